@@ -1,0 +1,268 @@
+"""Benchmark of the compiled-pipeline hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): a batched
+uneven panel of 2000 traces × 3001 float32 samples at 2 ms, live lengths
+U{1500..3001}, through demean → band-pass 3/6/70/90 Hz with a 50 Hz notch
+(2 Hz wide) → AGC 300 ms, src → dst. One step = one apply of the plan to one
+panel. Throughput is Msamples/s over the full stored width (rows × cols /
+time). Panels rotate through a pool larger than L2 so no step reads inputs
+left in cache by the previous one.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 it runs under torchrun, one rank per GPU, each on its own panel
+(weak scaling; traces are independent, there is no data-path exchange);
+timing is the max over ranks of the device-timed region.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ROWS, COLS, DT = 2000, 3001, 2.0
+WORKLOAD = "uneven panel 2000x3001 f32 @2ms, live U{1500..3001}: demean -> bandpass 3/6/70/90 Hz + 50 Hz notch (2 Hz) -> AGC 300 ms"
+METRIC = "Msamples/s, band-pass+AGC plan, 2000×3001 fp32; p50/p99 viewer-request latency"
+
+
+def flow():
+    import processseg_b200 as P
+    return [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(3, 6, 70, 90)).withNotch(50, 2)),
+            P.agcOp(300)]
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps=3, warmup=1):
+    """The oracle (the C++ restatement of the reference's path) through its
+    ProcessPool clone on all host cores, on the same panel."""
+    import numpy as np
+    import processseg_b200 as P
+    from processseg_b200 import synth
+    from oracle import oracle as O
+    g = synth.c2()
+    meta = g.meta()
+    live, start = meta.flat(COLS)
+    plan = O.OraclePlan(flow(), P.F32, DT, COLS)
+    cores = os.cpu_count() or 1
+    med, mn = plan.bench(g.data, live, start, threads=cores, warm=warmup, iters=steps)
+    return {"value": ROWS * COLS / med / 1e6, "unit": "Msamples/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} applies of the full 2000x3001 panel (median {med * 1e3:.1f} ms, "
+                      f"min {mn * 1e3:.1f} ms), ProcessPool clone, {cores} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    b = cpu_baseline(steps=max(1, args.steps), warmup=max(1, min(args.warmup, 3)))
+    line = {"impl": "reference", "metric": METRIC, "value": b["value"], "unit": "Msamples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "rows": ROWS, "cols": COLS},
+            "cpu_baseline": b,
+            "e2e": {"value": b["value"], "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import processseg_b200 as P
+    from processseg_b200 import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    g = synth.c2(seed=2 + rank)
+    meta = g.meta()
+    plan = P.initPipeline(flow()).compile(P.float32, DT, COLS)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=ROWS, cols=COLS)
+    # A pool of distinct panels larger than L2 (126 MB): 8 × (24 + 24) MB.
+    pool = 8
+    srcs = [torch.from_numpy(g.data).cuda() for _ in range(pool)]
+    for i, s in enumerate(srcs):
+        s.mul_(1.0 + 1e-3 * i)
+    dsts = [torch.empty_like(srcs[0]) for _ in range(pool)]
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        plan.apply(srcs[i % pool], dsts[i % pool], meta, ws)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            step(i)
+            ends[i].record(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        time.sleep(0.25)  # at least one clock sample after a short region
+    ms_total = e0.elapsed_time(e1)
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    ms_step = ms_total / args.steps
+    value = world * ROWS * COLS / (ms_step * 1e-3) / 1e6
+
+    # e2e: the public API with host buffers (pinned): copy in, apply, copy out.
+    hsrc = torch.from_numpy(g.data).pin_memory()
+    hdst = torch.empty_like(hsrc).pin_memory()
+    hs, hd = hsrc.numpy(), hdst.numpy()
+    for _ in range(2):
+        plan.apply(hs, hd, meta, ws)
+    e2e_steps = max(3, min(args.steps, 20))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plan.apply(hs, hd, meta, ws)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * ROWS * COLS / e2e_s / 1e6
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        kavg = statistics.mean(kernel_ms)
+        alg_bytes = 2 * ROWS * COLS * 4
+        achieved = alg_bytes / (kavg * 1e-3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+                traffic = json.load(f).get("pipeline_kernel_c2_bytes")
+        except Exception:
+            pass
+        line = {
+            "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows": ROWS, "cols": COLS, "parallelism": f"traces x{world}",
+                       "l2": "inputs larger than L2: 8 rotating src/dst panel pairs (384 MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "pipeline_kernel<float>", "algorithmic_bytes": alg_bytes},
+            "e2e": {"value": e2e, "unit": "Msamples/s",
+                    "h2d_bytes_per_step": ROWS * COLS * 4 + ROWS * 12,
+                    "d2h_bytes_per_step": ROWS * COLS * 4},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(steps=3, warmup=1)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,284 @@
+/*
+ * psg.h — C ABI of libpsgcuda.so, the B200 (sm_100a) implementation of
+ * processSEG's compiled-pipeline hot path.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns a
+ * `psg_status` and never throws or aborts. After a non-zero status,
+ * `psg_last_error` gives the message of the calling thread's last failure.
+ * PSG_EINVAL mirrors the reference's ValueError and is returned before any
+ * sample changes; PSG_EWORKSPACE mirrors its AssertionDefect for a workspace
+ * that was not reserved for the plan. Data never fails: NaN and Inf stay in
+ * their own row, as in the reference.
+ *
+ * Reference interfaces (paths within xrfez/processSEG v0.14.1) that each
+ * declaration replaces are cited beside it.
+ */
+#ifndef PSG_H
+#define PSG_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum psg_status {
+  PSG_OK = 0,
+  PSG_EINVAL = 1,     /* ValueError: bad op, plan, shape, interval, width    */
+  PSG_EWORKSPACE = 2, /* AssertionDefect: workspace not reserved for the plan */
+  PSG_ENOMEM = 3,     /* device memory or admission refused                  */
+  PSG_ETIMEOUT = 4,   /* a bounded wait ran out                              */
+  PSG_ECUDA = 5,      /* a CUDA call failed (message has the CUDA error)     */
+  PSG_ENODEV = 6      /* no usable sm_100 device                             */
+} psg_status;
+
+/* ------------------------------------------------------------- enumerations
+ * The numbering follows the reference's enums so that ops built in any host
+ * language keep their meaning.                                             */
+typedef enum psg_dtype { PSG_F32 = 0, PSG_F64 = 1 } psg_dtype;
+
+/* OpKind, src/processSEG/pipeline.nim:92-108 */
+typedef enum psg_op_kind {
+  PSG_OP_DEMEAN = 0, PSG_OP_DETREND = 1, PSG_OP_SCALE = 2, PSG_OP_GAIN_DB = 3,
+  PSG_OP_CLIP = 4, PSG_OP_POLARITY = 5, PSG_OP_MUTE_TOP = 6,
+  PSG_OP_MUTE_BOTTOM = 7, PSG_OP_FILTER = 8, PSG_OP_IIR = 9, PSG_OP_AGC = 10,
+  PSG_OP_NORMALIZE = 11, PSG_OP_GAIN_CURVE = 12, PSG_OP_CALIBRATE = 13,
+  PSG_OP_UNCALIBRATE = 14
+} psg_op_kind;
+
+/* TrendRemoval, src/processSEG/filter/edges.nim:9-14 */
+typedef enum psg_trend { PSG_TR_NONE = 0, PSG_TR_MEAN = 1, PSG_TR_LINEAR = 2 } psg_trend;
+/* ResponseKind, src/processSEG/filter/design.nim:69-72 */
+typedef enum psg_response_kind { PSG_RK_TRAPEZOID = 0, PSG_RK_BUTTERWORTH = 1 } psg_response_kind;
+/* AgcMode, src/processSEG/gain/gain.nim:92-95 */
+typedef enum psg_agc_mode { PSG_AGC_RMS = 0, PSG_AGC_MEAN_ABS = 1 } psg_agc_mode;
+/* NormStat / NormScope, src/processSEG/gain/gain.nim:72-81 */
+typedef enum psg_norm_stat { PSG_NORM_MAX = 0, PSG_NORM_RMS = 1, PSG_NORM_PERCENTILE = 2 } psg_norm_stat;
+typedef enum psg_norm_scope { PSG_PER_TRACE = 0, PSG_PER_PANEL = 1 } psg_norm_scope;
+/* GainCurveKind, src/processSEG/gain/curves.nim:65-69 */
+typedef enum psg_curve_kind { PSG_GC_KNOTS = 0, PSG_GC_POWER = 1, PSG_GC_EXPONENTIAL = 2 } psg_curve_kind;
+/* Trace status as ChunkMeta.isLive reads it, src/processSEG/core/types.nim:221-224 */
+typedef enum psg_trace_status {
+  PSG_TS_UNKNOWN = 0, PSG_TS_LIVE = 1, PSG_TS_DEAD = 2, PSG_TS_AUX = 3
+} psg_trace_status;
+/* CorrelationMode, src/processSEG/vibroseis/correlate.nim:61-64 */
+typedef enum psg_corr_mode { PSG_CM_CORRELATE = 0, PSG_CM_DECONVOLVE = 1 } psg_corr_mode;
+/* FoldNorm of stackInto, src/processSEG/vibroseis/vstack.nim:439 */
+typedef enum psg_fold_norm { PSG_FN_NONE = 0, PSG_FN_FOLD = 1, PSG_FN_SQRT_FOLD = 2 } psg_fold_norm;
+
+#define PSG_MAX_NOTCHES 8
+#define PSG_MAX_KNOTS 64
+
+/* ------------------------------------------------------------ op descriptors
+ * FilterSpec, src/processSEG/filter/design.nim:78-91 (notches inline).      */
+typedef struct psg_notch { double freq_hz, width_hz; } psg_notch;
+typedef struct psg_filter_spec {
+  int32_t kind;       /* psg_response_kind */
+  int32_t zero_dc;    /* withZeroDc */
+  int32_t n_notches;
+  int32_t _pad;
+  double f1, f2, f3, f4;                          /* trapezoid corners, Hz */
+  double low_hz, low_slope, high_hz, high_slope;  /* Butterworth */
+  psg_notch notches[PSG_MAX_NOTCHES];
+} psg_filter_spec;
+
+/* GainCurve, src/processSEG/gain/curves.nim:71-80 (knots inline). */
+typedef struct psg_gain_knot { double t_ms, db; } psg_gain_knot;
+typedef struct psg_gain_curve {
+  int32_t kind;       /* psg_curve_kind */
+  int32_t n_knots;
+  double power, ref_ms, min_ms, db_per_s;
+  psg_gain_knot knots[PSG_MAX_KNOTS];
+} psg_gain_curve;
+
+/* Op, src/processSEG/pipeline.nim:117-174, as one plain struct: the fields a
+ * kind does not use are ignored. */
+typedef struct psg_op {
+  int32_t kind;        /* psg_op_kind */
+  int32_t trend;       /* filter: psg_trend */
+  double factor;       /* scale: factor; gain dB: dB */
+  double lo, hi;       /* clip */
+  psg_filter_spec filter;
+  double window_ms, target, epsilon;  /* agc */
+  int32_t agc_mode;    /* psg_agc_mode */
+  int32_t norm_stat;   /* psg_norm_stat */
+  int32_t norm_scope;  /* psg_norm_scope */
+  int32_t _pad;
+  double norm_target, percentile;     /* normalize */
+  psg_gain_curve curve;
+  double t_min_ms, t_max_ms;          /* gain curve table span (NaN: record end) */
+} psg_op;
+
+/* ------------------------------------------------------------------ handles */
+typedef struct psg_plan psg_plan;           /* PipelinePlan[T]                 */
+typedef struct psg_workspace psg_workspace; /* Workspace (a device arena)      */
+typedef struct psg_corr_plan psg_corr_plan; /* CorrelationPlan[T]              */
+typedef struct psg_stack psg_stack;         /* RecordStack[T], rsVertical      */
+
+/* The calling thread's last error message (empty after success). */
+const char* psg_last_error(void);
+/* Selects and checks the device (sm_100 required). */
+int psg_init(int device);
+/* Library version string. */
+const char* psg_version(void);
+
+/* --------------------------------------------------------- lengths / margins */
+/* isFastLen / nextFastLen, src/processSEG/fft/plan.nim:105-118 */
+int psg_is_fast_len(int64_t n);
+int64_t psg_next_fast_len(int64_t n, int even);
+/* impulseLength, src/processSEG/filter/design.nim:353-366 */
+int psg_impulse_length(const psg_filter_spec* spec, double dt_ms, int32_t* out);
+/* response, src/processSEG/filter/design.nim:236-255 */
+int psg_response(const psg_filter_spec* spec, double f_hz, double dt_ms, double* out);
+/* Pipeline.requiredMargin, src/processSEG/pipeline.nim:525-548 */
+int psg_required_margin(const psg_op* ops, int32_t n_ops, double dt_ms, int32_t* out);
+/* decodeWindow, src/processSEG/pipeline.nim:550-560: out[0..1] = first, last */
+void psg_decode_window(int64_t shown_first, int64_t shown_last, int64_t margin,
+                       int64_t trace_len, int64_t* out);
+
+/* --------------------------------------------------------------- plans */
+/* compile, src/processSEG/pipeline.nim:466-523. Uploads the plan's tables to
+ * the current device once. */
+int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms,
+                     int32_t samples, int32_t record_samples, psg_plan** out);
+void psg_plan_destroy(psg_plan* plan);
+/* requiredMargin / generation / samples / recordSamples / partCount,
+ * src/processSEG/pipeline.nim:562-647 */
+int32_t psg_plan_margin(const psg_plan* plan);
+uint64_t psg_plan_generation(const psg_plan* plan);
+int32_t psg_plan_samples(const psg_plan* plan);
+int32_t psg_plan_record_samples(const psg_plan* plan);
+int32_t psg_plan_part_count(const psg_plan* plan);
+int32_t psg_plan_len(const psg_plan* plan);
+/* For step i of the plan: its FFT length (0 for steps without one) and the
+ * pad laid out each side (FilterPlan.nfft / pad, filter/apply.nim:161-164). */
+int32_t psg_plan_step_nfft(const psg_plan* plan, int32_t step);
+int32_t psg_plan_step_margin(const psg_plan* plan, int32_t step);
+/* Scratch bytes of device memory the plan needs for `rows` rows
+ * (WorkspaceSize, src/processSEG/pipeline.nim:599-602). */
+int64_t psg_plan_workspace_bytes(const psg_plan* plan, int64_t rows, int32_t cols);
+
+/* --------------------------------------------------------------- workspace */
+/* initWorkspace / reserve, src/processSEG/core/workspace.nim:50-96: a
+ * grow-only device arena, plus pinned host staging for the host-pointer
+ * entry points. One per thread (or stream) of callers. */
+int psg_workspace_create(psg_workspace** out);
+void psg_workspace_destroy(psg_workspace* ws);
+int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows,
+                          int32_t cols);
+int64_t psg_workspace_bytes(const psg_workspace* ws);
+
+/* --------------------------------------------------------------- rows
+ * ChunkMeta flattened (isLive, liveSamples, sampleTimeMs,
+ * src/processSEG/core/types.nim:212-240) into two per-row arrays on the host:
+ * live[r] = the samples to process (0: the row is not processed) and
+ * start_ms[r] = the time of column 0 (NaN when unknown). mode 0 is the
+ * processing rule (live or unknown status, not failed); mode 1 the
+ * correlation rule (not dead, not failed: auxiliary rows are correlated,
+ * src/processSEG/vibroseis/correlate.nim:442-443). `t0_ms` may be NULL (NaN). */
+int psg_rows_flatten(const int32_t* status, const int32_t* num_samples,
+                     const double* t0_ms, int64_t rows, int32_t first_sample,
+                     double dt_ms, const int64_t* failed, int64_t n_failed,
+                     int32_t cols, int32_t mode, int32_t* live_out,
+                     double* start_ms_out);
+
+/* --------------------------------------------------------------- apply
+ * apply(plan, src, dst, meta, ws), src/processSEG/pipeline.nim:736-772.
+ * Device pointers; `src` NULL (or equal to `dst`) runs in place. `live` and
+ * `start_ms` are device arrays of `rows` values (psg_rows_flatten). `dt_ms`
+ * is the rows' interval (ChunkMeta.dtMs), checked against the plan with
+ * sameInterval. Rows that are not live, and samples past a row's live
+ * length, are copied unchanged from src. Asynchronous on `stream`
+ * (a cudaStream_t; NULL: the legacy default stream). */
+int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst,
+              int64_t rows, int32_t cols, const int32_t* live, const double* start_ms,
+              double dt_ms, void* stream);
+/* The same from and to host memory (pinned memory overlaps best): the
+ * host→device copy of src, live and start_ms, the apply, and the
+ * device→host copy of dst, all on `stream`; returns after dst is written. */
+int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host,
+                   void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
+                   const double* start_ms_host, double dt_ms, void* stream);
+
+/* Parts API, src/processSEG/pipeline.nim:643-723: the per-panel factor of a
+ * part (NaN: the block is left alone) over the whole block, on the device;
+ * `factor_out` is a device double. */
+int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part,
+                     const void* block, int64_t rows, int32_t cols, const int32_t* live,
+                     double* factor_out, void* stream);
+
+/* ----------------------------------------------------------- statistics */
+/* traceStatsInto, src/processSEG/gain/stats.nim:186-199: rms and maxAbs per
+ * row (NaN for rows with live[r] == 0), device arrays of `rows` doubles. */
+int psg_trace_stats(const void* block, int32_t dtype, int64_t rows, int32_t cols,
+                    const int32_t* live, double* rms_out, double* max_abs_out,
+                    void* stream);
+/* panelStats, src/processSEG/gain/stats.nim:253-304. out (device) receives
+ * {rms, maxAbs, clip, rows, samples} as doubles. clip_percentile NaN skips
+ * the histogram. */
+int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t rows,
+                    int32_t cols, const int32_t* live, double clip_percentile,
+                    double* out, void* stream);
+
+/* ----------------------------------------------------------- vibroseis */
+/* linearSweep + sweepInto + generatePilot (taper shapes tpLinear, tpCosine,
+ * tpCos2, tpHamming, tpBlackman), src/processSEG/vibroseis/sweep.nim:185-342,
+ * taper.nim:125-179, pilot.nim:115-119. Phase in float64. `out` is host
+ * memory of *n_out values of dtype (NULL: just report the length). */
+int psg_linear_sweep(double f1_hz, double f2_hz, double length_ms, double dt_ms,
+                     double taper_start_ms, double taper_end_ms, int32_t taper_shape,
+                     double start_phase_deg, double amplitude,
+                     double max_nyquist_fraction, int32_t dtype, void* out,
+                     int64_t* n_out);
+/* initCorrelationPlan, src/processSEG/vibroseis/correlate.nim:82-160: the
+ * pilot (host samples of pilot_dtype) spectrum in float64, the multiplier
+ * stored as dtype on the device. */
+int psg_corr_plan_create(const void* pilot, int32_t pilot_dtype, int64_t pilot_len,
+                         double pilot_dt_ms, double pilot_t0_ms, int32_t dtype,
+                         double dt_ms, int32_t record_samples, int32_t out_samples,
+                         int32_t mode, double eps_percent, int32_t normalize,
+                         psg_corr_plan** out);
+void psg_corr_plan_destroy(psg_corr_plan* plan);
+int32_t psg_corr_plan_nfft(const psg_corr_plan* plan);
+int32_t psg_corr_plan_out_samples(const psg_corr_plan* plan);
+double psg_corr_plan_scale(const psg_corr_plan* plan);
+/* correlateInto (block form), src/processSEG/vibroseis/correlate.nim:421-464:
+ * device src [rows, cols ≤ recordSamples], dst [rows, outSamples]; `live`
+ * from psg_rows_flatten mode 1 (0: a zero row). */
+int psg_correlate(const psg_corr_plan* plan, const void* src, void* dst, int64_t rows,
+                  int32_t cols, const int32_t* live, double dt_ms, void* stream);
+
+/* RecordStack rsVertical, src/processSEG/vibroseis/vstack.nim:118-471:
+ * float64 sums and int32 counts on the device. */
+int psg_stack_create(int64_t rows, int32_t samples, double dt_ms, psg_stack** out);
+void psg_stack_destroy(psg_stack* st);
+int psg_stack_clear(psg_stack* st, void* stream);
+/* addRecord: rows of `block` (device, dtype) with live[r] > 0 into output
+ * row row_map[r] (device int32; NULL: r; < 0: skipped); a row with a
+ * non-finite sample is skipped. */
+int psg_stack_add(psg_stack* st, const void* block, int32_t dtype, int64_t rows,
+                  int32_t cols, const int32_t* live, const int32_t* row_map,
+                  void* stream);
+/* correlateInto fused with addRecord: each correlated row is also added to
+ * the stack in one launch. `live` selects the rows to correlate (mode 1);
+ * `stack_live` (device, NULL: outSamples for every row) the samples of each
+ * correlated row to add (0: not added; addRecord adds live rows only, mode
+ * 0 with cols = outSamples); row_map as psg_stack_add. `dst` may be NULL
+ * when only the stack is wanted. */
+int psg_correlate_stack(const psg_corr_plan* plan, psg_stack* st, const void* src,
+                        void* dst, int64_t rows, int32_t cols, const int32_t* live,
+                        const int32_t* stack_live, const int32_t* row_map, double dt_ms,
+                        void* stream);
+/* stackInto, src/processSEG/vibroseis/vstack.nim:439-471: dst device
+ * [rows, samples] of dtype. */
+int psg_stack_result(const psg_stack* st, void* dst, int32_t dtype, int32_t norm,
+                     void* stream);
+/* foldInto: counts, device int32 [rows, samples]. */
+int psg_stack_fold(const psg_stack* st, int32_t* dst, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSG_H */

@@ -1,0 +1,298 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU oracle
+(``oracle/libpsg_oracle.so``, built from ``oracle/psg_oracle.cpp`` by
+``oracle/Makefile``). Only the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline legs of ``bench.py`` use it, as the checker or the timed CPU
+reference; the product never does.
+
+The oracle restates the reference's Nim hot path (see the header of
+psg_oracle.cpp). It cannot be compared with the reference's own binaries
+(no Nim toolchain exists here): it is pinned by the reference's known-answer
+tests instead (tests/test_oracle_pins.py).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from processseg_b200 import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libpsg_oracle.so")
+_lib = None
+
+P, I32, I64, DBL = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+
+
+def build():
+    """Compiles the oracle with its Makefile (gcc only)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        sig = {
+            "orc_last_error": (C.c_char_p, []),
+            "orc_is_fast_len": (C.c_int, [I64]),
+            "orc_next_fast_len": (I64, [I64, C.c_int]),
+            "orc_fft_forward": (C.c_int, [C.c_int, I64, P, P, P]),
+            "orc_fft_inverse": (C.c_int, [C.c_int, I64, P, P, P]),
+            "orc_response": (C.c_int, [C.POINTER(A.FilterSpecC), DBL, DBL, C.POINTER(DBL)]),
+            "orc_impulse_length": (C.c_int, [C.POINTER(A.FilterSpecC), DBL, C.POINTER(I64)]),
+            "orc_filter_plan_info": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_int, DBL, I64, C.c_int,
+                                               C.POINTER(I64), C.POINTER(I64), C.POINTER(I64),
+                                               C.POINTER(C.c_int), C.POINTER(DBL), P]),
+            "orc_required_margin": (C.c_int, [C.POINTER(A.OpC), C.c_int, DBL, C.POINTER(I64)]),
+            "orc_plan_compile": (C.c_int, [C.POINTER(A.OpC), C.c_int, C.c_int, DBL, I64, I64,
+                                           C.POINTER(P)]),
+            "orc_plan_destroy": (None, [P]),
+            "orc_plan_margin": (I64, [P]),
+            "orc_plan_part_count": (C.c_int, [P]),
+            "orc_plan_step_nfft": (I64, [P, C.c_int]),
+            "orc_rows_flatten": (C.c_int, [P, P, P, I64, I32, DBL, P, I64, I32, I32, P, P]),
+            "orc_plan_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int]),
+            "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int,
+                                          C.POINTER(DBL), C.POINTER(DBL)]),
+            "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
+            "orc_panel_stats": (C.c_int, [C.c_int, P, I64, I64, P, DBL, P]),
+            "orc_percentile_abs": (C.c_int, [C.c_int, P, I64, DBL, C.POINTER(DBL)]),
+            "orc_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, C.c_int, DBL, DBL, C.c_int,
+                                           P, C.POINTER(I64)]),
+            "orc_correlate": (C.c_int, [P, I64, DBL, DBL, C.c_int, DBL, I64, I64, C.c_int, DBL,
+                                        C.c_int, P, P, I64, I64, P, C.POINTER(I64),
+                                        C.POINTER(DBL)]),
+            "orc_stack_add": (C.c_int, [C.c_int, P, I64, I64, P, P, P, P, I64]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _check(st):
+    if st != 0:
+        raise ValueError(lib().orc_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _dt(a):
+    return A.F32 if a.dtype == np.float32 else A.F64
+
+
+def is_fast_len(n):
+    return bool(lib().orc_is_fast_len(n))
+
+
+def next_fast_len(n, even=True):
+    return lib().orc_next_fast_len(n, 1 if even else 0)
+
+
+def fft_forward(x):
+    x = np.ascontiguousarray(x)
+    n = x.size
+    re = np.zeros(n // 2 + 1, x.dtype)
+    im = np.zeros(n // 2 + 1, x.dtype)
+    _check(lib().orc_fft_forward(_dt(x), n, _ptr(x), _ptr(re), _ptr(im)))
+    return re, im
+
+
+def fft_inverse(re, im, n):
+    re = np.ascontiguousarray(re)
+    im = np.ascontiguousarray(im)
+    x = np.zeros(n, re.dtype)
+    _check(lib().orc_fft_inverse(_dt(re), n, _ptr(re), _ptr(im), _ptr(x)))
+    return x
+
+
+def response(spec, f, dtMs):
+    out = C.c_double()
+    _check(lib().orc_response(C.byref(spec.to_c()), f, dtMs, C.byref(out)))
+    return out.value
+
+
+def impulse_length(spec, dtMs):
+    out = C.c_int64()
+    _check(lib().orc_impulse_length(C.byref(spec.to_c()), dtMs, C.byref(out)))
+    return out.value
+
+
+def filter_plan_info(spec, dtype, dtMs, samples, trend=A.TR_LINEAR, with_gain=False):
+    m, pad, nfft = C.c_int64(), C.c_int64(), C.c_int64()
+    refl, dc = C.c_int(), C.c_double()
+    s = spec.to_c()
+    _check(lib().orc_filter_plan_info(C.byref(s), dtype, dtMs, samples, trend, C.byref(m),
+                                      C.byref(pad), C.byref(nfft), C.byref(refl), C.byref(dc),
+                                      None))
+    info = dict(margin=m.value, pad=pad.value, nfft=nfft.value, reflect=bool(refl.value),
+                dcGain=dc.value)
+    if with_gain:
+        g = np.zeros(nfft.value // 2 + 1)
+        _check(lib().orc_filter_plan_info(C.byref(s), dtype, dtMs, samples, trend, C.byref(m),
+                                          C.byref(pad), C.byref(nfft), C.byref(refl), C.byref(dc),
+                                          _ptr(g)))
+        info["gain"] = g
+    return info
+
+
+def required_margin(ops, dtMs):
+    arr = A.ops_array(ops)
+    out = C.c_int64()
+    _check(lib().orc_required_margin(arr, len(ops), dtMs, C.byref(out)))
+    return out.value
+
+
+class OraclePlan:
+    """A compiled pipeline in the oracle (pipeline.nim:466-523)."""
+
+    def __init__(self, ops, dtype, dtMs, samples, recordSamples=0):
+        self.dtype = dtype
+        arr = A.ops_array(list(ops))
+        h = C.c_void_p()
+        _check(lib().orc_plan_compile(arr, len(list(ops)), dtype, dtMs, samples, recordSamples,
+                                      C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.orc_plan_destroy(self.h)
+            self.h = None
+
+    @property
+    def margin(self):
+        return lib().orc_plan_margin(self.h)
+
+    @property
+    def partCount(self):
+        return lib().orc_plan_part_count(self.h)
+
+    def step_nfft(self, i):
+        return lib().orc_plan_step_nfft(self.h, i)
+
+    def apply(self, src, live, startMs=None, threads=1, inplace=False):
+        """Runs the plan on ``src`` ([rows, cols], the plan's dtype): returns
+        dst (src → dst form; the copy fused per row as the reference)."""
+        src = np.ascontiguousarray(src)
+        rows, cols = src.shape
+        live = np.ascontiguousarray(live, dtype=np.int32)
+        st = None if startMs is None else np.ascontiguousarray(startMs, dtype=np.float64)
+        if inplace:
+            dst = src.copy()
+            _check(lib().orc_plan_apply(self.h, None, _ptr(dst), rows, cols, _ptr(live), _ptr(st),
+                                        threads))
+        else:
+            dst = np.zeros_like(src)
+            _check(lib().orc_plan_apply(self.h, _ptr(src), _ptr(dst), rows, cols, _ptr(live),
+                                        _ptr(st), threads))
+        return dst
+
+    def bench(self, src, live, startMs=None, threads=1, warm=3, iters=15):
+        """Median and minimum seconds of one src → dst apply through the pool
+        clone (bench/benchutil.nim:96-126 method)."""
+        src = np.ascontiguousarray(src)
+        rows, cols = src.shape
+        dst = np.zeros_like(src)
+        live = np.ascontiguousarray(live, dtype=np.int32)
+        st = None if startMs is None else np.ascontiguousarray(startMs, dtype=np.float64)
+        med, mn = C.c_double(), C.c_double()
+        _check(lib().orc_bench_apply(self.h, _ptr(src), _ptr(dst), rows, cols, _ptr(live), _ptr(st),
+                                     threads, warm, iters, C.byref(med), C.byref(mn)))
+        return med.value, mn.value
+
+
+def rows_flatten(status, numSamples, t0Ms, firstSample, dtMs, failed, cols, mode=0):
+    status = np.ascontiguousarray(status, dtype=np.int32)
+    ns = np.ascontiguousarray(numSamples, dtype=np.int32)
+    t0 = None if t0Ms is None else np.ascontiguousarray(t0Ms, dtype=np.float64)
+    fl = np.ascontiguousarray(failed if failed is not None else [], dtype=np.int64)
+    rows = status.size
+    live = np.zeros(rows, np.int32)
+    start = np.zeros(rows, np.float64)
+    _check(lib().orc_rows_flatten(_ptr(status), _ptr(ns), _ptr(t0), rows, firstSample, dtMs,
+                                  _ptr(fl), fl.size, cols, mode, _ptr(live), _ptr(start)))
+    return live, start
+
+
+def agc_row(x, windowMs, dtMs, mode=A.AGC_RMS, target=1.0, eps=1e-9):
+    y = np.ascontiguousarray(x).copy()
+    _check(lib().orc_agc_row(_dt(y), windowMs, dtMs, mode, target, eps, _ptr(y), y.size))
+    return y
+
+
+def panel_stats(b, live, clipP):
+    b = np.ascontiguousarray(b)
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    out = np.zeros(5)
+    _check(lib().orc_panel_stats(_dt(b), _ptr(b), b.shape[0], b.shape[1], _ptr(live), clipP,
+                                 _ptr(out)))
+    return dict(rms=out[0], maxAbs=out[1], clip=out[2], rows=int(out[3]), samples=int(out[4]))
+
+
+def percentile_abs(x, p):
+    x = np.ascontiguousarray(x)
+    out = C.c_double()
+    _check(lib().orc_percentile_abs(_dt(x), _ptr(x), x.size, p, C.byref(out)))
+    return out.value
+
+
+def linear_sweep(f1, f2, lengthMs, dtMs, taperStart=0.0, taperEnd=0.0, shape=2, phaseDeg=0.0,
+                 amplitude=1.0, dtype=np.float64):
+    n = C.c_int64()
+    dt = A.F32 if dtype == np.float32 else A.F64
+    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, phaseDeg,
+                                  amplitude, dt, None, C.byref(n)))
+    x = np.zeros(n.value, dtype)
+    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, phaseDeg,
+                                  amplitude, dt, _ptr(x), C.byref(n)))
+    return x
+
+
+def correlate(pilot, pilotDt, pilotT0, src, live, dtMs, recordSamples, outSamples=0,
+              mode=A.CM_CORRELATE, epsPercent=1.0, normalize=True):
+    pilot = np.ascontiguousarray(pilot, dtype=np.float64)
+    src = np.ascontiguousarray(src)
+    rows, cols = src.shape
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    nfft, scale = C.c_int64(), C.c_double()
+    # First the plan facts (no rows), then the rows.
+    _check(lib().orc_correlate(_ptr(pilot), pilot.size, pilotDt, pilotT0, _dt(src), dtMs,
+                               recordSamples, outSamples, mode, epsPercent, int(normalize), None,
+                               None, 0, cols, None, C.byref(nfft), C.byref(scale)))
+    outN = outSamples if outSamples else recordSamples - pilot.size
+    dst = np.zeros((rows, outN), src.dtype)
+    _check(lib().orc_correlate(_ptr(pilot), pilot.size, pilotDt, pilotT0, _dt(src), dtMs,
+                               recordSamples, outSamples, mode, epsPercent, int(normalize),
+                               _ptr(src), _ptr(dst), rows, cols, _ptr(live), C.byref(nfft),
+                               C.byref(scale)))
+    return dst, nfft.value, scale.value
+
+
+def stack_add(num, cnt, block, live, rowMap=None):
+    block = np.ascontiguousarray(block)
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    rm = None if rowMap is None else np.ascontiguousarray(rowMap, dtype=np.int32)
+    _check(lib().orc_stack_add(_dt(block), _ptr(block), block.shape[0], block.shape[1], _ptr(live),
+                               _ptr(rm), _ptr(num), _ptr(cnt), num.shape[1]))
+
+
+def stack_result(num, cnt, dtype, norm=A.FN_FOLD):
+    """stackInto, vibroseis/vstack.nim:439-471 (rsVertical)."""
+    c = cnt.astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if norm == A.FN_NONE:
+            v = num
+        elif norm == A.FN_FOLD:
+            v = num / c
+        else:
+            v = num / np.sqrt(c)
+    v = np.where(cnt == 0, 0.0, v)
+    return v.astype(dtype)

@@ -1,0 +1,1578 @@
+// psg_cuda.cu — the device side of libpsgcuda.so and its C ABI (include/psg.h).
+//
+// The hot path is one fused kernel per plan part (pipeline_kernel): each CTA
+// takes a trace, loads its live samples from HBM into shared memory once,
+// runs every step of the part on it there (demean/detrend/scale/clip/
+// polarity, the zero-phase FFT filter with its trend removal, padding and
+// trend add-back, AGC with block prefix/suffix sums in float64, per-trace
+// normalization with an exact radix selection, gain curves), and writes the
+// trace back once. src → dst copies of dead rows and of samples past the live
+// length ride in the same kernel. A per-panel normalization splits the plan
+// into parts; its factor is computed on the device by the panel-statistics
+// kernels and read by the next part's kernel (no host round trip).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "psg_device.cuh"
+#include "psg_internal.h"
+
+using namespace psgd;
+
+namespace psg {
+
+static thread_local std::string t_err;
+void set_error(const std::string& m) { t_err = m; }
+
+#define CUDA_OK(x)                                                                         \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ============================================================ device plan
+struct DevStep {
+  int kind, trend, reflect, zero_dc;
+  int agc_mode, stat, pad, nfft;
+  int half, table_len, table_on, _p;
+  double factor, lo, hi, dc_gain, target, epsilon, norm_target, percentile, t_min_ms, dt_ms;
+  FftDesc fft;
+  const void* gain;
+  const void* fall;
+  const void* tw;
+  const void* split;
+  const void* table;
+  psg_gain_curve curve;
+};
+
+struct PipeArgs {
+  const void* src;
+  void* dst;
+  long long rows;
+  int cols;
+  int x_elems;       // shared-memory trace buffer, elements
+  int work_off;      // byte offset of the work area
+  int first, last;   // steps [first, last)
+  const int* live;
+  const double* start_ms;
+  const double* factor;  // the part's panel factor (NaN: none) or NULL
+  const DevStep* steps;
+};
+
+// ----------------------------------------------------------- device helpers
+__device__ __forceinline__ bool fin_pos_d(double x) { return isfinite(x) && x > 0; }
+template <class T> __device__ __forceinline__ bool fits_d(double x) {
+  if (!fin_pos_d(x)) return false;
+  double y = (double)(T)x;
+  return isfinite(y) && y > 0;
+}
+
+// Row copies between global buffers and shared memory, 16-byte vectors where
+// the addresses allow it.
+template <class T> __device__ void load_row(const T* __restrict__ g, T* s, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+}
+template <> __device__ void load_row<float>(const float* __restrict__ g, float* s, int n) {
+  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
+  if (head > n) head = n;
+  for (int i = threadIdx.x; i < head; i += blockDim.x) s[i] = g[i];
+  int nv = (n - head) >> 2;
+  const float4* gv = reinterpret_cast<const float4*>(g + head);
+  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+    float4 q = __ldcs(gv + v);
+    int i = head + 4 * v;
+    s[i] = q.x; s[i + 1] = q.y; s[i + 2] = q.z; s[i + 3] = q.w;
+  }
+  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+}
+template <class T> __device__ void store_row(const T* s, T* __restrict__ g, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+}
+template <> __device__ void store_row<float>(const float* s, float* __restrict__ g, int n) {
+  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
+  if (head > n) head = n;
+  for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
+  int nv = (n - head) >> 2;
+  float4* gv = reinterpret_cast<float4*>(g + head);
+  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+    int i = head + 4 * v;
+    __stcs(gv + v, make_float4(s[i], s[i + 1], s[i + 2], s[i + 3]));
+  }
+  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+}
+template <class T> __device__ void copy_global(const T* __restrict__ a, T* __restrict__ b, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
+}
+
+// Σ x and Σ i·x over the live samples, in float64 (core/sums.nim).
+template <class T> __device__ double sum_x(const T* X, int n, double* red) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)X[i];
+  return block_sum(s, red);
+}
+template <class T> __device__ double sum_ix(const T* X, int n, double* red) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)i * (double)X[i];
+  return block_sum(s, red);
+}
+template <class T> __device__ double sum_sq(const T* X, int n, double* red) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = (double)X[i];
+    s += v * v;
+  }
+  return block_sum(s, red);
+}
+template <class T> __device__ double max_abs(const T* X, int n, unsigned long long* red) {
+  unsigned long long m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    unsigned long long b = abs_bits(X[i]);
+    m = b > m ? b : m;
+  }
+  m = block_max_u64(m, red);
+  return bits_value(m, (T)0);
+}
+
+// The k-th smallest |x| (0-based) as its bits, by an 8-bit radix selection
+// over the bit patterns in shared memory.
+template <class T>
+__device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* hist, int* sh) {
+  unsigned long long prefix = 0, mask = 0;
+  int kk = k;
+  for (int shift = (int)sizeof(T) * 8 - 8; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      unsigned long long key = abs_bits(X[i]);
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      int lane = threadIdx.x;
+      unsigned c[8], tot = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        c[j] = hist[lane * 8 + j];
+        tot += c[j];
+      }
+      unsigned incl = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+      }
+      unsigned excl = incl - tot;
+      if ((unsigned)kk >= excl && (unsigned)kk < incl) {
+        unsigned below = excl;
+        int d = 0;
+        for (; d < 8; d++) {
+          if ((unsigned)kk < below + c[d]) break;
+          below += c[d];
+        }
+        sh[0] = lane * 8 + d;
+        sh[1] = kk - (int)below;
+      }
+    }
+    __syncthreads();
+    prefix |= (unsigned long long)sh[0] << shift;
+    mask |= 255ull << shift;
+    kk = sh[1];
+    __syncthreads();
+  }
+  return prefix;
+}
+
+// ------------------------------------------------------------------ steps
+struct Shared {
+  double red[32];
+  unsigned long long redu[32];
+  unsigned hist[256];
+  int sh[4];
+};
+
+// filter/edges.nim:16-30
+template <class T> __device__ void trend_of(int trend, const T* X, int n, double& a, double& b, Shared& S) {
+  a = 0;
+  b = 0;
+  if (trend == PSG_TR_NONE) return;
+  double sx = sum_x(X, n, S.red);
+  double nf = (double)n, mean = sx / nf;
+  if (trend == PSG_TR_MEAN || n == 1) {
+    a = mean;
+    return;
+  }
+  double six = sum_ix(X, n, S.red);
+  double c = (nf - 1) / 2;
+  double slope = (six - c * sx) / (nf * (nf * nf - 1) / 12);
+  a = mean - slope * c;
+  b = slope;
+}
+
+// The zero-phase FFT filter with the reference's edge handling
+// (filter/apply.nim:194-231, 340-363) on the trace in shared memory.
+template <class T>
+__device__ void step_filter(const DevStep& st, T* X, int n, unsigned char* work, Shared& S) {
+  typedef typename C2<T>::type V;
+  const int p = st.pad, nfft = st.nfft, m = nfft / 2;
+  V* A = reinterpret_cast<V*>(work);
+  V* B = A + m;
+  double a, b;
+  trend_of(st.trend, X, n, a, b, S);
+  const T* fall = reinterpret_cast<const T*>(st.fall);
+  T* Ar = reinterpret_cast<T*>(A);
+  // packInto: the detrended samples at p .. p+n, odd reflections tapered by
+  // `fall` (or zeros) in the pads, zeros to nfft.
+  for (int j = threadIdx.x; j < nfft; j += blockDim.x) {
+    T v = (T)0;
+    if (j >= p && j < p + n) {
+      int i = j - p;
+      v = (T)((double)X[i] - (a + b * (double)i));
+    } else if (st.reflect && j < p) {
+      int k = p - j, i = min(k, n - 1);
+      T d0 = (T)((double)X[0] - a);
+      T r = (T)((double)X[i] - (a + b * (double)i));
+      v = (d0 + d0 - r) * __ldg(&fall[k - 1]);
+    } else if (st.reflect && j >= p + n && j < 2 * p + n) {
+      int k = j - (p + n - 1), i = n - 1 - min(k, n - 1);
+      T dn = (T)((double)X[n - 1] - (a + b * (double)(n - 1)));
+      T r = (T)((double)X[i] - (a + b * (double)i));
+      v = (dn + dn - r) * __ldg(&fall[k - 1]);
+    }
+    Ar[j] = v;
+  }
+  __syncthreads();
+  const V* tw = reinterpret_cast<const V*>(st.tw);
+  const V* split = reinterpret_cast<const V*>(st.split);
+  const T* gain = reinterpret_cast<const T*>(st.gain);
+  V* z = cfft_forward<T>(A, B, st.fft, tw);
+  split_mul_unsplit<T>(z, m, split, (T)1 / (T)nfft, [&](V x, int k) {
+    T g = __ldg(&gain[k]);
+    return V{x.x * g, x.y * g};
+  });
+  V* y = cfft_forward<T>(z, z == A ? B : A, st.fft, tw);
+  // unpackFrom: the output is swap(y); sample 2k is y[k].im, 2k+1 is y[k].re.
+  double gb = b * st.dc_gain;
+  double ga = st.zero_dc ? -gb * (double)(n - 1) / 2 : a * st.dc_gain;
+  bool plain = ga == 0 && gb == 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int idx = p + i;
+    V c = y[idx >> 1];
+    T v = (idx & 1) ? c.x : c.y;
+    X[i] = plain ? v : (T)((double)v + (ga + gb * (double)i));
+  }
+  __syncthreads();
+}
+
+// AGC (gain/gain.nim:351-461): per block of w = 2h + 1 samples, prefix and
+// suffix sums of the terms in float64 (a warp per block, no subtraction),
+// stored as T; then the gain step in T on means scaled by the trace RMS.
+template <class T>
+__device__ void step_agc(const DevStep& st, T* X, int n, unsigned char* work, Shared& S) {
+  const bool rms_mode = st.agc_mode == PSG_AGC_RMS;
+  double ss = sum_sq(X, n, S.red);
+  double rms = sqrt(ss / (double)n);
+  if (rms == 0) return;
+  if (!fits_d<T>(st.target / rms / st.epsilon)) return;  // also a NaN or Inf row
+  const int h = st.half, w = 2 * h + 1;
+  T* P = reinterpret_cast<T*>(work);          // n + 1 values
+  T* Sx = P + ((n + 1 + 3) & ~3);             // n values
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int nb = (n + w - 1) / w;
+  for (int blk = warp; blk < nb; blk += nwarps) {
+    const int bs = blk * w, be = min(bs + w, n), L = be - bs;
+    double carry = 0;
+    if (lane == 0) P[bs] = (T)0;
+    for (int c = 0; c < L; c += 32) {
+      int idx = c + lane;
+      double t = 0;
+      if (idx < L) {
+        double v = (double)X[bs + idx];
+        t = rms_mode ? v * v : fabs(v);
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        double u = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += u;
+      }
+      // p[e] for e = bs+idx+1 inside the block; the block end is the next
+      // block's start (0) unless it is the trace end.
+      int e = bs + idx + 1;
+      if (idx < L && (e < be || (be == n && (n % w) != 0))) P[e] = (T)(carry + t);
+      carry += __shfl_sync(0xffffffffu, t, 31);
+    }
+    carry = 0;
+    for (int c = 0; c < L; c += 32) {
+      int idx = c + lane;
+      double t = 0;
+      if (idx < L) {
+        double v = (double)X[be - 1 - idx];
+        t = rms_mode ? v * v : fabs(v);
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        double u = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += u;
+      }
+      if (idx < L) Sx[be - 1 - idx] = (T)(carry + t);
+      carry += __shfl_sync(0xffffffffu, t, 31);
+    }
+  }
+  if (threadIdx.x == 0 && n % w == 0) P[n] = (T)0;
+  __syncthreads();
+  const double unit = rms_mode ? 1 / (rms * rms) : 1 / rms;
+  const T k = (T)(st.target / rms), eps = (T)st.epsilon;
+  const int first = min(h, n), last = max(first, n - h);
+  const int headCut = min(max(n - h, 0), first);
+  const int lastBlock = (n - 1) / w * w;
+  const int tailCut = min(max(lastBlock + h, last), n);
+  const double pn = (double)P[n];
+  const double unitW = unit / (double)w;
+  const double headWhole = headCut < first ? pn * unit * (1 / (double)n) : 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double mean;
+    if (i < headCut) mean = (double)P[i + h + 1] * (unit * (1 / (double)(i + h + 1)));
+    else if (i < first) mean = headWhole;
+    else if (i < last) mean = ((double)Sx[i - h] + (double)P[i + h + 1]) * unitW;
+    else if (i < tailCut) mean = ((double)Sx[i - h] + pn) * (unit * (1 / (double)(w - (i + h + 1 - n))));
+    else mean = (double)Sx[i - h] * (unit * (1 / (double)(w - (i + h + 1 - n))));
+    T lv = rms_mode ? sqrt((T)mean) : (T)mean;
+    T gi = k / (lv + eps);
+    X[i] = (T)(X[i] * gi);
+  }
+  __syncthreads();
+}
+
+// Per-trace normalization (gain/gain.nim:198-219; stats.nim:129-182).
+template <class T> __device__ void step_norm_trace(const DevStep& st, T* X, int n, Shared& S) {
+  double level;
+  if (st.stat == PSG_NORM_MAX) {
+    level = max_abs(X, n, S.redu);
+  } else if (st.stat == PSG_NORM_RMS) {
+    level = sqrt(sum_sq(X, n, S.red) / (double)n);
+  } else {
+    double mx = max_abs(X, n, S.redu);
+    if (isnan(mx)) {
+      level = mx;
+    } else {
+      double hr = (double)(n - 1) * st.percentile / 100;
+      int k = min((int)floor(hr), n - 1);
+      double lower = bits_value(select_kth(X, n, k, S.hist, S.sh), (T)0);
+      if (k + 1 >= n) {
+        level = lower;
+      } else {
+        double upper = bits_value(select_kth(X, n, k + 1, S.hist, S.sh), (T)0);
+        double f = hr - (double)k;
+        level = f == 0 ? lower : lower + f * (upper - lower);
+      }
+    }
+  }
+  if (fin_pos_d(level) && fits_d<T>(st.norm_target / level)) {
+    T kf = (T)(st.norm_target / level);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * kf;
+  }
+  __syncthreads();
+}
+
+// gain/curves.nim:132-160 on the device, in float64.
+__device__ double factor_at_d(const psg_gain_curve& c, double t) {
+  if (isnan(t)) return t;
+  if (c.kind == PSG_GC_POWER) return pow(fmax(t, c.min_ms) / c.ref_ms, c.power);
+  double db;
+  if (c.kind == PSG_GC_KNOTS) {
+    int nk = c.n_knots;
+    if (t <= c.knots[0].t_ms) db = c.knots[0].db;
+    else if (t >= c.knots[nk - 1].t_ms) db = c.knots[nk - 1].db;
+    else {
+      int lo = 0, hi = nk - 1;
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (c.knots[mid].t_ms <= t) lo = mid; else hi = mid;
+      }
+      double f = (t - c.knots[lo].t_ms) / (c.knots[hi].t_ms - c.knots[lo].t_ms);
+      db = c.knots[lo].db + f * (c.knots[hi].db - c.knots[lo].db);
+    }
+  } else {
+    db = c.db_per_s * t / 1000;
+  }
+  return pow(10.0, db / 20);
+}
+
+// The gain curve on one row (gain/curves.nim:316-350 and the workspace form
+// :383-418): the table where the row's times fall on it (as it is on the
+// grid, linearly interpolated off it), the curve itself elsewhere.
+template <class T> __device__ void step_gain_curve(const DevStep& st, T* X, int n, double start) {
+  if (isnan(start)) return;
+  const T* tab = reinterpret_cast<const T*>(st.table);
+  double u = (start - st.t_min_ms) / st.dt_ms;
+  long long s = 0, j0 = n, j1 = n;
+  double f = 0;
+  bool on = false;
+  if (isfinite(u) && fabs(u) <= 1e15) {
+    double r = round(u);
+    on = fabs(u - r) <= 1e-9 * fmax(1.0, fabs(u));
+    s = (long long)(on ? r : floor(u));
+    f = u - (double)s;
+    long long last = (long long)st.table_len - (on ? 1 : 2);
+    j0 = min(max(-s, 0ll), (long long)n);
+    j1 = min(max(last - s + 1, j0), (long long)n);
+  }
+  const T tf = (T)f;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    T v = X[j];
+    if (j >= j0 && j < j1) {
+      T a = __ldg(&tab[s + j]);
+      X[j] = on ? v * a : v * (a + tf * (__ldg(&tab[s + j + 1]) - a));
+    } else if (v != (T)0) {
+      X[j] = v * (T)factor_at_d(st.curve, start + (double)j * st.dt_ms);
+    }
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------ the kernel
+template <class T>
+__global__ void __launch_bounds__(256) pipeline_kernel(PipeArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Shared S;
+  T* X = reinterpret_cast<T*>(smem);
+  unsigned char* work = smem + a.work_off;
+  const T* src = reinterpret_cast<const T*>(a.src);
+  T* dst = reinterpret_cast<T*>(a.dst);
+  const bool copy = src != nullptr && src != dst;
+  for (long long r = blockIdx.x; r < a.rows; r += gridDim.x) {
+    int n = a.live[r];
+    n = n < 0 ? 0 : (n > a.cols ? a.cols : n);
+    const T* srow = (copy ? src : dst) + r * (long long)a.cols;
+    T* drow = dst + r * (long long)a.cols;
+    if (copy && n < a.cols) copy_global(srow + n, drow + n, a.cols - n);
+    if (n == 0) continue;
+    load_row(srow, X, n);
+    __syncthreads();
+    if (a.factor) {
+      double f = *a.factor;
+      if (!isnan(f)) {
+        T k = (T)f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * k;
+        __syncthreads();
+      }
+    }
+    for (int si = a.first; si < a.last; si++) {
+      const DevStep& st = a.steps[si];
+      switch (st.kind) {
+        case ST_DEMEAN: {
+          double sx = sum_x(X, n, S.red);
+          T mean = (T)(sx / (double)n);
+          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] - mean;
+          __syncthreads();
+          break;
+        }
+        case ST_DETREND: {
+          double nf = (double)n, c = (nf - 1) / 2, sx = sum_x(X, n, S.red), mean = sx / nf;
+          double stt = nf * (nf * nf - 1) / 12;
+          double slope = n > 1 ? (sum_ix(X, n, S.red) - c * sx) / stt : 0.0;
+          T ta = (T)(mean - slope * c), tb = (T)slope;
+          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] - (ta + tb * (T)i);
+          __syncthreads();
+          break;
+        }
+        case ST_SCALE: {
+          T k = (T)st.factor;
+          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * k;
+          __syncthreads();
+          break;
+        }
+        case ST_CLIP: {
+          T lo = (T)st.lo, hi = (T)st.hi;
+          for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            T v = X[i];
+            X[i] = v > hi ? hi : (v < lo ? lo : v);
+          }
+          __syncthreads();
+          break;
+        }
+        case ST_POLARITY:
+          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = -X[i];
+          __syncthreads();
+          break;
+        case ST_FILTER: step_filter(st, X, n, work, S); break;
+        case ST_AGC: step_agc(st, X, n, work, S); break;
+        case ST_NORM_TRACE: step_norm_trace(st, X, n, S); break;
+        case ST_GAIN_CURVE: step_gain_curve(st, X, n, a.start_ms ? a.start_ms[r] : (double)NAN); break;
+        default: break;
+      }
+    }
+    store_row(X, drow, n);
+    __syncthreads();
+  }
+}
+
+// ======================================================= panel statistics
+// gain/stats.nim:253-304: per row Σx² and max |x| (pass 1), then one CTA
+// folds the usable rows, and for a percentile counts a 65536-bin histogram
+// of the float32 bits of |x| >> 15 and reads the order statistics from it.
+template <class T>
+__global__ void __launch_bounds__(256) row_stats_kernel(const T* __restrict__ b, long long rows, int cols,
+                                                        const int* __restrict__ live, double* __restrict__ ss,
+                                                        double* __restrict__ mx) {
+  __shared__ Shared S;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    int n = min(max(live[r], 0), cols);
+    const T* x = b + r * (long long)cols;
+    double s = 0;
+    unsigned long long m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double v = (double)x[i];
+      s += v * v;
+      unsigned long long bb = abs_bits(x[i]);
+      m = bb > m ? bb : m;
+    }
+    s = block_sum(s, S.red);
+    m = block_max_u64(m, S.redu);
+    if (threadIdx.x == 0) {
+      ss[r] = s;
+      mx[r] = n > 0 ? bits_value(m, (T)0) : (double)NAN;
+    }
+    __syncthreads();
+  }
+}
+
+struct PanelOut {
+  double rms, maxAbs, clip, rows, samples;
+  double factor;
+  double k_rank;
+  double pad;
+};
+
+__device__ __forceinline__ bool usable_d(double ssr, double mxr, int n) {
+  return n > 0 && !isnan(mxr) && !isinf(mxr) && !(ssr == INFINITY);
+}
+
+// One CTA: fold the rows; for `stat` < 0 no factor is computed.
+__global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int cols, const int* __restrict__ live,
+                                                          const double* __restrict__ ss, const double* __restrict__ mx,
+                                                          PanelOut* out) {
+  __shared__ Shared S;
+  double sum = 0, cnt = 0, nr = 0;
+  unsigned long long mb = 0;
+  for (long long r = threadIdx.x; r < rows; r += blockDim.x) {
+    int n = min(max(live[r], 0), cols);
+    if (!usable_d(ss[r], mx[r], n)) continue;
+    sum += ss[r];
+    cnt += (double)n;
+    nr += 1;
+    unsigned long long b = (unsigned long long)__double_as_longlong(mx[r]);
+    mb = b > mb ? b : mb;
+  }
+  sum = block_sum(sum, S.red);
+  cnt = block_sum(cnt, S.red);
+  nr = block_sum(nr, S.red);
+  mb = block_max_u64(mb, S.redu);
+  if (threadIdx.x == 0) {
+    out->rows = nr;
+    out->samples = cnt;
+    out->clip = NAN;
+    out->rms = cnt > 0 ? sqrt(sum / cnt) : 0.0;
+    out->maxAbs = cnt > 0 ? __longlong_as_double((long long)mb) : 0.0;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) panel_hist_kernel(const T* __restrict__ b, long long rows, int cols,
+                                                         const int* __restrict__ live, const double* __restrict__ ss,
+                                                         const double* __restrict__ mx, unsigned* __restrict__ hist) {
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    int n = min(max(live[r], 0), cols);
+    if (!usable_d(ss[r], mx[r], n)) continue;
+    const T* x = b + r * (long long)cols;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      float a = (float)fabs((double)x[i]);
+      unsigned key = min(__float_as_uint(a) >> 15, 0xFEFFu);
+      atomicAdd(&hist[key], 1u);
+    }
+  }
+}
+
+// orderStat (gain/stats.nim:237-251) for ranks j0 and j0 + 1, one CTA of 1024.
+__device__ double order_stat_from(const unsigned* hist, long long j, double mxv, int bin, long long below) {
+  if (bin == 0) return 0;
+  double c = (double)hist[bin];
+  double lo = (double)__uint_as_float((unsigned)bin << 15);
+  double hi = fmin((double)__uint_as_float((unsigned)(bin + 1) << 15), mxv);
+  return fmin(fmax(lo + ((double)(j - below) + 0.5) / c * (hi - lo), lo), mxv);
+}
+
+__global__ void __launch_bounds__(1024) panel_clip_kernel(const unsigned* __restrict__ hist, PanelOut* out,
+                                                          double clipP, int stat, double target, int dtype) {
+  __shared__ long long pre[1024];
+  __shared__ long long found_below[2];
+  __shared__ int found_bin[2];
+  const int per = 64;  // 65536 / 1024 bins per thread
+  const int maxKey = 0xFEFF;
+  long long tot = 0;
+  for (int k = 0; k < per; k++) {
+    int bin = threadIdx.x * per + k;
+    if (bin <= maxKey) tot += hist[bin];
+  }
+  pre[threadIdx.x] = tot;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
+    long long v = threadIdx.x >= o ? pre[threadIdx.x - o] : 0;
+    __syncthreads();
+    pre[threadIdx.x] += v;
+    __syncthreads();
+  }
+  double samples = out->samples, mxv = out->maxAbs;
+  bool have = samples > 0 && !isnan(clipP);
+  double rank = have ? (samples - 1) * clipP / 100 : 0;
+  long long k0 = have ? (long long)fmin(floor(rank), samples - 1) : 0;
+  if (threadIdx.x < 2) {
+    found_bin[threadIdx.x] = -1;
+    found_below[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  if (have) {
+    for (int q = 0; q < 2; q++) {
+      long long j = k0 + q;
+      long long excl = pre[threadIdx.x] - tot;
+      if (j >= excl && j < pre[threadIdx.x]) {
+        long long below = excl;
+        for (int k = 0; k < per; k++) {
+          int bin = threadIdx.x * per + k;
+          long long c = bin <= maxKey ? hist[bin] : 0;
+          if (below + c > j) {
+            found_bin[q] = bin;
+            found_below[q] = below;
+            break;
+          }
+          below += c;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double clip = NAN;
+    if (have) {
+      if (clipP == 100) {
+        clip = mxv;
+      } else {
+        double lower = found_bin[0] < 0 ? mxv : order_stat_from(hist, k0, mxv, found_bin[0], found_below[0]);
+        double f = rank - (double)k0;
+        if (f == 0 || (double)(k0 + 1) >= samples) clip = lower;
+        else {
+          double upper = found_bin[1] < 0 ? mxv : order_stat_from(hist, k0 + 1, mxv, found_bin[1], found_below[1]);
+          clip = lower + f * (upper - lower);
+        }
+      }
+    }
+    out->clip = clip;
+    double factor = NAN;
+    if (stat >= 0) {
+      double level = stat == PSG_NORM_MAX ? out->maxAbs : (stat == PSG_NORM_RMS ? out->rms : clip);
+      bool ok = dtype == PSG_F32 ? fits_d<float>(target / level) : fits_d<double>(target / level);
+      if (fin_pos_d(level) && ok) factor = target / level;
+    }
+    out->factor = factor;
+  }
+}
+
+// ============================================================ correlation
+struct CorrArgs {
+  const void* src;
+  void* dst;
+  long long rows;
+  int cols, out, nfft, shift, pilot_len, record;
+  const int* live;
+  const void* mul;    // V[bins]
+  const void* tw;
+  const void* split;
+  FftDesc fft;
+  void* gwork;        // per-CTA global scratch when shared memory is too small (else NULL)
+  // stack epilogue
+  double* num;
+  int* cnt;
+  int stack_samples;
+  long long stack_rows;
+  const int* row_map;
+  const int* stack_live;
+  int stack_on;
+};
+
+// correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
+// pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
+template <class T>
+__global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
+  typedef typename C2<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Shared S;
+  const int m = a.nfft / 2;
+  V* A = a.gwork ? reinterpret_cast<V*>(a.gwork) + (size_t)blockIdx.x * 2 * m : reinterpret_cast<V*>(smem);
+  V* B = A + m;
+  const T* src = reinterpret_cast<const T*>(a.src);
+  T* dst = reinterpret_cast<T*>(a.dst);
+  const V* mul = reinterpret_cast<const V*>(a.mul);
+  const V* tw = reinterpret_cast<const V*>(a.tw);
+  const V* split = reinterpret_cast<const V*>(a.split);
+  const int wrapped = min(max(1 - a.pilot_len - a.shift, 0), a.out);
+  const int direct = min(max(-a.shift, wrapped), a.out);
+  const int last = min(max(a.record - a.shift, direct), a.out);
+  for (long long r = blockIdx.x; r < a.rows; r += gridDim.x) {
+    int n = min(max(a.live[r], 0), a.cols);
+    V* y = nullptr;
+    if (n > 0) {
+      const T* x = src + r * (long long)a.cols;
+      T* Ar = reinterpret_cast<T*>(A);
+      for (int j = threadIdx.x; j < a.nfft; j += blockDim.x) Ar[j] = j < n ? x[j] : (T)0;
+      __syncthreads();
+      V* z = cfft_forward<T>(A, B, a.fft, tw);
+      split_mul_unsplit<T>(z, m, split, (T)1 / (T)a.nfft, [&](V v, int k) {
+        V w = __ldg(&mul[k]);
+        return V{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
+      });
+      y = cfft_forward<T>(z, z == A ? B : A, a.fft, tw);
+    }
+    // lagSpans / scatter: the output at column c reads lag c + shift
+    // (wrapped by nfft for negative lags).
+    auto value = [&](int c) -> T {
+      if (!y || c < wrapped || c >= last) return (T)0;
+      int idx = c < direct ? c + a.shift + a.nfft : c + a.shift;
+      V v = y[idx >> 1];
+      return (idx & 1) ? v.x : v.y;
+    };
+    if (dst) {
+      T* d = dst + r * (long long)a.out;
+      for (int c = threadIdx.x; c < a.out; c += blockDim.x) d[c] = value(c);
+    }
+    if (a.stack_on) {
+      int o = a.row_map ? a.row_map[r] : (int)r;
+      int sn = a.stack_live ? min(max(a.stack_live[r], 0), a.stack_samples) : min(a.out, a.stack_samples);
+      if (o >= 0 && o < a.stack_rows && sn > 0) {
+        double bad = 0;
+        for (int c = threadIdx.x; c < sn; c += blockDim.x) {
+          double v = (double)value(c);
+          bad += v - v;  // allFinite: x − x is 0 for finite x
+        }
+        bad = block_sum(bad, S.red);
+        if (bad == 0) {
+          double* nm = a.num + (long long)o * a.stack_samples;
+          int* ct = a.cnt + (long long)o * a.stack_samples;
+          for (int c = threadIdx.x; c < sn; c += blockDim.x) {
+            atomicAdd(nm + c, (double)value(c));
+            atomicAdd(ct + c, 1);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// RecordStack.addRecord for a block already in memory.
+template <class T>
+__global__ void __launch_bounds__(256) stack_add_kernel(const T* __restrict__ b, long long rows, int cols,
+                                                        const int* __restrict__ live, const int* __restrict__ row_map,
+                                                        double* num, int* cnt, int samples, long long out_rows) {
+  __shared__ Shared S;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    int o = row_map ? row_map[r] : (int)r;
+    int n = min(max(live[r], 0), min(cols, samples));
+    if (o < 0 || o >= out_rows || n == 0) continue;
+    const T* x = b + r * (long long)cols;
+    double bad = 0;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      double v = (double)x[c];
+      bad += v - v;
+    }
+    bad = block_sum(bad, S.red);
+    if (bad == 0) {
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        num[(long long)o * samples + c] += (double)x[c];
+        cnt[(long long)o * samples + c] += 1;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void stack_result_kernel(const double* __restrict__ num, const int* __restrict__ cnt, long long total,
+                                    int norm, T* __restrict__ d) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    double c = (double)cnt[i];
+    T v;
+    if (c == 0) v = (T)0;
+    else if (norm == PSG_FN_NONE) v = (T)num[i];
+    else if (norm == PSG_FN_FOLD) v = (T)(num[i] / c);
+    else v = (T)(num[i] / sqrt(c));
+    d[i] = v;
+  }
+}
+
+// ======================================================== host plumbing
+static int g_sm_count = 0, g_max_smem = 0, g_device = -1;
+
+static void ensure_device() {
+  int dev;
+  CUDA_OK(cudaGetDevice(&dev));
+  if (dev != g_device) {
+    cudaDeviceProp p;
+    CUDA_OK(cudaGetDeviceProperties(&p, dev));
+    if (p.major < 10) throw CudaError("libpsgcuda.so needs an sm_100 device, found sm_" + std::to_string(p.major * 10 + p.minor));
+    g_sm_count = p.multiProcessorCount;
+    g_max_smem = (int)p.sharedMemPerBlockOptin;
+    g_device = dev;
+  }
+}
+
+template <class K> static void allow_smem(K kernel) {
+  CUDA_OK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_max_smem - (int)sizeof(Shared) - 1024));
+}
+
+struct DeviceBuf {
+  void* p = nullptr;
+  ~DeviceBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+template <class T> static void* upload(std::vector<std::unique_ptr<DeviceBuf>>& keep, const std::vector<T>& v) {
+  if (v.empty()) return nullptr;
+  auto b = std::make_unique<DeviceBuf>();
+  CUDA_OK(cudaMalloc(&b->p, v.size() * sizeof(T)));
+  CUDA_OK(cudaMemcpy(b->p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  void* p = b->p;
+  keep.push_back(std::move(b));
+  return p;
+}
+template <class T> static std::vector<T> as_t(const std::vector<double>& v) {
+  return std::vector<T>(v.begin(), v.end());
+}
+template <class T>
+static std::vector<typename C2<T>::type> as_c(const std::vector<double>& re, const std::vector<double>& im) {
+  std::vector<typename C2<T>::type> o(re.size());
+  for (size_t i = 0; i < re.size(); i++) o[i] = {(T)re[i], (T)im[i]};
+  return o;
+}
+static FftDesc fft_desc(const FftTables& t) {
+  FftDesc d{};
+  d.m = (int)t.m;
+  d.npass = (int)t.radices.size();
+  if (d.npass > 24) throw InvalidArg("an FFT of more than 24 passes");
+  int64_t cur = t.m, off = 0;
+  for (int i = 0; i < d.npass; i++) {
+    d.radix[i] = t.radices[i];
+    d.twoff[i] = (int)off;
+    int64_t sub = cur / t.radices[i];
+    off += sub * (t.radices[i] - 1);
+    cur = sub;
+  }
+  return d;
+}
+
+}  // namespace psg
+
+using namespace psg;
+
+__global__ void trace_stats_finish(double* rms, double* mx, const int* live, long long rows, int cols);
+
+// =================================================================== plans
+struct psg_plan {
+  PlanHost host;
+  std::vector<std::unique_ptr<DeviceBuf>> keep;
+  DevStep* d_steps = nullptr;
+  int device = 0;
+  int threads = 256;
+  int x_elems = 0, work_off = 0;
+  size_t smem = 0;
+  int grid = 1;
+  bool needs_panel = false;
+};
+
+struct psg_workspace {
+  int device = -1;
+  void* d = nullptr;
+  int64_t bytes = 0;
+};
+
+struct psg_corr_plan {
+  CorrHost host;
+  int dtype = 0;
+  std::vector<std::unique_ptr<DeviceBuf>> keep;
+  void* mul = nullptr;
+  void* tw = nullptr;
+  void* split = nullptr;
+  void* gwork = nullptr;
+  size_t smem = 0;
+  int grid = 1;
+  FftDesc fft{};
+};
+
+struct psg_stack {
+  int64_t rows = 0;
+  int32_t samples = 0;
+  double dt_ms = 0;
+  double* num = nullptr;
+  int* cnt = nullptr;
+};
+
+template <class F> static int guarded(F&& f) {
+  try {
+    f();
+    t_err.clear();
+    return PSG_OK;
+  } catch (const InvalidArg& e) {
+    t_err = e.what();
+    return PSG_EINVAL;
+  } catch (const WorkspaceError& e) {
+    t_err = e.what();
+    return PSG_EWORKSPACE;
+  } catch (const CudaError& e) {
+    t_err = e.what();
+    std::string w = e.what();
+    if (w.find("out of memory") != std::string::npos) return PSG_ENOMEM;
+    if (w.find("needs an sm_100") != std::string::npos || w.find("no CUDA-capable") != std::string::npos) return PSG_ENODEV;
+    return PSG_ECUDA;
+  } catch (const std::bad_alloc&) {
+    t_err = "host allocation failed";
+    return PSG_ENOMEM;
+  } catch (const std::exception& e) {
+    t_err = e.what();
+    return PSG_EINVAL;
+  }
+}
+
+// Workspace layout (bytes): [0, 512) panel outputs and factors, then
+// rows × 16 B of per-row statistics, then the 65536-bin histogram, then the
+// host-path staging (live, start_ms, samples).
+static const int64_t kHist = 65536 * 4;
+static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
+static int64_t ws_device_bytes(int64_t rows) { return 512 + align256(rows * 16) + kHist; }
+static int64_t ws_host_bytes(int64_t rows, int32_t cols, int dtype) {
+  return ws_device_bytes(rows) + align256(rows * 4) + align256(rows * 8) +
+         align256(rows * (int64_t)cols * (dtype == PSG_F32 ? 4 : 8));
+}
+
+template <class T> static void build_device_steps(psg_plan* p) {
+  typedef typename C2<T>::type V;
+  std::vector<DevStep> ds;
+  int64_t work = 0;
+  for (auto& s : p->host.steps) {
+    DevStep d{};
+    d.kind = s.kind;
+    d.factor = s.factor;
+    d.lo = s.lo;
+    d.hi = s.hi;
+    d.dt_ms = p->host.dt_ms;
+    if (s.kind == ST_FILTER) {
+      const FilterHost& f = s.filter;
+      if (f.nfft > (1 << 24)) throw InvalidArg("the filter's FFT is too long for the device");
+      d.trend = f.trend;
+      d.reflect = f.reflect;
+      d.zero_dc = f.spec.zero_dc;
+      d.pad = (int)f.pad;
+      d.nfft = (int)f.nfft;
+      d.dc_gain = f.dc_gain;
+      d.fft = fft_desc(f.fft);
+      d.gain = upload(p->keep, as_t<T>(f.gain));
+      d.fall = upload(p->keep, as_t<T>(f.fall));
+      d.tw = upload(p->keep, as_c<T>(f.fft.tw_re, f.fft.tw_im));
+      d.split = upload(p->keep, as_c<T>(f.fft.split_re, f.fft.split_im));
+      work = std::max<int64_t>(work, 2 * f.fft.m * (int64_t)sizeof(V));
+    } else if (s.kind == ST_AGC) {
+      d.half = (int)s.half;
+      d.agc_mode = s.agc_mode;
+      d.target = s.target;
+      d.epsilon = s.epsilon;
+      int64_t n = p->host.samples;
+      work = std::max<int64_t>(work, (((n + 1 + 3) & ~3LL) + n) * (int64_t)sizeof(T));
+    } else if (s.kind == ST_NORM_TRACE || s.kind == ST_NORM_PANEL) {
+      d.stat = s.stat;
+      d.norm_target = s.norm_target;
+      d.percentile = s.percentile;
+    } else if (s.kind == ST_GAIN_CURVE) {
+      d.curve = s.curve;
+      d.t_min_ms = s.t_min_ms;
+      d.table_len = (int)s.table.size();
+      d.table = upload(p->keep, as_t<T>(s.table));
+    }
+    if (s.kind == ST_NORM_PANEL) p->needs_panel = true;
+    ds.push_back(d);
+  }
+  // Each part's panel statistics live in a 64-byte slot of the workspace's
+  // first 448 bytes.
+  if (p->host.parts.size() > 6) throw InvalidArg("a plan takes at most 5 per-panel normalizations after its first op");
+  p->x_elems = (int)((p->host.samples + 3) & ~3LL);
+  p->work_off = (int)align256(p->x_elems * (int64_t)sizeof(T));
+  p->smem = (size_t)(p->work_off + work);
+  int limit = g_max_smem - (int)sizeof(Shared) - 1024;
+  if ((int64_t)p->smem > limit)
+    throw InvalidArg("the plan's traces (" + std::to_string(p->host.samples) + " samples) and FFTs need " +
+                     std::to_string(p->smem) + " bytes of shared memory; the device gives " + std::to_string(limit));
+  if (!ds.empty()) {
+    DeviceBuf* b = new DeviceBuf();
+    p->keep.emplace_back(b);
+    CUDA_OK(cudaMalloc(&b->p, ds.size() * sizeof(DevStep)));
+    CUDA_OK(cudaMemcpy(b->p, ds.data(), ds.size() * sizeof(DevStep), cudaMemcpyHostToDevice));
+    p->d_steps = (DevStep*)b->p;
+  }
+  allow_smem(pipeline_kernel<T>);
+  int per_sm = 0;
+  CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel<T>, p->threads, p->smem));
+  p->grid = std::max(1, per_sm) * g_sm_count;
+}
+
+template <class T>
+static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
+                        int32_t cols, const int* live, const double* start, cudaStream_t stream) {
+  auto range = p->host.parts[part];
+  bool panel = range.first < range.second && p->host.steps[range.first].kind == ST_NORM_PANEL;
+  const double* factor = nullptr;
+  if (panel) {
+    // The factor over the whole block as the previous part left it (or src).
+    const StepHost& ns = p->host.steps[range.first];
+    const T* blk = reinterpret_cast<const T*>(src ? src : dst);
+    char* base = (char*)ws->d;
+    PanelOut* out = reinterpret_cast<PanelOut*>(base + 64 * part);
+    double* ss = reinterpret_cast<double*>(base + 512);
+    double* mx = ss + rows;
+    unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
+    int g = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
+    if (rows > 0) row_stats_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx);
+    panel_fold_kernel<<<1, 1024, 0, stream>>>(rows, cols, live, ss, mx, out);
+    double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
+    if (!std::isnan(clipP)) {
+      CUDA_OK(cudaMemsetAsync(hist, 0, kHist, stream));
+      if (rows > 0) panel_hist_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx, hist);
+    }
+    panel_clip_kernel<<<1, 1024, 0, stream>>>(hist, out, clipP, ns.stat, ns.norm_target, p->host.dtype);
+    factor = &out->factor;
+  }
+  PipeArgs a{};
+  a.src = src;
+  a.dst = dst;
+  a.rows = rows;
+  a.cols = cols;
+  a.x_elems = p->x_elems;
+  a.work_off = p->work_off;
+  a.first = panel ? range.first + 1 : range.first;
+  a.last = range.second;
+  a.live = live;
+  a.start_ms = start;
+  a.factor = factor;
+  a.steps = p->d_steps;
+  bool nothing = a.first >= a.last && !factor && (src == nullptr || src == dst);
+  if (nothing || rows == 0) return;
+  int grid = (int)std::min<int64_t>(rows, p->grid);
+  pipeline_kernel<T><<<grid, p->threads, p->smem, stream>>>(a);
+  CUDA_OK(cudaGetLastError());
+}
+
+template <class T> static void corr_upload(psg_corr_plan* p) {
+  typedef typename C2<T>::type V;
+  p->mul = upload(p->keep, as_c<T>(p->host.mul_re, p->host.mul_im));
+  p->tw = upload(p->keep, as_c<T>(p->host.fft.tw_re, p->host.fft.tw_im));
+  p->split = upload(p->keep, as_c<T>(p->host.fft.split_re, p->host.fft.split_im));
+  p->fft = fft_desc(p->host.fft);
+  size_t need = (size_t)(2 * p->host.fft.m * sizeof(V));
+  int limit = g_max_smem - (int)sizeof(Shared) - 1024;
+  allow_smem(corr_kernel<T>);
+  if ((int64_t)need <= limit) {
+    p->smem = need;
+    int per_sm = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, corr_kernel<T>, 256, p->smem));
+    p->grid = std::max(1, per_sm) * g_sm_count;
+  } else {
+    // Too long for shared memory: each CTA works in its own slice of global
+    // memory (mostly L2-resident at these lengths).
+    p->smem = 0;
+    p->grid = g_sm_count * 2;
+    auto b = std::make_unique<DeviceBuf>();
+    CUDA_OK(cudaMalloc(&b->p, need * p->grid));
+    p->gwork = b->p;
+    p->keep.push_back(std::move(b));
+  }
+}
+
+extern "C" {
+
+const char* psg_last_error(void) { return t_err.c_str(); }
+const char* psg_version(void) { return "processseg_b200 0.1 (sm_100a)"; }
+
+int psg_init(int device) {
+  return guarded([&] {
+    CUDA_OK(cudaSetDevice(device));
+    ensure_device();
+  });
+}
+
+int psg_is_fast_len(int64_t n) { return fast_len(n) ? 1 : 0; }
+int64_t psg_next_fast_len(int64_t n, int even) { return next_fast(n, even != 0); }
+
+int psg_impulse_length(const psg_filter_spec* spec, double dt_ms, int32_t* out) {
+  return guarded([&] {
+    if (!spec || !out) throw InvalidArg("null argument");
+    *out = (int32_t)spec_impulse_length(*spec, dt_ms);
+  });
+}
+int psg_response(const psg_filter_spec* spec, double f_hz, double dt_ms, double* out) {
+  return guarded([&] {
+    if (!spec || !out) throw InvalidArg("null argument");
+    *out = spec_response(*spec, f_hz, dt_ms);
+  });
+}
+int psg_required_margin(const psg_op* ops, int32_t n_ops, double dt_ms, int32_t* out) {
+  return guarded([&] {
+    if (!out || (n_ops > 0 && !ops)) throw InvalidArg("null argument");
+    *out = (int32_t)required_margin(ops, n_ops, dt_ms);
+  });
+}
+void psg_decode_window(int64_t a, int64_t b, int64_t margin, int64_t trace_len, int64_t* out) {
+  int64_t m = std::min(std::max<int64_t>(margin, 0), std::max<int64_t>(trace_len, 0));
+  out[0] = std::max<int64_t>(0, a - m);
+  out[1] = std::min(trace_len - 1, b + m);
+}
+
+int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms, int32_t samples,
+                     int32_t record_samples, psg_plan** out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    *out = nullptr;
+    std::unique_ptr<psg_plan> p(new psg_plan());
+    p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples);
+    ensure_device();
+    CUDA_OK(cudaGetDevice(&p->device));
+    if (dtype == PSG_F32) build_device_steps<float>(p.get());
+    else build_device_steps<double>(p.get());
+    *out = p.release();
+  });
+}
+void psg_plan_destroy(psg_plan* plan) { delete plan; }
+int32_t psg_plan_margin(const psg_plan* p) { return p ? (int32_t)p->host.margin : 0; }
+uint64_t psg_plan_generation(const psg_plan* p) { return p ? p->host.generation : 0; }
+int32_t psg_plan_samples(const psg_plan* p) { return p ? (int32_t)p->host.samples : 0; }
+int32_t psg_plan_record_samples(const psg_plan* p) { return p ? (int32_t)p->host.record_samples : 0; }
+int32_t psg_plan_part_count(const psg_plan* p) { return p ? (int32_t)p->host.parts.size() : 0; }
+int32_t psg_plan_len(const psg_plan* p) { return p ? (int32_t)p->host.steps.size() : 0; }
+int32_t psg_plan_step_nfft(const psg_plan* p, int32_t i) {
+  if (!p || i < 0 || i >= (int)p->host.steps.size()) return 0;
+  return p->host.steps[i].kind == ST_FILTER ? (int32_t)p->host.steps[i].filter.nfft : 0;
+}
+int32_t psg_plan_step_margin(const psg_plan* p, int32_t i) {
+  if (!p || i < 0 || i >= (int)p->host.steps.size()) return 0;
+  return (int32_t)p->host.steps[i].margin();
+}
+int64_t psg_plan_workspace_bytes(const psg_plan* p, int64_t rows, int32_t cols) {
+  return p ? ws_host_bytes(rows, cols, p->host.dtype) : 0;
+}
+
+int psg_workspace_create(psg_workspace** out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    *out = new psg_workspace();
+  });
+}
+void psg_workspace_destroy(psg_workspace* ws) {
+  if (!ws) return;
+  if (ws->d) cudaFree(ws->d);
+  delete ws;
+}
+static void ws_grow(psg_workspace* ws, int64_t need) {
+  int dev;
+  CUDA_OK(cudaGetDevice(&dev));
+  if (ws->d && ws->device != dev) throw InvalidArg("the workspace belongs to another device");
+  if (ws->bytes >= need) return;
+  if (ws->d) {
+    CUDA_OK(cudaDeviceSynchronize());
+    CUDA_OK(cudaFree(ws->d));
+    ws->d = nullptr;
+    ws->bytes = 0;
+  }
+  CUDA_OK(cudaMalloc(&ws->d, (size_t)need));
+  ws->bytes = need;
+  ws->device = dev;
+}
+int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows, int32_t cols) {
+  return guarded([&] {
+    if (!ws || !plan) throw InvalidArg("null argument");
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    ws_grow(ws, ws_host_bytes(rows, cols, plan->host.dtype));
+  });
+}
+int64_t psg_workspace_bytes(const psg_workspace* ws) { return ws ? ws->bytes : 0; }
+
+int psg_rows_flatten(const int32_t* status, const int32_t* num_samples, const double* t0_ms, int64_t rows,
+                     int32_t first_sample, double dt_ms, const int64_t* failed, int64_t n_failed, int32_t cols,
+                     int32_t mode, int32_t* live_out, double* start_ms_out) {
+  return guarded([&] {
+    if (rows < 0 || (rows > 0 && (!status || !num_samples || !live_out))) throw InvalidArg("null argument");
+    if (!(std::isfinite(dt_ms) && dt_ms > 0)) throw InvalidArg("dtMs must be finite and positive");
+    if (first_sample < 0) throw InvalidArg("firstSample must be ≥ 0");
+    // ChunkMeta's failed list is ascending and unique (core/types.nim:106-113).
+    for (int64_t i = 0; i < n_failed; i++) {
+      if (failed[i] < 0 || failed[i] >= rows) throw InvalidArg("failed row " + std::to_string(failed[i]) + " is outside 0 ..< " + std::to_string(rows));
+      if (i > 0 && failed[i] <= failed[i - 1]) throw InvalidArg("failed rows must be ascending and unique");
+    }
+    int64_t fi = 0;
+    for (int64_t r = 0; r < rows; r++) {
+      bool is_failed = false;
+      while (fi < n_failed && failed[fi] < r) fi++;
+      if (fi < n_failed && failed[fi] == r) is_failed = true;
+      int32_t st = status[r];
+      bool use = mode == 0 ? ((st == PSG_TS_LIVE || st == PSG_TS_UNKNOWN) && !is_failed)
+                           : (st != PSG_TS_DEAD && !is_failed);
+      int64_t n = std::min<int64_t>(std::max<int64_t>((int64_t)num_samples[r] - first_sample, 0), cols);
+      live_out[r] = use ? (int32_t)n : 0;
+      if (start_ms_out) start_ms_out[r] = (t0_ms ? t0_ms[r] : NAN) + (double)first_sample * dt_ms;
+    }
+  });
+}
+
+static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
+                        const int32_t* live, double dt_ms, bool need_ws) {
+  if (!plan) throw InvalidArg("a PipelinePlan must come from compile");
+  if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+  if (rows > 0 && (!dst || !live)) throw InvalidArg("dst and live are required");
+  int64_t esz = plan->host.dtype == PSG_F32 ? 4 : 8;
+  if (src && src != dst) {
+    uintptr_t s0 = (uintptr_t)src, d0 = (uintptr_t)dst, bytes = (uintptr_t)(rows * cols * esz);
+    if (s0 < d0 + bytes && d0 < s0 + bytes) throw InvalidArg("src and dst overlap without being the same block");
+  }
+  if (!same_interval(dt_ms, plan->host.dt_ms))
+    throw InvalidArg("the plan is for dtMs = " + std::to_string(plan->host.dt_ms) + ", the rows have " + std::to_string(dt_ms));
+  if (cols > plan->host.samples)
+    throw InvalidArg("the block has " + std::to_string(cols) + " columns, the plan takes " + std::to_string(plan->host.samples) + " samples");
+  if (need_ws) {
+    if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
+    int64_t need = plan->needs_panel ? ws_device_bytes(rows) : 0;
+    if (ws->bytes < need) throw WorkspaceError("reserve the workspace for the plan first");
+  }
+}
+
+int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
+              const int32_t* live, const double* start_ms, double dt_ms, void* stream) {
+  return guarded([&] {
+    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, true);
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int part = 0; part < (int)plan->host.parts.size(); part++) {
+      const void* from = part == 0 ? src : nullptr;
+      if (plan->host.dtype == PSG_F32) launch_part<float>(plan, ws, part, from, dst, rows, cols, live, start_ms, s);
+      else launch_part<double>(plan, ws, part, from, dst, rows, cols, live, start_ms, s);
+    }
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host, void* dst_host, int64_t rows,
+                   int32_t cols, const int32_t* live_host, const double* start_ms_host, double dt_ms, void* stream) {
+  return guarded([&] {
+    check_apply(plan, ws, src_host, dst_host, rows, cols, live_host, dt_ms, false);
+    if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
+    if (ws->bytes < ws_host_bytes(rows, cols, plan->host.dtype)) throw WorkspaceError("reserve the workspace for the plan first");
+    if (rows == 0) return;
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t esz = plan->host.dtype == PSG_F32 ? 4 : 8;
+    char* base = (char*)ws->d + ws_device_bytes(rows);
+    int32_t* d_live = (int32_t*)base;
+    double* d_start = (double*)(base + align256(rows * 4));
+    void* d_data = base + align256(rows * 4) + align256(rows * 8);
+    size_t bytes = (size_t)(rows * cols * esz);
+    const void* from = src_host ? src_host : dst_host;
+    CUDA_OK(cudaMemcpyAsync(d_data, from, bytes, cudaMemcpyHostToDevice, s));
+    CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, s));
+    if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, s));
+    for (int part = 0; part < (int)plan->host.parts.size(); part++) {
+      if (plan->host.dtype == PSG_F32)
+        launch_part<float>(plan, ws, part, nullptr, d_data, rows, cols, d_live, start_ms_host ? d_start : nullptr, s);
+      else
+        launch_part<double>(plan, ws, part, nullptr, d_data, rows, cols, d_live, start_ms_host ? d_start : nullptr, s);
+    }
+    CUDA_OK(cudaMemcpyAsync(dst_host, d_data, bytes, cudaMemcpyDeviceToHost, s));
+    CUDA_OK(cudaStreamSynchronize(s));
+  });
+}
+
+int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* block, int64_t rows, int32_t cols,
+                     const int32_t* live, double* factor_out, void* stream) {
+  return guarded([&] {
+    if (!plan) throw InvalidArg("a PipelinePlan must come from compile");
+    if (part < 0 || part >= (int)plan->host.parts.size()) throw WorkspaceError("no part " + std::to_string(part));
+    auto range = plan->host.parts[part];
+    if (!(range.first < range.second && plan->host.steps[range.first].kind == ST_NORM_PANEL))
+      throw WorkspaceError("part " + std::to_string(part) + " has no per-panel normalization");
+    if (!ws || ws->bytes < ws_device_bytes(rows)) throw WorkspaceError("reserve the workspace for the plan first");
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    const StepHost& ns = plan->host.steps[range.first];
+    char* base = (char*)ws->d;
+    PanelOut* out = reinterpret_cast<PanelOut*>(base + 64 * part);
+    double* ss = reinterpret_cast<double*>(base + 512);
+    double* mx = ss + rows;
+    unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)g_sm_count * 8));
+    double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
+    if (plan->host.dtype == PSG_F32) {
+      if (rows > 0) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
+    } else {
+      if (rows > 0) row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
+    }
+    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, out);
+    if (!std::isnan(clipP)) {
+      CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
+      if (rows > 0) {
+        if (plan->host.dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
+        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
+      }
+    }
+    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, out, clipP, ns.stat, ns.norm_target, plan->host.dtype);
+    CUDA_OK(cudaMemcpyAsync(factor_out, &out->factor, 8, cudaMemcpyDeviceToDevice, s));
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_trace_stats(const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live, double* rms_out,
+                    double* max_abs_out, void* stream) {
+  return guarded([&] {
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if (rows == 0) return;
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    int g = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
+    // Σx² into rms_out, max into max_abs_out, then rms = sqrt(Σx²/n) per row
+    if (dtype == PSG_F32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, rms_out, max_abs_out);
+    else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, rms_out, max_abs_out);
+    trace_stats_finish<<<(int)((rows + 255) / 256), 256, 0, s>>>(rms_out, max_abs_out, live, rows, cols);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live,
+                    double clip_percentile, double* out, void* stream) {
+  return guarded([&] {
+    if (!std::isnan(clip_percentile) && !(clip_percentile >= 0 && clip_percentile <= 100))
+      throw InvalidArg("a percentile must be in 0 .. 100, got " + std::to_string(clip_percentile));
+    if (!ws || ws->bytes < ws_device_bytes(rows)) throw WorkspaceError("reserve the workspace first (psg_workspace_reserve)");
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    char* base = (char*)ws->d;
+    PanelOut* po = reinterpret_cast<PanelOut*>(base + 448);
+    double* ss = reinterpret_cast<double*>(base + 512);
+    double* mx = ss + rows;
+    unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)g_sm_count * 8));
+    if (rows > 0) {
+      if (dtype == PSG_F32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
+      else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
+    }
+    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po);
+    if (!std::isnan(clip_percentile)) {
+      CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
+      if (rows > 0) {
+        if (dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
+        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
+      }
+    }
+    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
+    CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+// ------------------------------------------------------------- vibroseis
+int psg_linear_sweep(double f1, double f2, double length_ms, double dt_ms, double ts, double te, int32_t shape,
+                     double phase_deg, double amplitude, double max_nyq, int32_t dtype, void* out, int64_t* n_out) {
+  return guarded([&] {
+    if (!n_out) throw InvalidArg("null argument");
+    std::vector<double> x = linear_sweep(f1, f2, length_ms, dt_ms, ts, te, shape, phase_deg, amplitude, max_nyq);
+    *n_out = (int64_t)x.size();
+    if (out) {
+      if (dtype == PSG_F32)
+        for (size_t i = 0; i < x.size(); i++) ((float*)out)[i] = (float)x[i];
+      else
+        std::memcpy(out, x.data(), x.size() * 8);
+    }
+  });
+}
+
+int psg_corr_plan_create(const void* pilot, int32_t pilot_dtype, int64_t pilot_len, double pilot_dt_ms, double pilot_t0_ms,
+                         int32_t dtype, double dt_ms, int32_t record_samples, int32_t out_samples, int32_t mode,
+                         double eps_percent, int32_t normalize, psg_corr_plan** out) {
+  return guarded([&] {
+    if (!out || !pilot) throw InvalidArg("null argument");
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    std::vector<double> pv(pilot_len > 0 ? pilot_len : 0);
+    for (int64_t i = 0; i < pilot_len; i++)
+      pv[i] = pilot_dtype == PSG_F32 ? (double)((const float*)pilot)[i] : ((const double*)pilot)[i];
+    std::unique_ptr<psg_corr_plan> p(new psg_corr_plan());
+    p->host = corr_plan(pv.data(), pilot_len, pilot_dt_ms, pilot_t0_ms, dt_ms, record_samples, out_samples, mode,
+                        eps_percent, normalize != 0);
+    p->dtype = dtype;
+    ensure_device();
+    if (dtype == PSG_F32) corr_upload<float>(p.get());
+    else corr_upload<double>(p.get());
+    *out = p.release();
+  });
+}
+void psg_corr_plan_destroy(psg_corr_plan* p) { delete p; }
+int32_t psg_corr_plan_nfft(const psg_corr_plan* p) { return p ? (int32_t)p->host.n : 0; }
+int32_t psg_corr_plan_out_samples(const psg_corr_plan* p) { return p ? (int32_t)p->host.out : 0; }
+double psg_corr_plan_scale(const psg_corr_plan* p) { return p ? p->host.scale : 0; }
+
+static int corr_launch(const psg_corr_plan* plan, psg_stack* st, const void* src, void* dst, int64_t rows, int32_t cols,
+                       const int32_t* live, const int32_t* stack_live, const int32_t* row_map, double dt_ms, void* stream) {
+  return guarded([&] {
+    if (!plan) throw InvalidArg("a CorrelationPlan must come from initCorrelationPlan");
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if (cols > plan->host.record)
+      throw InvalidArg("the records are " + std::to_string(cols) + " samples, the plan takes " + std::to_string(plan->host.record));
+    if (!same_interval(dt_ms, plan->host.dt_ms))
+      throw InvalidArg("the records are at " + std::to_string(dt_ms) + " ms, the plan at " + std::to_string(plan->host.dt_ms) + " ms");
+    if (st && !same_interval(st->dt_ms, dt_ms)) throw InvalidArg("the stack is at another interval");
+    if (st && !row_map && rows > st->rows) throw InvalidArg("a record of " + std::to_string(rows) + " rows into a stack of " + std::to_string(st->rows) + " (pass a rowMap)");
+    if (rows == 0) return;
+    if (!src || !live || (!dst && !st)) throw InvalidArg("null argument");
+    ensure_device();
+    CorrArgs a{};
+    a.src = src;
+    a.dst = dst;
+    a.rows = rows;
+    a.cols = cols;
+    a.out = (int)plan->host.out;
+    a.nfft = (int)plan->host.n;
+    a.shift = (int)plan->host.shift;
+    a.pilot_len = (int)plan->host.pilot_len;
+    a.record = (int)plan->host.record;
+    a.live = live;
+    a.mul = plan->mul;
+    a.tw = plan->tw;
+    a.split = plan->split;
+    a.fft = plan->fft;
+    a.gwork = plan->gwork;
+    if (st) {
+      a.stack_on = 1;
+      a.num = st->num;
+      a.cnt = st->cnt;
+      a.stack_samples = st->samples;
+      a.stack_rows = st->rows;
+      a.row_map = row_map;
+      a.stack_live = stack_live;
+    }
+    int grid = (int)std::min<int64_t>(rows, plan->grid);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (plan->dtype == PSG_F32) corr_kernel<float><<<grid, 256, plan->smem, s>>>(a);
+    else corr_kernel<double><<<grid, 256, plan->smem, s>>>(a);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_correlate(const psg_corr_plan* plan, const void* src, void* dst, int64_t rows, int32_t cols, const int32_t* live,
+                  double dt_ms, void* stream) {
+  if (!dst && rows > 0) {
+    t_err = "dst is required";
+    return PSG_EINVAL;
+  }
+  return corr_launch(plan, nullptr, src, dst, rows, cols, live, nullptr, nullptr, dt_ms, stream);
+}
+
+int psg_stack_create(int64_t rows, int32_t samples, double dt_ms, psg_stack** out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    if (rows < 0 || samples < 0) throw InvalidArg("rows and samples must be ≥ 0");
+    if (!(std::isfinite(dt_ms) && dt_ms > 0)) throw InvalidArg("dtMs must be finite and positive");
+    ensure_device();
+    std::unique_ptr<psg_stack> s(new psg_stack());
+    s->rows = rows;
+    s->samples = samples;
+    s->dt_ms = dt_ms;
+    size_t n = (size_t)(rows * samples);
+    if (n) {
+      CUDA_OK(cudaMalloc(&s->num, n * 8));
+      CUDA_OK(cudaMalloc(&s->cnt, n * 4));
+      CUDA_OK(cudaMemset(s->num, 0, n * 8));
+      CUDA_OK(cudaMemset(s->cnt, 0, n * 4));
+    }
+    *out = s.release();
+  });
+}
+void psg_stack_destroy(psg_stack* s) {
+  if (!s) return;
+  if (s->num) cudaFree(s->num);
+  if (s->cnt) cudaFree(s->cnt);
+  delete s;
+}
+int psg_stack_clear(psg_stack* st, void* stream) {
+  return guarded([&] {
+    if (!st) throw InvalidArg("null argument");
+    size_t n = (size_t)(st->rows * st->samples);
+    if (n) {
+      CUDA_OK(cudaMemsetAsync(st->num, 0, n * 8, (cudaStream_t)stream));
+      CUDA_OK(cudaMemsetAsync(st->cnt, 0, n * 4, (cudaStream_t)stream));
+    }
+  });
+}
+int psg_stack_add(psg_stack* st, const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live,
+                  const int32_t* row_map, void* stream) {
+  return guarded([&] {
+    if (!st) throw InvalidArg("null argument");
+    if (cols > st->samples) throw InvalidArg("the record has " + std::to_string(cols) + " samples, the stack " + std::to_string(st->samples));
+    if (!row_map && rows > st->rows) throw InvalidArg("a record of " + std::to_string(rows) + " rows into a stack of " + std::to_string(st->rows) + " (pass a rowMap)");
+    if (rows == 0) return;
+    ensure_device();
+    int g = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == PSG_F32) stack_add_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, row_map, st->num, st->cnt, st->samples, st->rows);
+    else stack_add_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, row_map, st->num, st->cnt, st->samples, st->rows);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+int psg_correlate_stack(const psg_corr_plan* plan, psg_stack* st, const void* src, void* dst, int64_t rows, int32_t cols,
+                        const int32_t* live, const int32_t* stack_live, const int32_t* row_map, double dt_ms, void* stream) {
+  if (!st) {
+    t_err = "a stack is required";
+    return PSG_EINVAL;
+  }
+  return corr_launch(plan, st, src, dst, rows, cols, live, stack_live, row_map, dt_ms, stream);
+}
+int psg_stack_result(const psg_stack* st, void* dst, int32_t dtype, int32_t norm, void* stream) {
+  return guarded([&] {
+    if (!st || !dst) throw InvalidArg("null argument");
+    long long total = (long long)st->rows * st->samples;
+    if (!total) return;
+    ensure_device();
+    int g = (int)std::min<long long>((total + 255) / 256, (long long)g_sm_count * 16);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dtype == PSG_F32) stack_result_kernel<float><<<g, 256, 0, s>>>(st->num, st->cnt, total, norm, (float*)dst);
+    else stack_result_kernel<double><<<g, 256, 0, s>>>(st->num, st->cnt, total, norm, (double*)dst);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+int psg_stack_fold(const psg_stack* st, int32_t* dst, void* stream) {
+  return guarded([&] {
+    if (!st || !dst) throw InvalidArg("null argument");
+    size_t n = (size_t)(st->rows * st->samples);
+    if (n) CUDA_OK(cudaMemcpyAsync(dst, st->cnt, n * 4, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  });
+}
+
+}  // extern "C"
+
+// traceStatsInto's finish: rms = sqrt(Σx²/n) for live rows, NaN for others.
+__global__ void trace_stats_finish(double* rms, double* mx, const int* live, long long rows, int cols) {
+  long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  int n = min(max(live[r], 0), cols);
+  if (n == 0) {
+    rms[r] = NAN;
+    mx[r] = NAN;
+  } else {
+    rms[r] = sqrt(rms[r] / (double)n);
+  }
+}

@@ -1,0 +1,113 @@
+// psg_internal.h — shared by the host plan compiler (psg_plan.cpp) and the
+// device side (psg_cuda.cu) of libpsgcuda.so. Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/psg.h"
+
+namespace psg {
+
+// A ValueError of the reference: an invalid op, plan, shape or interval.
+struct InvalidArg : std::runtime_error {
+  explicit InvalidArg(const std::string& m) : std::runtime_error(m) {}
+};
+// An AssertionDefect of the reference: a workspace not reserved for the plan.
+struct WorkspaceError : std::runtime_error {
+  explicit WorkspaceError(const std::string& m) : std::runtime_error(m) {}
+};
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+void set_error(const std::string& m);
+
+// ------------------------------------------------------------------- lengths
+bool fast_len(int64_t n);
+int64_t next_fast(int64_t n, bool even = true);
+
+// ------------------------------------------------------------------ FFT plan
+// The complex FFT of length m that a real FFT of length n = 2m runs: the
+// Stockham passes (radix per pass, first pass first) and their twiddles,
+// generated in float64. The device reads the twiddles as T.
+struct FftTables {
+  int64_t n = 0, m = 0;
+  std::vector<int> radices;
+  std::vector<double> tw_re, tw_im;       // per pass: sub·(r − 1) values
+  std::vector<double> split_re, split_im; // exp(−2πik/n), k = 0 .. m
+};
+FftTables fft_tables(int64_t n);
+
+// --------------------------------------------------------------- filter plan
+struct FilterHost {
+  psg_filter_spec spec{};
+  int trend = PSG_TR_LINEAR;
+  int64_t margin = 0, pad = 0, nfft = 0;
+  bool reflect = false;
+  double dc_gain = 0;
+  std::vector<double> gain;  // nfft/2 + 1 bins
+  std::vector<double> fall;  // pad values
+  FftTables fft;
+};
+void validate_spec(const psg_filter_spec& s, double dt_ms);
+double spec_response(const psg_filter_spec& s, double f_hz, double dt_ms);
+int64_t spec_impulse_length(const psg_filter_spec& s, double dt_ms);
+FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend);
+
+// ---------------------------------------------------------------- the plan
+enum StepKind {
+  ST_DEMEAN = 0, ST_DETREND, ST_SCALE, ST_CLIP, ST_POLARITY, ST_FILTER, ST_AGC,
+  ST_NORM_TRACE, ST_NORM_PANEL, ST_GAIN_CURVE
+};
+
+struct StepHost {
+  int kind = 0;
+  double factor = 0, lo = 0, hi = 0;
+  FilterHost filter;
+  // AGC
+  int64_t half = 0;
+  int agc_mode = 0;
+  double target = 1, epsilon = 1e-9;
+  // normalize
+  int stat = 0, scope = 0;
+  double norm_target = 1, percentile = 99;
+  // gain curve
+  psg_gain_curve curve{};
+  std::vector<double> table;
+  double t_min_ms = 0;
+  int64_t margin() const { return kind == ST_FILTER ? filter.margin : (kind == ST_AGC ? half : 0); }
+};
+
+struct PlanHost {
+  int dtype = PSG_F32;
+  double dt_ms = 0;
+  int64_t samples = 0, record_samples = 0, margin = 0;
+  uint64_t generation = 0;
+  std::vector<StepHost> steps;
+  std::vector<std::pair<int, int>> parts;  // [a, b)
+};
+
+PlanHost compile_plan(const psg_op* ops, int n_ops, int dtype, double dt_ms, int64_t samples,
+                      int64_t record_samples);
+int64_t required_margin(const psg_op* ops, int n_ops, double dt_ms);
+double gain_factor_at(const psg_gain_curve& c, double t_ms);
+bool same_interval(double dt, double plan_dt);
+
+// ----------------------------------------------------------- correlation
+struct CorrHost {
+  int64_t n = 0, shift = 0, record = 0, out = 0, pilot_len = 0;
+  double dt_ms = 0, scale = 1;
+  int mode = 0;
+  std::vector<double> mul_re, mul_im;
+  FftTables fft;
+};
+CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
+                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize);
+std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
+                                 double t_end, int shape, double phase_deg, double amplitude,
+                                 double max_nyq_fraction);
+
+}  // namespace psg

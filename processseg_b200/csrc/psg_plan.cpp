@@ -1,0 +1,643 @@
+// psg_plan.cpp — host side of libpsgcuda.so: validating ops and compiling a
+// pipeline into the tables the device kernels read (filter responses, FFT
+// twiddles, pad tapers, gain tables, correlation multipliers), all generated
+// in float64. The arithmetic on samples runs on the GPU (psg_cuda.cu).
+//
+// Reference: src/processSEG/pipeline.nim (compile), filter/design.nim
+// (responses, impulse length), filter/apply.nim:118-151 (filter plan),
+// gain/gain.nim:272-302 (AGC plan), gain/curves.nim:214-247 (gain tables),
+// vibroseis/correlate.nim:82-160, sweep.nim, taper.nim (correlation plan).
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <limits>
+
+#include "psg_internal.h"
+
+namespace psg {
+
+namespace {
+const double kPi = 3.14159265358979323846;
+const double kInf = std::numeric_limits<double>::infinity();
+const double kNaN = std::numeric_limits<double>::quiet_NaN();
+typedef std::complex<double> cd;
+
+std::string num(double v) {
+  char b[48];
+  snprintf(b, sizeof b, "%g", v);
+  return b;
+}
+bool fin(double x) { return std::isfinite(x); }
+bool fin_pos(double x) {
+  int c = std::fpclassify(x);
+  return (c == FP_NORMAL || c == FP_SUBNORMAL) && x > 0;
+}
+template <class T> bool fits(double x) { return fin_pos(x) && fin_pos((double)(T)x); }
+bool fits_dtype(int dtype, double x) { return dtype == PSG_F32 ? fits<float>(x) : fits<double>(x); }
+double as_dtype(int dtype, double x) { return dtype == PSG_F32 ? (double)(float)x : x; }
+
+// A mixed-radix decimation-in-time FFT in float64 on the host, for the
+// plan-time transforms (impulse lengths, pilot spectra). `w` holds
+// exp(sign·2πi·j/N) for the top length N; a sub-transform reads it at a stride.
+void dit(const cd* in, int64_t istride, cd* out, int64_t n, const std::vector<cd>& w, int64_t wstride,
+         std::vector<cd>& tmp) {
+  if (n == 1) {
+    out[0] = in[0];
+    return;
+  }
+  int r = n % 4 == 0 ? 4 : (n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : 5));
+  int64_t m = n / r;
+  for (int q = 0; q < r; q++) dit(in + q * istride, istride * r, out + q * m, m, w, wstride * r, tmp);
+  const int64_t N = (int64_t)w.size();
+  cd t[5];
+  for (int64_t k = 0; k < m; k++) {
+    for (int q = 0; q < r; q++) t[q] = out[q * m + k] * w[(q * k * wstride) % N];
+    for (int s = 0; s < r; s++) {
+      cd acc = 0;
+      for (int q = 0; q < r; q++) acc += t[q] * w[((int64_t)q * s * m * wstride) % N];
+      tmp[k + m * s] = acc;
+    }
+  }
+  std::copy(tmp.begin(), tmp.begin() + n, out);
+}
+// Forward (sign −1) or unscaled inverse (sign +1) complex FFT of a 2·3·5-smooth length.
+std::vector<cd> cfft(const std::vector<cd>& x, int sign) {
+  int64_t n = (int64_t)x.size();
+  std::vector<cd> w(n), out(n), tmp(n);
+  for (int64_t j = 0; j < n; j++) {
+    double a = sign * 2 * kPi * (double)j / (double)n;
+    w[j] = cd(std::cos(a), std::sin(a));
+  }
+  dit(x.data(), 1, out.data(), n, w, 1, tmp);
+  return out;
+}
+}  // namespace
+
+bool same_interval(double dt, double plan_dt) { return std::fabs(dt - plan_dt) <= 1e-9 * plan_dt; }
+
+// ----------------------------------------------------------------- lengths
+// fft/plan.nim:105-118
+bool fast_len(int64_t n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+int64_t next_fast(int64_t n, bool even) {
+  int64_t r = n < 1 ? 1 : n;
+  while (!fast_len(r) || (even && (r & 1))) r++;
+  return r;
+}
+
+// -------------------------------------------------------------- FFT tables
+// The device runs Stockham passes of radix 8, 4, 2, 3 and 5 (largest powers
+// of two first, so fewer passes than the reference's 4/2/3/5 order). The
+// twiddle of output k of butterfly p in a pass of `cur` points is
+// exp(−2πi·(p·k mod cur)/cur), as fft/plan.nim:146-155 builds them.
+FftTables fft_tables(int64_t n) {
+  if (!fast_len(n) || n % 2 != 0) throw InvalidArg("the device FFT needs an even 2·3·5-smooth length, got " + std::to_string(n));
+  FftTables t;
+  t.n = n;
+  t.m = n / 2;
+  int64_t k = t.m;
+  while (k % 8 == 0) { t.radices.push_back(8); k /= 8; }
+  if (k % 4 == 0) { t.radices.push_back(4); k /= 4; }
+  if (k % 2 == 0) { t.radices.push_back(2); k /= 2; }
+  while (k % 3 == 0) { t.radices.push_back(3); k /= 3; }
+  while (k % 5 == 0) { t.radices.push_back(5); k /= 5; }
+  int64_t cur = t.m;
+  for (int r : t.radices) {
+    int64_t sub = cur / r;
+    for (int64_t p = 0; p < sub; p++)
+      for (int q = 1; q < r; q++) {
+        double a = -2 * kPi * (double)((p * q) % cur) / (double)cur;
+        t.tw_re.push_back(std::cos(a));
+        t.tw_im.push_back(std::sin(a));
+      }
+    cur = sub;
+  }
+  for (int64_t j = 0; j <= t.m; j++) {
+    double a = -2 * kPi * (double)j / (double)n;
+    t.split_re.push_back(std::cos(a));
+    t.split_im.push_back(std::sin(a));
+  }
+  return t;
+}
+
+// ------------------------------------------------------------------ design
+namespace {
+bool low_cut(const psg_filter_spec& s) { return s.f2 > 0; }
+bool high_cut(const psg_filter_spec& s) { return s.f3 < kInf; }
+void need(bool ok, const std::string& m) {
+  if (!ok) throw InvalidArg(m);
+}
+// filter/design.nim:103-137
+void check_spec_shape(const psg_filter_spec& s) {
+  if (s.kind == PSG_RK_TRAPEZOID) {
+    need(!(std::isnan(s.f1) || std::isnan(s.f2) || std::isnan(s.f3) || std::isnan(s.f4)), "a corner is NaN");
+    if (low_cut(s)) need(s.f1 >= 0 && s.f1 < s.f2, "a low cut needs 0 ≤ f1 < f2 (a sloped ramp), got f1 = " + num(s.f1) + ", f2 = " + num(s.f2));
+    else need(s.f1 == 0 && s.f2 == 0, "no low cut needs f1 = f2 = 0");
+    if (high_cut(s)) need(s.f3 < s.f4 && s.f4 < kInf, "a high cut needs f3 < f4 < Inf (a sloped ramp), got f3 = " + num(s.f3) + ", f4 = " + num(s.f4));
+    else need(s.f4 == kInf, "no high cut needs f3 = f4 = Inf");
+    if (low_cut(s) && high_cut(s)) need(s.f2 <= s.f3, "a band-pass needs f2 ≤ f3");
+  } else if (s.kind == PSG_RK_BUTTERWORTH) {
+    need(s.low_hz >= 0 && s.low_hz < kInf, "a low-cut corner must be finite and ≥ 0 (0: none), got " + num(s.low_hz));
+    need(s.high_hz > 0, "a high-cut corner must be > 0 (Inf: none), got " + num(s.high_hz));
+    if (s.low_hz > 0) need(s.low_slope > 0 && s.low_slope < kInf, "a slope must be finite and > 0 dB/octave, got " + num(s.low_slope));
+    if (s.high_hz < kInf) need(s.high_slope > 0 && s.high_slope < kInf, "a slope must be finite and > 0 dB/octave, got " + num(s.high_slope));
+    need(s.low_hz < s.high_hz, "the low-cut corner must be below the high-cut one");
+  } else {
+    throw InvalidArg("unknown response kind " + std::to_string(s.kind));
+  }
+  need(s.n_notches >= 0 && s.n_notches <= PSG_MAX_NOTCHES, "at most 8 notches");
+  for (int i = 0; i < s.n_notches; i++) {
+    need(s.notches[i].freq_hz > 0 && s.notches[i].freq_hz < kInf, "a notch frequency must be finite and > 0, got " + num(s.notches[i].freq_hz));
+    need(s.notches[i].width_hz > 0 && s.notches[i].width_hz < kInf, "a notch width must be finite and > 0, got " + num(s.notches[i].width_hz));
+  }
+}
+double tan_warp(double f, double dt_ms) {
+  double x = kPi * f * dt_ms / 1000;
+  return x >= kPi / 2 ? kInf : std::tan(x);
+}
+double sin2_ramp(double x) {
+  if (x <= 0) return 0.0;
+  if (x >= 1) return 1.0;
+  double s = std::sin(kPi / 2 * x);
+  return s * s;
+}
+double narrowest(const psg_filter_spec& s) {
+  double r = kInf;
+  if (s.kind == PSG_RK_TRAPEZOID) {
+    if (low_cut(s)) r = std::min(r, s.f2 - s.f1);
+    if (high_cut(s)) r = std::min(r, s.f4 - s.f3);
+  } else {
+    if (s.low_hz > 0) r = std::min(r, s.low_hz * std::min(1.0, 24 / s.low_slope) / 2);
+    if (s.high_hz < kInf) r = std::min(r, s.high_hz * std::min(1.0, 24 / s.high_slope) / 2);
+  }
+  for (int i = 0; i < s.n_notches; i++) r = std::min(r, s.notches[i].width_hz / 2);
+  return r;
+}
+// The bin gains of an FFT of `nfft` points (filter/design.nim:257-265).
+std::vector<double> bin_gains(const psg_filter_spec& s, double dt_ms, int64_t nfft) {
+  int64_t bins = nfft / 2 + 1;
+  std::vector<double> h(bins);
+  double df = 1000 / ((double)nfft * dt_ms);
+  for (int64_t k = 0; k < bins; k++) h[k] = spec_response(s, (double)k * df, dt_ms);
+  if (s.zero_dc && bins > 0) h[0] = 0;
+  return h;
+}
+// The half length holding 99.9 % of the energy of a symmetric impulse whose
+// centre sample is `c` (filter/design.nim:288-298).
+int64_t half_energy(const std::vector<double>& h, double c) {
+  int64_t n = (int64_t)h.size();
+  double total = c * c;
+  for (int64_t j = 1; j < n; j++) total += h[j] * h[j];
+  double e = c * c;
+  int64_t L = 0;
+  while (e < 0.999 * total && L < n / 2) {
+    ++L;
+    e += h[L] * h[L] + (n - L != L ? h[n - L] * h[n - L] : 0.0);
+  }
+  return L;
+}
+// One feature's impulse length, the longer of H and 1 − H, on a grid grown
+// until the impulse fits in an eighth of it (filter/design.nim:300-325).
+int64_t feature_len(const psg_filter_spec& s, double dt_ms) {
+  const int64_t max_grid = 1 << 24;
+  double feat = narrowest(s);
+  if (feat == kInf) return 0;
+  double start = std::ceil(16 * (1000 / dt_ms) / feat);
+  int64_t n = start > (double)max_grid ? max_grid + 1 : next_fast(std::max<int64_t>(64, (int64_t)start));
+  while (true) {
+    if (n > max_grid)
+      throw InvalidArg("the filter's impulse response is longer than " + std::to_string(max_grid / 8) +
+                       " samples at " + num(dt_ms) + " ms (narrowest ramp " + num(feat) + " Hz)");
+    std::vector<double> g = bin_gains(s, dt_ms, n);
+    std::vector<cd> full(n);
+    for (int64_t k = 0; k < (int64_t)g.size(); k++) {
+      full[k] = g[k];
+      if (k > 0 && k < n - k) full[n - k] = g[k];
+    }
+    std::vector<cd> t = cfft(full, +1);
+    std::vector<double> h(n);
+    for (int64_t j = 0; j < n; j++) h[j] = t[j].real() / (double)n;
+    int64_t L = std::max(half_energy(h, h[0]), half_energy(h, 1 - h[0]));
+    if (L <= n / 8) return L;
+    n = next_fast(2 * n);
+  }
+}
+}  // namespace
+
+// filter/design.nim:143-173
+void validate_spec(const psg_filter_spec& s, double dt_ms) {
+  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and > 0, got " + num(dt_ms));
+  check_spec_shape(s);
+  double nyq = 500 / dt_ms;
+  if (s.kind == PSG_RK_TRAPEZOID) {
+    if (high_cut(s)) need(!(s.f4 > nyq), "f4 = " + num(s.f4) + " Hz is above Nyquist (" + num(nyq) + " Hz at " + num(dt_ms) + " ms)");
+    if (low_cut(s)) need(!(s.f2 >= nyq), "f2 = " + num(s.f2) + " Hz is not below Nyquist (" + num(nyq) + " Hz)");
+  } else {
+    if (s.high_hz < kInf) need(!(s.high_hz >= nyq), "the high-cut corner " + num(s.high_hz) + " Hz is not below Nyquist (" + num(nyq) + " Hz)");
+    need(!(s.low_hz >= nyq), "the low-cut corner " + num(s.low_hz) + " Hz is not below Nyquist (" + num(nyq) + " Hz)");
+  }
+  for (int i = 0; i < s.n_notches; i++)
+    need(!(s.notches[i].freq_hz >= nyq), "a notch at " + num(s.notches[i].freq_hz) + " Hz is not below Nyquist (" + num(nyq) + " Hz)");
+}
+
+// filter/design.nim:236-255
+double spec_response(const psg_filter_spec& s, double f, double dt_ms) {
+  double g = 1.0;
+  if (s.kind == PSG_RK_TRAPEZOID) {
+    if (low_cut(s)) g *= sin2_ramp((f - s.f1) / (s.f2 - s.f1));
+    if (high_cut(s)) g *= 1 - sin2_ramp((f - s.f3) / (s.f4 - s.f3));
+  } else {
+    double wf = tan_warp(f, dt_ms);
+    if (s.low_hz > 0) g *= f <= 0 ? 0.0 : 1 / (1 + std::pow(tan_warp(s.low_hz, dt_ms) / wf, s.low_slope / 6));
+    if (s.high_hz < kInf) g *= wf == kInf ? 0.0 : 1 / (1 + std::pow(wf / tan_warp(s.high_hz, dt_ms), s.high_slope / 6));
+  }
+  for (int i = 0; i < s.n_notches; i++) g *= sin2_ramp(std::fabs(f - s.notches[i].freq_hz) / (s.notches[i].width_hz / 2));
+  return g;
+}
+
+// filter/design.nim:327-366: each edge and notch measured on its own.
+int64_t spec_impulse_length(const psg_filter_spec& s, double dt_ms) {
+  validate_spec(s, dt_ms);
+  psg_filter_spec flat{};
+  flat.kind = PSG_RK_TRAPEZOID;
+  flat.f3 = flat.f4 = kInf;
+  std::vector<psg_filter_spec> parts;
+  if (s.kind == PSG_RK_TRAPEZOID) {
+    if (low_cut(s)) { psg_filter_spec a = flat; a.f1 = s.f1; a.f2 = s.f2; parts.push_back(a); }
+    if (high_cut(s)) { psg_filter_spec a = flat; a.f3 = s.f3; a.f4 = s.f4; parts.push_back(a); }
+  } else {
+    psg_filter_spec b{};
+    b.kind = PSG_RK_BUTTERWORTH;
+    b.low_slope = s.low_slope;
+    b.high_slope = s.high_slope;
+    if (s.low_hz > 0) { psg_filter_spec a = b; a.low_hz = s.low_hz; a.high_hz = kInf; parts.push_back(a); }
+    if (s.high_hz < kInf) { psg_filter_spec a = b; a.low_hz = 0; a.high_hz = s.high_hz; parts.push_back(a); }
+  }
+  for (int i = 0; i < s.n_notches; i++) {
+    psg_filter_spec a = flat;
+    a.n_notches = 1;
+    a.notches[0] = s.notches[i];
+    parts.push_back(a);
+  }
+  int64_t L = 0;
+  for (auto& p : parts) L = std::max(L, feature_len(p, dt_ms));
+  return L;
+}
+
+// filter/apply.nim:118-151
+FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend) {
+  need(samples >= 1, "a filter plan needs samples ≥ 1, got " + std::to_string(samples));
+  need(trend >= PSG_TR_NONE && trend <= PSG_TR_LINEAR, "unknown trend removal " + std::to_string(trend));
+  validate_spec(s, dt_ms);
+  FilterHost f;
+  f.spec = s;
+  f.trend = trend;
+  f.margin = spec_impulse_length(s, dt_ms);
+  f.dc_gain = spec_response(s, 0, dt_ms);
+  f.reflect = f.dc_gain >= 0.5 || trend != PSG_TR_LINEAR;
+  f.pad = f.reflect ? f.margin : std::min(f.margin, samples);
+  int64_t n = samples + (f.reflect ? 4 : 2) * f.pad;
+  double rmp = narrowest(s);
+  if (rmp < kInf && f.pad == f.margin) n = std::max(n, (int64_t)std::ceil(2000 / (rmp * dt_ms)));
+  f.nfft = next_fast(n);
+  f.gain = bin_gains(s, dt_ms, f.nfft);
+  f.fall.resize(f.pad);
+  for (int64_t k = 1; k <= f.pad; k++) {
+    double c = std::cos(kPi / 2 * (double)k / (double)(f.pad + 1));
+    f.fall[k - 1] = c * c;
+  }
+  f.fft = fft_tables(f.nfft);
+  return f;
+}
+
+// ------------------------------------------------------------- gain curves
+// gain/curves.nim:132-160
+double gain_factor_at(const psg_gain_curve& c, double t) {
+  if (std::isnan(t)) return kNaN;
+  if (c.kind == PSG_GC_POWER) return std::pow(std::max(t, c.min_ms) / c.ref_ms, c.power);
+  double db;
+  if (c.kind == PSG_GC_KNOTS) {
+    if (c.n_knots == 0) return kNaN;
+    const psg_gain_knot* k = c.knots;
+    int n = c.n_knots;
+    if (t <= k[0].t_ms) db = k[0].db;
+    else if (t >= k[n - 1].t_ms) db = k[n - 1].db;
+    else {
+      int lo = 0, hi = n - 1;
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        (k[mid].t_ms <= t ? lo : hi) = mid;
+      }
+      double f = (t - k[lo].t_ms) / (k[hi].t_ms - k[lo].t_ms);
+      db = k[lo].db + f * (k[hi].db - k[lo].db);
+    }
+  } else {
+    db = c.db_per_s * t / 1000;
+  }
+  return std::pow(10.0, db / 20);
+}
+namespace {
+void check_curve(const psg_gain_curve& c) {
+  if (c.kind == PSG_GC_KNOTS) {
+    need(c.n_knots >= 1, "the curve has no knots: build it with knotGain, powerGain or exponentialGain");
+    need(c.n_knots <= PSG_MAX_KNOTS, "at most 64 knots");
+    for (int i = 0; i < c.n_knots; i++) {
+      need(fin(c.knots[i].t_ms) && fin(c.knots[i].db), "knot " + std::to_string(i) + " is not finite");
+      if (i > 0) need(c.knots[i].t_ms > c.knots[i - 1].t_ms, "knot times must strictly increase");
+    }
+  } else if (c.kind == PSG_GC_POWER) {
+    need(fin(c.power), "a power must be finite, got " + num(c.power));
+    need(fin(c.ref_ms) && c.ref_ms > 0, "refMs must be finite and positive, got " + num(c.ref_ms));
+    need(fin(c.min_ms) && c.min_ms > 0, "minMs must be finite and positive, got " + num(c.min_ms));
+  } else if (c.kind == PSG_GC_EXPONENTIAL) {
+    need(fin(c.db_per_s), "dbPerS must be finite, got " + num(c.db_per_s));
+  } else {
+    throw InvalidArg("unknown gain curve kind " + std::to_string(c.kind));
+  }
+}
+
+const char* op_name(int k) {
+  static const char* names[] = {"opDemean", "opDetrend", "opScale", "opGainDb", "opClip",
+                                "opPolarity", "opMuteTop", "opMuteBottom", "opFilter", "opIir",
+                                "opAgc", "opNormalize", "opGainCurve", "opCalibrate", "opUncalibrate"};
+  return (k >= 0 && k < 15) ? names[k] : "op?";
+}
+
+// gain/gain.nim:272-296
+int64_t agc_half(double window_ms, double dt_ms, int64_t samples, double target, double epsilon) {
+  need(fin_pos(dt_ms), "dtMs must be finite and positive, got " + num(dt_ms));
+  need(samples >= 1 && samples <= 2147483647LL, "an AGC plan needs samples in 1 .. int32.high, got " + std::to_string(samples));
+  need(fin_pos(window_ms), "an AGC window must be finite and positive, got " + num(window_ms) + " ms");
+  double h = std::round(window_ms / (2 * dt_ms));
+  need(h >= 1, "an AGC window of " + num(window_ms) + " ms is under 3 samples at " + num(dt_ms) + " ms");
+  need(h <= (double)(1 << 26), "an AGC window of " + num(window_ms) + " ms is too long");
+  need(fin_pos(target), "an AGC target must be finite and positive, got " + num(target));
+  need(fin_pos(epsilon), "an AGC epsilon must be finite and positive, got " + num(epsilon));
+  return (int64_t)h;
+}
+
+// pipeline.nim:392-447
+StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, int64_t record) {
+  StepHost s;
+  switch (op.kind) {
+    case PSG_OP_DEMEAN: s.kind = ST_DEMEAN; break;
+    case PSG_OP_DETREND: s.kind = ST_DETREND; break;
+    case PSG_OP_POLARITY: s.kind = ST_POLARITY; break;
+    case PSG_OP_SCALE:
+      need(fin(op.factor), "the factor must be finite, got " + num(op.factor));
+      need(fin(as_dtype(dtype, op.factor)), "a factor of " + num(op.factor) + " overflows " + (dtype ? "float64" : "float32"));
+      s.kind = ST_SCALE;
+      s.factor = op.factor;
+      break;
+    case PSG_OP_GAIN_DB: {
+      need(fin(op.factor), "the gain must be finite, got " + num(op.factor) + " dB");
+      double f = std::pow(10.0, op.factor / 20);
+      need(fin(f) && fin(as_dtype(dtype, f)), "a gain of " + num(op.factor) + " dB overflows " + (dtype ? "float64" : "float32"));
+      s.kind = ST_SCALE;
+      s.factor = f;
+      break;
+    }
+    case PSG_OP_CLIP:
+      need(!(std::isnan(op.lo) || std::isnan(op.hi) || op.lo > op.hi),
+           "clip limits must satisfy lo ≤ hi, got " + num(op.lo) + " .. " + num(op.hi));
+      s.kind = ST_CLIP;
+      s.lo = op.lo;
+      s.hi = op.hi;
+      break;
+    case PSG_OP_FILTER:
+      s.kind = ST_FILTER;
+      s.filter = filter_plan(op.filter, dt_ms, samples, op.trend);
+      break;
+    case PSG_OP_AGC:
+      need(op.agc_mode == PSG_AGC_RMS || op.agc_mode == PSG_AGC_MEAN_ABS, "unknown AGC mode");
+      s.kind = ST_AGC;
+      s.half = agc_half(op.window_ms, dt_ms, samples, op.target, op.epsilon);
+      s.agc_mode = op.agc_mode;
+      s.target = op.target;
+      s.epsilon = op.epsilon;
+      break;
+    case PSG_OP_NORMALIZE:
+      // gain/gain.nim:153-167
+      need(samples >= 1, "a normalize plan needs samples ≥ 1");
+      need(fin_pos(op.norm_target), "a normalize target must be finite and positive, got " + num(op.norm_target));
+      need(op.percentile >= 0 && op.percentile <= 100, "a percentile must be in 0 .. 100, got " + num(op.percentile));
+      need(op.norm_stat >= 0 && op.norm_stat <= 2, "unknown normalization statistic");
+      need(op.norm_scope == PSG_PER_TRACE || op.norm_scope == PSG_PER_PANEL, "unknown normalization scope");
+      s.kind = op.norm_scope == PSG_PER_PANEL ? ST_NORM_PANEL : ST_NORM_TRACE;
+      s.stat = op.norm_stat;
+      s.scope = op.norm_scope;
+      s.norm_target = op.norm_target;
+      s.percentile = op.percentile;
+      break;
+    case PSG_OP_GAIN_CURVE: {
+      // gain/curves.nim:214-247, tabulated over the record (pipeline.nim:441-443)
+      check_curve(op.curve);
+      double hi = std::isnan(op.t_max_ms) ? op.t_min_ms + (double)(record - 1) * dt_ms : op.t_max_ms;
+      need(fin(op.t_min_ms) && fin(hi), "the table limits must be finite, got " + num(op.t_min_ms) + " .. " + num(hi));
+      need(!(hi < op.t_min_ms), "tMaxMs " + num(hi) + " is before tMinMs " + num(op.t_min_ms));
+      double span = std::floor((hi - op.t_min_ms) / dt_ms + 1e-9);
+      need(span < (double)(1 << 26), "a gain table of " + num(span) + " samples is too long");
+      s.kind = ST_GAIN_CURVE;
+      s.curve = op.curve;
+      s.t_min_ms = op.t_min_ms;
+      s.table.resize((size_t)span + 1);
+      for (size_t k = 0; k < s.table.size(); k++) {
+        double t = op.t_min_ms + (double)k * dt_ms;
+        double g = gain_factor_at(op.curve, t);
+        need(!(std::isinf(as_dtype(dtype, g)) || std::isnan(g)), "the gain at " + num(t) + " ms (" + num(g) + ") overflows");
+        s.table[k] = g;
+      }
+      break;
+    }
+    case PSG_OP_MUTE_TOP:
+    case PSG_OP_MUTE_BOTTOM:
+    case PSG_OP_IIR:
+    case PSG_OP_CALIBRATE:
+    case PSG_OP_UNCALIBRATE:
+      throw InvalidArg("this op is not part of the GPU hot path yet");
+    default:
+      throw InvalidArg("unknown op kind " + std::to_string(op.kind));
+  }
+  return s;
+}
+
+std::atomic<uint64_t> g_generation{0};
+}  // namespace
+
+// pipeline.nim:466-523
+PlanHost compile_plan(const psg_op* ops, int n_ops, int dtype, double dt_ms, int64_t samples,
+                      int64_t record_samples) {
+  need(dtype == PSG_F32 || dtype == PSG_F64, "dtype must be float32 or float64");
+  need(fin(dt_ms) && dt_ms > 0, "dtMs must be finite and positive, got " + num(dt_ms));
+  need(samples >= 1, "a pipeline needs samples ≥ 1, got " + std::to_string(samples));
+  need(samples <= (1 << 20), "a pipeline takes at most 2²⁰ samples per trace on the device");
+  need(record_samples == 0 || record_samples >= samples,
+       "recordSamples (" + std::to_string(record_samples) + ") must be 0 or ≥ samples (" + std::to_string(samples) +
+           "): it is the length of the traces a window of `samples` is cut from");
+  need(n_ops >= 0 && (n_ops == 0 || ops != nullptr), "no ops");
+  PlanHost p;
+  p.dtype = dtype;
+  p.dt_ms = dt_ms;
+  p.samples = samples;
+  p.record_samples = std::max(samples, record_samples);
+  for (int i = 0; i < n_ops; i++) {
+    try {
+      p.steps.push_back(compile_op(ops[i], dtype, dt_ms, samples, p.record_samples));
+    } catch (const InvalidArg& e) {
+      throw InvalidArg(std::string("op ") + std::to_string(i) + " (" + op_name(ops[i].kind) + "): " + e.what());
+    }
+  }
+  int start = 0;
+  for (int i = 0; i < (int)p.steps.size(); i++) {
+    p.margin += p.steps[i].margin();
+    if (p.steps[i].kind == ST_NORM_PANEL && i > start) {
+      p.parts.push_back({start, i});
+      start = i;
+    }
+  }
+  p.parts.push_back({start, (int)p.steps.size()});
+  p.generation = g_generation.fetch_add(1) + 1;
+  return p;
+}
+
+// pipeline.nim:525-548
+int64_t required_margin(const psg_op* ops, int n_ops, double dt_ms) {
+  need(fin(dt_ms) && dt_ms > 0, "dtMs must be finite and positive, got " + num(dt_ms));
+  int64_t m = 0;
+  for (int i = 0; i < n_ops; i++) {
+    try {
+      if (ops[i].kind == PSG_OP_FILTER) m += spec_impulse_length(ops[i].filter, dt_ms);
+      else if (ops[i].kind == PSG_OP_AGC) m += agc_half(ops[i].window_ms, dt_ms, 1, ops[i].target, ops[i].epsilon);
+    } catch (const InvalidArg& e) {
+      throw InvalidArg(std::string("op ") + std::to_string(i) + " (" + op_name(ops[i].kind) + "): " + e.what());
+    }
+  }
+  return m;
+}
+
+// --------------------------------------------------------------- vibroseis
+namespace {
+// vibroseis/taper.nim:125-145 for the shapes that need no special function.
+double taper_weight(int shape, double x) {
+  x = std::min(1.0, std::max(0.0, x));
+  switch (shape) {
+    case 0: return x;
+    case 1: return std::sin(kPi / 2 * x);
+    case 2: return 0.5 - 0.5 * std::cos(kPi * x);
+    case 3: return 0.54 - 0.46 * std::cos(kPi * x);
+    case 4: return 0.42 - 0.5 * std::cos(kPi * x) + 0.08 * std::cos(2 * kPi * x);
+    case 5: return 0.35875 - 0.48829 * std::cos(kPi * x) + 0.14128 * std::cos(2 * kPi * x) - 0.01168 * std::cos(3 * kPi * x);
+    default: throw InvalidArg("taper shape " + std::to_string(shape) + " is not supported");
+  }
+}
+}  // namespace
+
+// vibroseis/sweep.nim:126-192 (validate, linearSweep), :292-301 (linear
+// phase, float64), :331-342 (sweepInto), taper.nim:160-179 (applyTaper).
+std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
+                                 double t_end, int shape, double phase_deg, double amplitude,
+                                 double max_nyq_fraction) {
+  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and positive, got " + num(dt_ms));
+  need(length_ms >= dt_ms && length_ms < kInf, "lengthMs must be at least one sample interval, got " + num(length_ms));
+  double steps = length_ms / dt_ms;
+  need(steps <= 2147483647.0, "a sweep is over 2³¹ samples");
+  need(std::fabs(steps - std::round(steps)) <= 1e-6, "lengthMs = " + num(length_ms) + " must be a whole number of samples of " + num(dt_ms) + " ms");
+  need(max_nyq_fraction > 0 && max_nyq_fraction <= 1, "maxNyquistFraction must be in (0, 1]");
+  need(fin(amplitude), "the amplitude must be finite");
+  need(fin(phase_deg), "startPhaseDeg must be finite");
+  double nyq = 500 / dt_ms, limit = max_nyq_fraction * nyq;
+  for (double f : {f1, f2}) {
+    need(f > 0 && f < kInf, "a sweep frequency must be > 0 Hz, got " + num(f));
+    need(!(f > nyq), "a sweep frequency of " + num(f) + " Hz is above Nyquist (" + num(nyq) + " Hz)");
+    need(!(f > limit * (1 + 1e-12)), "a sweep frequency of " + num(f) + " Hz is above the anti-alias limit " + num(limit) + " Hz");
+  }
+  double ts = std::isnan(t_start) ? 0.0 : t_start, te = std::isnan(t_end) ? 0.0 : t_end;
+  need(ts >= 0 && ts < kInf && te >= 0 && te < kInf, "a taper length must be ≥ 0 and finite");
+  need(!(ts + te > length_ms * (1 + 1e-9)), "the sweep tapers overlap");
+  int64_t n = (int64_t)std::round(steps);
+  std::vector<double> x(n);
+  double dt = dt_ms / 1000, T = length_ms / 1000, rate = (f2 - f1) / T;
+  double p0 = phase_deg * (kPi / 180);
+  for (int64_t j = 0; j < n; j++) {
+    double t = (double)j * dt;
+    x[j] = amplitude * std::sin(p0 + 2 * kPi * (f1 * t + 0.5 * rate * t * t));
+  }
+  double sweep_ms = (double)n * dt_ms;
+  if (ts > 0)
+    for (int64_t j = 0; j < n && (double)j * dt_ms < ts; j++) x[j] *= taper_weight(shape, (double)j * dt_ms / ts);
+  if (te > 0)
+    for (int64_t j = n - 1; j >= 0 && sweep_ms - (double)j * dt_ms < te; j--)
+      x[j] *= taper_weight(shape, (sweep_ms - (double)j * dt_ms) / te);
+  return x;
+}
+
+// vibroseis/correlate.nim:82-160
+CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
+                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize) {
+  need(plen >= 2, "a pilot needs at least two samples, got " + std::to_string(plen));
+  need(pilot_dt > 0 && pilot_dt < kInf, "a pilot's dtMs must be finite and positive");
+  need(fin(pilot_t0), "a pilot's t0Ms must be finite, got " + num(pilot_t0));
+  double energy = 0;
+  for (int64_t i = 0; i < plen; i++) {
+    need(fin(pilot[i]), "pilot sample " + std::to_string(i) + " is not finite");
+    energy += pilot[i] * pilot[i];
+  }
+  need(energy != 0, "the pilot is all zeros");
+  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and positive, got " + num(dt_ms));
+  need(same_interval(pilot_dt, dt_ms), "the pilot is sampled at " + num(pilot_dt) + " ms, the records at " + num(dt_ms) + " ms: resample the pilot first (resamplePilot)");
+  need(record >= 1, "recordSamples must be ≥ 1, got " + std::to_string(record));
+  int64_t out_n = out == 0 ? record - plen : out;
+  need(out_n >= 1, "the pilot (" + std::to_string(plen) + " samples) is not shorter than the record (" + std::to_string(record) + "): no listen time; pass outSamples");
+  need(out >= 0 && out_n <= record, "outSamples must be in 0 .. recordSamples, got " + std::to_string(out));
+  need(mode == PSG_CM_CORRELATE || mode == PSG_CM_DECONVOLVE, "unknown correlation mode");
+  if (mode == PSG_CM_DECONVOLVE) need(eps_percent > 0 && eps_percent < kInf, "epsPercent must be finite and positive, got " + num(eps_percent));
+  double s = pilot_t0 / dt_ms;
+  need(std::fabs(s) < (double)(record + plen), "the pilot starts " + num(pilot_t0) + " ms from the time break: no lag reaches the output");
+  CorrHost c;
+  int64_t whole = (int64_t)std::round(s);
+  double frac = s - (double)whole;
+  c.n = next_fast(record + plen + 64 + std::llabs(whole));
+  int64_t bins = c.n / 2 + 1;
+  std::vector<cd> x(c.n, cd(0, 0));
+  for (int64_t j = 0; j < plen; j++) x[j] = pilot[j];
+  std::vector<cd> P = cfft(x, -1);
+  double peak_pow = 0;
+  for (int64_t k = 0; k < bins; k++) peak_pow = std::max(peak_pow, std::norm(P[k]));
+  double eps = mode == PSG_CM_DECONVOLVE ? eps_percent / 100 * peak_pow : 0.0;
+  std::vector<double> w(bins);
+  double peak = 0;
+  for (int64_t k = 0; k < bins; k++) {
+    double p2 = std::norm(P[k]);
+    w[k] = mode == PSG_CM_DECONVOLVE ? 1 / (p2 + eps) : 1.0;
+    double g = p2 * w[k];
+    peak += (k == 0 || (c.n % 2 == 0 && k == bins - 1)) ? g : 2 * g;
+  }
+  peak /= (double)c.n;
+  c.scale = normalize ? 1 / peak : 1.0;
+  c.mul_re.resize(bins);
+  c.mul_im.resize(bins);
+  for (int64_t k = 0; k < bins; k++) {
+    double th = 2 * kPi * (double)k * frac / (double)c.n;
+    cd m = std::conj(P[k]) * (w[k] * c.scale) * cd(std::cos(th), std::sin(th));
+    c.mul_re[k] = m.real();
+    c.mul_im[k] = m.imag();
+  }
+  c.mul_im[bins - 1] = 0;  // the inverse takes Nyquist as real
+  c.shift = whole;
+  c.record = record;
+  c.out = out_n;
+  c.pilot_len = plen;
+  c.dt_ms = dt_ms;
+  c.mode = mode;
+  c.fft = fft_tables(c.n);
+  return c;
+}
+
+}  // namespace psg

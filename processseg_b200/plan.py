@@ -1,0 +1,206 @@
+"""``compile``, ``PipelinePlan``, ``Workspace`` and ``apply``: the host side
+of src/processSEG/pipeline.nim:466-772 over the C ABI of libpsgcuda.so.
+
+``apply`` takes either CUDA tensors (torch, C-contiguous ``[rows, cols]``;
+the work is queued on the current torch stream and nothing is copied) or
+numpy arrays (host memory: the library copies the block in, runs the plan
+and copies it back before returning). Errors follow the reference:
+``ValueError`` before any sample changes for a bad shape, width, interval
+or overlap; ``AssertionError`` (the reference's AssertionDefect) for a
+workspace that was not reserved for the plan.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Optional
+
+import numpy as np
+
+from . import _abi as A
+from .meta import ChunkMeta
+
+
+def _dtype_code(T) -> int:
+    if T in (A.F32, np.float32, "float32") or getattr(T, "__name__", "") == "float32":
+        return A.F32
+    if T in (A.F64, np.float64, float, "float64") or getattr(T, "__name__", "") == "float64":
+        return A.F64
+    try:
+        import torch
+        if T == torch.float32:
+            return A.F32
+        if T == torch.float64:
+            return A.F64
+    except ImportError:
+        pass
+    raise ValueError(f"a sample type must be float32 or float64, got {T!r}")
+
+
+class Workspace:
+    """The scratch of ``apply`` on the device (workspace.nim:50-96): a
+    grow-only arena, one per thread or stream of callers."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        A.check(A.lib().psg_workspace_create(C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and A._lib is not None:
+            A._lib.psg_workspace_destroy(h)
+            self.h = None
+
+    def reserve(self, plan: "PipelinePlan", rows: int = 65536, cols: int = 0):
+        """Grows the arena to hold ``plan``'s scratch for up to ``rows`` rows,
+        and, with ``cols``, the staging a host-memory ``apply`` of
+        ``rows × cols`` needs. A no-op when it already fits."""
+        A.check(A.lib().psg_workspace_reserve(self.h, plan.h, int(rows), int(cols)))
+
+    @property
+    def bytes(self) -> int:
+        return A.lib().psg_workspace_bytes(self.h)
+
+
+def initWorkspace() -> Workspace:
+    return Workspace()
+
+
+def _is_torch(x) -> bool:
+    try:
+        import torch
+        return isinstance(x, torch.Tensor)
+    except ImportError:
+        return False
+
+
+class PipelinePlan:
+    """A compiled pipeline (pipeline.nim:200-211): immutable, shared by any
+    number of callers, each with its own ``Workspace``."""
+
+    def __init__(self, h, dtype: int, dtMs: float):
+        self.h = h
+        self.dtype = dtype
+        self._dtMs = dtMs
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and A._lib is not None:
+            A._lib.psg_plan_destroy(h)
+            self.h = None
+
+    # ------------------------------------------------------------ accessors
+    @property
+    def generation(self) -> int:
+        return A.lib().psg_plan_generation(self.h)
+
+    @property
+    def requiredMargin(self) -> int:
+        return A.lib().psg_plan_margin(self.h)
+
+    @property
+    def samples(self) -> int:
+        return A.lib().psg_plan_samples(self.h)
+
+    @property
+    def recordSamples(self) -> int:
+        return A.lib().psg_plan_record_samples(self.h)
+
+    @property
+    def dtMs(self) -> float:
+        return self._dtMs
+
+    @property
+    def partCount(self) -> int:
+        return A.lib().psg_plan_part_count(self.h)
+
+    def __len__(self):
+        return A.lib().psg_plan_len(self.h)
+
+    def stepNfft(self, i: int) -> int:
+        return A.lib().psg_plan_step_nfft(self.h, i)
+
+    def stepMargin(self, i: int) -> int:
+        return A.lib().psg_plan_step_margin(self.h, i)
+
+    # ---------------------------------------------------------------- apply
+    def _check_block(self, x, name):
+        if x.ndim != 2:
+            raise ValueError(f"{name} must be a [rows, cols] tensor, got rank {x.ndim}")
+        want = np.float32 if self.dtype == A.F32 else np.float64
+        if _is_torch(x):
+            import torch
+            tw = torch.float32 if self.dtype == A.F32 else torch.float64
+            if x.dtype != tw:
+                raise ValueError(f"{name} is {x.dtype}, the plan is for {tw}")
+            if not x.is_contiguous():
+                raise ValueError(f"{name} must be C-contiguous (row-major)")
+            if not x.is_cuda:
+                raise ValueError(f"{name} must be a CUDA tensor or a numpy array")
+        else:
+            if x.dtype != want:
+                raise ValueError(f"{name} is {x.dtype}, the plan is for {np.dtype(want)}")
+            if not x.flags.c_contiguous:
+                raise ValueError(f"{name} must be C-contiguous (row-major)")
+
+    def apply(self, *args, stream=None):
+        """``apply(b, meta, ws)`` in place, or ``apply(src, dst, meta, ws)``
+        from src into dst (pipeline.nim:736-772)."""
+        if len(args) == 3:
+            src, (dst, meta, ws) = None, args
+        elif len(args) == 4:
+            src, dst, meta, ws = args
+        else:
+            raise TypeError("apply(b, meta, ws) or apply(src, dst, meta, ws)")
+        if self.h is None:
+            raise ValueError("a PipelinePlan must come from compile")
+        self._check_block(dst, "dst")
+        rows, cols = int(dst.shape[0]), int(dst.shape[1])
+        if src is not None:
+            self._check_block(src, "src")
+            if tuple(src.shape) != tuple(dst.shape):
+                raise ValueError(f"src is {src.shape[0]} × {src.shape[1]}, dst {rows} × {cols}")
+            if _is_torch(src) != _is_torch(dst):
+                raise ValueError("src and dst must both be CUDA tensors or both numpy arrays")
+        meta.checkShape(rows)
+        if _is_torch(dst):
+            import torch
+            live, start = meta.device(cols, 0, dst.device.index)
+            st = stream if stream is not None else torch.cuda.current_stream(dst.device).cuda_stream
+            A.check(A.lib().psg_apply(self.h, ws.h, None if src is None else src.data_ptr(),
+                                      dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
+                                      meta.dtMs, st))
+        else:
+            live, start = meta.flat(cols, 0)
+            p = lambda a: a.ctypes.data_as(C.c_void_p)
+            A.check(A.lib().psg_apply_host(self.h, ws.h, None if src is None else p(src), p(dst), rows,
+                                           cols, p(live), p(start), meta.dtMs,
+                                           stream if stream is not None else None))
+
+    def panelFactorOf(self, b, meta: ChunkMeta, part: int, ws: Workspace) -> float:
+        """The per-panel factor of part ``part`` over the block ``b`` (a CUDA
+        tensor), NaN when it leaves the block alone (pipeline.nim:656-669)."""
+        import torch
+        self._check_block(b, "b")
+        rows, cols = int(b.shape[0]), int(b.shape[1])
+        live, _ = meta.device(cols, 0, b.device.index)
+        out = torch.empty(1, dtype=torch.float64, device=b.device)
+        st = torch.cuda.current_stream(b.device).cuda_stream
+        A.check(A.lib().psg_panel_factor(self.h, ws.h, part, b.data_ptr(), rows, cols,
+                                         live.data_ptr(), out.data_ptr(), st))
+        return float(out.item())
+
+
+def compile(pipeline, T, dtMs: float, samples: int, recordSamples: int = 0) -> PipelinePlan:
+    """Validates every op for blocks of up to ``samples`` samples at
+    ``dtMs`` and uploads its tables to the current device
+    (pipeline.nim:466-523). ``ValueError`` names the op:
+    ``op 1 (opFilter): ...``."""
+    dt = _dtype_code(T)
+    ops = list(pipeline)
+    arr = A.ops_array(ops)
+    h = C.c_void_p()
+    A.check(A.lib().psg_plan_compile(arr, len(ops), dt, float(dtMs), int(samples),
+                                     int(recordSamples), C.byref(h)))
+    return PipelinePlan(h, dt, float(dtMs))

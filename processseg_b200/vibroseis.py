@@ -1,0 +1,222 @@
+"""Vibroseis correlation and vertical stacking: the host side of
+src/processSEG/vibroseis/{sweep,taper,pilot,correlate,vstack}.nim over the
+C ABI. Sweeps are synthesised in float64 (closed-form linear phase); the
+pilot spectrum and the correlation multiplier are computed in float64 at
+plan time; correlation and the stack run on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi as A
+from .meta import ChunkMeta
+
+tpLinear, tpCosine, tpCos2, tpHamming, tpBlackman, tpBlackmanHarris = range(6)
+
+
+@dataclass(frozen=True)
+class SweepTaper:
+    """taper.nim:60-77 (the shapes without a special function)."""
+    startMs: float = 0.0
+    endMs: float = 0.0
+    shape: int = tpCos2
+
+
+def initSweepTaper(startMs: float, endMs: float, shape: int = tpCos2) -> SweepTaper:
+    for name, v in (("startMs", startMs), ("endMs", endMs)):
+        if not math.isnan(v) and not (v >= 0 and v < math.inf):
+            raise ValueError(f"a taper {name} must be ≥ 0 and finite (or NaN for none), got {v}")
+    return SweepTaper(startMs, endMs, shape)
+
+
+def noTaper() -> SweepTaper:
+    return SweepTaper(0.0, 0.0, tpLinear)
+
+
+@dataclass(frozen=True)
+class SweepSpec:
+    """A linear sweep (sweep.nim:81-95, law slLinear)."""
+    f1Hz: float
+    f2Hz: float
+    lengthMs: float
+    dtMs: float
+    taper: SweepTaper = SweepTaper(0.0, 0.0, tpLinear)
+    startPhaseDeg: float = 0.0
+    amplitude: float = 1.0
+    maxNyquistFraction: float = 0.8
+
+    def samples(self, dtype=np.float64) -> np.ndarray:
+        """sweepSamples (sweep.nim:331-348): phase in float64."""
+        n = C.c_int64()
+        dt = A.F32 if dtype == np.float32 else A.F64
+        args = (self.f1Hz, self.f2Hz, self.lengthMs, self.dtMs, self.taper.startMs,
+                self.taper.endMs, self.taper.shape, self.startPhaseDeg, self.amplitude,
+                self.maxNyquistFraction, dt)
+        A.check(A.lib().psg_linear_sweep(*args, None, C.byref(n)))
+        x = np.zeros(n.value, dtype)
+        A.check(A.lib().psg_linear_sweep(*args, x.ctypes.data_as(C.c_void_p), C.byref(n)))
+        return x
+
+
+def linearSweep(f1Hz, f2Hz, lengthMs, dtMs, taper: SweepTaper = None, startPhaseDeg=0.0,
+                amplitude=1.0, maxNyquistFraction=0.8) -> SweepSpec:
+    s = SweepSpec(f1Hz, f2Hz, lengthMs, dtMs, taper or noTaper(), startPhaseDeg, amplitude,
+                  maxNyquistFraction)
+    s.samples()  # validates (sweep.nim:126-178)
+    return s
+
+
+@dataclass
+class Pilot:
+    """pilot.nim:55-62."""
+    samples: np.ndarray
+    dtMs: float
+    t0Ms: float = 0.0
+    sweep: Optional[SweepSpec] = None
+
+    def __len__(self):
+        return int(self.samples.size)
+
+
+def generatePilot(spec: SweepSpec, dtype=np.float64) -> Pilot:
+    return Pilot(spec.samples(dtype), spec.dtMs, 0.0, spec)
+
+
+def initPilot(samples, dtMs, t0Ms=0.0) -> Pilot:
+    return Pilot(np.asarray(samples), float(dtMs), float(t0Ms))
+
+
+class CorrelationPlan:
+    """correlate.nim:66-160."""
+
+    def __init__(self, T, pilot: Pilot, dtMs: float, recordSamples: int, outSamples: int = 0,
+                 mode: int = A.CM_CORRELATE, epsPercent: float = 1.0, normalize: bool = True):
+        from .plan import _dtype_code
+        self.dtype = _dtype_code(T)
+        ps = np.ascontiguousarray(pilot.samples)
+        pdt = A.F32 if ps.dtype == np.float32 else A.F64
+        if ps.dtype not in (np.float32, np.float64):
+            ps = ps.astype(np.float64)
+            pdt = A.F64
+        h = C.c_void_p()
+        A.check(A.lib().psg_corr_plan_create(ps.ctypes.data_as(C.c_void_p), pdt, ps.size, pilot.dtMs,
+                                             pilot.t0Ms, self.dtype, dtMs, recordSamples, outSamples,
+                                             mode, epsPercent, int(normalize), C.byref(h)))
+        self.h = h
+        self.dtMs = float(dtMs)
+        self.recordSamples = int(recordSamples)
+        self.pilotSamples = int(ps.size)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and A._lib is not None:
+            A._lib.psg_corr_plan_destroy(h)
+            self.h = None
+
+    @property
+    def nfft(self) -> int:
+        return A.lib().psg_corr_plan_nfft(self.h)
+
+    @property
+    def outSamples(self) -> int:
+        return A.lib().psg_corr_plan_out_samples(self.h)
+
+    @property
+    def scale(self) -> float:
+        return A.lib().psg_corr_plan_scale(self.h)
+
+    def correlateInto(self, src, dst, meta: ChunkMeta, stack: "RecordStack" = None, rowMap=None):
+        """correlate.nim:421-464 on CUDA tensors; with ``stack`` the
+        correlated live rows are also added to it (vstack.nim:357-380) in the
+        same launch."""
+        import torch
+        rows, cols = int(src.shape[0]), int(src.shape[1])
+        meta.checkShape(rows)
+        if dst is not None:
+            meta.checkShape(int(dst.shape[0]))
+            if int(dst.shape[1]) != self.outSamples:
+                raise ValueError(f"dst must be {self.outSamples} samples wide, got {dst.shape[1]}")
+        if meta.firstSample != 0:
+            raise ValueError(f"correlation needs whole records from sample 0, got firstSample "
+                             f"{meta.firstSample}")
+        live, _ = meta.device(cols, 1, src.device.index)
+        st = torch.cuda.current_stream(src.device).cuda_stream
+        dptr = None if dst is None else dst.data_ptr()
+        if stack is None:
+            A.check(A.lib().psg_correlate(self.h, src.data_ptr(), dptr, rows, cols, live.data_ptr(),
+                                          meta.dtMs, st))
+        else:
+            slive, _ = meta.device(self.outSamples, 0, src.device.index)
+            rm = None
+            if rowMap is not None:
+                rm = torch.as_tensor(np.asarray(rowMap, np.int32), device=src.device)
+                self._rm = rm
+            A.check(A.lib().psg_correlate_stack(self.h, stack.h, src.data_ptr(), dptr, rows, cols,
+                                                live.data_ptr(), slive.data_ptr(),
+                                                None if rm is None else rm.data_ptr(), meta.dtMs, st))
+
+
+def initCorrelationPlan(T, pilot: Pilot, dtMs: float, recordSamples: int, outSamples: int = 0,
+                        mode: int = A.CM_CORRELATE, epsPercent: float = 1.0,
+                        normalize: bool = True) -> CorrelationPlan:
+    return CorrelationPlan(T, pilot, dtMs, recordSamples, outSamples, mode, epsPercent, normalize)
+
+
+class RecordStack:
+    """A vertical record stack (vstack.nim:95-150, rsVertical): float64 sums
+    and int32 counts on the device."""
+
+    def __init__(self, rows: int, samples: int, dtMs: float):
+        h = C.c_void_p()
+        A.check(A.lib().psg_stack_create(rows, samples, dtMs, C.byref(h)))
+        self.h = h
+        self.rows, self.samples, self.dtMs = rows, samples, dtMs
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and A._lib is not None:
+            A._lib.psg_stack_destroy(h)
+            self.h = None
+
+    def clear(self):
+        import torch
+        A.check(A.lib().psg_stack_clear(self.h, torch.cuda.current_stream().cuda_stream))
+
+    def addRecord(self, b, meta: ChunkMeta, rowMap=None):
+        """vstack.nim:357-380 on a CUDA tensor."""
+        import torch
+        rows, cols = int(b.shape[0]), int(b.shape[1])
+        meta.checkShape(rows)
+        if cols > self.samples:
+            raise ValueError(f"the record has {cols} samples, the stack {self.samples}")
+        live, _ = meta.device(cols, 0, b.device.index)
+        rm = None
+        if rowMap is not None:
+            rm = torch.as_tensor(np.asarray(rowMap, np.int32), device=b.device)
+            self._rm = rm
+        dt = A.F32 if b.dtype == torch.float32 else A.F64
+        A.check(A.lib().psg_stack_add(self.h, b.data_ptr(), dt, rows, cols, live.data_ptr(),
+                                      None if rm is None else rm.data_ptr(),
+                                      torch.cuda.current_stream(b.device).cuda_stream))
+
+    def stackInto(self, dst, norm: int = A.FN_FOLD):
+        import torch
+        if tuple(dst.shape) != (self.rows, self.samples):
+            raise ValueError(f"dst must be a [{self.rows}, {self.samples}] tensor, got {tuple(dst.shape)}")
+        dt = A.F32 if dst.dtype == torch.float32 else A.F64
+        A.check(A.lib().psg_stack_result(self.h, dst.data_ptr(), dt, norm,
+                                         torch.cuda.current_stream(dst.device).cuda_stream))
+
+    def foldInto(self, dst):
+        import torch
+        A.check(A.lib().psg_stack_fold(self.h, dst.data_ptr(),
+                                       torch.cuda.current_stream(dst.device).cuda_stream))
+
+
+def initRecordStack(rows: int, samples: int, dtMs: float) -> RecordStack:
+    return RecordStack(rows, samples, dtMs)

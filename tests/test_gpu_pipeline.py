@@ -1,0 +1,226 @@
+"""Parity of the device pipeline (libpsgcuda.so through its C ABI) with the
+CPU oracle, on seeded synthetic panels. The bar: each
+output trace within 1e-5 of its RMS of the oracle's float32 apply, and
+within 1e-12 of its RMS for float64 plans. Non-live rows and samples past a
+row's live length are copied bit for bit."""
+import math
+
+import numpy as np
+import pytest
+
+import processseg_b200 as P
+from processseg_b200 import synth
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("built")]
+
+C1_FLOW = [P.demeanOp(), P.bandPassOp(P.Corners(4, 8, 60, 80)), P.agcOp(500)]
+C2_FLOW = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(3, 6, 70, 90)).withNotch(50, 2)),
+           P.agcOp(300)]
+
+
+def rel_rms_err(got, want, live):
+    """max over live traces of max|got − want| / rms(want) on the live part."""
+    worst = 0.0
+    for r in range(want.shape[0]):
+        n = int(live[r])
+        if n == 0:
+            continue
+        w = want[r, :n].astype(np.float64)
+        g = got[r, :n].astype(np.float64)
+        rms = math.sqrt(float(np.mean(w * w)))
+        if rms == 0:
+            assert np.all(g == 0)
+            continue
+        worst = max(worst, float(np.max(np.abs(g - w))) / rms)
+    return worst
+
+
+def run_gpu(flow, data, meta, dtype, dtMs, samples=None, record=0, inplace=False, host=False):
+    plan = P.initPipeline(flow).compile(dtype, dtMs, samples or data.shape[1], record)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=data.shape[0], cols=data.shape[1])
+    if host:
+        dst = np.zeros_like(data)
+        plan.apply(data, dst, meta, ws)
+        return dst
+    src = torch.from_numpy(data).cuda()
+    if inplace:
+        plan.apply(src, meta, ws)
+        torch.cuda.synchronize()
+        return src.cpu().numpy()
+    dst = torch.zeros_like(src)
+    plan.apply(src, dst, meta, ws)
+    torch.cuda.synchronize()
+    return dst.cpu().numpy()
+
+
+def run_oracle(flow, data, meta, dtype, dtMs, samples=None, record=0):
+    plan = O.OraclePlan(flow, dtype, dtMs, samples or data.shape[1], record)
+    live, start = meta.flat(data.shape[1], 0)
+    return plan.apply(data, live, start)
+
+
+def test_c1_plain_plan_matches_oracle():
+    g = synth.c1()
+    meta = g.meta()
+    got = run_gpu(C1_FLOW, g.data, meta, P.float32, 2.0)
+    want = run_oracle(C1_FLOW, g.data, meta, P.F32, 2.0)
+    live = meta.flat(2001)[0]
+    assert rel_rms_err(got, want, live) <= 1e-5
+    # and against the float64 oracle
+    want64 = run_oracle(C1_FLOW, g.data.astype(np.float64), meta, P.F64, 2.0)
+    assert rel_rms_err(got, want64, live) <= 1e-5
+
+
+def test_c2_uneven_panel_src_dst_and_in_place():
+    g = synth.c2(rows=300)
+    g.status[[5, 77]] = P.tsDead
+    g.status[[9]] = P.tsAux
+    g.failed = np.array([13, 200], np.int64)
+    meta = g.meta()
+    want = run_oracle(C2_FLOW, g.data, meta, P.F32, 2.0)
+    live = meta.flat(3001)[0]
+    for inplace in (False, True):
+        got = run_gpu(C2_FLOW, g.data, meta, P.float32, 2.0, inplace=inplace)
+        assert rel_rms_err(got, want, live) <= 1e-5
+        for r in range(g.data.shape[0]):
+            n = live[r]
+            assert np.array_equal(got[r, n:], g.data[r, n:]), r  # dead rows and padding
+    host = run_gpu(C2_FLOW, g.data, meta, P.float32, 2.0, host=True)
+    dev = run_gpu(C2_FLOW, g.data, meta, P.float32, 2.0)
+    assert np.array_equal(host, dev)
+
+
+def test_float64_plan_matches_oracle_to_1e12():
+    g = synth.c2(rows=64, dtype=np.float64)
+    meta = g.meta()
+    got = run_gpu(C2_FLOW, g.data, meta, P.float64, 2.0)
+    want = run_oracle(C2_FLOW, g.data, meta, P.F64, 2.0)
+    assert rel_rms_err(got, want, meta.flat(3001)[0]) <= 1e-12
+
+
+FLOWS = {
+    "basic": [P.detrendOp(), P.scaleOp(2.5), P.gainDbOp(-3), P.clipOp(-1.5, 1.2), P.polarityOp(),
+              P.demeanOp()],
+    "highcut_reflect": [P.filterOp(P.highCut(60, 80))],
+    "zero_dc": [P.filterOp(P.highCut(60, 80).withZeroDc())],
+    "trend_none": [P.filterOp(P.lowCut(2, 4), P.trNone)],
+    "trend_mean": [P.filterOp(P.bandPass(P.Corners(4, 8, 60, 80)), P.trMean)],
+    "butter": [P.filterOp(P.butterBandPass(5, 100, 24)), P.gainCurveOp(P.powerGain(2))],
+    "agc_meanabs": [P.agcOp(200, P.agcMeanAbs, target=2.0)],
+    "norm_max": [P.normalizeOp(P.normMax, target=3.0)],
+    "norm_rms": [P.bandPassOp(P.Corners(4, 8, 60, 80)), P.normalizeOp(P.normRms)],
+    "norm_pct": [P.normalizeOp(P.normPercentile, percentile=99.0)],
+    "norm_pct_low": [P.normalizeOp(P.normPercentile, percentile=37.5)],
+    "panel_rms": [P.agcOp(200), P.normalizeOp(P.normRms, P.perPanel, target=3.0), P.demeanOp()],
+    "panel_max": [P.normalizeOp(P.normMax, P.perPanel), P.agcOp(100)],
+    "panel_pct": [P.demeanOp(), P.normalizeOp(P.normPercentile, P.perPanel, percentile=99.0)],
+    "curves": [P.gainCurveOp(P.exponentialGain(3)),
+               P.gainCurveOp(P.knotGain([P.GainKnot(0, 0), P.GainKnot(900, 6), P.GainKnot(3000, 20)]))],
+}
+
+
+@pytest.mark.parametrize("name", sorted(FLOWS))
+@pytest.mark.parametrize("dtype", [P.F32, P.F64])
+def test_op_flows_match_oracle(name, dtype):
+    npd = np.float32 if dtype == P.F32 else np.float64
+    g = synth.shot_gather(40, 1201, 2.0, seed=11, dtype=npd, live_range=(2, 1201), sine_hz=30.0,
+                          workload="flows")
+    g.status[[3]] = P.tsDead
+    g.t0Ms = np.linspace(-10, 40, 40)
+    g.numSamples[7] = 1
+    meta = g.meta()
+    flow = FLOWS[name]
+    got = run_gpu(flow, g.data, meta, dtype, 2.0)
+    want = run_oracle(flow, g.data, meta, dtype, 2.0)
+    tol = 1e-5 if dtype == P.F32 else 1e-12
+    if name.startswith("panel_pct"):
+        tol = max(tol, 1e-9)  # the histogram bin position is exact; sums reorder in f64
+    assert rel_rms_err(got, want, meta.flat(1201)[0]) <= tol
+
+
+def test_gain_curve_zoom_window_matches_whole_record_plan():
+    # tests/tpipeline.nim:333-361: a window compiled for its width with the
+    # record's length gives the bits of the whole-record plan.
+    ns, first, cols = 6001, 3700, 1101
+    g = synth.shot_gather(12, ns, 2.0, seed=5, workload="zoom")
+    win = np.ascontiguousarray(g.data[:, first:first + cols])
+    meta = P.initChunkMeta(g.status, g.numSamples, 2.0, g.t0Ms, first)
+    for curve in (P.powerGain(2), P.exponentialGain(3),
+                  P.knotGain([P.GainKnot(0, 0), P.GainKnot(9000, 20)])):
+        flow = [P.gainCurveOp(curve)]
+        a = run_gpu(flow, win, meta, P.float32, 2.0, samples=ns)
+        b = run_gpu(flow, win, meta, P.float32, 2.0, samples=cols, record=ns)
+        assert np.array_equal(a, b)
+        want = run_oracle(flow, win, meta, P.F32, 2.0, samples=cols, record=ns)
+        assert rel_rms_err(b, want, meta.flat(cols)[0]) <= 1e-6
+
+
+def test_nan_stays_in_its_row():
+    g = synth.shot_gather(6, 500, 2.0, seed=2, workload="nan")
+    g.data[2, 250] = np.nan
+    meta = g.meta()
+    got = run_gpu(C1_FLOW, g.data, meta, P.float32, 2.0)
+    assert np.isnan(got[2]).any()
+    for r in (0, 1, 3, 4, 5):
+        assert np.all(np.isfinite(got[r]))
+
+
+def test_errors_change_nothing():
+    # tests/tpipeline.nim:227-249
+    g = synth.shot_gather(20, 500, 2.0, seed=3, workload="err")
+    meta = g.meta()
+    src = torch.from_numpy(g.data).cuda()
+    orig = src.clone()
+    flow = P.initPipeline([P.demeanOp(), P.agcOp(100)])
+    ws = P.initWorkspace()
+    narrow = flow.compile(P.float32, 2.0, 400)
+    ws.reserve(narrow)
+    with pytest.raises(ValueError):
+        narrow.apply(src, meta, ws)
+    other = flow.compile(P.float32, 4.0, 500)
+    with pytest.raises(ValueError):
+        other.apply(src, meta, ws)
+    ok = flow.compile(P.float32, 2.0, 500)
+    with pytest.raises(ValueError):
+        ok.apply(src, torch.zeros(19, 500, device="cuda"), meta, ws)
+    with pytest.raises(ValueError):
+        ok.apply(src, torch.zeros(20, 499, device="cuda"), meta, ws)
+    with pytest.raises(ValueError):
+        ok.apply(src[:, :250], src[:, 250:], meta, ws)  # not contiguous
+    with pytest.raises(ValueError):
+        ok.apply(src.double(), meta, ws)
+    buf = torch.zeros(24, 500, device="cuda")
+    with pytest.raises(ValueError, match="overlap"):
+        P.initPipeline([P.scaleOp(2)]).compile(P.float32, 2.0, 500).apply(buf[0:20], buf[2:22], meta, ws)
+    torch.cuda.synchronize()
+    assert torch.equal(src, orig)
+    panel = P.initPipeline([P.normalizeOp(P.normRms, P.perPanel)]).compile(P.float32, 2.0, 500)
+    with pytest.raises(AssertionError):
+        panel.apply(src, meta, P.initWorkspace())
+    with pytest.raises(ValueError, match=r"^op 1 \(opFilter\): "):
+        P.initPipeline([P.demeanOp(), P.bandPassOp(P.Corners(4, 8, 200, 260))]).compile(P.float32, 2.0, 500)
+
+
+def test_empty_pipeline_copies():
+    g = synth.shot_gather(10, 100, 2.0, seed=1, workload="empty")
+    meta = g.meta()
+    got = run_gpu([], g.data, meta, P.float32, 2.0)
+    assert np.array_equal(got, g.data)
+    same = run_gpu([], g.data, meta, P.float32, 2.0, inplace=True)
+    assert np.array_equal(same, g.data)
+
+
+def test_panel_factor_matches_oracle():
+    g = synth.shot_gather(50, 800, 2.0, seed=8, workload="pf", live_range=(100, 800))
+    meta = g.meta()
+    flow = P.initPipeline([P.agcOp(50), P.normalizeOp(P.normPercentile, P.perPanel, target=2)])
+    plan = flow.compile(P.float32, 2.0, 800)
+    ws = P.initWorkspace()
+    ws.reserve(plan)
+    b = torch.from_numpy(g.data).cuda()
+    f = plan.panelFactorOf(b, meta, 1, ws)
+    st = O.panel_stats(g.data, meta.flat(800)[0], 99.0)
+    assert abs(f - 2 / st["clip"]) <= 1e-12 * abs(f)
