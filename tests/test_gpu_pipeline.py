@@ -37,6 +37,27 @@ def rel_rms_err(got, want, live):
     return worst
 
 
+def assert_parity(got, flow, data, meta, dtype, dtMs, samples=None, record=0, tol=None):
+    """The device output against the oracle of the same precision: within
+    ``tol`` (1e-5 float32, 1e-12 float64) of each trace's RMS. Where the
+    oracle's own float32 output is further than that from the float64
+    oracle (float32 rounding of a large offset under a low-cut, say), the
+    device must be no further from the float64 oracle than twice the
+    oracle's own float32 error."""
+    tol = tol if tol is not None else (1e-5 if dtype == P.F32 else 1e-12)
+    live = meta.flat(data.shape[1])[0]
+    want = run_oracle(flow, data, meta, dtype, dtMs, samples, record)
+    e = rel_rms_err(got, want, live)
+    if e <= tol or dtype == P.F64:
+        assert e <= tol, e
+        return e
+    want64 = run_oracle(flow, data.astype(np.float64), meta, P.F64, dtMs, samples, record)
+    own = rel_rms_err(want, want64, live)
+    mine = rel_rms_err(got, want64, live)
+    assert mine <= max(tol, 2 * own), (e, mine, own)
+    return mine
+
+
 def run_gpu(flow, data, meta, dtype, dtMs, samples=None, record=0, inplace=False, host=False):
     plan = P.initPipeline(flow).compile(dtype, dtMs, samples or data.shape[1], record)
     ws = P.initWorkspace()
@@ -134,11 +155,10 @@ def test_op_flows_match_oracle(name, dtype):
     meta = g.meta()
     flow = FLOWS[name]
     got = run_gpu(flow, g.data, meta, dtype, 2.0)
-    want = run_oracle(flow, g.data, meta, dtype, 2.0)
     tol = 1e-5 if dtype == P.F32 else 1e-12
     if name.startswith("panel_pct"):
         tol = max(tol, 1e-9)  # the histogram bin position is exact; sums reorder in f64
-    assert rel_rms_err(got, want, meta.flat(1201)[0]) <= tol
+    assert_parity(got, flow, g.data, meta, dtype, 2.0, tol=tol)
 
 
 def test_gain_curve_zoom_window_matches_whole_record_plan():
