@@ -222,6 +222,25 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
                     int32_t cols, const int32_t* live, double clip_percentile,
                     double* out, void* stream);
 
+/* panelStats without allocating: the same computation and output as
+ * psg_panel_stats, for callers that cannot call cudaMalloc, such as a
+ * viewer's frame loop that reads display-gain statistics every frame from
+ * inside a fixed device-memory budget, or code that must not allocate on a
+ * stream it shares with other work. No counterpart in the reference (its
+ * panelStats takes a Workspace the caller grew beforehand).
+ * Its scratch is a fixed array inside the library, about 1.25 MiB, that every
+ * GPU which loads the library holds until the process exits; it takes at
+ * most PSG_STATIC_MAX_ROWS rows (PSG_EINVAL beyond). The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress): make
+ * that first call before any stream capture. Every call shares the one
+ * array and it keeps the last call's contents, so calls that overlap on the
+ * GPU (on different streams, or from different host threads) race: order
+ * them on one stream. */
+#define PSG_STATIC_MAX_ROWS 65536
+int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32_t cols,
+                           const int32_t* live, double clip_percentile, double* out,
+                           void* stream);
+
 /* ----------------------------------------------------------- vibroseis */
 /* linearSweep + sweepInto + generatePilot (taper shapes tpLinear, tpCosine,
  * tpCos2, tpHamming, tpBlackman), src/processSEG/vibroseis/sweep.nim:185-342,

@@ -126,6 +126,7 @@ def _declare(lib):
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_trace_stats": (C.c_int, [P, I32, I64, I32, P, P, P, P]),
         "psg_panel_stats": (C.c_int, [P, P, I32, I64, I32, P, DBL, P, P]),
+        "psg_panel_stats_static": (C.c_int, [P, I32, I64, I32, P, DBL, P, P]),
         "psg_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, I32, DBL, DBL, DBL, I32, P,
                                        C.POINTER(I64)]),
         "psg_corr_plan_create": (C.c_int, [P, I32, I64, DBL, DBL, I32, DBL, I32, I32, I32, DBL, I32,

@@ -1386,6 +1386,72 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
   });
 }
 
+// ------------------------------------------------- panel stats, no allocation
+// psg_panel_stats for callers that cannot allocate device memory: its scratch
+// (the panel output, per-row Σx² and max |x|, and the 65536-bin histogram)
+// is a fixed array of this file, sized for PSG_STATIC_MAX_ROWS rows, that
+// every GPU which loads the library holds until the process exits. Host code
+// must not pass the array's name to a kernel (on the host it is a stand-in,
+// not a device address): the device address is looked up once per device
+// with cudaGetSymbolAddress and cached.
+}  // extern "C"
+static const int64_t kStaticBytes = 512 + (int64_t)PSG_STATIC_MAX_ROWS * 16 + kHist;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+static std::mutex g_static_mu;
+static void* g_static_addr[128];
+extern "C" {
+
+int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live,
+                           double clip_percentile, double* out, void* stream) {
+  return guarded([&] {
+    if (!std::isnan(clip_percentile) && !(clip_percentile >= 0 && clip_percentile <= 100))
+      throw InvalidArg("a percentile must be in 0 .. 100, got " + std::to_string(clip_percentile));
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if (rows > PSG_STATIC_MAX_ROWS)
+      throw InvalidArg("psg_panel_stats_static takes at most " + std::to_string(PSG_STATIC_MAX_ROWS) +
+                       " rows, got " + std::to_string(rows) + " (use psg_panel_stats with a workspace)");
+    if (rows > 0 && (!block || !live)) throw InvalidArg("null argument");
+    if (!out) throw InvalidArg("null argument");
+    ensure_device();
+    int dev;
+    CUDA_OK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) throw InvalidArg("device ordinal out of range");
+    char* base;
+    {
+      std::lock_guard<std::mutex> g(g_static_mu);
+      if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) throw CudaError(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_static_addr[dev] = p;
+      }
+      base = (char*)g_static_addr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    PanelOut* po = reinterpret_cast<PanelOut*>(base + 448);
+    double* ss = reinterpret_cast<double*>(base + 512);
+    double* mx = ss + rows;
+    unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + (int64_t)PSG_STATIC_MAX_ROWS * 16);
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)g_sm_count * 8));
+    if (rows > 0) {
+      if (dtype == PSG_F32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
+      else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
+    }
+    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po);
+    if (!std::isnan(clip_percentile)) {
+      // The array keeps the previous call's counts: the histogram starts at zero.
+      CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
+      if (rows > 0) {
+        if (dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
+        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
+      }
+    }
+    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
+    CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
 // ------------------------------------------------------------- vibroseis
 int psg_linear_sweep(double f1, double f2, double length_ms, double dt_ms, double ts, double te, int32_t shape,
                      double phase_deg, double amplitude, double max_nyq, int32_t dtype, void* out, int64_t* n_out) {
