@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 OUT = os.path.join(PKG, "libpsgcuda.so")
 SOURCES = ["psg_cuda.cu", "psg_plan.cpp"]
-DEPS = SOURCES + ["psg_device.cuh", "psg_internal.h", os.path.join("..", "..", "include", "psg.h")]
+DEPS = SOURCES + ["psg_device.cuh", "psg_internal.h", "psg_dft_consts.h", os.path.join("..", "..", "include", "psg.h")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr", "-Xptxas", "-v"]

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -41,7 +42,7 @@ void set_error(const std::string& m) { t_err = m; }
 struct DevStep {
   int kind, trend, reflect, zero_dc;
   int agc_mode, stat, pad, nfft;
-  int half, table_len, table_on, _p;
+  int half, table_len, need, need_next;
   double factor, lo, hi, dc_gain, target, epsilon, norm_target, percentile, t_min_ms, dt_ms;
   FftDesc fft;
   const void* gain;
@@ -64,6 +65,8 @@ struct PipeArgs {
   const double* start_ms;
   const double* factor;  // the part's panel factor (NaN: none) or NULL
   const DevStep* steps;
+  int x_bytes;           // bytes of one row buffer (two of them with the bulk prefetch)
+  int* status;           // set to 1 when a bounded wait gives up
 };
 
 // ----------------------------------------------------------- device helpers
@@ -109,35 +112,6 @@ template <> __device__ void store_row<float>(const float* s, float* __restrict__
 }
 template <class T> __device__ void copy_global(const T* __restrict__ a, T* __restrict__ b, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
-}
-
-// Σ x and Σ i·x over the live samples, in float64 (core/sums.nim).
-template <class T> __device__ double sum_x(const T* X, int n, double* red) {
-  double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)X[i];
-  return block_sum(s, red);
-}
-template <class T> __device__ double sum_ix(const T* X, int n, double* red) {
-  double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)i * (double)X[i];
-  return block_sum(s, red);
-}
-template <class T> __device__ double sum_sq(const T* X, int n, double* red) {
-  double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double v = (double)X[i];
-    s += v * v;
-  }
-  return block_sum(s, red);
-}
-template <class T> __device__ double max_abs(const T* X, int n, unsigned long long* red) {
-  unsigned long long m = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    unsigned long long b = abs_bits(X[i]);
-    m = b > m ? b : m;
-  }
-  m = block_max_u64(m, red);
-  return bits_value(m, (T)0);
 }
 
 // The k-th smallest |x| (0-based) as its bits, by an 8-bit radix selection
@@ -190,59 +164,227 @@ __device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* his
 }
 
 // ------------------------------------------------------------------ steps
+// Statistics a step needs of its input, accumulated in the loop that wrote
+// that input (the load, or the previous step's output loop), so that no step
+// makes a pass of its own for them.
+enum { NEED_S1 = 1, NEED_SI = 2, NEED_S2 = 4, NEED_MX = 8 };
+
 struct Shared {
-  double red[32];
+  double red[4][32];
   unsigned long long redu[32];
+  double sv[32];
+  int sf[32];
+  double pv[32];
   unsigned hist[256];
   int sh[4];
+  double out[4];
 };
 
-// filter/edges.nim:16-30
-template <class T> __device__ void trend_of(int trend, const T* X, int n, double& a, double& b, Shared& S) {
+struct Stats {
+  double s1, si, s2, mx;
+};
+
+// Per-thread partial sums: Σx, Σi·x, Σx² in float64 and the largest |x| bits,
+// for the statistics NEED asks for (a compile-time set, so the loops carry
+// no per-sample branch on it).
+template <class T> struct Acc {
+  double s1 = 0, si = 0, s2 = 0;
+  unsigned long long mx = 0;
+  template <int NEED> __device__ __forceinline__ void add(T v, int i) {
+    if (NEED & (NEED_S1 | NEED_SI | NEED_S2)) {
+      double d = (double)v;
+      if (NEED & NEED_S1) s1 += d;
+      if (NEED & NEED_SI) si += (double)i * d;
+      if (NEED & NEED_S2) s2 += d * d;
+    }
+    if (NEED & NEED_MX) {
+      unsigned long long b = abs_bits(v);
+      mx = b > mx ? b : mx;
+    }
+  }
+};
+
+// Calls f with the statistics set `need` as a compile-time constant.
+template <int K> struct NeedC { static constexpr int value = K; };
+template <class F> __device__ __forceinline__ auto with_need(int need, F&& f) {
+  switch (need) {
+    case 0: return f(NeedC<0>());
+    case NEED_S1: return f(NeedC<NEED_S1>());
+    case NEED_S1 | NEED_SI: return f(NeedC<NEED_S1 | NEED_SI>());
+    case NEED_S2: return f(NeedC<NEED_S2>());
+    case NEED_MX: return f(NeedC<NEED_MX>());
+    default: return f(NeedC<NEED_S1 | NEED_SI | NEED_S2 | NEED_MX>());
+  }
+}
+
+// Folds the partial sums over the block. Always ends with a __syncthreads(),
+// so the loop's writes to the trace are visible to the next step.
+template <class T> __device__ __forceinline__ Stats reduce_stats(const Acc<T>& a, int need, Shared& S) {
+  Stats r{0, 0, 0, 0};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (need == 0) {
+    __syncthreads();
+    return r;
+  }
+  double v0 = a.s1, v1 = a.si, v2 = a.s2;
+  unsigned long long m = a.mx;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    if (need & NEED_S1) v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+    if (need & NEED_SI) v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    if (need & NEED_S2) v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+    if (need & NEED_MX) {
+      unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
+      m = u > m ? u : m;
+    }
+  }
+  if (lane == 0) {
+    S.red[0][warp] = v0;
+    S.red[1][warp] = v1;
+    S.red[2][warp] = v2;
+    S.redu[warp] = m;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    v0 = lane < nw ? S.red[0][lane] : 0.0;
+    v1 = lane < nw ? S.red[1][lane] : 0.0;
+    v2 = lane < nw ? S.red[2][lane] : 0.0;
+    m = lane < nw ? S.redu[lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+      v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+      v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+      unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
+      m = u > m ? u : m;
+    }
+    if (lane == 0) {
+      S.out[0] = v0;
+      S.out[1] = v1;
+      S.out[2] = v2;
+      S.out[3] = bits_value(m, (T)0);
+    }
+  }
+  __syncthreads();
+  r.s1 = S.out[0];
+  r.si = S.out[1];
+  r.s2 = S.out[2];
+  r.mx = S.out[3];
+  return r;
+}
+
+// The elementwise loop of a step: X[i] = op(X[i], i) over the live samples,
+// accumulating what the next step needs.
+template <class T, class Op>
+__device__ __forceinline__ Stats map_trace(T* X, int n, int need, Shared& S, Op op) {
+  return with_need(need, [&](auto K) {
+    constexpr int NEED = decltype(K)::value;
+    Acc<T> acc;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const T o = op(X[i], i);
+      X[i] = o;
+      acc.template add<NEED>(o, i);
+    }
+    return reduce_stats(acc, NEED, S);
+  });
+}
+
+// A pass over the unchanged trace when a step left it as it was.
+template <class T> __device__ __forceinline__ Stats stats_pass(const T* X, int n, int need, Shared& S) {
+  return with_need(need, [&](auto K) {
+    constexpr int NEED = decltype(K)::value;
+    Acc<T> acc;
+    if (NEED)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) acc.template add<NEED>(X[i], i);
+    return reduce_stats(acc, NEED, S);
+  });
+}
+
+// Loads the live samples into shared memory (16-byte vectors where the row
+// allows), scaled by a panel factor when there is one, accumulating what the
+// first step needs.
+template <class T>
+__device__ __forceinline__ Stats load_trace(const T* __restrict__ g, T* s, int n, bool scale, T k, int need,
+                                            Shared& S) {
+  return with_need(need, [&](auto K) {
+    constexpr int NEED = decltype(K)::value;
+    Acc<T> acc;
+    int head = 0, nv = 0;
+    if (sizeof(T) == 4) {
+      head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
+      if (head > n) head = n;
+      nv = (n - head) >> 2;
+      const float4* gv = reinterpret_cast<const float4*>(g + head);
+      for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        float4 q = __ldcs(gv + v);
+        const int i = head + 4 * v;
+        T e[4] = {(T)q.x, (T)q.y, (T)q.z, (T)q.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const T y = scale ? e[u] * k : e[u];
+          s[i + u] = y;
+          acc.template add<NEED>(y, i + u);
+        }
+      }
+    }
+    // the unaligned head and the tail
+    const int tail0 = head + 4 * nv;
+    const int rest = head + (n - tail0);
+    for (int t = threadIdx.x; t < rest; t += blockDim.x) {
+      const int i = t < head ? t : tail0 + (t - head);
+      const T y = scale ? g[i] * k : g[i];
+      s[i] = y;
+      acc.template add<NEED>(y, i);
+    }
+    return reduce_stats(acc, NEED, S);
+  });
+}
+
+// filter/edges.nim:16-30, from the sums of the step's input.
+__device__ __forceinline__ void trend_from(int trend, const Stats& st, int n, double& a, double& b) {
   a = 0;
   b = 0;
   if (trend == PSG_TR_NONE) return;
-  double sx = sum_x(X, n, S.red);
-  double nf = (double)n, mean = sx / nf;
+  double nf = (double)n, mean = st.s1 / nf;
   if (trend == PSG_TR_MEAN || n == 1) {
     a = mean;
     return;
   }
-  double six = sum_ix(X, n, S.red);
   double c = (nf - 1) / 2;
-  double slope = (six - c * sx) / (nf * (nf * nf - 1) / 12);
+  double slope = (st.si - c * st.s1) / (nf * (nf * nf - 1) / 12);
   a = mean - slope * c;
   b = slope;
 }
 
 // The zero-phase FFT filter with the reference's edge handling
 // (filter/apply.nim:194-231, 340-363) on the trace in shared memory.
-template <class T>
-__device__ void step_filter(const DevStep& st, T* X, int n, unsigned char* work, Shared& S) {
+template <class T, int MAXR>
+__device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
   typedef typename C2<T>::type V;
   const int p = st.pad, nfft = st.nfft, m = nfft / 2;
-  V* A = reinterpret_cast<V*>(work);
-  V* B = A + m;
+  const InShared mem;
+  const int ao = work_off / (int)sizeof(V), bo = ao + m;  // offsets of the two buffers
+  V* A = reinterpret_cast<V*>(psg_dyn_smem) + ao;
   double a, b;
-  trend_of(st.trend, X, n, a, b, S);
+  trend_from(st.trend, in, n, a, b);
   const T* fall = reinterpret_cast<const T*>(st.fall);
   T* Ar = reinterpret_cast<T*>(A);
   // packInto: the detrended samples at p .. p+n, odd reflections tapered by
   // `fall` (or zeros) in the pads, zeros to nfft.
   for (int j = threadIdx.x; j < nfft; j += blockDim.x) {
     T v = (T)0;
-    if (j >= p && j < p + n) {
-      int i = j - p;
+    const int i = j - p;
+    if (i >= 0 && i < n) {
       v = (T)((double)X[i] - (a + b * (double)i));
-    } else if (st.reflect && j < p) {
-      int k = p - j, i = min(k, n - 1);
+    } else if (st.reflect && i < 0) {
+      int k = -i, ii = min(k, n - 1);
       T d0 = (T)((double)X[0] - a);
-      T r = (T)((double)X[i] - (a + b * (double)i));
+      T r = (T)((double)X[ii] - (a + b * (double)ii));
       v = (d0 + d0 - r) * __ldg(&fall[k - 1]);
-    } else if (st.reflect && j >= p + n && j < 2 * p + n) {
-      int k = j - (p + n - 1), i = n - 1 - min(k, n - 1);
+    } else if (st.reflect && i >= n && i < n + p) {
+      int k = i - (n - 1), ii = n - 1 - min(k, n - 1);
       T dn = (T)((double)X[n - 1] - (a + b * (double)(n - 1)));
-      T r = (T)((double)X[i] - (a + b * (double)i));
+      T r = (T)((double)X[ii] - (a + b * (double)ii));
       v = (dn + dn - r) * __ldg(&fall[k - 1]);
     }
     Ar[j] = v;
@@ -251,80 +393,166 @@ __device__ void step_filter(const DevStep& st, T* X, int n, unsigned char* work,
   const V* tw = reinterpret_cast<const V*>(st.tw);
   const V* split = reinterpret_cast<const V*>(st.split);
   const T* gain = reinterpret_cast<const T*>(st.gain);
-  V* z = cfft_forward<T>(A, B, st.fft, tw);
-  split_mul_unsplit<T>(z, m, split, (T)1 / (T)nfft, [&](V x, int k) {
+  const int zo = cfft_forward<T, MAXR>(mem, ao, bo, st.fft, tw);
+  split_mul_unsplit<T>(mem, zo, m, split, (T)1 / (T)nfft, [&](V x, int k) {
     T g = __ldg(&gain[k]);
     return V{x.x * g, x.y * g};
   });
-  V* y = cfft_forward<T>(z, z == A ? B : A, st.fft, tw);
+  const int yo = cfft_forward<T, MAXR>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
+  const V* y = reinterpret_cast<const V*>(psg_dyn_smem) + yo;
   // unpackFrom: the output is swap(y); sample 2k is y[k].im, 2k+1 is y[k].re.
-  double gb = b * st.dc_gain;
-  double ga = st.zero_dc ? -gb * (double)(n - 1) / 2 : a * st.dc_gain;
-  bool plain = ga == 0 && gb == 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int idx = p + i;
-    V c = y[idx >> 1];
-    T v = (idx & 1) ? c.x : c.y;
-    X[i] = plain ? v : (T)((double)v + (ga + gb * (double)i));
-  }
-  __syncthreads();
+  const double gb = b * st.dc_gain;
+  const double ga = st.zero_dc ? -gb * (double)(n - 1) / 2 : a * st.dc_gain;
+  const bool plain = ga == 0 && gb == 0;
+  return map_trace(X, n, st.need_next, S, [&](T, int i) {
+    const int idx = p + i;
+    const V c = y[idx >> 1];
+    const T v = (idx & 1) ? c.x : c.y;
+    return plain ? v : (T)((double)v + (ga + gb * (double)i));
+  });
 }
 
-// AGC (gain/gain.nim:351-461): per block of w = 2h + 1 samples, prefix and
-// suffix sums of the terms in float64 (a warp per block, no subtraction),
-// stored as T; then the gain step in T on means scaled by the trace RMS.
-template <class T>
-__device__ void step_agc(const DevStep& st, T* X, int n, unsigned char* work, Shared& S) {
-  const bool rms_mode = st.agc_mode == PSG_AGC_RMS;
-  double ss = sum_sq(X, n, S.red);
-  double rms = sqrt(ss / (double)n);
-  if (rms == 0) return;
-  if (!fits_d<T>(st.target / rms / st.epsilon)) return;  // also a NaN or Inf row
-  const int h = st.half, w = 2 * h + 1;
-  T* P = reinterpret_cast<T*>(work);          // n + 1 values
-  T* Sx = P + ((n + 1 + 3) & ~3);             // n values
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int nb = (n + w - 1) / w;
-  for (int blk = warp; blk < nb; blk += nwarps) {
-    const int bs = blk * w, be = min(bs + w, n), L = be - bs;
-    double carry = 0;
-    if (lane == 0) P[bs] = (T)0;
-    for (int c = 0; c < L; c += 32) {
-      int idx = c + lane;
-      double t = 0;
-      if (idx < L) {
-        double v = (double)X[bs + idx];
-        t = rms_mode ? v * v : fabs(v);
-      }
+// An exclusive scan over the threads, in thread order (or reversed), of
+// segment sums that restart where a segment starts a new AGC block: the
+// running sum carried into each thread's segment.
+template <bool REV> __device__ double carry_scan(double v, bool f, Shared& S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  int ff = f ? 1 : 0;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        double u = __shfl_up_sync(0xffffffffu, t, o);
-        if (lane >= o) t += u;
-      }
-      // p[e] for e = bs+idx+1 inside the block; the block end is the next
-      // block's start (0) unless it is the trace end.
-      int e = bs + idx + 1;
-      if (idx < L && (e < be || (be == n && (n % w) != 0))) P[e] = (T)(carry + t);
-      carry += __shfl_sync(0xffffffffu, t, 31);
-    }
-    carry = 0;
-    for (int c = 0; c < L; c += 32) {
-      int idx = c + lane;
-      double t = 0;
-      if (idx < L) {
-        double v = (double)X[be - 1 - idx];
-        t = rms_mode ? v * v : fabs(v);
-      }
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        double u = __shfl_up_sync(0xffffffffu, t, o);
-        if (lane >= o) t += u;
-      }
-      if (idx < L) Sx[be - 1 - idx] = (T)(carry + t);
-      carry += __shfl_sync(0xffffffffu, t, 31);
+  for (int o = 1; o < 32; o <<= 1) {
+    double vv = REV ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
+    int fo = REV ? __shfl_down_sync(0xffffffffu, ff, o) : __shfl_up_sync(0xffffffffu, ff, o);
+    bool in = REV ? lane + o < 32 : lane >= o;
+    if (in) {
+      if (!ff) v += vv;
+      ff |= fo;
     }
   }
-  if (threadIdx.x == 0 && n % w == 0) P[n] = (T)0;
+  // warp totals: the last lane in scan order holds its warp's inclusive value
+  if (lane == (REV ? 0 : 31)) {
+    S.sv[warp] = v;
+    S.sf[warp] = ff;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // exclusive scan of the warp totals in scan order
+    int wi = REV ? nw - 1 - lane : lane;  // position of this lane's warp in scan order
+    double wv = (lane < nw) ? S.sv[REV ? (nw - 1 - lane) : lane] : 0.0;
+    int wf = (lane < nw) ? S.sf[REV ? (nw - 1 - lane) : lane] : 0;
+    (void)wi;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      double vv = __shfl_up_sync(0xffffffffu, wv, o);
+      int fo = __shfl_up_sync(0xffffffffu, wf, o);
+      if (lane >= o) {
+        if (!wf) wv += vv;
+        wf |= fo;
+      }
+    }
+    double ex = __shfl_up_sync(0xffffffffu, wv, 1);
+    if (lane == 0) ex = 0.0;
+    if (lane < nw) S.pv[REV ? (nw - 1 - lane) : lane] = ex;
+  }
+  __syncthreads();
+  const double cw = S.pv[warp];
+  const double incl = ff ? v : v + cw;
+  double prev = REV ? __shfl_down_sync(0xffffffffu, incl, 1) : __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane == (REV ? 31 : 0)) prev = cw;
+  return prev;
+}
+
+// AGC (gain/gain.nim:351-461). Window sums come from per-block prefix and
+// suffix sums of the terms in float64 (blocks of w = 2h + 1 samples, no
+// subtraction): each thread runs them over a contiguous segment of the trace
+// and a segmented scan across the threads carries the sums between
+// segments. The prefix and suffix arrays are stored as T; the gain step runs
+// in T on means scaled by the trace RMS.
+template <class T>
+__device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
+  const int need = st.need_next;
+  const bool rms_mode = st.agc_mode == PSG_AGC_RMS;
+  const double rms = sqrt(in.s2 / (double)n);
+  if (rms == 0 || !fits_d<T>(st.target / rms / st.epsilon)) return stats_pass(X, n, need, S);
+  const int h = st.half, w = 2 * h + 1;
+  T* P = reinterpret_cast<T*>(psg_dyn_smem + work_off);  // n + 1 values
+  T* Sx = P + ((n + 1 + 3) & ~3);          // n values
+  // An odd segment length keeps the strided reads free of bank conflicts.
+  int seg = (n + blockDim.x - 1) / blockDim.x;
+  seg |= 1;
+  const int g0 = min((int)threadIdx.x * seg, n), g1 = min(g0 + seg, n);
+  auto term = [&](int g) {
+    const double v = (double)X[g];
+    return rms_mode ? v * v : fabs(v);
+  };
+  // The first block start at or after g0, and the last block end (a sample
+  // whose successor starts a block) at or before g1 − 1.
+  const int firstStart = g0 + (g0 % w == 0 ? 0 : w - g0 % w);
+  const int lastEnd = g1 - 1 - ((g1 % w) == 0 ? 0 : (g1 % w));  // (lastEnd + 1) % w == 0
+  // Local sums: the prefix chain restarts at block starts, the suffix chain
+  // (run backwards) at block ends; between those the loops have no branch.
+  double rp = 0, rs = 0;
+  bool fp = false, fs = false;
+  {
+    int g = g0;
+    int next = firstStart;
+    while (g < g1) {
+      if (g == next) {
+        rp = 0;
+        fp = true;
+        next += w;
+      }
+      const int stop = min(g1, next);
+      for (; g < stop; g++) rp += term(g);
+    }
+    g = g1 - 1;
+    int end = lastEnd;
+    while (g >= g0) {
+      if (g == end) {
+        rs = 0;
+        fs = true;
+        end -= w;
+      }
+      const int stop = max(g0 - 1, end);
+      for (; g > stop; g--) rs += term(g);
+    }
+  }
+  const double cp = carry_scan<false>(g0 < g1 ? rp : 0.0, fp, S);
+  const double cs = carry_scan<true>(g0 < g1 ? rs : 0.0, fs, S);
+  {
+    // p[e]: the sum from the block start to e − 1, 0 at a block start;
+    // p[n] is the last block's sum unless n starts a block.
+    double run = cp;
+    int g = g0;
+    int next = firstStart;
+    while (g < g1) {
+      if (g == next) {
+        run = 0;
+        P[g] = (T)0;
+        next += w;
+      }
+      const int stop = min(g1, next);
+      for (; g < stop; g++) {
+        run += term(g);
+        if (g + 1 != next) P[g + 1] = (T)run;
+      }
+    }
+    if (g1 == n && g0 < g1 && n % w == 0) P[n] = (T)0;
+    // s[i]: the sum from i to its block's end (or n − 1)
+    run = cs;
+    g = g1 - 1;
+    int end = lastEnd;
+    while (g >= g0) {
+      if (g == end) {
+        run = 0;
+        end -= w;
+      }
+      const int stop = max(g0 - 1, end);
+      for (; g > stop; g--) {
+        run += term(g);
+        Sx[g] = (T)run;
+      }
+    }
+  }
   __syncthreads();
   const double unit = rms_mode ? 1 / (rms * rms) : 1 / rms;
   const T k = (T)(st.target / rms), eps = (T)st.epsilon;
@@ -332,52 +560,56 @@ __device__ void step_agc(const DevStep& st, T* X, int n, unsigned char* work, Sh
   const int headCut = min(max(n - h, 0), first);
   const int lastBlock = (n - 1) / w * w;
   const int tailCut = min(max(lastBlock + h, last), n);
-  const double pn = (double)P[n];
-  const double unitW = unit / (double)w;
-  const double headWhole = headCut < first ? pn * unit * (1 / (double)n) : 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double mean;
-    if (i < headCut) mean = (double)P[i + h + 1] * (unit * (1 / (double)(i + h + 1)));
+  const T pn = P[n];
+  const T unitW = (T)(unit / (double)w);
+  const T headWhole = headCut < first ? (T)((double)pn * unit * (1 / (double)n)) : (T)0;
+  return map_trace(X, n, need, S, [&](T x, int i) {
+    T mean;
+    if (i >= first && i < last) mean = (Sx[i - h] + P[i + h + 1]) * unitW;
+    else if (i < headCut) mean = (T)((double)P[i + h + 1] * (unit * (1 / (double)(i + h + 1))));
     else if (i < first) mean = headWhole;
-    else if (i < last) mean = ((double)Sx[i - h] + (double)P[i + h + 1]) * unitW;
-    else if (i < tailCut) mean = ((double)Sx[i - h] + pn) * (unit * (1 / (double)(w - (i + h + 1 - n))));
-    else mean = (double)Sx[i - h] * (unit * (1 / (double)(w - (i + h + 1 - n))));
-    T lv = rms_mode ? sqrt((T)mean) : (T)mean;
-    T gi = k / (lv + eps);
-    X[i] = (T)(X[i] * gi);
-  }
-  __syncthreads();
+    else if (i < tailCut) mean = (T)(((double)Sx[i - h] + (double)pn) * (unit * (1 / (double)(w - (i + h + 1 - n)))));
+    else mean = (T)((double)Sx[i - h] * (unit * (1 / (double)(w - (i + h + 1 - n)))));
+    T lv;
+    if (rms_mode) {
+      if (sizeof(T) == 4) lv = mean > (T)0 ? (T)(mean * rsqrtf((float)mean)) : (T)0;
+      else lv = sqrt(mean);
+    } else {
+      lv = mean;
+    }
+    T gi;
+    if (sizeof(T) == 4) gi = (T)__fdividef((float)k, (float)(lv + eps));
+    else gi = k / (lv + eps);
+    return (T)(x * gi);
+  });
 }
 
 // Per-trace normalization (gain/gain.nim:198-219; stats.nim:129-182).
-template <class T> __device__ void step_norm_trace(const DevStep& st, T* X, int n, Shared& S) {
+template <class T>
+__device__ __forceinline__ Stats step_norm_trace(const DevStep& st, const Stats& in, T* X, int n, Shared& S) {
+  const int need = st.need_next;
   double level;
   if (st.stat == PSG_NORM_MAX) {
-    level = max_abs(X, n, S.redu);
+    level = in.mx;
   } else if (st.stat == PSG_NORM_RMS) {
-    level = sqrt(sum_sq(X, n, S.red) / (double)n);
+    level = sqrt(in.s2 / (double)n);
+  } else if (isnan(in.mx)) {
+    level = in.mx;
   } else {
-    double mx = max_abs(X, n, S.redu);
-    if (isnan(mx)) {
-      level = mx;
+    double hr = (double)(n - 1) * st.percentile / 100;
+    int k = min((int)floor(hr), n - 1);
+    double lower = bits_value(select_kth(X, n, k, S.hist, S.sh), (T)0);
+    if (k + 1 >= n) {
+      level = lower;
     } else {
-      double hr = (double)(n - 1) * st.percentile / 100;
-      int k = min((int)floor(hr), n - 1);
-      double lower = bits_value(select_kth(X, n, k, S.hist, S.sh), (T)0);
-      if (k + 1 >= n) {
-        level = lower;
-      } else {
-        double upper = bits_value(select_kth(X, n, k + 1, S.hist, S.sh), (T)0);
-        double f = hr - (double)k;
-        level = f == 0 ? lower : lower + f * (upper - lower);
-      }
+      double upper = bits_value(select_kth(X, n, k + 1, S.hist, S.sh), (T)0);
+      double f = hr - (double)k;
+      level = f == 0 ? lower : lower + f * (upper - lower);
     }
   }
-  if (fin_pos_d(level) && fits_d<T>(st.norm_target / level)) {
-    T kf = (T)(st.norm_target / level);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * kf;
-  }
-  __syncthreads();
+  if (!(fin_pos_d(level) && fits_d<T>(st.norm_target / level))) return stats_pass(X, n, need, S);
+  const T kf = (T)(st.norm_target / level);
+  return map_trace(X, n, need, S, [&](T x, int) { return x * kf; });
 }
 
 // gain/curves.nim:132-160 on the device, in float64.
@@ -407,8 +639,10 @@ __device__ double factor_at_d(const psg_gain_curve& c, double t) {
 // The gain curve on one row (gain/curves.nim:316-350 and the workspace form
 // :383-418): the table where the row's times fall on it (as it is on the
 // grid, linearly interpolated off it), the curve itself elsewhere.
-template <class T> __device__ void step_gain_curve(const DevStep& st, T* X, int n, double start) {
-  if (isnan(start)) return;
+template <class T>
+__device__ __forceinline__ Stats step_gain_curve(const DevStep& st, T* X, int n, double start, Shared& S) {
+  const int need = st.need_next;
+  if (isnan(start)) return stats_pass(X, n, need, S);
   const T* tab = reinterpret_cast<const T*>(st.table);
   double u = (start - st.t_min_ms) / st.dt_ms;
   long long s = 0, j0 = n, j1 = n;
@@ -424,91 +658,157 @@ template <class T> __device__ void step_gain_curve(const DevStep& st, T* X, int 
     j1 = min(max(last - s + 1, j0), (long long)n);
   }
   const T tf = (T)f;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    T v = X[j];
+  return map_trace(X, n, need, S, [&](T v, int j) {
     if (j >= j0 && j < j1) {
       T a = __ldg(&tab[s + j]);
-      X[j] = on ? v * a : v * (a + tf * (__ldg(&tab[s + j + 1]) - a));
-    } else if (v != (T)0) {
-      X[j] = v * (T)factor_at_d(st.curve, start + (double)j * st.dt_ms);
+      return on ? v * a : v * (a + tf * (__ldg(&tab[s + j + 1]) - a));
     }
-  }
-  __syncthreads();
+    if (v != (T)0) return v * (T)factor_at_d(st.curve, start + (double)j * st.dt_ms);
+    return v;
+  });
 }
 
 // ------------------------------------------------------------ the kernel
-template <class T>
-__global__ void __launch_bounds__(256) pipeline_kernel(PipeArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// Stores a row from shared memory, 16-byte vectors where the row allows.
+template <class T> __device__ __forceinline__ void store_out(const T* s, T* __restrict__ g, int n) {
+  if (sizeof(T) == 4) {
+    const int head = min((int)((4 - (((uintptr_t)g >> 2) & 3)) & 3), n);
+    const int nv = (n - head) >> 2;
+    for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
+    float4* gv = reinterpret_cast<float4*>(g + head);
+    const float* sf = reinterpret_cast<const float*>(s) + head;
+    for (int v = threadIdx.x; v < nv; v += blockDim.x)
+      __stcs(gv + v, make_float4(sf[4 * v], sf[4 * v + 1], sf[4 * v + 2], sf[4 * v + 3]));
+    for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+  }
+}
+
+struct RowSlot {
+  int head, body, len, off;  // ragged head (elements), bulk bytes, elements, byte offset of X in the buffer
+};
+
+// PF: prefetch the next row into the second buffer while this one is
+// processed (when the second buffer costs no occupancy); otherwise one buffer,
+// loaded at the top of each row.
+template <class T, int MAXR, bool PF>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
   __shared__ Shared S;
-  T* X = reinterpret_cast<T*>(smem);
-  unsigned char* work = smem + a.work_off;
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ RowSlot slot[2];
   const T* src = reinterpret_cast<const T*>(a.src);
   T* dst = reinterpret_cast<T*>(a.dst);
   const bool copy = src != nullptr && src != dst;
-  for (long long r = blockIdx.x; r < a.rows; r += gridDim.x) {
-    int n = a.live[r];
-    n = n < 0 ? 0 : (n > a.cols ? a.cols : n);
-    const T* srow = (copy ? src : dst) + r * (long long)a.cols;
-    T* drow = dst + r * (long long)a.cols;
-    if (copy && n < a.cols) copy_global(srow + n, drow + n, a.cols - n);
-    if (n == 0) continue;
-    load_row(srow, X, n);
-    __syncthreads();
-    if (a.factor) {
-      double f = *a.factor;
-      if (!isnan(f)) {
-        T k = (T)f;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * k;
-        __syncthreads();
+  const T* from = copy ? src : dst;
+  const double pf = a.factor ? *a.factor : (double)NAN;
+  const bool scale = !isnan(pf);
+  const T kf = scale ? (T)pf : (T)1;
+  const int need0 = a.first < a.last ? a.steps[a.first].need : 0;
+  constexpr int esz = (int)sizeof(T);
+  // Thread 0 starts the bulk copy of a row into buffer b: the 16-byte aligned
+  // body of the part we need (the whole row for src → dst, the live samples
+  // in place); the few ragged elements at either end are read directly.
+  auto issue = [&](long long row, int b) {
+    int n = min(max(a.live[row], 0), a.cols);
+    int len = copy ? a.cols : n;
+    const T* g = from + row * (long long)a.cols;
+    uintptr_t ga = (uintptr_t)g;
+    int head = (int)(((16 - (ga & 15)) & 15) / esz);
+    head = min(head, len);
+    int body = ((len - head) * esz) & ~15;
+    int off = (16 - (head * esz) % 16) % 16;
+    unsigned char* xb = psg_dyn_smem + b * a.x_bytes;
+    slot[b] = RowSlot{head, body, len, off};
+    if (body > 0) {
+      mbar_arrive_expect_tx(&bars[b], (uint32_t)body);
+      bulk_load(xb + off + head * esz, g + head, (uint32_t)body, &bars[b]);
+    } else {
+      mbar_arrive(&bars[b]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init_fence();
+    if (PF && blockIdx.x < a.rows) issue(blockIdx.x, 0);
+  }
+  __syncthreads();
+  uint32_t phase[2] = {0, 0};
+  int cur = 0;
+  for (long long r = blockIdx.x; r < a.rows; r += gridDim.x, cur = PF ? cur ^ 1 : 0) {
+    const long long rn = r + gridDim.x;
+    if (threadIdx.x == 0) {
+      // the buffer's last reads (the previous row's store) come before the copy into it
+      if (PF && rn < a.rows) {
+        fence_proxy_async();
+        issue(rn, cur ^ 1);
+      } else if (!PF) {
+        fence_proxy_async();
+        issue(r, 0);
       }
     }
-    for (int si = a.first; si < a.last; si++) {
-      const DevStep& st = a.steps[si];
-      switch (st.kind) {
+    if (!mbar_wait(&bars[cur], phase[cur], 1ll << 26)) {
+      if (threadIdx.x == 0) atomicExch(a.status, 1);
+      mbar_wait(&bars[cur], phase[cur], 1ll << 26);
+      return;
+    }
+    phase[cur] ^= 1;
+    const RowSlot sl = slot[cur];
+    T* X = reinterpret_cast<T*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
+    const T* g = from + r * (long long)a.cols;
+    const int tail0 = sl.head + sl.body / esz;
+    for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = g[i];
+    for (int i = tail0 + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = g[i];
+    __syncthreads();  // the ragged ends are read by other threads below
+    int n = min(max(a.live[r], 0), a.cols);
+    Stats st{0, 0, 0, 0};
+    if (n > 0) {
+      // the panel factor of a part that starts with one, and the first
+      // step's statistics
+      if (scale) st = map_trace(X, n, need0, S, [&](T x, int) { return x * kf; });
+      else st = stats_pass(X, n, need0, S);
+    } else {
+      __syncthreads();
+    }
+    for (int si = a.first; n > 0 && si < a.last; si++) {
+      const DevStep& d = a.steps[si];
+      const int need = d.need_next;
+      switch (d.kind) {
         case ST_DEMEAN: {
-          double sx = sum_x(X, n, S.red);
-          T mean = (T)(sx / (double)n);
-          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] - mean;
-          __syncthreads();
+          const T mean = (T)(st.s1 / (double)n);
+          st = map_trace(X, n, need, S, [&](T x, int) { return x - mean; });
           break;
         }
         case ST_DETREND: {
-          double nf = (double)n, c = (nf - 1) / 2, sx = sum_x(X, n, S.red), mean = sx / nf;
+          double nf = (double)n, c = (nf - 1) / 2, mean = st.s1 / nf;
           double stt = nf * (nf * nf - 1) / 12;
-          double slope = n > 1 ? (sum_ix(X, n, S.red) - c * sx) / stt : 0.0;
-          T ta = (T)(mean - slope * c), tb = (T)slope;
-          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] - (ta + tb * (T)i);
-          __syncthreads();
+          double slope = n > 1 ? (st.si - c * st.s1) / stt : 0.0;
+          const T ta = (T)(mean - slope * c), tb = (T)slope;
+          st = map_trace(X, n, need, S, [&](T x, int i) { return x - (ta + tb * (T)i); });
           break;
         }
         case ST_SCALE: {
-          T k = (T)st.factor;
-          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = X[i] * k;
-          __syncthreads();
+          const T k = (T)d.factor;
+          st = map_trace(X, n, need, S, [&](T x, int) { return x * k; });
           break;
         }
         case ST_CLIP: {
-          T lo = (T)st.lo, hi = (T)st.hi;
-          for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            T v = X[i];
-            X[i] = v > hi ? hi : (v < lo ? lo : v);
-          }
-          __syncthreads();
+          const T lo = (T)d.lo, hi = (T)d.hi;
+          st = map_trace(X, n, need, S, [&](T v, int) { return v > hi ? hi : (v < lo ? lo : v); });
           break;
         }
         case ST_POLARITY:
-          for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = -X[i];
-          __syncthreads();
+          st = map_trace(X, n, need, S, [&](T x, int) { return -x; });
           break;
-        case ST_FILTER: step_filter(st, X, n, work, S); break;
-        case ST_AGC: step_agc(st, X, n, work, S); break;
-        case ST_NORM_TRACE: step_norm_trace(st, X, n, S); break;
-        case ST_GAIN_CURVE: step_gain_curve(st, X, n, a.start_ms ? a.start_ms[r] : (double)NAN); break;
+        case ST_FILTER: st = step_filter<T, MAXR>(d, st, X, n, a.work_off, S); break;
+        case ST_AGC: st = step_agc(d, st, X, n, a.work_off, S); break;
+        case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
+        case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, a.start_ms ? a.start_ms[r] : (double)NAN, S); break;
         default: break;
       }
     }
-    store_row(X, drow, n);
+    if (copy || n > 0) store_out(X, dst + r * (long long)a.cols, copy ? a.cols : n);
     __syncthreads();
   }
 }
@@ -533,7 +833,7 @@ __global__ void __launch_bounds__(256) row_stats_kernel(const T* __restrict__ b,
       unsigned long long bb = abs_bits(x[i]);
       m = bb > m ? bb : m;
     }
-    s = block_sum(s, S.red);
+    s = block_sum(s, S.red[0]);
     m = block_max_u64(m, S.redu);
     if (threadIdx.x == 0) {
       ss[r] = s;
@@ -570,9 +870,9 @@ __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int co
     unsigned long long b = (unsigned long long)__double_as_longlong(mx[r]);
     mb = b > mb ? b : mb;
   }
-  sum = block_sum(sum, S.red);
-  cnt = block_sum(cnt, S.red);
-  nr = block_sum(nr, S.red);
+  sum = block_sum(sum, S.red[0]);
+  cnt = block_sum(cnt, S.red[0]);
+  nr = block_sum(nr, S.red[0]);
   mb = block_max_u64(mb, S.redu);
   if (threadIdx.x == 0) {
     out->rows = nr;
@@ -707,14 +1007,11 @@ struct CorrArgs {
 
 // correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
 // pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
-template <class T>
-__global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
+template <class T, class M>
+__device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Shared& S) {
   typedef typename C2<T>::type V;
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ Shared S;
   const int m = a.nfft / 2;
-  V* A = a.gwork ? reinterpret_cast<V*>(a.gwork) + (size_t)blockIdx.x * 2 * m : reinterpret_cast<V*>(smem);
-  V* B = A + m;
+  V* buf = reinterpret_cast<V*>(mem.base());
   const T* src = reinterpret_cast<const T*>(a.src);
   T* dst = reinterpret_cast<T*>(a.dst);
   const V* mul = reinterpret_cast<const V*>(a.mul);
@@ -725,18 +1022,19 @@ __global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
   const int last = min(max(a.record - a.shift, direct), a.out);
   for (long long r = blockIdx.x; r < a.rows; r += gridDim.x) {
     int n = min(max(a.live[r], 0), a.cols);
-    V* y = nullptr;
+    const V* y = nullptr;
     if (n > 0) {
       const T* x = src + r * (long long)a.cols;
-      T* Ar = reinterpret_cast<T*>(A);
+      T* Ar = reinterpret_cast<T*>(buf);
       for (int j = threadIdx.x; j < a.nfft; j += blockDim.x) Ar[j] = j < n ? x[j] : (T)0;
       __syncthreads();
-      V* z = cfft_forward<T>(A, B, a.fft, tw);
-      split_mul_unsplit<T>(z, m, split, (T)1 / (T)a.nfft, [&](V v, int k) {
+      constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
+      const int zo = cfft_forward<T, MAXR>(mem, 0, m, a.fft, tw);
+      split_mul_unsplit<T>(mem, zo, m, split, (T)1 / (T)a.nfft, [&](V v, int k) {
         V w = __ldg(&mul[k]);
         return V{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
       });
-      y = cfft_forward<T>(z, z == A ? B : A, a.fft, tw);
+      y = buf + cfft_forward<T, MAXR>(mem, zo, zo == 0 ? m : 0, a.fft, tw);
     }
     // lagSpans / scatter: the output at column c reads lag c + shift
     // (wrapped by nfft for negative lags).
@@ -759,7 +1057,7 @@ __global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
           double v = (double)value(c);
           bad += v - v;  // allFinite: x − x is 0 for finite x
         }
-        bad = block_sum(bad, S.red);
+        bad = block_sum(bad, S.red[0]);
         if (bad == 0) {
           double* nm = a.num + (long long)o * a.stack_samples;
           int* ct = a.cnt + (long long)o * a.stack_samples;
@@ -771,6 +1069,20 @@ __global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
       }
     }
     __syncthreads();
+  }
+}
+
+// correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
+// pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
+template <class T>
+__global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
+  __shared__ Shared S;
+  if (a.gwork) {
+    typedef typename C2<T>::type V;
+    InGlobal g{reinterpret_cast<unsigned char*>(a.gwork) + (size_t)blockIdx.x * a.nfft * sizeof(V)};
+    corr_rows<T>(a, g, S);
+  } else {
+    corr_rows<T>(a, InShared(), S);
   }
 }
 
@@ -790,7 +1102,7 @@ __global__ void __launch_bounds__(256) stack_add_kernel(const T* __restrict__ b,
       double v = (double)x[c];
       bad += v - v;
     }
-    bad = block_sum(bad, S.red);
+    bad = block_sum(bad, S.red[0]);
     if (bad == 0) {
       for (int c = threadIdx.x; c < n; c += blockDim.x) {
         num[(long long)o * samples + c] += (double)x[c];
@@ -889,7 +1201,9 @@ struct psg_plan {
   DevStep* d_steps = nullptr;
   int device = 0;
   int threads = 256;
-  int x_elems = 0, work_off = 0;
+  int max_radix = 12;  // the largest FFT radix compiled into the plan's kernel
+  int x_elems = 0, work_off = 0, x_bytes = 0;
+  bool prefetch = false;
   size_t smem = 0;
   int grid = 1;
   bool needs_panel = false;
@@ -899,6 +1213,11 @@ struct psg_workspace {
   int device = -1;
   void* d = nullptr;
   int64_t bytes = 0;
+  // Streams and events of the chunked host-memory apply (created on first use).
+  static const int kLanes = 4;
+  cudaStream_t lane[kLanes] = {};
+  cudaEvent_t start_ev = nullptr, done_ev[kLanes] = {};
+  bool lanes_ready = false;
 };
 
 struct psg_corr_plan {
@@ -959,6 +1278,12 @@ static int64_t ws_host_bytes(int64_t rows, int32_t cols, int dtype) {
          align256(rows * (int64_t)cols * (dtype == PSG_F32 ? 4 : 8));
 }
 
+// The pipeline kernel of a sample type and largest radix.
+template <class T> static void (*pipe_kernel_for(int max_radix, bool pf))(PipeArgs) {
+  if (sizeof(T) == 8 || max_radix <= 8) return pf ? pipeline_kernel<T, 8, true> : pipeline_kernel<T, 8, false>;
+  return pf ? pipeline_kernel<T, 12, true> : pipeline_kernel<T, 12, false>;
+}
+
 template <class T> static void build_device_steps(psg_plan* p) {
   typedef typename C2<T>::type V;
   std::vector<DevStep> ds;
@@ -1003,13 +1328,41 @@ template <class T> static void build_device_steps(psg_plan* p) {
       d.table = upload(p->keep, as_t<T>(s.table));
     }
     if (s.kind == ST_NORM_PANEL) p->needs_panel = true;
+    // what the step needs of its input (accumulated by the loop before it)
+    switch (s.kind) {
+      case ST_DEMEAN: d.need = NEED_S1; break;
+      case ST_DETREND: d.need = NEED_S1 | NEED_SI; break;
+      case ST_FILTER:
+        d.need = s.filter.trend == PSG_TR_LINEAR ? (NEED_S1 | NEED_SI) : (s.filter.trend == PSG_TR_MEAN ? NEED_S1 : 0);
+        break;
+      case ST_AGC: d.need = NEED_S2; break;
+      case ST_NORM_TRACE: d.need = s.stat == PSG_NORM_RMS ? NEED_S2 : NEED_MX; break;
+      default: d.need = 0;
+    }
     ds.push_back(d);
   }
+  for (size_t i = 0; i < ds.size(); i++)
+    ds[i].need_next = (i + 1 < ds.size() && ds[i + 1].kind != ST_NORM_PANEL) ? ds[i + 1].need : 0;
   // Each part's panel statistics live in a 64-byte slot of the workspace's
   // first 448 bytes.
   if (p->host.parts.size() > 6) throw InvalidArg("a plan takes at most 5 per-panel normalizations after its first op");
   p->x_elems = (int)((p->host.samples + 3) & ~3LL);
-  p->work_off = (int)align256(p->x_elems * (int64_t)sizeof(T));
+  // Row buffers with room for the 16-byte alignment of a row's body: two
+  // (the next row's bulk load lands in the other) when that keeps as many
+  // CTAs on an SM as one does, else one.
+  p->x_bytes = (int)align256((p->host.samples + 8) * (int64_t)sizeof(T));
+  auto occupancy = [&](bool pf) {
+    size_t sm = (size_t)((pf ? 2 : 1) * p->x_bytes + work);
+    auto k = pipe_kernel_for<T>(p->max_radix, pf);
+    allow_smem(k);
+    int per_sm = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, p->threads, sm));
+    return per_sm;
+  };
+  int one = occupancy(false), two = occupancy(true);
+  p->prefetch = two > 0 && two >= one;
+  if (const char* e = getenv("PSG_PREFETCH")) p->prefetch = atoi(e) != 0 && two > 0;
+  p->work_off = (p->prefetch ? 2 : 1) * p->x_bytes;
   p->smem = (size_t)(p->work_off + work);
   int limit = g_max_smem - (int)sizeof(Shared) - 1024;
   if ((int64_t)p->smem > limit)
@@ -1022,9 +1375,10 @@ template <class T> static void build_device_steps(psg_plan* p) {
     CUDA_OK(cudaMemcpy(b->p, ds.data(), ds.size() * sizeof(DevStep), cudaMemcpyHostToDevice));
     p->d_steps = (DevStep*)b->p;
   }
-  allow_smem(pipeline_kernel<T>);
+  auto kern = pipe_kernel_for<T>(p->max_radix, p->prefetch);
+  allow_smem(kern);
   int per_sm = 0;
-  CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipeline_kernel<T>, p->threads, p->smem));
+  CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p->threads, p->smem));
   p->grid = std::max(1, per_sm) * g_sm_count;
 }
 
@@ -1067,10 +1421,12 @@ static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const vo
   a.start_ms = start;
   a.factor = factor;
   a.steps = p->d_steps;
+  a.x_bytes = p->x_bytes;
+  a.status = reinterpret_cast<int*>((char*)ws->d + 504);
   bool nothing = a.first >= a.last && !factor && (src == nullptr || src == dst);
   if (nothing || rows == 0) return;
   int grid = (int)std::min<int64_t>(rows, p->grid);
-  pipeline_kernel<T><<<grid, p->threads, p->smem, stream>>>(a);
+  pipe_kernel_for<T>(p->max_radix, p->prefetch)<<<grid, p->threads, p->smem, stream>>>(a);
   CUDA_OK(cudaGetLastError());
 }
 
@@ -1145,7 +1501,9 @@ int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_
     if (!out) throw InvalidArg("null argument");
     *out = nullptr;
     std::unique_ptr<psg_plan> p(new psg_plan());
-    p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples);
+    p->max_radix = dtype == PSG_F32 ? 12 : 8;
+    if (const char* e = getenv("PSG_MAX_RADIX")) p->max_radix = std::min(p->max_radix, std::max(2, atoi(e)));
+    p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples, p->max_radix);
     ensure_device();
     CUDA_OK(cudaGetDevice(&p->device));
     if (dtype == PSG_F32) build_device_steps<float>(p.get());
@@ -1180,6 +1538,13 @@ int psg_workspace_create(psg_workspace** out) {
 }
 void psg_workspace_destroy(psg_workspace* ws) {
   if (!ws) return;
+  if (ws->lanes_ready) {
+    for (int i = 0; i < psg_workspace::kLanes; i++) {
+      cudaStreamDestroy(ws->lane[i]);
+      cudaEventDestroy(ws->done_ev[i]);
+    }
+    cudaEventDestroy(ws->start_ev);
+  }
   if (ws->d) cudaFree(ws->d);
   delete ws;
 }
@@ -1195,6 +1560,7 @@ static void ws_grow(psg_workspace* ws, int64_t need) {
     ws->bytes = 0;
   }
   CUDA_OK(cudaMalloc(&ws->d, (size_t)need));
+  CUDA_OK(cudaMemset(ws->d, 0, 512));  // panel slots and the kernels' status word
   ws->bytes = need;
   ws->device = dev;
 }
@@ -1250,7 +1616,7 @@ static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src
     throw InvalidArg("the block has " + std::to_string(cols) + " columns, the plan takes " + std::to_string(plan->host.samples) + " samples");
   if (need_ws) {
     if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
-    int64_t need = plan->needs_panel ? ws_device_bytes(rows) : 0;
+    int64_t need = plan->needs_panel ? ws_device_bytes(rows) : 512;
     if (ws->bytes < need) throw WorkspaceError("reserve the workspace for the plan first");
   }
 }
@@ -1270,6 +1636,12 @@ int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* ds
   });
 }
 
+// The host-memory apply. A plan without per-panel normalizations runs
+// chunk by chunk of rows on the workspace's streams, so that the copy in of
+// one chunk, the kernel of the one before and the copy out of the one before
+// that overlap (the device's two copy engines and its SMs). A plan with one
+// needs the whole block on the device before its factor: copy in, apply,
+// copy out.
 int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host, void* dst_host, int64_t rows,
                    int32_t cols, const int32_t* live_host, const double* start_ms_host, double dt_ms, void* stream) {
   return guarded([&] {
@@ -1283,19 +1655,57 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
     char* base = (char*)ws->d + ws_device_bytes(rows);
     int32_t* d_live = (int32_t*)base;
     double* d_start = (double*)(base + align256(rows * 4));
-    void* d_data = base + align256(rows * 4) + align256(rows * 8);
-    size_t bytes = (size_t)(rows * cols * esz);
-    const void* from = src_host ? src_host : dst_host;
-    CUDA_OK(cudaMemcpyAsync(d_data, from, bytes, cudaMemcpyHostToDevice, s));
-    CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, s));
-    if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, s));
-    for (int part = 0; part < (int)plan->host.parts.size(); part++) {
-      if (plan->host.dtype == PSG_F32)
-        launch_part<float>(plan, ws, part, nullptr, d_data, rows, cols, d_live, start_ms_host ? d_start : nullptr, s);
-      else
-        launch_part<double>(plan, ws, part, nullptr, d_data, rows, cols, d_live, start_ms_host ? d_start : nullptr, s);
+    char* d_data = base + align256(rows * 4) + align256(rows * 8);
+    const char* from = (const char*)(src_host ? src_host : dst_host);
+    const double* dstart = start_ms_host ? d_start : nullptr;
+    auto run_parts = [&](int64_t r0, int64_t nr, cudaStream_t st) {
+      void* blk = d_data + r0 * cols * esz;
+      for (int part = 0; part < (int)plan->host.parts.size(); part++) {
+        if (plan->host.dtype == PSG_F32)
+          launch_part<float>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st);
+        else
+          launch_part<double>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st);
+      }
+    };
+    const int64_t row_bytes = (int64_t)cols * esz;
+    const int64_t chunk = std::max<int64_t>(64, std::min<int64_t>(rows, (4 << 20) / std::max<int64_t>(1, row_bytes)));
+    if (plan->needs_panel || rows <= chunk) {
+      CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, s));
+      if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, s));
+      CUDA_OK(cudaMemcpyAsync(d_data, from, (size_t)(rows * row_bytes), cudaMemcpyHostToDevice, s));
+      run_parts(0, rows, s);
+      CUDA_OK(cudaMemcpyAsync(dst_host, d_data, (size_t)(rows * row_bytes), cudaMemcpyDeviceToHost, s));
+      CUDA_OK(cudaStreamSynchronize(s));
+      return;
     }
-    CUDA_OK(cudaMemcpyAsync(dst_host, d_data, bytes, cudaMemcpyDeviceToHost, s));
+    if (!ws->lanes_ready) {
+      for (int i = 0; i < psg_workspace::kLanes; i++) {
+        CUDA_OK(cudaStreamCreateWithFlags(&ws->lane[i], cudaStreamNonBlocking));
+        CUDA_OK(cudaEventCreateWithFlags(&ws->done_ev[i], cudaEventDisableTiming));
+      }
+      CUDA_OK(cudaEventCreateWithFlags(&ws->start_ev, cudaEventDisableTiming));
+      ws->lanes_ready = true;
+    }
+    // The chunk streams start after what the caller queued on its stream.
+    CUDA_OK(cudaEventRecord(ws->start_ev, s));
+    for (int i = 0; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamWaitEvent(ws->lane[i], ws->start_ev, 0));
+    CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, ws->lane[0]));
+    if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, ws->lane[0]));
+    CUDA_OK(cudaEventRecord(ws->done_ev[0], ws->lane[0]));
+    for (int i = 1; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamWaitEvent(ws->lane[i], ws->done_ev[0], 0));
+    int k = 0;
+    for (int64_t r0 = 0; r0 < rows; r0 += chunk, k++) {
+      int64_t nr = std::min(chunk, rows - r0);
+      cudaStream_t st = ws->lane[k % psg_workspace::kLanes];
+      size_t off = (size_t)(r0 * row_bytes), nb = (size_t)(nr * row_bytes);
+      CUDA_OK(cudaMemcpyAsync(d_data + off, from + off, nb, cudaMemcpyHostToDevice, st));
+      run_parts(r0, nr, st);
+      CUDA_OK(cudaMemcpyAsync((char*)dst_host + off, d_data + off, nb, cudaMemcpyDeviceToHost, st));
+    }
+    for (int i = 0; i < psg_workspace::kLanes; i++) {
+      CUDA_OK(cudaEventRecord(ws->done_ev[i], ws->lane[i]));
+      CUDA_OK(cudaStreamWaitEvent(s, ws->done_ev[i], 0));
+    }
     CUDA_OK(cudaStreamSynchronize(s));
   });
 }
@@ -1479,7 +1889,7 @@ int psg_corr_plan_create(const void* pilot, int32_t pilot_dtype, int64_t pilot_l
       pv[i] = pilot_dtype == PSG_F32 ? (double)((const float*)pilot)[i] : ((const double*)pilot)[i];
     std::unique_ptr<psg_corr_plan> p(new psg_corr_plan());
     p->host = corr_plan(pv.data(), pilot_len, pilot_dt_ms, pilot_t0_ms, dt_ms, record_samples, out_samples, mode,
-                        eps_percent, normalize != 0);
+                        eps_percent, normalize != 0, dtype == PSG_F32 ? 16 : 8);
     p->dtype = dtype;
     ensure_device();
     if (dtype == PSG_F32) corr_upload<float>(p.get());

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "psg_dft_consts.h"
+
 namespace psgd {
 
 template <class T> struct C2;
@@ -132,36 +134,106 @@ template <class V, class T> __device__ __forceinline__ void dft8(V* v) {
   v[7] = csub(e[3], o3);
 }
 
+// Multiplication by a compile-time constant twiddle (c, s); quarter turns
+// fold to swaps and negations.
+template <class V, class T> __device__ __forceinline__ V cmul_k(V a, double c, double s) {
+  if (c == 1.0 && s == 0.0) return a;
+  if (c == 0.0 && s == -1.0) return V{a.y, -a.x};
+  if (c == -1.0 && s == 0.0) return V{-a.x, -a.y};
+  if (c == 0.0 && s == 1.0) return V{-a.y, a.x};
+  const T tc = (T)c, ts = (T)s;
+  return V{a.x * tc - a.y * ts, a.x * ts + a.y * tc};
+}
+
+template <class V, class T, int R> struct Dft;
+template <class V, class T> struct Dft<V, T, 2> { static __device__ __forceinline__ void run(V* v) { dft2<V, T>(v); } };
+template <class V, class T> struct Dft<V, T, 3> { static __device__ __forceinline__ void run(V* v) { dft3<V, T>(v); } };
+template <class V, class T> struct Dft<V, T, 4> { static __device__ __forceinline__ void run(V* v) { dft4<V, T>(v); } };
+template <class V, class T> struct Dft<V, T, 5> { static __device__ __forceinline__ void run(V* v) { dft5<V, T>(v); } };
+template <class V, class T> struct Dft<V, T, 8> { static __device__ __forceinline__ void run(V* v) { dft8<V, T>(v); } };
+
+// A DFT of R = A·B points in registers: B DFTs of A points on the inputs
+// B apart, twiddles ω_R^{j2·k1}, then A DFTs of B points:
+//   X[k1 + A·k2] = Σ_j2 ω_B^{j2·k2} ω_R^{j2·k1} Σ_j1 x[B·j1 + j2] ω_A^{j1·k1}
+template <class V, class T, int A, int B> struct DftAB {
+  static __device__ __forceinline__ void run(V* v) {
+    constexpr int R = A * B;
+    V y[R];
+#pragma unroll
+    for (int j2 = 0; j2 < B; j2++) {
+      V u[A];
+#pragma unroll
+      for (int j1 = 0; j1 < A; j1++) u[j1] = v[B * j1 + j2];
+      Dft<V, T, A>::run(u);
+#pragma unroll
+      for (int k1 = 0; k1 < A; k1++) {
+        const int e = (j2 * k1) % R;
+        y[j2 * A + k1] = cmul_k<V, T>(u[k1], DftW<R>::c(e), DftW<R>::s(e));
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; k1++) {
+      V z[B];
+#pragma unroll
+      for (int j2 = 0; j2 < B; j2++) z[j2] = y[j2 * A + k1];
+      Dft<V, T, B>::run(z);
+#pragma unroll
+      for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = z[k2];
+    }
+  }
+};
+template <class V, class T> struct Dft<V, T, 6> : DftAB<V, T, 2, 3> {};
+template <class V, class T> struct Dft<V, T, 9> : DftAB<V, T, 3, 3> {};
+template <class V, class T> struct Dft<V, T, 10> : DftAB<V, T, 2, 5> {};
+template <class V, class T> struct Dft<V, T, 12> : DftAB<V, T, 4, 3> {};
+template <class V, class T> struct Dft<V, T, 15> : DftAB<V, T, 3, 5> {};
+template <class V, class T> struct Dft<V, T, 16> : DftAB<V, T, 4, 4> {};
+
+// The block's dynamic shared memory. The FFT buffers are addressed as
+// offsets from this symbol, so the compiler emits shared-memory loads and
+// stores with 32-bit addresses (a pointer chosen at run time between two
+// buffers would fall back to generic 64-bit addressing).
+extern __shared__ __align__(16) unsigned char psg_dyn_smem[];
+
+// Where an FFT's two work buffers live: the block's dynamic shared memory,
+// or (for transforms longer than it holds) a slice of global memory.
+struct InShared {
+  __device__ __forceinline__ unsigned char* base() const { return psg_dyn_smem; }
+};
+struct InGlobal {
+  unsigned char* b;
+  __device__ __forceinline__ unsigned char* base() const { return b; }
+};
+
 // One decimation-in-frequency Stockham pass of radix R over `s · sub`
 // butterflies (fft/plan.nim:187-190):
 //   y[q + s·(R·p + k)] = (Σ_j x[q + s·(p + j·sub)]·ω_R^{jk})·ω_cur^{pk}
-// with the pass's twiddles tw[p·(R − 1) + k − 1] = ω_cur^{pk}.
-template <int R, class T>
-__device__ __forceinline__ void fft_pass(const typename C2<T>::type* __restrict__ x,
-                                         typename C2<T>::type* __restrict__ y, int s, int sub,
+// with the pass's twiddles tw[p·(R − 1) + k − 1] = ω_cur^{pk}; x and y are
+// element offsets into the buffer memory.
+template <int R, class T, class M>
+__device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, int sub,
                                          const typename C2<T>::type* __restrict__ tw) {
   typedef typename C2<T>::type V;
+  V* buf = reinterpret_cast<V*>(mem.base());
   const int total = s * sub;
   const float inv_s = 1.0f / (float)s;
+  const int step = total;  // s · sub: the distance between a butterfly's inputs
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
     int p = (int)((float)b * inv_s);
     if (p * s > b) p--;
     else if ((p + 1) * s <= b) p++;
     const int q = b - p * s;
     V v[R];
+    const int xi = xo + q + s * p;
 #pragma unroll
-    for (int j = 0; j < R; j++) v[j] = x[q + s * (p + j * sub)];
-    if (R == 2) dft2<V, T>(v);
-    else if (R == 3) dft3<V, T>(v);
-    else if (R == 4) dft4<V, T>(v);
-    else if (R == 5) dft5<V, T>(v);
-    else dft8<V, T>(v);
+    for (int j = 0; j < R; j++) v[j] = buf[xi + j * step];
+    Dft<V, T, R>::run(v);
     const V* t = tw + p * (R - 1);
 #pragma unroll
     for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&t[k - 1]));
-    V* o = y + q + s * R * p;
+    const int yi = yo + q + s * R * p;
 #pragma unroll
-    for (int k = 0; k < R; k++) o[s * k] = v[k];
+    for (int k = 0; k < R; k++) buf[yi + s * k] = v[k];
   }
 }
 
@@ -173,30 +245,37 @@ struct FftDesc {
   int twoff[24];  // offset of each pass's twiddles
 };
 
-// Forward complex FFT of `a` (m points), `b` the second buffer. Returns the
-// buffer holding the result. Ends with a __syncthreads().
-template <class T>
-__device__ typename C2<T>::type* cfft_forward(typename C2<T>::type* a, typename C2<T>::type* b,
-                                              const FftDesc& d, const typename C2<T>::type* tw) {
+// Forward complex FFT of the m points at offset `ao`, `bo` the second
+// buffer. Returns the offset holding the result; ends with a
+// __syncthreads(). MAXR bounds the radices compiled in (and with them the
+// registers a pass needs); the plan's factorization never uses a larger one.
+template <class T, int MAXR, class M>
+__device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const FftDesc& d,
+                                            const typename C2<T>::type* tw) {
   typedef typename C2<T>::type V;
-  V* x = a;
-  V* y = b;
+  int x = ao, y = bo;
   int cur = d.m, s = 1;
   for (int i = 0; i < d.npass; i++) {
     const int r = d.radix[i];
     const int sub = cur / r;
     const V* t = tw + d.twoff[i];
     switch (r) {
-      case 8: fft_pass<8, T>(x, y, s, sub, t); break;
-      case 4: fft_pass<4, T>(x, y, s, sub, t); break;
-      case 2: fft_pass<2, T>(x, y, s, sub, t); break;
-      case 3: fft_pass<3, T>(x, y, s, sub, t); break;
-      default: fft_pass<5, T>(x, y, s, sub, t); break;
+      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T>(mem, x, y, s, sub, t); break;
+      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T>(mem, x, y, s, sub, t); break;
+      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T>(mem, x, y, s, sub, t); break;
+      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T>(mem, x, y, s, sub, t); break;
+      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T>(mem, x, y, s, sub, t); break;
+      case 8: fft_pass<8, T>(mem, x, y, s, sub, t); break;
+      case 6: fft_pass<6, T>(mem, x, y, s, sub, t); break;
+      case 5: fft_pass<5, T>(mem, x, y, s, sub, t); break;
+      case 4: fft_pass<4, T>(mem, x, y, s, sub, t); break;
+      case 3: fft_pass<3, T>(mem, x, y, s, sub, t); break;
+      default: fft_pass<2, T>(mem, x, y, s, sub, t); break;
     }
     __syncthreads();
     cur = sub;
     s *= r;
-    V* tmp = x;
+    const int tmp = x;
     x = y;
     y = tmp;
   }
@@ -209,10 +288,11 @@ __device__ typename C2<T>::type* cfft_forward(typename C2<T>::type* a, typename 
 // (k, m − k): split into the spectrum X[k], multiply by the bin's complex
 // factor (a real gain: im = 0), and un-split into swap(Z'), scaled by 1/n,
 // ready for the forward transform that inverts it.
-template <class T, class MulFn>
-__device__ void split_mul_unsplit(typename C2<T>::type* z, int m, const typename C2<T>::type* split,
-                                  T scale, MulFn mul) {
+template <class T, class M, class MulFn>
+__device__ __forceinline__ void split_mul_unsplit(const M& mem, int zo, int m, const typename C2<T>::type* split,
+                                                  T scale, MulFn mul) {
   typedef typename C2<T>::type V;
+  V* z = reinterpret_cast<V*>(mem.base()) + zo;
   const T half = (T)0.5;
   for (int k = threadIdx.x; k <= m / 2; k += blockDim.x) {
     if (k == 0) {
@@ -257,6 +337,56 @@ __device__ void split_mul_unsplit(typename C2<T>::type* z, int m, const typename
     if (j != k) z[j] = Zj;
   }
   __syncthreads();
+}
+
+// ------------------------------------------------- bulk copies (TMA, 1-D)
+// A row moves from global into shared memory with one cp.async.bulk issued
+// by one thread, completion tracked by an mbarrier carrying the byte count.
+// Both addresses and the size are multiples of 16 bytes. No multicast: the
+// destination is this CTA's own shared memory.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory
+// before later async-proxy (bulk copy) writes to it.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst_smem)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for a phase of `bar`, giving up after `limit` polls (each poll may
+// suspend the thread for a while in hardware). Returns false on give-up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
 }
 
 }  // namespace psgd

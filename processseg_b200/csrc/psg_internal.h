@@ -39,7 +39,7 @@ struct FftTables {
   std::vector<double> tw_re, tw_im;       // per pass: sub·(r − 1) values
   std::vector<double> split_re, split_im; // exp(−2πik/n), k = 0 .. m
 };
-FftTables fft_tables(int64_t n);
+FftTables fft_tables(int64_t n, int max_radix = 16);
 
 // --------------------------------------------------------------- filter plan
 struct FilterHost {
@@ -55,7 +55,7 @@ struct FilterHost {
 void validate_spec(const psg_filter_spec& s, double dt_ms);
 double spec_response(const psg_filter_spec& s, double f_hz, double dt_ms);
 int64_t spec_impulse_length(const psg_filter_spec& s, double dt_ms);
-FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend);
+FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend, int max_radix = 16);
 
 // ---------------------------------------------------------------- the plan
 enum StepKind {
@@ -91,7 +91,7 @@ struct PlanHost {
 };
 
 PlanHost compile_plan(const psg_op* ops, int n_ops, int dtype, double dt_ms, int64_t samples,
-                      int64_t record_samples);
+                      int64_t record_samples, int max_radix = 12);
 int64_t required_margin(const psg_op* ops, int n_ops, double dt_ms);
 double gain_factor_at(const psg_gain_curve& c, double t_ms);
 bool same_interval(double dt, double plan_dt);
@@ -105,7 +105,7 @@ struct CorrHost {
   FftTables fft;
 };
 CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
-                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize);
+                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize, int max_radix = 16);
 std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
                                  double t_end, int shape, double phase_deg, double amplitude,
                                  double max_nyq_fraction);

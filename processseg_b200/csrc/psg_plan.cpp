@@ -93,21 +93,78 @@ int64_t next_fast(int64_t n, bool even) {
 }
 
 // -------------------------------------------------------------- FFT tables
-// The device runs Stockham passes of radix 8, 4, 2, 3 and 5 (largest powers
-// of two first, so fewer passes than the reference's 4/2/3/5 order). The
-// twiddle of output k of butterfly p in a pass of `cur` points is
+// The device runs Stockham passes of radix 2, 3, 4, 5, 6, 8, 9, 10, 12, 15 or
+// 16 (the composite ones as small DFTs in registers). The factorization of m
+// minimizes a cost model of a pass on a CTA of `threads`: ceil(butterflies /
+// threads) rounds of R elements each, at the small DFT's arithmetic per
+// element plus the pass's shared-memory traffic and twiddle multiply.
+// The twiddle of output k of butterfly p in a pass of `cur` points is
 // exp(−2πi·(p·k mod cur)/cur), as fft/plan.nim:146-155 builds them.
-FftTables fft_tables(int64_t n) {
+namespace {
+double radix_cost(int r) {
+  switch (r) {
+    case 2: return 2.0;
+    case 3: return 5.3;
+    case 4: return 4.0;
+    case 5: return 6.8;
+    case 6: return 6.2;
+    case 8: return 6.0;
+    case 9: return 8.0;
+    case 10: return 7.4;
+    case 12: return 7.3;
+    case 15: return 8.6;
+    case 16: return 7.0;
+  }
+  return 1e9;
+}
+std::vector<int> plan_radices(int64_t m, int threads, int max_radix) {
+  static const int kRadix[] = {16, 15, 12, 10, 9, 8, 6, 5, 4, 3, 2};
+  // best[d] for every divisor d of m: the cheapest passes whose product is d
+  std::vector<int64_t> divs;
+  for (int64_t d = 1; d * d <= m; d++)
+    if (m % d == 0) {
+      divs.push_back(d);
+      if (d * d != m) divs.push_back(m / d);
+    }
+  std::sort(divs.begin(), divs.end());
+  std::vector<double> best(divs.size(), 1e300);
+  std::vector<int> choice(divs.size(), 0);
+  auto index = [&](int64_t d) { return (int)(std::lower_bound(divs.begin(), divs.end(), d) - divs.begin()); };
+  best[0] = 0;  // d = 1
+  for (size_t i = 1; i < divs.size(); i++) {
+    int64_t d = divs[i];
+    for (int r : kRadix) {
+      if (r > max_radix || d % r != 0) continue;
+      double bf = (double)(m / r);
+      double rounds = std::ceil(bf / threads);
+      double pass = rounds * r * (radix_cost(r) + 2.0 + 5.0 * (r - 1) / r + 10.0 / r);
+      double c = best[index(d / r)] + pass;
+      if (c < best[i] - 1e-9) {
+        best[i] = c;
+        choice[i] = r;
+      }
+    }
+  }
+  std::vector<int> out;
+  int64_t d = m;
+  while (d > 1) {
+    int r = choice[index(d)];
+    if (r == 0) throw InvalidArg("no FFT factorization of " + std::to_string(m));
+    out.push_back(r);
+    d /= r;
+  }
+  // larger radices first: their passes have the fewest butterflies
+  std::sort(out.begin(), out.end(), std::greater<int>());
+  return out;
+}
+}  // namespace
+
+FftTables fft_tables(int64_t n, int max_radix) {
   if (!fast_len(n) || n % 2 != 0) throw InvalidArg("the device FFT needs an even 2·3·5-smooth length, got " + std::to_string(n));
   FftTables t;
   t.n = n;
   t.m = n / 2;
-  int64_t k = t.m;
-  while (k % 8 == 0) { t.radices.push_back(8); k /= 8; }
-  if (k % 4 == 0) { t.radices.push_back(4); k /= 4; }
-  if (k % 2 == 0) { t.radices.push_back(2); k /= 2; }
-  while (k % 3 == 0) { t.radices.push_back(3); k /= 3; }
-  while (k % 5 == 0) { t.radices.push_back(5); k /= 5; }
+  t.radices = plan_radices(t.m, 256, max_radix);
   int64_t cur = t.m;
   for (int r : t.radices) {
     int64_t sub = cur / r;
@@ -292,7 +349,7 @@ int64_t spec_impulse_length(const psg_filter_spec& s, double dt_ms) {
 }
 
 // filter/apply.nim:118-151
-FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend) {
+FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend, int max_radix) {
   need(samples >= 1, "a filter plan needs samples ≥ 1, got " + std::to_string(samples));
   need(trend >= PSG_TR_NONE && trend <= PSG_TR_LINEAR, "unknown trend removal " + std::to_string(trend));
   validate_spec(s, dt_ms);
@@ -313,7 +370,7 @@ FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, 
     double c = std::cos(kPi / 2 * (double)k / (double)(f.pad + 1));
     f.fall[k - 1] = c * c;
   }
-  f.fft = fft_tables(f.nfft);
+  f.fft = fft_tables(f.nfft, max_radix);
   return f;
 }
 
@@ -384,7 +441,7 @@ int64_t agc_half(double window_ms, double dt_ms, int64_t samples, double target,
 }
 
 // pipeline.nim:392-447
-StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, int64_t record) {
+StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, int64_t record, int max_radix) {
   StepHost s;
   switch (op.kind) {
     case PSG_OP_DEMEAN: s.kind = ST_DEMEAN; break;
@@ -413,7 +470,7 @@ StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, 
       break;
     case PSG_OP_FILTER:
       s.kind = ST_FILTER;
-      s.filter = filter_plan(op.filter, dt_ms, samples, op.trend);
+      s.filter = filter_plan(op.filter, dt_ms, samples, op.trend, max_radix);
       break;
     case PSG_OP_AGC:
       need(op.agc_mode == PSG_AGC_RMS || op.agc_mode == PSG_AGC_MEAN_ABS, "unknown AGC mode");
@@ -473,7 +530,7 @@ std::atomic<uint64_t> g_generation{0};
 
 // pipeline.nim:466-523
 PlanHost compile_plan(const psg_op* ops, int n_ops, int dtype, double dt_ms, int64_t samples,
-                      int64_t record_samples) {
+                      int64_t record_samples, int max_radix) {
   need(dtype == PSG_F32 || dtype == PSG_F64, "dtype must be float32 or float64");
   need(fin(dt_ms) && dt_ms > 0, "dtMs must be finite and positive, got " + num(dt_ms));
   need(samples >= 1, "a pipeline needs samples ≥ 1, got " + std::to_string(samples));
@@ -489,7 +546,7 @@ PlanHost compile_plan(const psg_op* ops, int n_ops, int dtype, double dt_ms, int
   p.record_samples = std::max(samples, record_samples);
   for (int i = 0; i < n_ops; i++) {
     try {
-      p.steps.push_back(compile_op(ops[i], dtype, dt_ms, samples, p.record_samples));
+      p.steps.push_back(compile_op(ops[i], dtype, dt_ms, samples, p.record_samples, max_radix));
     } catch (const InvalidArg& e) {
       throw InvalidArg(std::string("op ") + std::to_string(i) + " (" + op_name(ops[i].kind) + "): " + e.what());
     }
@@ -580,7 +637,7 @@ std::vector<double> linear_sweep(double f1, double f2, double length_ms, double 
 
 // vibroseis/correlate.nim:82-160
 CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
-                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize) {
+                   int64_t record, int64_t out, int mode, double eps_percent, bool normalize, int max_radix) {
   need(plen >= 2, "a pilot needs at least two samples, got " + std::to_string(plen));
   need(pilot_dt > 0 && pilot_dt < kInf, "a pilot's dtMs must be finite and positive");
   need(fin(pilot_t0), "a pilot's t0Ms must be finite, got " + num(pilot_t0));
@@ -636,7 +693,7 @@ CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pi
   c.pilot_len = plen;
   c.dt_ms = dt_ms;
   c.mode = mode;
-  c.fft = fft_tables(c.n);
+  c.fft = fft_tables(c.n, max_radix);
   return c;
 }
 

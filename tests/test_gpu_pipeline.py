@@ -112,6 +112,12 @@ def test_c2_uneven_panel_src_dst_and_in_place():
     host = run_gpu(C2_FLOW, g.data, meta, P.float32, 2.0, host=True)
     dev = run_gpu(C2_FLOW, g.data, meta, P.float32, 2.0)
     assert np.array_equal(host, dev)
+    # every op alone: in place gives the bits of src -> dst
+    for flow in ([P.demeanOp()], C2_FLOW[1:2], C2_FLOW[2:]):
+        a = run_gpu(flow, g.data, meta, P.float32, 2.0)
+        b = run_gpu(flow, g.data, meta, P.float32, 2.0, inplace=True)
+        assert np.array_equal(a, b)
+        assert_parity(a, flow, g.data, meta, P.F32, 2.0)
 
 
 def test_float64_plan_matches_oracle_to_1e12():
