@@ -118,6 +118,90 @@ def cpu_baseline(steps=3, warmup=1):
                       f"min {mn * 1e3:.1f} ms), ProcessPool clone, {cores} threads"}
 
 
+def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
+    """The served viewer load (Poisson arrivals at ``rate_hz``; trace counts
+    log-uniform in 48..5000; shown windows log-uniform in 200..4000 samples
+    of a 6001-sample record, decoded with each plan's margin; three plans):
+    the request loop against the plain per-call apply on the same request
+    sequence. Latency is arrival to completion."""
+    import threading
+    import numpy as np
+    import torch
+    import processseg_b200 as P
+    from processseg_b200 import synth
+    flows = synth.viewer_flows()
+    margins = [P.initPipeline(f).requiredMargin(DT) for f in flows]
+    reqs = synth.viewer_requests(n_req, rate_hz=rate_hz, margins=margins)
+    plans = {}
+    for r in reqs:
+        key = (r.flow, r.cols)
+        if key not in plans:
+            plans[key] = P.initPipeline(flows[r.flow]).compile(P.float32, DT, r.cols, recordSamples=6001)
+    maxn = max(r.rows * r.cols for r in reqs)
+    g = synth.shot_gather(5000, 6001, DT, seed=9, workload="c4", live_range=(3000, 6001))
+    pool = torch.from_numpy(g.data.reshape(-1)[:maxn].copy()).pin_memory().numpy()
+    outs = [torch.empty(maxn, dtype=torch.float32).pin_memory().numpy() for _ in range(slots)]
+    metas = {}
+    jobs = []
+    for i, r in enumerate(reqs):
+        key = (r.rows, r.first, r.cols)
+        if key not in metas:
+            metas[key] = P.initChunkMeta(g.status[:r.rows], g.numSamples[:r.rows], DT, g.t0Ms[:r.rows], r.first)
+            metas[key].flat(r.cols)
+        src = pool[:r.rows * r.cols].reshape(r.rows, r.cols)
+        dst = outs[i % slots][:r.rows * r.cols].reshape(r.rows, r.cols)
+        jobs.append((r.arrival_s, plans[(r.flow, r.cols)], src, dst, metas[key]))
+    total = sum(r.rows * r.cols for r in reqs)
+    # plain per-call: one caller, in arrival order
+    ws = P.initWorkspace()
+    for _, plan, src, dst, meta in jobs[:3]:
+        ws.reserve(plan, rows=5000, cols=src.shape[1])
+        plan.apply(src, dst, meta, ws)
+    for _, plan, src, dst, meta in jobs:
+        ws.reserve(plan, rows=5000, cols=src.shape[1])
+    lat = []
+    t0 = time.perf_counter()
+    for arr, plan, src, dst, meta in jobs:
+        while time.perf_counter() - t0 < arr:
+            pass
+        plan.apply(src, dst, meta, ws)
+        lat.append(time.perf_counter() - t0 - arr)
+    plain_span = time.perf_counter() - t0
+    plain = {"p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
+             "msamples_per_s": total / plain_span / 1e6}
+    # the request loop: submits at the arrival times, a second thread waits
+    with P.Server(arena_bytes=3 << 30) as srv:
+        for _, plan, src, dst, meta in jobs[:3]:
+            srv.wait(srv.submit(plan, src, dst, meta))
+        srv.stats(reset=True)
+        tickets = []
+        done = threading.Event()
+
+        def waiter():
+            k = 0
+            while k < len(jobs):
+                if k < len(tickets):
+                    srv.wait(tickets[k], 60000)
+                    k += 1
+                else:
+                    time.sleep(0.0001)
+            done.set()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        for arr, plan, src, dst, meta in jobs:
+            while time.perf_counter() - t0 < arr:
+                pass
+            tickets.append(srv.submit(plan, src, dst, meta))
+        th.join()
+        st = srv.stats()
+    return {"workload": "served viewer load: Poisson 2000 req/s, traces log-U[48,5000], windows log-U[200,4000] of 6001 + plan margins, 3 plans",
+            "requests": n_req, "offered_rps": rate_hz, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+            "msamples_per_s": st["msamples_per_s"], "requests_per_launch": st["requests_per_launch"],
+            "plain_per_call": plain}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -242,6 +326,8 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }
+        if not args.no_serving:
+            line["serving"] = serving_leg()
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(steps=3, warmup=1)
         print(json.dumps(line), flush=True)
@@ -257,6 +343,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-load leg")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -297,6 +297,30 @@ int psg_stack_result(const psg_stack* st, void* dst, int32_t dtype, int32_t norm
 /* foldInto: counts, device int32 [rows, samples]. */
 int psg_stack_fold(const psg_stack* st, int32_t* dst, void* stream);
 
+/* ------------------------------------------------------------- serving
+ * A request loop for a viewer (the reference's viewer loop,
+ * tests/utils/viewersim.nim:155-200, calls pool.apply per stale entry; here
+ * requests from any thread are batched on the GPU as they arrive). Requests
+ * are admitted by device footprint into a fixed arena of `arena_bytes`,
+ * copied in, run together in one launch of the batched pipeline kernel
+ * (each trace with its own request's plan and width), and copied out, so the
+ * copies of one request overlap the kernels of others. Float32 plans without
+ * a per-panel normalization. Results equal psg_apply_host's bit for bit. */
+typedef struct psg_server psg_server;
+int psg_server_create(int device, int64_t arena_bytes, psg_server** out);
+void psg_server_destroy(psg_server* server);
+/* Queues a request (host buffers; pinned memory overlaps best). Returns
+ * PSG_ENOMEM when the request alone needs more than the arena holds. The plan
+ * and the buffers must stay valid until psg_wait returns. */
+int psg_submit(psg_server* server, const psg_plan* plan, const void* src_host, void* dst_host,
+               int64_t rows, int32_t cols, const int32_t* live_host,
+               const double* start_ms_host, double dt_ms, uint64_t* ticket);
+/* Waits for a request (PSG_ETIMEOUT after timeout_ms) and releases its ticket. */
+int psg_wait(psg_server* server, uint64_t ticket, double timeout_ms);
+/* out[8]: completed, samples, launches, requests per launch, p50 and p99
+ * latency (s, submit to completion), Msamples/s, refused; reset != 0 clears. */
+int psg_server_stats(psg_server* server, double* out, int reset);
+
 #ifdef __cplusplus
 }
 #endif

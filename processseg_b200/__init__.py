@@ -29,3 +29,4 @@ from .plan import PipelinePlan, Workspace, compile, initWorkspace
 from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepSpec, SweepTaper, generatePilot,
                         initCorrelationPlan, initPilot, initRecordStack, initSweepTaper, linearSweep,
                         noTaper, tpCos2, tpCosine, tpLinear)
+from .server import Server

@@ -143,6 +143,11 @@ def _declare(lib):
         "psg_correlate_stack": (C.c_int, [P, P, P, P, I64, I32, P, P, P, DBL, P]),
         "psg_stack_result": (C.c_int, [P, P, I32, I32, P]),
         "psg_stack_fold": (C.c_int, [P, P, P]),
+        "psg_server_create": (C.c_int, [C.c_int, I64, C.POINTER(P)]),
+        "psg_server_destroy": (None, [P]),
+        "psg_submit": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, C.POINTER(C.c_uint64)]),
+        "psg_wait": (C.c_int, [P, C.c_uint64, DBL]),
+        "psg_server_stats": (C.c_int, [P, C.POINTER(DBL), C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -53,18 +53,25 @@ struct DevStep {
   psg_gain_curve curve;
 };
 
-struct PipeArgs {
-  const void* src;
+// One apply: a block of rows and the plan steps of one part.
+struct Job {
+  const void* src;  // NULL or == dst: in place
   void* dst;
-  long long rows;
-  int cols;
-  int x_elems;       // shared-memory trace buffer, elements
-  int work_off;      // byte offset of the work area
-  int first, last;   // steps [first, last)
   const int* live;
   const double* start_ms;
-  const double* factor;  // the part's panel factor (NaN: none) or NULL
   const DevStep* steps;
+  long long rows;
+  int cols, first, last, _pad;
+};
+
+struct PipeArgs {
+  Job job;                     // the apply (single-job launches)
+  const Job* jobs;             // batched launches: the jobs, and the first
+  const long long* row_begin;  // global row of each (ascending)
+  int njobs;
+  long long total_rows;
+  const double* factor;  // the part's panel factor (NaN: none) or NULL
+  int work_off;          // byte offset of the work area
   int x_bytes;           // bytes of one row buffer (two of them with the bulk prefetch)
   int* status;           // set to 1 when a bounded wait gives up
 };
@@ -689,40 +696,74 @@ struct RowSlot {
   int head, body, len, off;  // ragged head (elements), bulk bytes, elements, byte offset of X in the buffer
 };
 
+// What one row of a launch needs: its job's pointers and plan, and its live
+// length. Batched launches find the job by a binary search of row_begin.
+template <class T> struct RowCtx {
+  const T* from;  // the row to read (src, or dst in place)
+  T* to;          // the row to write
+  const DevStep* steps;
+  double start;
+  int n, cols, first, last;
+  bool copy;
+};
+template <class T, bool BATCH>
+__device__ __forceinline__ RowCtx<T> row_ctx(const PipeArgs& a, long long t) {
+  long long r = t;
+  const Job* J = &a.job;
+  if (BATCH) {
+    int lo = 0, hi = a.njobs - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (a.row_begin[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    J = &a.jobs[lo];
+    r = t - a.row_begin[lo];
+  }
+  RowCtx<T> c;
+  const T* src = reinterpret_cast<const T*>(J->src);
+  T* dst = reinterpret_cast<T*>(J->dst);
+  c.copy = src != nullptr && src != dst;
+  c.cols = J->cols;
+  c.from = (c.copy ? src : dst) + r * (long long)c.cols;
+  c.to = dst + r * (long long)c.cols;
+  c.n = min(max(J->live[r], 0), c.cols);
+  c.start = J->start_ms ? J->start_ms[r] : (double)NAN;
+  c.steps = J->steps;
+  c.first = J->first;
+  c.last = J->last;
+  return c;
+}
+
 // PF: prefetch the next row into the second buffer while this one is
 // processed (when the second buffer costs no occupancy); otherwise one buffer,
-// loaded at the top of each row.
-template <class T, int MAXR, bool PF>
+// loaded at the top of each row. BATCH: the rows of several jobs (several
+// plans, widths and blocks) in one launch.
+template <class T, int MAXR, bool PF, bool BATCH>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
   __shared__ Shared S;
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ RowSlot slot[2];
-  const T* src = reinterpret_cast<const T*>(a.src);
-  T* dst = reinterpret_cast<T*>(a.dst);
-  const bool copy = src != nullptr && src != dst;
-  const T* from = copy ? src : dst;
   const double pf = a.factor ? *a.factor : (double)NAN;
   const bool scale = !isnan(pf);
   const T kf = scale ? (T)pf : (T)1;
-  const int need0 = a.first < a.last ? a.steps[a.first].need : 0;
+  const long long total = BATCH ? a.total_rows : a.job.rows;
   constexpr int esz = (int)sizeof(T);
-  // Thread 0 starts the bulk copy of a row into buffer b: the 16-byte aligned
+  // Thread 0 starts the bulk copy of row t into buffer b: the 16-byte aligned
   // body of the part we need (the whole row for src → dst, the live samples
   // in place); the few ragged elements at either end are read directly.
-  auto issue = [&](long long row, int b) {
-    int n = min(max(a.live[row], 0), a.cols);
-    int len = copy ? a.cols : n;
-    const T* g = from + row * (long long)a.cols;
-    uintptr_t ga = (uintptr_t)g;
-    int head = (int)(((16 - (ga & 15)) & 15) / esz);
-    head = min(head, len);
+  auto issue = [&](long long t, int b) {
+    const RowCtx<T> c = row_ctx<T, BATCH>(a, t);
+    int len = c.copy ? c.cols : c.n;
+    uintptr_t ga = (uintptr_t)c.from;
+    int head = min((int)(((16 - (ga & 15)) & 15) / esz), len);
     int body = ((len - head) * esz) & ~15;
     int off = (16 - (head * esz) % 16) % 16;
     unsigned char* xb = psg_dyn_smem + b * a.x_bytes;
     slot[b] = RowSlot{head, body, len, off};
     if (body > 0) {
       mbar_arrive_expect_tx(&bars[b], (uint32_t)body);
-      bulk_load(xb + off + head * esz, g + head, (uint32_t)body, &bars[b]);
+      bulk_load(xb + off + head * esz, c.from + head, (uint32_t)body, &bars[b]);
     } else {
       mbar_arrive(&bars[b]);
     }
@@ -731,21 +772,21 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     mbar_init_fence();
-    if (PF && blockIdx.x < a.rows) issue(blockIdx.x, 0);
+    if (PF && blockIdx.x < total) issue(blockIdx.x, 0);
   }
   __syncthreads();
   uint32_t phase[2] = {0, 0};
   int cur = 0;
-  for (long long r = blockIdx.x; r < a.rows; r += gridDim.x, cur = PF ? cur ^ 1 : 0) {
-    const long long rn = r + gridDim.x;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x, cur = PF ? cur ^ 1 : 0) {
+    const long long tn = t + gridDim.x;
     if (threadIdx.x == 0) {
       // the buffer's last reads (the previous row's store) come before the copy into it
-      if (PF && rn < a.rows) {
+      if (PF && tn < total) {
         fence_proxy_async();
-        issue(rn, cur ^ 1);
+        issue(tn, cur ^ 1);
       } else if (!PF) {
         fence_proxy_async();
-        issue(r, 0);
+        issue(t, 0);
       }
     }
     if (!mbar_wait(&bars[cur], phase[cur], 1ll << 26)) {
@@ -754,14 +795,15 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
       return;
     }
     phase[cur] ^= 1;
+    const RowCtx<T> c = row_ctx<T, BATCH>(a, t);
     const RowSlot sl = slot[cur];
     T* X = reinterpret_cast<T*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
-    const T* g = from + r * (long long)a.cols;
     const int tail0 = sl.head + sl.body / esz;
-    for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = g[i];
-    for (int i = tail0 + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = g[i];
+    for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = c.from[i];
+    for (int i = tail0 + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = c.from[i];
     __syncthreads();  // the ragged ends are read by other threads below
-    int n = min(max(a.live[r], 0), a.cols);
+    const int n = c.n;
+    const int need0 = c.first < c.last ? c.steps[c.first].need : 0;
     Stats st{0, 0, 0, 0};
     if (n > 0) {
       // the panel factor of a part that starts with one, and the first
@@ -771,8 +813,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
     } else {
       __syncthreads();
     }
-    for (int si = a.first; n > 0 && si < a.last; si++) {
-      const DevStep& d = a.steps[si];
+    for (int si = c.first; n > 0 && si < c.last; si++) {
+      const DevStep& d = c.steps[si];
       const int need = d.need_next;
       switch (d.kind) {
         case ST_DEMEAN: {
@@ -781,10 +823,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
           break;
         }
         case ST_DETREND: {
-          double nf = (double)n, c = (nf - 1) / 2, mean = st.s1 / nf;
+          double nf = (double)n, cc = (nf - 1) / 2, mean = st.s1 / nf;
           double stt = nf * (nf * nf - 1) / 12;
-          double slope = n > 1 ? (st.si - c * st.s1) / stt : 0.0;
-          const T ta = (T)(mean - slope * c), tb = (T)slope;
+          double slope = n > 1 ? (st.si - cc * st.s1) / stt : 0.0;
+          const T ta = (T)(mean - slope * cc), tb = (T)slope;
           st = map_trace(X, n, need, S, [&](T x, int i) { return x - (ta + tb * (T)i); });
           break;
         }
@@ -804,11 +846,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
         case ST_FILTER: st = step_filter<T, MAXR>(d, st, X, n, a.work_off, S); break;
         case ST_AGC: st = step_agc(d, st, X, n, a.work_off, S); break;
         case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
-        case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, a.start_ms ? a.start_ms[r] : (double)NAN, S); break;
+        case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, c.start, S); break;
         default: break;
       }
     }
-    if (copy || n > 0) store_out(X, dst + r * (long long)a.cols, copy ? a.cols : n);
+    if (c.copy || n > 0) store_out(X, c.to, c.copy ? c.cols : n);
     __syncthreads();
   }
 }
@@ -1252,6 +1294,9 @@ template <class F> static int guarded(F&& f) {
   } catch (const WorkspaceError& e) {
     t_err = e.what();
     return PSG_EWORKSPACE;
+  } catch (const NoMemory& e) {
+    t_err = e.what();
+    return PSG_ENOMEM;
   } catch (const CudaError& e) {
     t_err = e.what();
     std::string w = e.what();
@@ -1280,8 +1325,14 @@ static int64_t ws_host_bytes(int64_t rows, int32_t cols, int dtype) {
 
 // The pipeline kernel of a sample type and largest radix.
 template <class T> static void (*pipe_kernel_for(int max_radix, bool pf))(PipeArgs) {
-  if (sizeof(T) == 8 || max_radix <= 8) return pf ? pipeline_kernel<T, 8, true> : pipeline_kernel<T, 8, false>;
-  return pf ? pipeline_kernel<T, 12, true> : pipeline_kernel<T, 12, false>;
+  if (sizeof(T) == 8 || max_radix <= 8)
+    return pf ? pipeline_kernel<T, 8, true, false> : pipeline_kernel<T, 8, false, false>;
+  return pf ? pipeline_kernel<T, 12, true, false> : pipeline_kernel<T, 12, false, false>;
+}
+// The batched form (float32 plans of one largest radix).
+static void (*batch_kernel_for(int max_radix, bool pf))(PipeArgs) {
+  if (max_radix <= 8) return pf ? pipeline_kernel<float, 8, true, true> : pipeline_kernel<float, 8, false, true>;
+  return pf ? pipeline_kernel<float, 12, true, true> : pipeline_kernel<float, 12, false, true>;
 }
 
 template <class T> static void build_device_steps(psg_plan* p) {
@@ -1409,21 +1460,20 @@ static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const vo
     factor = &out->factor;
   }
   PipeArgs a{};
-  a.src = src;
-  a.dst = dst;
-  a.rows = rows;
-  a.cols = cols;
-  a.x_elems = p->x_elems;
+  a.job.src = src;
+  a.job.dst = dst;
+  a.job.rows = rows;
+  a.job.cols = cols;
+  a.job.first = panel ? range.first + 1 : range.first;
+  a.job.last = range.second;
+  a.job.live = live;
+  a.job.start_ms = start;
+  a.job.steps = p->d_steps;
   a.work_off = p->work_off;
-  a.first = panel ? range.first + 1 : range.first;
-  a.last = range.second;
-  a.live = live;
-  a.start_ms = start;
   a.factor = factor;
-  a.steps = p->d_steps;
   a.x_bytes = p->x_bytes;
   a.status = reinterpret_cast<int*>((char*)ws->d + 504);
-  bool nothing = a.first >= a.last && !factor && (src == nullptr || src == dst);
+  bool nothing = a.job.first >= a.job.last && !factor && (src == nullptr || src == dst);
   if (nothing || rows == 0) return;
   int grid = (int)std::min<int64_t>(rows, p->grid);
   pipe_kernel_for<T>(p->max_radix, p->prefetch)<<<grid, p->threads, p->smem, stream>>>(a);
@@ -2052,3 +2102,459 @@ __global__ void trace_stats_finish(double* rms, double* mx, const int* live, lon
     rms[r] = sqrt(rms[r] / (double)n);
   }
 }
+
+// ================================================================ serving
+// A request loop for a viewer's zoom-window and panel requests (different
+// trace counts, widths and plans). Requests are admitted by their device
+// footprint into a fixed arena (no allocation per request), copied in on
+// one stream, run together in one launch of the batched pipeline kernel (each
+// trace with its own request's plan), and copied out on another stream, so
+// that requests arriving while others are on the GPU join the next launch
+// and the copies of one overlap the kernels of others. The results are those
+// of the plain apply: the kernel computes each trace the same way alone or
+// in a batch.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
+#include <unordered_map>
+
+namespace psg {
+namespace {
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Arena {
+  int64_t size = 0;
+  std::map<int64_t, int64_t> free_;  // offset → bytes
+  void init(int64_t n) {
+    size = n;
+    free_.clear();
+    free_[0] = n;
+  }
+  int64_t alloc(int64_t n) {
+    n = (n + 255) / 256 * 256;
+    for (auto it = free_.begin(); it != free_.end(); ++it)
+      if (it->second >= n) {
+        int64_t off = it->first, rest = it->second - n;
+        free_.erase(it);
+        if (rest) free_[off + n] = rest;
+        return off;
+      }
+    return -1;
+  }
+  void release(int64_t off, int64_t n) {
+    n = (n + 255) / 256 * 256;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && off + n == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct Req {
+  uint64_t ticket = 0;
+  const psg_plan* plan = nullptr;
+  const void* src = nullptr;
+  void* dst = nullptr;
+  const int32_t* live = nullptr;
+  const double* start = nullptr;
+  int64_t rows = 0;
+  int32_t cols = 0;
+  int64_t off = -1, bytes = 0;
+  double t_submit = 0, t_done = 0;
+  int status = PSG_OK;
+  bool done = false;
+  cudaEvent_t in = nullptr;  // its copy in finished
+};
+
+struct Batch {
+  std::vector<Req*> reqs;
+  cudaEvent_t kern = nullptr;  // its kernel finished
+  cudaEvent_t done = nullptr;  // its copies out finished
+  int slot = 0;
+};
+}  // namespace
+}  // namespace psg
+
+struct psg_server {
+  int device = 0;
+  char* arena_d = nullptr;
+  Arena arena;
+  cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+  static const int kSlots = 4, kMaxJobs = 64;
+  Job* jobs_h = nullptr;  // pinned, kSlots × kMaxJobs
+  long long* begin_h = nullptr;
+  Job* jobs_d = nullptr;
+  long long* begin_d = nullptr;
+  int* status_d = nullptr;
+  bool slot_busy[kSlots] = {};
+  std::thread sched;
+  std::mutex mu;
+  std::condition_variable cv, cv_done;
+  bool stop = false;
+  std::deque<Req*> pending;
+  std::vector<Req*> staged;
+  std::vector<Batch*> inflight;
+  std::vector<cudaEvent_t> events;  // a pool of reusable events
+  cudaEvent_t last_kernel = nullptr;
+  std::unordered_map<uint64_t, Req*> by_ticket;
+  uint64_t next_ticket = 1;
+  // statistics
+  int64_t completed = 0, samples = 0, launches = 0, batched_reqs = 0, refused = 0;
+  std::vector<double> lat;
+  double t_first = 0, t_last = 0;
+  std::string error;
+};
+
+namespace psg {
+namespace {
+int64_t req_bytes(const Req& r) {
+  return align256(r.rows * (int64_t)r.cols * 4) + align256(r.rows * 4) + align256(r.rows * 8);
+}
+
+cudaEvent_t get_event(psg_server* S) {
+  if (!S->events.empty()) {
+    cudaEvent_t e = S->events.back();
+    S->events.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return e;
+}
+void put_event(psg_server* S, cudaEvent_t e) {
+  if (e) S->events.push_back(e);
+}
+
+// Moves pending requests that fit the arena to staged, starting their copies in.
+void admit(psg_server* S) {
+  while (!S->pending.empty()) {
+    Req* r = S->pending.front();
+    int64_t off = S->arena.alloc(r->bytes);
+    if (off < 0) break;  // waits for memory to free up (FIFO)
+    S->pending.pop_front();
+    r->off = off;
+    char* base = S->arena_d + off;
+    size_t db = (size_t)(r->rows * (int64_t)r->cols * 4);
+    CUDA_OK(cudaMemcpyAsync(base, r->src, db, cudaMemcpyHostToDevice, S->s_in));
+    CUDA_OK(cudaMemcpyAsync(base + align256((int64_t)db), r->live, r->rows * 4, cudaMemcpyHostToDevice, S->s_in));
+    if (r->start)
+      CUDA_OK(cudaMemcpyAsync(base + align256((int64_t)db) + align256(r->rows * 4), r->start, r->rows * 8,
+                              cudaMemcpyHostToDevice, S->s_in));
+    r->in = get_event(S);
+    CUDA_OK(cudaEventRecord(r->in, S->s_in));
+    S->staged.push_back(r);
+  }
+}
+
+// One launch over every staged request whose copy in has finished (up to
+// kMaxJobs), then their copies out. Called when no kernel is running, so
+// that requests arriving meanwhile join the next launch.
+void launch_batch(psg_server* S) {
+  int slot = -1;
+  for (int i = 0; i < psg_server::kSlots; i++)
+    if (!S->slot_busy[i]) {
+      slot = i;
+      break;
+    }
+  if (slot < 0 || S->staged.empty()) return;
+  Batch* b = new Batch();
+  b->slot = slot;
+  for (size_t i = 0; i < S->staged.size() && b->reqs.size() < (size_t)psg_server::kMaxJobs;) {
+    Req* r = S->staged[i];
+    if (cudaEventQuery(r->in) == cudaSuccess) {
+      put_event(S, r->in);
+      r->in = nullptr;
+      b->reqs.push_back(r);
+      S->staged.erase(S->staged.begin() + i);
+    } else {
+      i++;
+    }
+  }
+  if (b->reqs.empty()) {
+    delete b;
+    return;
+  }
+  size_t take = b->reqs.size();
+  Job* jh = S->jobs_h + slot * psg_server::kMaxJobs;
+  long long* bh = S->begin_h + slot * psg_server::kMaxJobs;
+  long long total = 0;
+  int xb = 0, maxr = 12;
+  size_t work = 0;
+  for (size_t i = 0; i < take; i++) {
+    Req* r = b->reqs[i];
+    const psg_plan* p = r->plan;
+    char* base = S->arena_d + r->off;
+    size_t db = (size_t)(r->rows * (int64_t)r->cols * 4);
+    Job j{};
+    j.src = nullptr;
+    j.dst = base;
+    j.live = (const int*)(base + align256((int64_t)db));
+    j.start_ms = r->start ? (const double*)(base + align256((int64_t)db) + align256(r->rows * 4)) : nullptr;
+    j.steps = p->d_steps;
+    j.rows = r->rows;
+    j.cols = r->cols;
+    j.first = p->host.parts[0].first;
+    j.last = p->host.parts[0].second;
+    jh[i] = j;
+    bh[i] = total;
+    total += r->rows;
+    xb = std::max(xb, p->x_bytes);
+    work = std::max(work, p->smem - (size_t)p->work_off);
+    maxr = std::min(maxr, p->max_radix);
+  }
+  CUDA_OK(cudaMemcpyAsync(S->jobs_d + slot * psg_server::kMaxJobs, jh, take * sizeof(Job), cudaMemcpyHostToDevice, S->s_comp));
+  CUDA_OK(cudaMemcpyAsync(S->begin_d + slot * psg_server::kMaxJobs, bh, take * sizeof(long long), cudaMemcpyHostToDevice, S->s_comp));
+  PipeArgs a{};
+  a.jobs = S->jobs_d + slot * psg_server::kMaxJobs;
+  a.row_begin = S->begin_d + slot * psg_server::kMaxJobs;
+  a.njobs = (int)take;
+  a.total_rows = total;
+  a.x_bytes = xb;
+  a.status = S->status_d;
+  // one row buffer, or two when the prefetch costs no occupancy
+  auto occ = [&](bool pf, size_t& sm) {
+    sm = (size_t)((pf ? 2 : 1) * xb) + work;
+    auto k = batch_kernel_for(maxr, pf);
+    allow_smem(k);
+    int per = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, sm));
+    return per;
+  };
+  size_t sm1, sm2;
+  int o1 = occ(false, sm1), o2 = occ(true, sm2);
+  bool pf = o2 > 0 && o2 >= o1;
+  a.work_off = (pf ? 2 : 1) * xb;
+  int per = pf ? o2 : o1;
+  if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
+  int grid = (int)std::min<long long>(total, (long long)per * g_sm_count);
+  if (total > 0) batch_kernel_for(maxr, pf)<<<grid, 256, pf ? sm2 : sm1, S->s_comp>>>(a);
+  CUDA_OK(cudaGetLastError());
+  b->kern = get_event(S);
+  CUDA_OK(cudaEventRecord(b->kern, S->s_comp));
+  S->last_kernel = b->kern;
+  CUDA_OK(cudaStreamWaitEvent(S->s_out, b->kern, 0));
+  for (Req* r : b->reqs)
+    CUDA_OK(cudaMemcpyAsync(r->dst, S->arena_d + r->off, (size_t)(r->rows * (int64_t)r->cols * 4),
+                            cudaMemcpyDeviceToHost, S->s_out));
+  b->done = get_event(S);
+  CUDA_OK(cudaEventRecord(b->done, S->s_out));
+  S->slot_busy[slot] = true;
+  S->inflight.push_back(b);
+  S->launches++;
+  S->batched_reqs += (int64_t)take;
+}
+
+// Retires finished batches: their requests are done and their memory free.
+bool retire(psg_server* S) {
+  bool any = false;
+  for (size_t i = 0; i < S->inflight.size();) {
+    Batch* b = S->inflight[i];
+    cudaError_t e = cudaEventQuery(b->done);
+    if (e == cudaErrorNotReady) {
+      i++;
+      continue;
+    }
+    double t = now_s();
+    for (Req* r : b->reqs) {
+      r->status = e == cudaSuccess ? PSG_OK : PSG_ECUDA;
+      r->t_done = t;
+      r->done = true;
+      S->arena.release(r->off, r->bytes);
+      S->completed++;
+      S->samples += r->rows * (int64_t)r->cols;
+      S->lat.push_back(t - r->t_submit);
+      S->t_last = t;
+    }
+    if (S->last_kernel == b->kern) S->last_kernel = nullptr;
+    put_event(S, b->kern);
+    put_event(S, b->done);
+    S->slot_busy[b->slot] = false;
+    delete b;
+    S->inflight.erase(S->inflight.begin() + i);
+    any = true;
+  }
+  return any;
+}
+
+void sched_loop(psg_server* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  while (true) {
+    if (S->stop && S->pending.empty() && S->staged.empty() && S->inflight.empty()) break;
+    try {
+      admit(S);
+      // launch when no kernel is running: arrivals during a kernel join the next launch
+      bool gpu_idle = S->last_kernel == nullptr || cudaEventQuery(S->last_kernel) == cudaSuccess;
+      if (!S->staged.empty() && gpu_idle) launch_batch(S);
+      if (retire(S)) S->cv_done.notify_all();
+    } catch (const std::exception& e) {
+      S->error = e.what();
+      for (Req* r : S->staged) {
+        r->status = PSG_ECUDA;
+        r->done = true;
+      }
+      S->staged.clear();
+      S->cv_done.notify_all();
+    }
+    if (S->inflight.empty() && S->pending.empty() && S->staged.empty())
+      S->cv.wait_for(lk, std::chrono::milliseconds(5));
+    else {
+      lk.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      lk.lock();
+    }
+  }
+}
+}  // namespace
+}  // namespace psg
+
+extern "C" {
+
+int psg_server_create(int device, int64_t arena_bytes, psg_server** out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    if (arena_bytes < (1 << 20)) throw InvalidArg("the arena needs at least 1 MiB");
+    CUDA_OK(cudaSetDevice(device));
+    ensure_device();
+    std::unique_ptr<psg_server> S(new psg_server());
+    S->device = device;
+    CUDA_OK(cudaMalloc(&S->arena_d, (size_t)arena_bytes));
+    S->arena.init(arena_bytes);
+    CUDA_OK(cudaStreamCreateWithFlags(&S->s_in, cudaStreamNonBlocking));
+    CUDA_OK(cudaStreamCreateWithFlags(&S->s_comp, cudaStreamNonBlocking));
+    CUDA_OK(cudaStreamCreateWithFlags(&S->s_out, cudaStreamNonBlocking));
+    const int nj = psg_server::kSlots * psg_server::kMaxJobs;
+    CUDA_OK(cudaMallocHost(&S->jobs_h, nj * sizeof(Job)));
+    CUDA_OK(cudaMallocHost(&S->begin_h, nj * sizeof(long long)));
+    CUDA_OK(cudaMalloc(&S->jobs_d, nj * sizeof(Job)));
+    CUDA_OK(cudaMalloc(&S->begin_d, nj * sizeof(long long)));
+    CUDA_OK(cudaMalloc(&S->status_d, 256));
+    CUDA_OK(cudaMemset(S->status_d, 0, 256));
+    psg_server* raw = S.release();
+    raw->sched = std::thread(sched_loop, raw);
+    *out = raw;
+  });
+}
+
+void psg_server_destroy(psg_server* S) {
+  if (!S) return;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  if (S->sched.joinable()) S->sched.join();
+  for (auto& kv : S->by_ticket) delete kv.second;
+  for (cudaEvent_t e : S->events) cudaEventDestroy(e);
+  cudaFree(S->arena_d);
+  cudaFree(S->jobs_d);
+  cudaFree(S->begin_d);
+  cudaFree(S->status_d);
+  cudaFreeHost(S->jobs_h);
+  cudaFreeHost(S->begin_h);
+  cudaStreamDestroy(S->s_in);
+  cudaStreamDestroy(S->s_comp);
+  cudaStreamDestroy(S->s_out);
+  delete S;
+}
+
+int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* dst_host, int64_t rows, int32_t cols,
+               const int32_t* live_host, const double* start_ms_host, double dt_ms, uint64_t* ticket) {
+  return guarded([&] {
+    if (!S || !ticket) throw InvalidArg("null argument");
+    check_apply(plan, nullptr, src_host, dst_host, rows, cols, live_host, dt_ms, false);
+    if (plan->host.dtype != PSG_F32) throw InvalidArg("the request loop serves float32 plans");
+    if (plan->host.parts.size() != 1) throw InvalidArg("the request loop serves plans without a per-panel normalization");
+    if (!src_host) throw InvalidArg("src is required");
+    std::unique_ptr<Req> r(new Req());
+    r->plan = plan;
+    r->src = src_host;
+    r->dst = dst_host;
+    r->rows = rows;
+    r->cols = cols;
+    r->live = live_host;
+    r->start = start_ms_host;
+    r->bytes = req_bytes(*r);
+    r->t_submit = now_s();
+    std::lock_guard<std::mutex> g(S->mu);
+    if (r->bytes > S->arena.size) {
+      S->refused++;
+      throw NoMemory("admission refused: the request needs " + std::to_string(r->bytes) +
+                               " bytes of device memory, the loop holds " + std::to_string(S->arena.size));
+    }
+    if (S->completed == 0 && S->by_ticket.empty()) S->t_first = r->t_submit;
+    r->ticket = S->next_ticket++;
+    *ticket = r->ticket;
+    S->by_ticket[r->ticket] = r.get();
+    S->pending.push_back(r.release());
+    S->cv.notify_all();
+  });
+}
+
+int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
+  if (!S) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->by_ticket.find(ticket);
+  if (it == S->by_ticket.end()) {
+    t_err = "unknown ticket " + std::to_string(ticket);
+    return PSG_EINVAL;
+  }
+  Req* r = it->second;
+  auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000));
+  while (!r->done) {
+    if (S->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !r->done) {
+      t_err = "the request did not finish within " + std::to_string(timeout_ms) + " ms";
+      return PSG_ETIMEOUT;
+    }
+  }
+  int st = r->status;
+  S->by_ticket.erase(it);
+  delete r;
+  if (st != PSG_OK) t_err = S->error.empty() ? "a CUDA call of the request loop failed" : S->error;
+  return st;
+}
+
+// {completed, samples, launches, mean requests per launch, p50 s, p99 s,
+//  Msamples/s over the first submit to the last completion, refused}
+int psg_server_stats(psg_server* S, double* out8, int reset) {
+  if (!S || !out8) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::lock_guard<std::mutex> g(S->mu);
+  std::vector<double> l = S->lat;
+  std::sort(l.begin(), l.end());
+  auto q = [&](double f) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(f * (l.size() - 1) + 0.5))]; };
+  out8[0] = (double)S->completed;
+  out8[1] = (double)S->samples;
+  out8[2] = (double)S->launches;
+  out8[3] = S->launches ? (double)S->batched_reqs / (double)S->launches : 0.0;
+  out8[4] = q(0.50);
+  out8[5] = q(0.99);
+  out8[6] = S->t_last > S->t_first ? (double)S->samples / (S->t_last - S->t_first) / 1e6 : 0.0;
+  out8[7] = (double)S->refused;
+  if (reset) {
+    S->completed = S->samples = S->launches = S->batched_reqs = S->refused = 0;
+    S->lat.clear();
+    S->t_first = S->t_last = 0;
+  }
+  return PSG_OK;
+}
+
+}  // extern "C"

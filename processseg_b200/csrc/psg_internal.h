@@ -19,6 +19,10 @@ struct InvalidArg : std::runtime_error {
 struct WorkspaceError : std::runtime_error {
   explicit WorkspaceError(const std::string& m) : std::runtime_error(m) {}
 };
+// Admission refused: the work needs more device memory than it may hold.
+struct NoMemory : std::runtime_error {
+  explicit NoMemory(const std::string& m) : std::runtime_error(m) {}
+};
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& m) : std::runtime_error(m) {}
 };

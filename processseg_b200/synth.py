@@ -122,3 +122,45 @@ def vibroseis_records(pilot, channels=240, samples=10001, sweeps=4, seed=3, p=0.
     for s in range(sweeps):
         out[s] = conv + noise * g.standard_normal((channels, samples))
     return out
+
+
+# ------------------------------------------------------------ viewer load
+def viewer_flows():
+    """The three plans of the served viewer load: band-pass 4-8-60-80 + AGC
+    500 ms; band-pass + RMS normalization per trace; Butterworth 5-100 Hz
+    (24 dB/octave effective slope, 4 poles) + t² gain."""
+    from . import (Corners, agcOp, bandPassOp, butterBandPass, filterOp, gainCurveOp,
+                   normalizeOp, normRms, powerGain)
+    bp = Corners(4, 8, 60, 80)
+    return [[bandPassOp(bp), agcOp(500)],
+            [bandPassOp(bp), normalizeOp(normRms)],
+            [filterOp(butterBandPass(5, 100, 24)), gainCurveOp(powerGain(2))]]
+
+
+@dataclass
+class ViewerRequest:
+    arrival_s: float
+    flow: int        # index into viewer_flows()
+    rows: int
+    first: int       # decode window within the record
+    cols: int
+
+
+def viewer_requests(n, rate_hz=2000.0, record=6001, dtMs=2.0, seed=4, margins=None):
+    """``n`` requests of the served viewer load: Poisson arrivals at
+    ``rate_hz``, trace counts log-uniform in 48 .. 5000, shown windows
+    log-uniform in 200 .. 4000 samples placed uniformly in the record, decoded
+    with each plan's margin (decodeWindow), plans drawn uniformly."""
+    from .ops import decodeWindow
+    g = rng_for("c4", seed)
+    t = np.cumsum(g.exponential(1.0 / rate_hz, n))
+    out = []
+    for i in range(n):
+        flow = int(g.integers(0, 3))
+        rows = int(round(math.exp(g.uniform(math.log(48), math.log(5000)))))
+        width = int(round(math.exp(g.uniform(math.log(200), math.log(4000)))))
+        a = int(g.integers(0, record - width + 1))
+        m = margins[flow] if margins is not None else 0
+        lo, hi = decodeWindow(a, a + width - 1, m, record)
+        out.append(ViewerRequest(float(t[i]), flow, rows, lo, hi - lo + 1))
+    return out
