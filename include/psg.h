@@ -151,6 +151,9 @@ uint64_t psg_plan_generation(const psg_plan* plan);
 int32_t psg_plan_samples(const psg_plan* plan);
 int32_t psg_plan_record_samples(const psg_plan* plan);
 int32_t psg_plan_part_count(const psg_plan* plan);
+/* partNeedsPanel, src/processSEG/pipeline.nim:649-654: 1 when part `part`
+ * starts with a per-panel normalization, else 0 (also for no such part). */
+int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part);
 int32_t psg_plan_len(const psg_plan* plan);
 /* For step i of the plan: its FFT length (0 for steps without one) and the
  * pad laid out each side (FilterPlan.nfft / pad, filter/apply.nim:161-164). */
@@ -208,6 +211,35 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
 int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part,
                      const void* block, int64_t rows, int32_t cols, const int32_t* live,
                      double* factor_out, void* stream);
+/* runPart, src/processSEG/pipeline.nim:690-723: the steps of part `part` on
+ * the rows of dst (copied from `src` first when it is not NULL: the first
+ * part of a src → dst apply only). For a part that starts with a per-panel
+ * normalization, `factor` is a device double (from psg_panel_factor or
+ * psg_panel_factor_from) that scales the live rows first; NaN or NULL
+ * leaves them alone. Checks as psg_apply (checkApply). */
+int psg_run_part(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src,
+                 void* dst, int64_t rows, int32_t cols, const int32_t* live,
+                 const double* start_ms, double dt_ms, const double* factor, void* stream);
+
+/* A panel split by traces over several devices (or calls): the per-panel
+ * factor of panelFactor (src/processSEG/gain/gain.nim:221-240, over
+ * panelStats, gain/stats.nim:253-304) from statistics that merge.
+ * psg_panel_partials writes, for this shard's rows, PSG_PANEL_PARTIAL_DOUBLES
+ * device doubles: [0] Σx², [1] samples, [2] rows (over the usable rows: live,
+ * finite, Σx² not overflowing), [3] maxAbs, then 65536 histogram counts of
+ * the float32 bits of |x| >> 15 (exact integers; zeros unless the part's
+ * statistic is a percentile). Shards merge by summing every entry except
+ * [3], which takes the maximum (two all-reduces over the ranks).
+ * psg_panel_factor_from turns merged partials into the factor (a device
+ * double). One shard's partials give the same factor, bit for bit, as
+ * psg_panel_factor over that shard. */
+#define PSG_PANEL_PARTIAL_HEAD 4
+#define PSG_PANEL_PARTIAL_DOUBLES (PSG_PANEL_PARTIAL_HEAD + 65536)
+int psg_panel_partials(const psg_plan* plan, psg_workspace* ws, int32_t part,
+                       const void* block, int64_t rows, int32_t cols, const int32_t* live,
+                       double* partial, void* stream);
+int psg_panel_factor_from(const psg_plan* plan, psg_workspace* ws, int32_t part,
+                          const double* partial, double* factor_out, void* stream);
 
 /* ----------------------------------------------------------- statistics */
 /* traceStatsInto, src/processSEG/gain/stats.nim:186-199: rms and maxAbs per

@@ -37,6 +37,9 @@ AGC_RMS, AGC_MEAN_ABS = 0, 1
 # psg_norm_stat / psg_norm_scope
 NORM_MAX, NORM_RMS, NORM_PERCENTILE = 0, 1, 2
 PER_TRACE, PER_PANEL = 0, 1
+# psg_panel_partials: [Σx², samples, rows, maxAbs] + 65536 histogram counts
+PANEL_PARTIAL_HEAD = 4
+PANEL_PARTIAL_DOUBLES = PANEL_PARTIAL_HEAD + 65536
 # psg_curve_kind
 GC_KNOTS, GC_POWER, GC_EXPONENTIAL = 0, 1, 2
 # psg_trace_status
@@ -112,6 +115,7 @@ def _declare(lib):
         "psg_plan_samples": (I32, [P]),
         "psg_plan_record_samples": (I32, [P]),
         "psg_plan_part_count": (I32, [P]),
+        "psg_plan_part_needs_panel": (I32, [P, I32]),
         "psg_plan_len": (I32, [P]),
         "psg_plan_step_nfft": (I32, [P, I32]),
         "psg_plan_step_margin": (I32, [P, I32]),
@@ -124,6 +128,9 @@ def _declare(lib):
         "psg_apply": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
         "psg_apply_host": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
+        "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),
+        "psg_panel_partials": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
+        "psg_panel_factor_from": (C.c_int, [P, P, I32, P, P, P]),
         "psg_trace_stats": (C.c_int, [P, I32, I64, I32, P, P, P, P]),
         "psg_panel_stats": (C.c_int, [P, P, I32, I64, I32, P, DBL, P, P]),
         "psg_panel_stats_static": (C.c_int, [P, I32, I64, I32, P, DBL, P, P]),

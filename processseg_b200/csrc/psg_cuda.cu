@@ -472,8 +472,9 @@ template <bool REV> __device__ double carry_scan(double v, bool f, Shared& S) {
 // suffix sums of the terms in float64 (blocks of w = 2h + 1 samples, no
 // subtraction): each thread runs them over a contiguous segment of the trace
 // and a segmented scan across the threads carries the sums between
-// segments. The prefix and suffix arrays are stored as T; the gain step runs
-// in T on means scaled by the trace RMS.
+// segments. The prefix and suffix arrays are stored as T; each window mean
+// is formed in float64 and rounded once to T, and the gain step runs in T on
+// means scaled by the trace RMS.
 template <class T>
 __device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
   const int need = st.need_next;
@@ -568,25 +569,19 @@ __device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T*
   const int lastBlock = (n - 1) / w * w;
   const int tailCut = min(max(lastBlock + h, last), n);
   const T pn = P[n];
-  const T unitW = (T)(unit / (double)w);
+  const double unitWd = unit / (double)w;
   const T headWhole = headCut < first ? (T)((double)pn * unit * (1 / (double)n)) : (T)0;
   return map_trace(X, n, need, S, [&](T x, int i) {
     T mean;
-    if (i >= first && i < last) mean = (Sx[i - h] + P[i + h + 1]) * unitW;
+    // the window mean in float64, rounded once to T, as the reference
+    if (i >= first && i < last) mean = (T)(((double)Sx[i - h] + (double)P[i + h + 1]) * unitWd);
     else if (i < headCut) mean = (T)((double)P[i + h + 1] * (unit * (1 / (double)(i + h + 1))));
     else if (i < first) mean = headWhole;
     else if (i < tailCut) mean = (T)(((double)Sx[i - h] + (double)pn) * (unit * (1 / (double)(w - (i + h + 1 - n)))));
     else mean = (T)((double)Sx[i - h] * (unit * (1 / (double)(w - (i + h + 1 - n)))));
-    T lv;
-    if (rms_mode) {
-      if (sizeof(T) == 4) lv = mean > (T)0 ? (T)(mean * rsqrtf((float)mean)) : (T)0;
-      else lv = sqrt(mean);
-    } else {
-      lv = mean;
-    }
-    T gi;
-    if (sizeof(T) == 4) gi = (T)__fdividef((float)k, (float)(lv + eps));
-    else gi = k / (lv + eps);
+    // levelOf in T, correctly rounded (gain/gain.nim:392-402)
+    const T lv = rms_mode ? sqrt(mean) : mean;
+    const T gi = k / (lv + eps);
     return (T)(x * gi);
   });
 }
@@ -889,7 +884,7 @@ struct PanelOut {
   double rms, maxAbs, clip, rows, samples;
   double factor;
   double k_rank;
-  double pad;
+  double sum_sq;  // Σx² of the usable rows
 };
 
 __device__ __forceinline__ bool usable_d(double ssr, double mxr, int n) {
@@ -922,6 +917,7 @@ __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int co
     out->clip = NAN;
     out->rms = cnt > 0 ? sqrt(sum / cnt) : 0.0;
     out->maxAbs = cnt > 0 ? __longlong_as_double((long long)mb) : 0.0;
+    out->sum_sq = sum;
   }
 }
 
@@ -941,8 +937,11 @@ __global__ void __launch_bounds__(256) panel_hist_kernel(const T* __restrict__ b
   }
 }
 
-// orderStat (gain/stats.nim:237-251) for ranks j0 and j0 + 1, one CTA of 1024.
-__device__ double order_stat_from(const unsigned* hist, long long j, double mxv, int bin, long long below) {
+// orderStat (gain/stats.nim:237-251) for ranks j0 and j0 + 1, one CTA of
+// 1024. The counts are uint32 (one device's histogram) or float64 (the
+// merged histogram of several shards, exact integers).
+template <class C>
+__device__ double order_stat_from(const C* hist, long long j, double mxv, int bin, long long below) {
   if (bin == 0) return 0;
   double c = (double)hist[bin];
   double lo = (double)__uint_as_float((unsigned)bin << 15);
@@ -950,7 +949,8 @@ __device__ double order_stat_from(const unsigned* hist, long long j, double mxv,
   return fmin(fmax(lo + ((double)(j - below) + 0.5) / c * (hi - lo), lo), mxv);
 }
 
-__global__ void __launch_bounds__(1024) panel_clip_kernel(const unsigned* __restrict__ hist, PanelOut* out,
+template <class C>
+__global__ void __launch_bounds__(1024) panel_clip_kernel(const C* __restrict__ hist, PanelOut* out,
                                                           double clipP, int stat, double target, int dtype) {
   __shared__ long long pre[1024];
   __shared__ long long found_below[2];
@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(1024) panel_clip_kernel(const unsigned* __rest
   long long tot = 0;
   for (int k = 0; k < per; k++) {
     int bin = threadIdx.x * per + k;
-    if (bin <= maxKey) tot += hist[bin];
+    if (bin <= maxKey) tot += (long long)hist[bin];
   }
   pre[threadIdx.x] = tot;
   __syncthreads();
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(1024) panel_clip_kernel(const unsigned* __rest
         long long below = excl;
         for (int k = 0; k < per; k++) {
           int bin = threadIdx.x * per + k;
-          long long c = bin <= maxKey ? hist[bin] : 0;
+          long long c = bin <= maxKey ? (long long)hist[bin] : 0;
           if (below + c > j) {
             found_bin[q] = bin;
             found_below[q] = below;
@@ -1023,6 +1023,32 @@ __global__ void __launch_bounds__(1024) panel_clip_kernel(const unsigned* __rest
     }
     out->factor = factor;
   }
+}
+
+
+// Mergeable statistics of a shard of a panel: {Σx², samples, rows, maxAbs}
+// of its usable rows, then the 65536 histogram counts as float64 (exact).
+// Shards merge by summing every entry but maxAbs, which takes the maximum.
+__global__ void panel_partial_head_kernel(const PanelOut* fold, double* partial) {
+  partial[0] = fold->sum_sq;
+  partial[1] = fold->samples;
+  partial[2] = fold->rows;
+  partial[3] = fold->maxAbs;
+}
+
+__global__ void hist_to_f64_kernel(const unsigned* __restrict__ hist, double* __restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < 65536) out[k] = (double)hist[k];
+}
+
+// The panel output of merged partials: rms, maxAbs, rows and samples.
+__global__ void partial_to_out_kernel(const double* __restrict__ partial, PanelOut* out) {
+  double cnt = partial[1];
+  out->samples = cnt;
+  out->rows = partial[2];
+  out->rms = cnt > 0 ? sqrt(partial[0] / cnt) : 0.0;
+  out->maxAbs = cnt > 0 ? partial[3] : 0.0;
+  out->clip = NAN;
 }
 
 // ============================================================ correlation
@@ -1318,9 +1344,23 @@ template <class F> static int guarded(F&& f) {
 static const int64_t kHist = 65536 * 4;
 static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
 static int64_t ws_device_bytes(int64_t rows) { return 512 + align256(rows * 16) + kHist; }
-static int64_t ws_host_bytes(int64_t rows, int32_t cols, int dtype) {
-  return ws_device_bytes(rows) + align256(rows * 4) + align256(rows * 8) +
-         align256(rows * (int64_t)cols * (dtype == PSG_F32 ? 4 : 8));
+// The host path streams a block through the device in chunks of about
+// kChunkBytes, one staging buffer per lane stream, so that a block larger
+// than the device's memory still runs; a plan with a per-panel
+// normalization stages the whole block (its factor reads every row).
+static const int64_t kChunkBytes = 4 << 20;
+static int64_t host_chunk_rows(int64_t rows, int32_t cols, int64_t esz) {
+  return std::max<int64_t>(64, std::min<int64_t>(rows, kChunkBytes / std::max<int64_t>(1, cols * esz)));
+}
+static bool host_whole_block(bool needs_panel, int64_t rows, int32_t cols, int64_t esz) {
+  return needs_panel || rows <= host_chunk_rows(rows, cols, esz);
+}
+static int64_t ws_host_bytes(bool needs_panel, int64_t rows, int32_t cols, int dtype) {
+  int64_t esz = dtype == PSG_F32 ? 4 : 8;
+  int64_t stage_rows = host_whole_block(needs_panel, rows, cols, esz)
+                           ? rows
+                           : psg_workspace::kLanes * host_chunk_rows(rows, cols, esz);
+  return ws_device_bytes(rows) + align256(rows * 4) + align256(rows * 8) + align256(stage_rows * (int64_t)cols * esz);
 }
 
 // The pipeline kernel of a sample type and largest radix.
@@ -1433,32 +1473,44 @@ template <class T> static void build_device_steps(psg_plan* p) {
   p->grid = std::max(1, per_sm) * g_sm_count;
 }
 
+// The per-panel factor of part `part` (which starts with a per-panel
+// normalization) over the whole block, left in the part's workspace slot;
+// returns its device address.
 template <class T>
-static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
-                        int32_t cols, const int* live, const double* start, cudaStream_t stream) {
-  auto range = p->host.parts[part];
-  bool panel = range.first < range.second && p->host.steps[range.first].kind == ST_NORM_PANEL;
-  const double* factor = nullptr;
-  if (panel) {
-    // The factor over the whole block as the previous part left it (or src).
-    const StepHost& ns = p->host.steps[range.first];
-    const T* blk = reinterpret_cast<const T*>(src ? src : dst);
-    char* base = (char*)ws->d;
-    PanelOut* out = reinterpret_cast<PanelOut*>(base + 64 * part);
-    double* ss = reinterpret_cast<double*>(base + 512);
-    double* mx = ss + rows;
-    unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
-    int g = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
-    if (rows > 0) row_stats_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx);
-    panel_fold_kernel<<<1, 1024, 0, stream>>>(rows, cols, live, ss, mx, out);
-    double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
-    if (!std::isnan(clipP)) {
-      CUDA_OK(cudaMemsetAsync(hist, 0, kHist, stream));
-      if (rows > 0) panel_hist_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx, hist);
-    }
-    panel_clip_kernel<<<1, 1024, 0, stream>>>(hist, out, clipP, ns.stat, ns.norm_target, p->host.dtype);
-    factor = &out->factor;
+static const double* panel_factor_dev(const psg_plan* p, psg_workspace* ws, int part, const T* blk, int64_t rows,
+                                      int32_t cols, const int* live, cudaStream_t stream) {
+  const StepHost& ns = p->host.steps[p->host.parts[part].first];
+  char* base = (char*)ws->d;
+  PanelOut* out = reinterpret_cast<PanelOut*>(base + 64 * part);
+  double* ss = reinterpret_cast<double*>(base + 512);
+  double* mx = ss + rows;
+  unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
+  int g = (int)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)g_sm_count * 8));
+  if (rows > 0) row_stats_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx);
+  panel_fold_kernel<<<1, 1024, 0, stream>>>(rows, cols, live, ss, mx, out);
+  double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
+  if (!std::isnan(clipP)) {
+    CUDA_OK(cudaMemsetAsync(hist, 0, kHist, stream));
+    if (rows > 0) panel_hist_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx, hist);
   }
+  panel_clip_kernel<unsigned><<<1, 1024, 0, stream>>>(hist, out, clipP, ns.stat, ns.norm_target, p->host.dtype);
+  return &out->factor;
+}
+
+static bool part_needs_panel(const psg_plan* p, int part) {
+  auto range = p->host.parts[part];
+  return range.first < range.second && p->host.steps[range.first].kind == ST_NORM_PANEL;
+}
+
+// runPart (pipeline.nim:690-723): the steps of part `part` after its
+// per-panel normalization, if any, whose factor (a device double, NaN: the
+// rows are left alone) scales the live rows first; `src` (first part only)
+// is copied in.
+template <class T>
+static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
+                     int32_t cols, const int* live, const double* start, const double* factor, cudaStream_t stream) {
+  auto range = p->host.parts[part];
+  bool panel = part_needs_panel(p, part);
   PipeArgs a{};
   a.job.src = src;
   a.job.dst = dst;
@@ -1478,6 +1530,15 @@ static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const vo
   int grid = (int)std::min<int64_t>(rows, p->grid);
   pipe_kernel_for<T>(p->max_radix, p->prefetch)<<<grid, p->threads, p->smem, stream>>>(a);
   CUDA_OK(cudaGetLastError());
+}
+
+template <class T>
+static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
+                        int32_t cols, const int* live, const double* start, cudaStream_t stream) {
+  const double* factor = nullptr;
+  if (part_needs_panel(p, part))
+    factor = panel_factor_dev<T>(p, ws, part, reinterpret_cast<const T*>(src ? src : dst), rows, cols, live, stream);
+  run_part<T>(p, ws, part, src, dst, rows, cols, live, start, factor, stream);
 }
 
 template <class T> static void corr_upload(psg_corr_plan* p) {
@@ -1572,12 +1633,17 @@ int32_t psg_plan_step_nfft(const psg_plan* p, int32_t i) {
   if (!p || i < 0 || i >= (int)p->host.steps.size()) return 0;
   return p->host.steps[i].kind == ST_FILTER ? (int32_t)p->host.steps[i].filter.nfft : 0;
 }
+
+int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part) {
+  if (!plan || part < 0 || part >= (int)plan->host.parts.size()) return 0;
+  return part_needs_panel(plan, part) ? 1 : 0;
+}
 int32_t psg_plan_step_margin(const psg_plan* p, int32_t i) {
   if (!p || i < 0 || i >= (int)p->host.steps.size()) return 0;
   return (int32_t)p->host.steps[i].margin();
 }
 int64_t psg_plan_workspace_bytes(const psg_plan* p, int64_t rows, int32_t cols) {
-  return p ? ws_host_bytes(rows, cols, p->host.dtype) : 0;
+  return p ? ws_host_bytes(p->needs_panel, rows, cols, p->host.dtype) : 0;
 }
 
 int psg_workspace_create(psg_workspace** out) {
@@ -1618,7 +1684,7 @@ int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows,
   return guarded([&] {
     if (!ws || !plan) throw InvalidArg("null argument");
     if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
-    ws_grow(ws, ws_host_bytes(rows, cols, plan->host.dtype));
+    ws_grow(ws, ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype));
   });
 }
 int64_t psg_workspace_bytes(const psg_workspace* ws) { return ws ? ws->bytes : 0; }
@@ -1697,7 +1763,7 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
   return guarded([&] {
     check_apply(plan, ws, src_host, dst_host, rows, cols, live_host, dt_ms, false);
     if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
-    if (ws->bytes < ws_host_bytes(rows, cols, plan->host.dtype)) throw WorkspaceError("reserve the workspace for the plan first");
+    if (ws->bytes < ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype)) throw WorkspaceError("reserve the workspace for the plan first");
     if (rows == 0) return;
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -1708,8 +1774,7 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
     char* d_data = base + align256(rows * 4) + align256(rows * 8);
     const char* from = (const char*)(src_host ? src_host : dst_host);
     const double* dstart = start_ms_host ? d_start : nullptr;
-    auto run_parts = [&](int64_t r0, int64_t nr, cudaStream_t st) {
-      void* blk = d_data + r0 * cols * esz;
+    auto run_parts = [&](void* blk, int64_t r0, int64_t nr, cudaStream_t st) {
       for (int part = 0; part < (int)plan->host.parts.size(); part++) {
         if (plan->host.dtype == PSG_F32)
           launch_part<float>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st);
@@ -1718,12 +1783,12 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
       }
     };
     const int64_t row_bytes = (int64_t)cols * esz;
-    const int64_t chunk = std::max<int64_t>(64, std::min<int64_t>(rows, (4 << 20) / std::max<int64_t>(1, row_bytes)));
-    if (plan->needs_panel || rows <= chunk) {
+    const int64_t chunk = host_chunk_rows(rows, cols, esz);
+    if (host_whole_block(plan->needs_panel, rows, cols, esz)) {
       CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, s));
       if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, s));
       CUDA_OK(cudaMemcpyAsync(d_data, from, (size_t)(rows * row_bytes), cudaMemcpyHostToDevice, s));
-      run_parts(0, rows, s);
+      run_parts(d_data, 0, rows, s);
       CUDA_OK(cudaMemcpyAsync(dst_host, d_data, (size_t)(rows * row_bytes), cudaMemcpyDeviceToHost, s));
       CUDA_OK(cudaStreamSynchronize(s));
       return;
@@ -1744,13 +1809,17 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
     CUDA_OK(cudaEventRecord(ws->done_ev[0], ws->lane[0]));
     for (int i = 1; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamWaitEvent(ws->lane[i], ws->done_ev[0], 0));
     int k = 0;
+    // Lane k % kLanes reuses its own staging buffer: on its stream the copy
+    // in of a chunk queues after the copy out of that lane's previous one.
     for (int64_t r0 = 0; r0 < rows; r0 += chunk, k++) {
       int64_t nr = std::min(chunk, rows - r0);
-      cudaStream_t st = ws->lane[k % psg_workspace::kLanes];
+      int lane = k % psg_workspace::kLanes;
+      cudaStream_t st = ws->lane[lane];
+      char* buf = d_data + (size_t)lane * (size_t)(chunk * row_bytes);
       size_t off = (size_t)(r0 * row_bytes), nb = (size_t)(nr * row_bytes);
-      CUDA_OK(cudaMemcpyAsync(d_data + off, from + off, nb, cudaMemcpyHostToDevice, st));
-      run_parts(r0, nr, st);
-      CUDA_OK(cudaMemcpyAsync((char*)dst_host + off, d_data + off, nb, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(buf, from + off, nb, cudaMemcpyHostToDevice, st));
+      run_parts(buf, r0, nr, st);
+      CUDA_OK(cudaMemcpyAsync((char*)dst_host + off, buf, nb, cudaMemcpyDeviceToHost, st));
     }
     for (int i = 0; i < psg_workspace::kLanes; i++) {
       CUDA_OK(cudaEventRecord(ws->done_ev[i], ws->lane[i]));
@@ -1760,39 +1829,94 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
   });
 }
 
+static void check_panel_part(const psg_plan* plan, int32_t part) {
+  if (!plan) throw InvalidArg("a PipelinePlan must come from compile");
+  if (part < 0 || part >= (int)plan->host.parts.size()) throw WorkspaceError("no part " + std::to_string(part));
+  if (!part_needs_panel(plan, part))
+    throw WorkspaceError("part " + std::to_string(part) + " has no per-panel normalization");
+}
+
 int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* block, int64_t rows, int32_t cols,
                      const int32_t* live, double* factor_out, void* stream) {
   return guarded([&] {
-    if (!plan) throw InvalidArg("a PipelinePlan must come from compile");
-    if (part < 0 || part >= (int)plan->host.parts.size()) throw WorkspaceError("no part " + std::to_string(part));
-    auto range = plan->host.parts[part];
-    if (!(range.first < range.second && plan->host.steps[range.first].kind == ST_NORM_PANEL))
-      throw WorkspaceError("part " + std::to_string(part) + " has no per-panel normalization");
+    check_panel_part(plan, part);
     if (!ws || ws->bytes < ws_device_bytes(rows)) throw WorkspaceError("reserve the workspace for the plan first");
+    if (!factor_out) throw InvalidArg("null argument");
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
-    const StepHost& ns = plan->host.steps[range.first];
+    const double* f = plan->host.dtype == PSG_F32
+                          ? panel_factor_dev<float>(plan, ws, part, (const float*)block, rows, cols, live, s)
+                          : panel_factor_dev<double>(plan, ws, part, (const double*)block, rows, cols, live, s);
+    CUDA_OK(cudaMemcpyAsync(factor_out, f, 8, cudaMemcpyDeviceToDevice, s));
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_run_part(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src, void* dst, int64_t rows,
+                 int32_t cols, const int32_t* live, const double* start_ms, double dt_ms, const double* factor,
+                 void* stream) {
+  return guarded([&] {
+    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, false);
+    if (part < 0 || part >= (int)plan->host.parts.size()) throw WorkspaceError("no part " + std::to_string(part));
+    if (!ws || ws->bytes < 512) throw WorkspaceError("reserve the workspace for the plan first");
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    const double* f = part_needs_panel(plan, part) ? factor : nullptr;
+    if (plan->host.dtype == PSG_F32) run_part<float>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s);
+    else run_part<double>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s);
+  });
+}
+
+int psg_panel_partials(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* block, int64_t rows,
+                       int32_t cols, const int32_t* live, double* partial, void* stream) {
+  return guarded([&] {
+    check_panel_part(plan, part);
+    if (!ws || ws->bytes < ws_device_bytes(rows)) throw WorkspaceError("reserve the workspace for the plan first");
+    if (!partial) throw InvalidArg("null argument");
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    const StepHost& ns = plan->host.steps[plan->host.parts[part].first];
     char* base = (char*)ws->d;
     PanelOut* out = reinterpret_cast<PanelOut*>(base + 64 * part);
     double* ss = reinterpret_cast<double*>(base + 512);
     double* mx = ss + rows;
     unsigned* hist = reinterpret_cast<unsigned*>(base + 512 + align256(rows * 16));
     int g = (int)std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t)g_sm_count * 8));
-    double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
-    if (plan->host.dtype == PSG_F32) {
-      if (rows > 0) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
-    } else {
-      if (rows > 0) row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
+    bool f32 = plan->host.dtype == PSG_F32;
+    if (rows > 0) {
+      if (f32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
+      else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
     }
     panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, out);
-    if (!std::isnan(clipP)) {
+    panel_partial_head_kernel<<<1, 1, 0, s>>>(out, partial);
+    if (ns.stat == PSG_NORM_PERCENTILE) {
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
       if (rows > 0) {
-        if (plan->host.dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
+        if (f32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
         else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
       }
+      hist_to_f64_kernel<<<256, 256, 0, s>>>(hist, partial + PSG_PANEL_PARTIAL_HEAD);
+    } else {
+      CUDA_OK(cudaMemsetAsync(partial + PSG_PANEL_PARTIAL_HEAD, 0, 65536 * sizeof(double), s));
     }
-    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, out, clipP, ns.stat, ns.norm_target, plan->host.dtype);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+
+int psg_panel_factor_from(const psg_plan* plan, psg_workspace* ws, int32_t part, const double* partial,
+                          double* factor_out, void* stream) {
+  return guarded([&] {
+    check_panel_part(plan, part);
+    if (!ws || ws->bytes < 512) throw WorkspaceError("reserve the workspace for the plan first");
+    if (!partial || !factor_out) throw InvalidArg("null argument");
+    ensure_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    const StepHost& ns = plan->host.steps[plan->host.parts[part].first];
+    PanelOut* out = reinterpret_cast<PanelOut*>((char*)ws->d + 64 * part);
+    double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
+    partial_to_out_kernel<<<1, 1, 0, s>>>(partial, out);
+    panel_clip_kernel<double><<<1, 1024, 0, s>>>(partial + PSG_PANEL_PARTIAL_HEAD, out, clipP, ns.stat,
+                                                 ns.norm_target, plan->host.dtype);
     CUDA_OK(cudaMemcpyAsync(factor_out, &out->factor, 8, cudaMemcpyDeviceToDevice, s));
     CUDA_OK(cudaGetLastError());
   });
@@ -1840,7 +1964,7 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
         else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
       }
     }
-    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
+    panel_clip_kernel<unsigned><<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
     CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
     CUDA_OK(cudaGetLastError());
   });
@@ -1906,7 +2030,7 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
         else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
       }
     }
-    panel_clip_kernel<<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
+    panel_clip_kernel<unsigned><<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
     CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
     CUDA_OK(cudaGetLastError());
   });

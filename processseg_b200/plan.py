@@ -178,6 +178,60 @@ class PipelinePlan:
                                            cols, p(live), p(start), meta.dtMs,
                                            stream if stream is not None else None))
 
+    def partNeedsPanel(self, part: int) -> bool:
+        """Part ``part`` starts with a per-panel normalization
+        (pipeline.nim:649-654)."""
+        return bool(A.lib().psg_plan_part_needs_panel(self.h, int(part)))
+
+    def _device_call(self, dst, meta, cols):
+        import torch
+        live, start = meta.device(cols, 0, dst.device.index)
+        return live, start, torch.cuda.current_stream(dst.device).cuda_stream
+
+    def runPart(self, src, dst, meta: ChunkMeta, part: int, factor, ws: Workspace):
+        """runPart (pipeline.nim:690-723) on CUDA tensors: the steps of part
+        ``part`` on ``dst`` (copied from ``src`` first unless it is None:
+        the first part of a src → dst apply only). ``factor`` is a CUDA
+        float64 tensor of one value (``panelFactorOf``/``panelFactorFrom``)
+        or None; NaN or None leaves the rows alone."""
+        self._check_block(dst, "dst")
+        rows, cols = int(dst.shape[0]), int(dst.shape[1])
+        if src is not None:
+            self._check_block(src, "src")
+            if tuple(src.shape) != tuple(dst.shape):
+                raise ValueError(f"src is {src.shape[0]} × {src.shape[1]}, dst {rows} × {cols}")
+        meta.checkShape(rows)
+        live, start, st = self._device_call(dst, meta, cols)
+        A.check(A.lib().psg_run_part(self.h, ws.h, int(part), None if src is None else src.data_ptr(),
+                                     dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
+                                     meta.dtMs, None if factor is None else factor.data_ptr(), st))
+
+    def panelPartials(self, b, meta: ChunkMeta, part: int, ws: Workspace):
+        """The mergeable statistics of part ``part``'s per-panel
+        normalization over this shard ``b`` of a panel: a CUDA float64
+        tensor of ``PANEL_PARTIAL_DOUBLES`` values ([Σx², samples, rows,
+        maxAbs] then 65536 histogram counts). Shards merge by summing every
+        entry but maxAbs, which takes the maximum."""
+        import torch
+        self._check_block(b, "b")
+        rows, cols = int(b.shape[0]), int(b.shape[1])
+        meta.checkShape(rows)
+        live, _, st = self._device_call(b, meta, cols)
+        out = torch.empty(A.PANEL_PARTIAL_DOUBLES, dtype=torch.float64, device=b.device)
+        A.check(A.lib().psg_panel_partials(self.h, ws.h, int(part), b.data_ptr(), rows, cols,
+                                           live.data_ptr(), out.data_ptr(), st))
+        return out
+
+    def panelFactorFrom(self, partial, part: int, ws: Workspace):
+        """The factor (a CUDA float64 tensor of one value, NaN when the
+        normalization leaves the panel alone) of merged partials."""
+        import torch
+        out = torch.empty(1, dtype=torch.float64, device=partial.device)
+        st = torch.cuda.current_stream(partial.device).cuda_stream
+        A.check(A.lib().psg_panel_factor_from(self.h, ws.h, int(part), partial.data_ptr(),
+                                              out.data_ptr(), st))
+        return out
+
     def panelFactorOf(self, b, meta: ChunkMeta, part: int, ws: Workspace) -> float:
         """The per-panel factor of part ``part`` over the block ``b`` (a CUDA
         tensor), NaN when it leaves the block alone (pipeline.nim:656-669)."""

@@ -64,15 +64,15 @@ class Gather:
 
 
 def shot_gather(rows, cols, dtMs, seed, dtype=np.float32, live_range=None, sine_hz=None,
-                sine_amp=0.3, noise=0.1, events=5, workload="gather", channels=240):
+                sine_amp=0.3, noise=0.1, events=5, workload="gather", channels=240, row0=0):
     """A gather of ``rows`` traces: ``events`` Rickers (25 Hz) on hyperbolas,
-    t0 ~ U(200, 3500) ms, amp ~ N(0, 1), offsets 25 m × (row mod channels);
+    t0 ~ U(200, 3500) ms, amp ~ N(0, 1), offsets 25 m × ((row0 + row) mod channels);
     noise N(0, σ); a DC offset U(−0.5, 0.5) per trace; optional sinusoid;
     live lengths U{live_range} with zeros past them."""
     g = rng_for(workload, seed)
     t0s = g.uniform(200.0, 3500.0, events)
     amps = g.standard_normal(events)
-    offsets = 25.0 * (np.arange(rows) % channels)
+    offsets = 25.0 * ((row0 + np.arange(rows)) % channels)
     if live_range is None:
         live = np.full(rows, cols, np.int64)
     else:
@@ -101,9 +101,22 @@ def c2(seed=2, dtype=np.float32, rows=2000):
                        workload="c2")
 
 
-def c5(seed=5, dtype=np.float32, rows=50000):
-    """50000 traces × 6001 samples at 1 ms, live U{4000..6001}."""
-    return shot_gather(rows, 6001, 1.0, seed, dtype, live_range=(4000, 6001), workload="c5")
+def c5(seed=5, dtype=np.float32, rows=50000, shot=5000):
+    """50000 traces × 6001 samples at 1 ms, live U{4000..6001}: consecutive
+    shot gathers of ``shot`` traces, each with its own events and noise
+    (seeded per shot), generated one at a time."""
+    out = None
+    for k, a in enumerate(range(0, rows, shot)):
+        n = min(shot, rows - a)
+        g = shot_gather(n, 6001, 1.0, seed * 65536 + k, dtype, live_range=(4000, 6001), workload="c5",
+                        row0=a)
+        if out is None:
+            out = Gather(np.empty((rows, 6001), dtype), np.empty(rows, np.int32), np.empty(rows, np.int32),
+                         np.zeros(rows), 1.0, np.zeros(0, np.int64))
+        out.data[a:a + n] = g.data
+        out.status[a:a + n] = g.status
+        out.numSamples[a:a + n] = g.numSamples
+    return out
 
 
 def vibroseis_records(pilot, channels=240, samples=10001, sweeps=4, seed=3, p=0.02, noise=0.05,
