@@ -1345,12 +1345,19 @@ static const int64_t kHist = 65536 * 4;
 static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
 static int64_t ws_device_bytes(int64_t rows) { return 512 + align256(rows * 16) + kHist; }
 // The host path streams a block through the device in chunks of about
-// kChunkBytes, one staging buffer per lane stream, so that a block larger
+// chunk_bytes() (4 MiB; PSG_HOST_CHUNK_BYTES overrides), one staging buffer per lane stream, so that a block larger
 // than the device's memory still runs; a plan with a per-panel
 // normalization stages the whole block (its factor reads every row).
-static const int64_t kChunkBytes = 4 << 20;
+static int64_t chunk_bytes() {
+  static const int64_t b = [] {
+    const char* e = getenv("PSG_HOST_CHUNK_BYTES");
+    int64_t v = e ? atoll(e) : 0;
+    return v >= (64 << 10) ? v : (int64_t)(4 << 20);
+  }();
+  return b;
+}
 static int64_t host_chunk_rows(int64_t rows, int32_t cols, int64_t esz) {
-  return std::max<int64_t>(64, std::min<int64_t>(rows, kChunkBytes / std::max<int64_t>(1, cols * esz)));
+  return std::max<int64_t>(16, std::min<int64_t>(rows, chunk_bytes() / std::max<int64_t>(1, cols * esz)));
 }
 static bool host_whole_block(bool needs_panel, int64_t rows, int32_t cols, int64_t esz) {
   return needs_panel || rows <= host_chunk_rows(rows, cols, esz);
