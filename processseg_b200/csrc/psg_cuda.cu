@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <complex>
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
@@ -38,817 +39,11 @@ void set_error(const std::string& m) { t_err = m; }
     if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-// ============================================================ device plan
-struct DevStep {
-  int kind, trend, reflect, zero_dc;
-  int agc_mode, stat, pad, nfft;
-  int half, table_len, need, need_next;
-  double factor, lo, hi, dc_gain, target, epsilon, norm_target, percentile, t_min_ms, dt_ms;
-  FftDesc fft;
-  const void* gain;
-  const void* fall;
-  const void* tw;
-  const void* split;
-  const void* table;
-  psg_gain_curve curve;
-};
+}  // namespace psg
 
-// One apply: a block of rows and the plan steps of one part.
-struct Job {
-  const void* src;  // NULL or == dst: in place
-  void* dst;
-  const int* live;
-  const double* start_ms;
-  const DevStep* steps;
-  long long rows;
-  int cols, first, last, _pad;
-};
+#include "psg_kernel.cuh"
 
-struct PipeArgs {
-  Job job;                     // the apply (single-job launches)
-  const Job* jobs;             // batched launches: the jobs, and the first
-  const long long* row_begin;  // global row of each (ascending)
-  int njobs;
-  long long total_rows;
-  const double* factor;  // the part's panel factor (NaN: none) or NULL
-  int work_off;          // byte offset of the work area
-  int x_bytes;           // bytes of one row buffer (two of them with the bulk prefetch)
-  int* status;           // set to 1 when a bounded wait gives up
-};
-
-// ----------------------------------------------------------- device helpers
-__device__ __forceinline__ bool fin_pos_d(double x) { return isfinite(x) && x > 0; }
-template <class T> __device__ __forceinline__ bool fits_d(double x) {
-  if (!fin_pos_d(x)) return false;
-  double y = (double)(T)x;
-  return isfinite(y) && y > 0;
-}
-
-// Row copies between global buffers and shared memory, 16-byte vectors where
-// the addresses allow it.
-template <class T> __device__ void load_row(const T* __restrict__ g, T* s, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
-}
-template <> __device__ void load_row<float>(const float* __restrict__ g, float* s, int n) {
-  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
-  if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += blockDim.x) s[i] = g[i];
-  int nv = (n - head) >> 2;
-  const float4* gv = reinterpret_cast<const float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
-    float4 q = __ldcs(gv + v);
-    int i = head + 4 * v;
-    s[i] = q.x; s[i + 1] = q.y; s[i + 2] = q.z; s[i + 3] = q.w;
-  }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
-}
-template <class T> __device__ void store_row(const T* s, T* __restrict__ g, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
-}
-template <> __device__ void store_row<float>(const float* s, float* __restrict__ g, int n) {
-  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
-  if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
-  int nv = (n - head) >> 2;
-  float4* gv = reinterpret_cast<float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
-    int i = head + 4 * v;
-    __stcs(gv + v, make_float4(s[i], s[i + 1], s[i + 2], s[i + 3]));
-  }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
-}
-template <class T> __device__ void copy_global(const T* __restrict__ a, T* __restrict__ b, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
-}
-
-// The k-th smallest |x| (0-based) as its bits, by an 8-bit radix selection
-// over the bit patterns in shared memory.
-template <class T>
-__device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* hist, int* sh) {
-  unsigned long long prefix = 0, mask = 0;
-  int kk = k;
-  for (int shift = (int)sizeof(T) * 8 - 8; shift >= 0; shift -= 8) {
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      unsigned long long key = abs_bits(X[i]);
-      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      int lane = threadIdx.x;
-      unsigned c[8], tot = 0;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        c[j] = hist[lane * 8 + j];
-        tot += c[j];
-      }
-      unsigned incl = tot;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += u;
-      }
-      unsigned excl = incl - tot;
-      if ((unsigned)kk >= excl && (unsigned)kk < incl) {
-        unsigned below = excl;
-        int d = 0;
-        for (; d < 8; d++) {
-          if ((unsigned)kk < below + c[d]) break;
-          below += c[d];
-        }
-        sh[0] = lane * 8 + d;
-        sh[1] = kk - (int)below;
-      }
-    }
-    __syncthreads();
-    prefix |= (unsigned long long)sh[0] << shift;
-    mask |= 255ull << shift;
-    kk = sh[1];
-    __syncthreads();
-  }
-  return prefix;
-}
-
-// ------------------------------------------------------------------ steps
-// Statistics a step needs of its input, accumulated in the loop that wrote
-// that input (the load, or the previous step's output loop), so that no step
-// makes a pass of its own for them.
-enum { NEED_S1 = 1, NEED_SI = 2, NEED_S2 = 4, NEED_MX = 8 };
-
-struct Shared {
-  double red[4][32];
-  unsigned long long redu[32];
-  double sv[32];
-  int sf[32];
-  double pv[32];
-  unsigned hist[256];
-  int sh[4];
-  double out[4];
-};
-
-struct Stats {
-  double s1, si, s2, mx;
-};
-
-// Per-thread partial sums: Σx, Σi·x, Σx² in float64 and the largest |x| bits,
-// for the statistics NEED asks for (a compile-time set, so the loops carry
-// no per-sample branch on it).
-template <class T> struct Acc {
-  double s1 = 0, si = 0, s2 = 0;
-  unsigned long long mx = 0;
-  template <int NEED> __device__ __forceinline__ void add(T v, int i) {
-    if (NEED & (NEED_S1 | NEED_SI | NEED_S2)) {
-      double d = (double)v;
-      if (NEED & NEED_S1) s1 += d;
-      if (NEED & NEED_SI) si += (double)i * d;
-      if (NEED & NEED_S2) s2 += d * d;
-    }
-    if (NEED & NEED_MX) {
-      unsigned long long b = abs_bits(v);
-      mx = b > mx ? b : mx;
-    }
-  }
-};
-
-// Calls f with the statistics set `need` as a compile-time constant.
-template <int K> struct NeedC { static constexpr int value = K; };
-template <class F> __device__ __forceinline__ auto with_need(int need, F&& f) {
-  switch (need) {
-    case 0: return f(NeedC<0>());
-    case NEED_S1: return f(NeedC<NEED_S1>());
-    case NEED_S1 | NEED_SI: return f(NeedC<NEED_S1 | NEED_SI>());
-    case NEED_S2: return f(NeedC<NEED_S2>());
-    case NEED_MX: return f(NeedC<NEED_MX>());
-    default: return f(NeedC<NEED_S1 | NEED_SI | NEED_S2 | NEED_MX>());
-  }
-}
-
-// Folds the partial sums over the block. Always ends with a __syncthreads(),
-// so the loop's writes to the trace are visible to the next step.
-template <class T> __device__ __forceinline__ Stats reduce_stats(const Acc<T>& a, int need, Shared& S) {
-  Stats r{0, 0, 0, 0};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if (need == 0) {
-    __syncthreads();
-    return r;
-  }
-  double v0 = a.s1, v1 = a.si, v2 = a.s2;
-  unsigned long long m = a.mx;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    if (need & NEED_S1) v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-    if (need & NEED_SI) v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-    if (need & NEED_S2) v2 += __shfl_xor_sync(0xffffffffu, v2, o);
-    if (need & NEED_MX) {
-      unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
-      m = u > m ? u : m;
-    }
-  }
-  if (lane == 0) {
-    S.red[0][warp] = v0;
-    S.red[1][warp] = v1;
-    S.red[2][warp] = v2;
-    S.redu[warp] = m;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    v0 = lane < nw ? S.red[0][lane] : 0.0;
-    v1 = lane < nw ? S.red[1][lane] : 0.0;
-    v2 = lane < nw ? S.red[2][lane] : 0.0;
-    m = lane < nw ? S.redu[lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-      v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-      v2 += __shfl_xor_sync(0xffffffffu, v2, o);
-      unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
-      m = u > m ? u : m;
-    }
-    if (lane == 0) {
-      S.out[0] = v0;
-      S.out[1] = v1;
-      S.out[2] = v2;
-      S.out[3] = bits_value(m, (T)0);
-    }
-  }
-  __syncthreads();
-  r.s1 = S.out[0];
-  r.si = S.out[1];
-  r.s2 = S.out[2];
-  r.mx = S.out[3];
-  return r;
-}
-
-// The elementwise loop of a step: X[i] = op(X[i], i) over the live samples,
-// accumulating what the next step needs.
-template <class T, class Op>
-__device__ __forceinline__ Stats map_trace(T* X, int n, int need, Shared& S, Op op) {
-  return with_need(need, [&](auto K) {
-    constexpr int NEED = decltype(K)::value;
-    Acc<T> acc;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const T o = op(X[i], i);
-      X[i] = o;
-      acc.template add<NEED>(o, i);
-    }
-    return reduce_stats(acc, NEED, S);
-  });
-}
-
-// A pass over the unchanged trace when a step left it as it was.
-template <class T> __device__ __forceinline__ Stats stats_pass(const T* X, int n, int need, Shared& S) {
-  return with_need(need, [&](auto K) {
-    constexpr int NEED = decltype(K)::value;
-    Acc<T> acc;
-    if (NEED)
-      for (int i = threadIdx.x; i < n; i += blockDim.x) acc.template add<NEED>(X[i], i);
-    return reduce_stats(acc, NEED, S);
-  });
-}
-
-// Loads the live samples into shared memory (16-byte vectors where the row
-// allows), scaled by a panel factor when there is one, accumulating what the
-// first step needs.
-template <class T>
-__device__ __forceinline__ Stats load_trace(const T* __restrict__ g, T* s, int n, bool scale, T k, int need,
-                                            Shared& S) {
-  return with_need(need, [&](auto K) {
-    constexpr int NEED = decltype(K)::value;
-    Acc<T> acc;
-    int head = 0, nv = 0;
-    if (sizeof(T) == 4) {
-      head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
-      if (head > n) head = n;
-      nv = (n - head) >> 2;
-      const float4* gv = reinterpret_cast<const float4*>(g + head);
-      for (int v = threadIdx.x; v < nv; v += blockDim.x) {
-        float4 q = __ldcs(gv + v);
-        const int i = head + 4 * v;
-        T e[4] = {(T)q.x, (T)q.y, (T)q.z, (T)q.w};
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const T y = scale ? e[u] * k : e[u];
-          s[i + u] = y;
-          acc.template add<NEED>(y, i + u);
-        }
-      }
-    }
-    // the unaligned head and the tail
-    const int tail0 = head + 4 * nv;
-    const int rest = head + (n - tail0);
-    for (int t = threadIdx.x; t < rest; t += blockDim.x) {
-      const int i = t < head ? t : tail0 + (t - head);
-      const T y = scale ? g[i] * k : g[i];
-      s[i] = y;
-      acc.template add<NEED>(y, i);
-    }
-    return reduce_stats(acc, NEED, S);
-  });
-}
-
-// filter/edges.nim:16-30, from the sums of the step's input.
-__device__ __forceinline__ void trend_from(int trend, const Stats& st, int n, double& a, double& b) {
-  a = 0;
-  b = 0;
-  if (trend == PSG_TR_NONE) return;
-  double nf = (double)n, mean = st.s1 / nf;
-  if (trend == PSG_TR_MEAN || n == 1) {
-    a = mean;
-    return;
-  }
-  double c = (nf - 1) / 2;
-  double slope = (st.si - c * st.s1) / (nf * (nf * nf - 1) / 12);
-  a = mean - slope * c;
-  b = slope;
-}
-
-// The zero-phase FFT filter with the reference's edge handling
-// (filter/apply.nim:194-231, 340-363) on the trace in shared memory.
-template <class T, int MAXR>
-__device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
-  typedef typename C2<T>::type V;
-  const int p = st.pad, nfft = st.nfft, m = nfft / 2;
-  const InShared mem;
-  const int ao = work_off / (int)sizeof(V), bo = ao + m;  // offsets of the two buffers
-  V* A = reinterpret_cast<V*>(psg_dyn_smem) + ao;
-  double a, b;
-  trend_from(st.trend, in, n, a, b);
-  const T* fall = reinterpret_cast<const T*>(st.fall);
-  T* Ar = reinterpret_cast<T*>(A);
-  // packInto: the detrended samples at p .. p+n, odd reflections tapered by
-  // `fall` (or zeros) in the pads, zeros to nfft.
-  for (int j = threadIdx.x; j < nfft; j += blockDim.x) {
-    T v = (T)0;
-    const int i = j - p;
-    if (i >= 0 && i < n) {
-      v = (T)((double)X[i] - (a + b * (double)i));
-    } else if (st.reflect && i < 0) {
-      int k = -i, ii = min(k, n - 1);
-      T d0 = (T)((double)X[0] - a);
-      T r = (T)((double)X[ii] - (a + b * (double)ii));
-      v = (d0 + d0 - r) * __ldg(&fall[k - 1]);
-    } else if (st.reflect && i >= n && i < n + p) {
-      int k = i - (n - 1), ii = n - 1 - min(k, n - 1);
-      T dn = (T)((double)X[n - 1] - (a + b * (double)(n - 1)));
-      T r = (T)((double)X[ii] - (a + b * (double)ii));
-      v = (dn + dn - r) * __ldg(&fall[k - 1]);
-    }
-    Ar[j] = v;
-  }
-  __syncthreads();
-  const V* tw = reinterpret_cast<const V*>(st.tw);
-  const V* split = reinterpret_cast<const V*>(st.split);
-  const T* gain = reinterpret_cast<const T*>(st.gain);
-  const int zo = cfft_forward<T, MAXR>(mem, ao, bo, st.fft, tw);
-  split_mul_unsplit<T>(mem, zo, m, split, (T)1 / (T)nfft, [&](V x, int k) {
-    T g = __ldg(&gain[k]);
-    return V{x.x * g, x.y * g};
-  });
-  const int yo = cfft_forward<T, MAXR>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
-  const V* y = reinterpret_cast<const V*>(psg_dyn_smem) + yo;
-  // unpackFrom: the output is swap(y); sample 2k is y[k].im, 2k+1 is y[k].re.
-  const double gb = b * st.dc_gain;
-  const double ga = st.zero_dc ? -gb * (double)(n - 1) / 2 : a * st.dc_gain;
-  const bool plain = ga == 0 && gb == 0;
-  return map_trace(X, n, st.need_next, S, [&](T, int i) {
-    const int idx = p + i;
-    const V c = y[idx >> 1];
-    const T v = (idx & 1) ? c.x : c.y;
-    return plain ? v : (T)((double)v + (ga + gb * (double)i));
-  });
-}
-
-// An exclusive scan over the threads, in thread order (or reversed), of
-// segment sums that restart where a segment starts a new AGC block: the
-// running sum carried into each thread's segment.
-template <bool REV> __device__ double carry_scan(double v, bool f, Shared& S) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  int ff = f ? 1 : 0;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    double vv = REV ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
-    int fo = REV ? __shfl_down_sync(0xffffffffu, ff, o) : __shfl_up_sync(0xffffffffu, ff, o);
-    bool in = REV ? lane + o < 32 : lane >= o;
-    if (in) {
-      if (!ff) v += vv;
-      ff |= fo;
-    }
-  }
-  // warp totals: the last lane in scan order holds its warp's inclusive value
-  if (lane == (REV ? 0 : 31)) {
-    S.sv[warp] = v;
-    S.sf[warp] = ff;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    // exclusive scan of the warp totals in scan order
-    int wi = REV ? nw - 1 - lane : lane;  // position of this lane's warp in scan order
-    double wv = (lane < nw) ? S.sv[REV ? (nw - 1 - lane) : lane] : 0.0;
-    int wf = (lane < nw) ? S.sf[REV ? (nw - 1 - lane) : lane] : 0;
-    (void)wi;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      double vv = __shfl_up_sync(0xffffffffu, wv, o);
-      int fo = __shfl_up_sync(0xffffffffu, wf, o);
-      if (lane >= o) {
-        if (!wf) wv += vv;
-        wf |= fo;
-      }
-    }
-    double ex = __shfl_up_sync(0xffffffffu, wv, 1);
-    if (lane == 0) ex = 0.0;
-    if (lane < nw) S.pv[REV ? (nw - 1 - lane) : lane] = ex;
-  }
-  __syncthreads();
-  const double cw = S.pv[warp];
-  const double incl = ff ? v : v + cw;
-  double prev = REV ? __shfl_down_sync(0xffffffffu, incl, 1) : __shfl_up_sync(0xffffffffu, incl, 1);
-  if (lane == (REV ? 31 : 0)) prev = cw;
-  return prev;
-}
-
-// AGC (gain/gain.nim:351-461). Window sums come from per-block prefix and
-// suffix sums of the terms in float64 (blocks of w = 2h + 1 samples, no
-// subtraction): each thread runs them over a contiguous segment of the trace
-// and a segmented scan across the threads carries the sums between
-// segments. The prefix and suffix arrays are stored as T; each window mean
-// is formed in float64 and rounded once to T, and the gain step runs in T on
-// means scaled by the trace RMS.
-template <class T>
-__device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
-  const int need = st.need_next;
-  const bool rms_mode = st.agc_mode == PSG_AGC_RMS;
-  const double rms = sqrt(in.s2 / (double)n);
-  if (rms == 0 || !fits_d<T>(st.target / rms / st.epsilon)) return stats_pass(X, n, need, S);
-  const int h = st.half, w = 2 * h + 1;
-  T* P = reinterpret_cast<T*>(psg_dyn_smem + work_off);  // n + 1 values
-  T* Sx = P + ((n + 1 + 3) & ~3);          // n values
-  // An odd segment length keeps the strided reads free of bank conflicts.
-  int seg = (n + blockDim.x - 1) / blockDim.x;
-  seg |= 1;
-  const int g0 = min((int)threadIdx.x * seg, n), g1 = min(g0 + seg, n);
-  auto term = [&](int g) {
-    const double v = (double)X[g];
-    return rms_mode ? v * v : fabs(v);
-  };
-  // The first block start at or after g0, and the last block end (a sample
-  // whose successor starts a block) at or before g1 − 1.
-  const int firstStart = g0 + (g0 % w == 0 ? 0 : w - g0 % w);
-  const int lastEnd = g1 - 1 - ((g1 % w) == 0 ? 0 : (g1 % w));  // (lastEnd + 1) % w == 0
-  // Local sums: the prefix chain restarts at block starts, the suffix chain
-  // (run backwards) at block ends; between those the loops have no branch.
-  double rp = 0, rs = 0;
-  bool fp = false, fs = false;
-  {
-    int g = g0;
-    int next = firstStart;
-    while (g < g1) {
-      if (g == next) {
-        rp = 0;
-        fp = true;
-        next += w;
-      }
-      const int stop = min(g1, next);
-      for (; g < stop; g++) rp += term(g);
-    }
-    g = g1 - 1;
-    int end = lastEnd;
-    while (g >= g0) {
-      if (g == end) {
-        rs = 0;
-        fs = true;
-        end -= w;
-      }
-      const int stop = max(g0 - 1, end);
-      for (; g > stop; g--) rs += term(g);
-    }
-  }
-  const double cp = carry_scan<false>(g0 < g1 ? rp : 0.0, fp, S);
-  const double cs = carry_scan<true>(g0 < g1 ? rs : 0.0, fs, S);
-  {
-    // p[e]: the sum from the block start to e − 1, 0 at a block start;
-    // p[n] is the last block's sum unless n starts a block.
-    double run = cp;
-    int g = g0;
-    int next = firstStart;
-    while (g < g1) {
-      if (g == next) {
-        run = 0;
-        P[g] = (T)0;
-        next += w;
-      }
-      const int stop = min(g1, next);
-      for (; g < stop; g++) {
-        run += term(g);
-        if (g + 1 != next) P[g + 1] = (T)run;
-      }
-    }
-    if (g1 == n && g0 < g1 && n % w == 0) P[n] = (T)0;
-    // s[i]: the sum from i to its block's end (or n − 1)
-    run = cs;
-    g = g1 - 1;
-    int end = lastEnd;
-    while (g >= g0) {
-      if (g == end) {
-        run = 0;
-        end -= w;
-      }
-      const int stop = max(g0 - 1, end);
-      for (; g > stop; g--) {
-        run += term(g);
-        Sx[g] = (T)run;
-      }
-    }
-  }
-  __syncthreads();
-  const double unit = rms_mode ? 1 / (rms * rms) : 1 / rms;
-  const T k = (T)(st.target / rms), eps = (T)st.epsilon;
-  const int first = min(h, n), last = max(first, n - h);
-  const int headCut = min(max(n - h, 0), first);
-  const int lastBlock = (n - 1) / w * w;
-  const int tailCut = min(max(lastBlock + h, last), n);
-  const T pn = P[n];
-  const double unitWd = unit / (double)w;
-  const T headWhole = headCut < first ? (T)((double)pn * unit * (1 / (double)n)) : (T)0;
-  return map_trace(X, n, need, S, [&](T x, int i) {
-    T mean;
-    // the window mean in float64, rounded once to T, as the reference
-    if (i >= first && i < last) mean = (T)(((double)Sx[i - h] + (double)P[i + h + 1]) * unitWd);
-    else if (i < headCut) mean = (T)((double)P[i + h + 1] * (unit * (1 / (double)(i + h + 1))));
-    else if (i < first) mean = headWhole;
-    else if (i < tailCut) mean = (T)(((double)Sx[i - h] + (double)pn) * (unit * (1 / (double)(w - (i + h + 1 - n)))));
-    else mean = (T)((double)Sx[i - h] * (unit * (1 / (double)(w - (i + h + 1 - n)))));
-    // levelOf in T, correctly rounded (gain/gain.nim:392-402)
-    const T lv = rms_mode ? sqrt(mean) : mean;
-    const T gi = k / (lv + eps);
-    return (T)(x * gi);
-  });
-}
-
-// Per-trace normalization (gain/gain.nim:198-219; stats.nim:129-182).
-template <class T>
-__device__ __forceinline__ Stats step_norm_trace(const DevStep& st, const Stats& in, T* X, int n, Shared& S) {
-  const int need = st.need_next;
-  double level;
-  if (st.stat == PSG_NORM_MAX) {
-    level = in.mx;
-  } else if (st.stat == PSG_NORM_RMS) {
-    level = sqrt(in.s2 / (double)n);
-  } else if (isnan(in.mx)) {
-    level = in.mx;
-  } else {
-    double hr = (double)(n - 1) * st.percentile / 100;
-    int k = min((int)floor(hr), n - 1);
-    double lower = bits_value(select_kth(X, n, k, S.hist, S.sh), (T)0);
-    if (k + 1 >= n) {
-      level = lower;
-    } else {
-      double upper = bits_value(select_kth(X, n, k + 1, S.hist, S.sh), (T)0);
-      double f = hr - (double)k;
-      level = f == 0 ? lower : lower + f * (upper - lower);
-    }
-  }
-  if (!(fin_pos_d(level) && fits_d<T>(st.norm_target / level))) return stats_pass(X, n, need, S);
-  const T kf = (T)(st.norm_target / level);
-  return map_trace(X, n, need, S, [&](T x, int) { return x * kf; });
-}
-
-// gain/curves.nim:132-160 on the device, in float64.
-__device__ double factor_at_d(const psg_gain_curve& c, double t) {
-  if (isnan(t)) return t;
-  if (c.kind == PSG_GC_POWER) return pow(fmax(t, c.min_ms) / c.ref_ms, c.power);
-  double db;
-  if (c.kind == PSG_GC_KNOTS) {
-    int nk = c.n_knots;
-    if (t <= c.knots[0].t_ms) db = c.knots[0].db;
-    else if (t >= c.knots[nk - 1].t_ms) db = c.knots[nk - 1].db;
-    else {
-      int lo = 0, hi = nk - 1;
-      while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (c.knots[mid].t_ms <= t) lo = mid; else hi = mid;
-      }
-      double f = (t - c.knots[lo].t_ms) / (c.knots[hi].t_ms - c.knots[lo].t_ms);
-      db = c.knots[lo].db + f * (c.knots[hi].db - c.knots[lo].db);
-    }
-  } else {
-    db = c.db_per_s * t / 1000;
-  }
-  return pow(10.0, db / 20);
-}
-
-// The gain curve on one row (gain/curves.nim:316-350 and the workspace form
-// :383-418): the table where the row's times fall on it (as it is on the
-// grid, linearly interpolated off it), the curve itself elsewhere.
-template <class T>
-__device__ __forceinline__ Stats step_gain_curve(const DevStep& st, T* X, int n, double start, Shared& S) {
-  const int need = st.need_next;
-  if (isnan(start)) return stats_pass(X, n, need, S);
-  const T* tab = reinterpret_cast<const T*>(st.table);
-  double u = (start - st.t_min_ms) / st.dt_ms;
-  long long s = 0, j0 = n, j1 = n;
-  double f = 0;
-  bool on = false;
-  if (isfinite(u) && fabs(u) <= 1e15) {
-    double r = round(u);
-    on = fabs(u - r) <= 1e-9 * fmax(1.0, fabs(u));
-    s = (long long)(on ? r : floor(u));
-    f = u - (double)s;
-    long long last = (long long)st.table_len - (on ? 1 : 2);
-    j0 = min(max(-s, 0ll), (long long)n);
-    j1 = min(max(last - s + 1, j0), (long long)n);
-  }
-  const T tf = (T)f;
-  return map_trace(X, n, need, S, [&](T v, int j) {
-    if (j >= j0 && j < j1) {
-      T a = __ldg(&tab[s + j]);
-      return on ? v * a : v * (a + tf * (__ldg(&tab[s + j + 1]) - a));
-    }
-    if (v != (T)0) return v * (T)factor_at_d(st.curve, start + (double)j * st.dt_ms);
-    return v;
-  });
-}
-
-// ------------------------------------------------------------ the kernel
-// Stores a row from shared memory, 16-byte vectors where the row allows.
-template <class T> __device__ __forceinline__ void store_out(const T* s, T* __restrict__ g, int n) {
-  if (sizeof(T) == 4) {
-    const int head = min((int)((4 - (((uintptr_t)g >> 2) & 3)) & 3), n);
-    const int nv = (n - head) >> 2;
-    for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
-    float4* gv = reinterpret_cast<float4*>(g + head);
-    const float* sf = reinterpret_cast<const float*>(s) + head;
-    for (int v = threadIdx.x; v < nv; v += blockDim.x)
-      __stcs(gv + v, make_float4(sf[4 * v], sf[4 * v + 1], sf[4 * v + 2], sf[4 * v + 3]));
-    for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
-  } else {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
-  }
-}
-
-struct RowSlot {
-  int head, body, len, off;  // ragged head (elements), bulk bytes, elements, byte offset of X in the buffer
-};
-
-// What one row of a launch needs: its job's pointers and plan, and its live
-// length. Batched launches find the job by a binary search of row_begin.
-template <class T> struct RowCtx {
-  const T* from;  // the row to read (src, or dst in place)
-  T* to;          // the row to write
-  const DevStep* steps;
-  double start;
-  int n, cols, first, last;
-  bool copy;
-};
-template <class T, bool BATCH>
-__device__ __forceinline__ RowCtx<T> row_ctx(const PipeArgs& a, long long t) {
-  long long r = t;
-  const Job* J = &a.job;
-  if (BATCH) {
-    int lo = 0, hi = a.njobs - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (a.row_begin[mid] <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    J = &a.jobs[lo];
-    r = t - a.row_begin[lo];
-  }
-  RowCtx<T> c;
-  const T* src = reinterpret_cast<const T*>(J->src);
-  T* dst = reinterpret_cast<T*>(J->dst);
-  c.copy = src != nullptr && src != dst;
-  c.cols = J->cols;
-  c.from = (c.copy ? src : dst) + r * (long long)c.cols;
-  c.to = dst + r * (long long)c.cols;
-  c.n = min(max(J->live[r], 0), c.cols);
-  c.start = J->start_ms ? J->start_ms[r] : (double)NAN;
-  c.steps = J->steps;
-  c.first = J->first;
-  c.last = J->last;
-  return c;
-}
-
-// PF: prefetch the next row into the second buffer while this one is
-// processed (when the second buffer costs no occupancy); otherwise one buffer,
-// loaded at the top of each row. BATCH: the rows of several jobs (several
-// plans, widths and blocks) in one launch.
-template <class T, int MAXR, bool PF, bool BATCH>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
-  __shared__ Shared S;
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ RowSlot slot[2];
-  const double pf = a.factor ? *a.factor : (double)NAN;
-  const bool scale = !isnan(pf);
-  const T kf = scale ? (T)pf : (T)1;
-  const long long total = BATCH ? a.total_rows : a.job.rows;
-  constexpr int esz = (int)sizeof(T);
-  // Thread 0 starts the bulk copy of row t into buffer b: the 16-byte aligned
-  // body of the part we need (the whole row for src → dst, the live samples
-  // in place); the few ragged elements at either end are read directly.
-  auto issue = [&](long long t, int b) {
-    const RowCtx<T> c = row_ctx<T, BATCH>(a, t);
-    int len = c.copy ? c.cols : c.n;
-    uintptr_t ga = (uintptr_t)c.from;
-    int head = min((int)(((16 - (ga & 15)) & 15) / esz), len);
-    int body = ((len - head) * esz) & ~15;
-    int off = (16 - (head * esz) % 16) % 16;
-    unsigned char* xb = psg_dyn_smem + b * a.x_bytes;
-    slot[b] = RowSlot{head, body, len, off};
-    if (body > 0) {
-      mbar_arrive_expect_tx(&bars[b], (uint32_t)body);
-      bulk_load(xb + off + head * esz, c.from + head, (uint32_t)body, &bars[b]);
-    } else {
-      mbar_arrive(&bars[b]);
-    }
-  };
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_init_fence();
-    if (PF && blockIdx.x < total) issue(blockIdx.x, 0);
-  }
-  __syncthreads();
-  uint32_t phase[2] = {0, 0};
-  int cur = 0;
-  for (long long t = blockIdx.x; t < total; t += gridDim.x, cur = PF ? cur ^ 1 : 0) {
-    const long long tn = t + gridDim.x;
-    if (threadIdx.x == 0) {
-      // the buffer's last reads (the previous row's store) come before the copy into it
-      if (PF && tn < total) {
-        fence_proxy_async();
-        issue(tn, cur ^ 1);
-      } else if (!PF) {
-        fence_proxy_async();
-        issue(t, 0);
-      }
-    }
-    if (!mbar_wait(&bars[cur], phase[cur], 1ll << 26)) {
-      if (threadIdx.x == 0) atomicExch(a.status, 1);
-      mbar_wait(&bars[cur], phase[cur], 1ll << 26);
-      return;
-    }
-    phase[cur] ^= 1;
-    const RowCtx<T> c = row_ctx<T, BATCH>(a, t);
-    const RowSlot sl = slot[cur];
-    T* X = reinterpret_cast<T*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
-    const int tail0 = sl.head + sl.body / esz;
-    for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = c.from[i];
-    for (int i = tail0 + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = c.from[i];
-    __syncthreads();  // the ragged ends are read by other threads below
-    const int n = c.n;
-    const int need0 = c.first < c.last ? c.steps[c.first].need : 0;
-    Stats st{0, 0, 0, 0};
-    if (n > 0) {
-      // the panel factor of a part that starts with one, and the first
-      // step's statistics
-      if (scale) st = map_trace(X, n, need0, S, [&](T x, int) { return x * kf; });
-      else st = stats_pass(X, n, need0, S);
-    } else {
-      __syncthreads();
-    }
-    for (int si = c.first; n > 0 && si < c.last; si++) {
-      const DevStep& d = c.steps[si];
-      const int need = d.need_next;
-      switch (d.kind) {
-        case ST_DEMEAN: {
-          const T mean = (T)(st.s1 / (double)n);
-          st = map_trace(X, n, need, S, [&](T x, int) { return x - mean; });
-          break;
-        }
-        case ST_DETREND: {
-          double nf = (double)n, cc = (nf - 1) / 2, mean = st.s1 / nf;
-          double stt = nf * (nf * nf - 1) / 12;
-          double slope = n > 1 ? (st.si - cc * st.s1) / stt : 0.0;
-          const T ta = (T)(mean - slope * cc), tb = (T)slope;
-          st = map_trace(X, n, need, S, [&](T x, int i) { return x - (ta + tb * (T)i); });
-          break;
-        }
-        case ST_SCALE: {
-          const T k = (T)d.factor;
-          st = map_trace(X, n, need, S, [&](T x, int) { return x * k; });
-          break;
-        }
-        case ST_CLIP: {
-          const T lo = (T)d.lo, hi = (T)d.hi;
-          st = map_trace(X, n, need, S, [&](T v, int) { return v > hi ? hi : (v < lo ? lo : v); });
-          break;
-        }
-        case ST_POLARITY:
-          st = map_trace(X, n, need, S, [&](T x, int) { return -x; });
-          break;
-        case ST_FILTER: st = step_filter<T, MAXR>(d, st, X, n, a.work_off, S); break;
-        case ST_AGC: st = step_agc(d, st, X, n, a.work_off, S); break;
-        case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
-        case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, c.start, S); break;
-        default: break;
-      }
-    }
-    if (c.copy || n > 0) store_out(X, c.to, c.copy ? c.cols : n);
-    __syncthreads();
-  }
-}
+namespace psg {
 
 // ======================================================= panel statistics
 // gain/stats.nim:253-304: per row Σx² and max |x| (pass 1), then one CTA
@@ -1058,9 +253,8 @@ struct CorrArgs {
   long long rows;
   int cols, out, nfft, shift, pilot_len, record;
   const int* live;
-  const void* mul;    // V[bins]
+  const void* bridge;  // Quad<T>[m]: the split · multiplier · unsplit map of each bin pair
   const void* tw;
-  const void* split;
   FftDesc fft;
   void* gwork;        // per-CTA global scratch when shared memory is too small (else NULL)
   // stack epilogue
@@ -1082,9 +276,7 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
   V* buf = reinterpret_cast<V*>(mem.base());
   const T* src = reinterpret_cast<const T*>(a.src);
   T* dst = reinterpret_cast<T*>(a.dst);
-  const V* mul = reinterpret_cast<const V*>(a.mul);
   const V* tw = reinterpret_cast<const V*>(a.tw);
-  const V* split = reinterpret_cast<const V*>(a.split);
   const int wrapped = min(max(1 - a.pilot_len - a.shift, 0), a.out);
   const int direct = min(max(-a.shift, wrapped), a.out);
   const int last = min(max(a.record - a.shift, direct), a.out);
@@ -1098,10 +290,7 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
       __syncthreads();
       constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
       const int zo = cfft_forward<T, MAXR>(mem, 0, m, a.fft, tw);
-      split_mul_unsplit<T>(mem, zo, m, split, (T)1 / (T)a.nfft, [&](V v, int k) {
-        V w = __ldg(&mul[k]);
-        return V{v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x};
-      });
+      split_bridge<T>(mem, zo, m, reinterpret_cast<const Quad<T>*>(a.bridge));
       y = buf + cfft_forward<T, MAXR>(mem, zo, zo == 0 ? m : 0, a.fft, tw);
     }
     // lagSpans / scatter: the output at column c reads lag c + shift
@@ -1211,7 +400,7 @@ static void ensure_device() {
   }
 }
 
-template <class K> static void allow_smem(K kernel) {
+static void allow_smem(const void* kernel) {
   CUDA_OK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_max_smem - (int)sizeof(Shared) - 1024));
 }
 
@@ -1240,18 +429,45 @@ static std::vector<typename C2<T>::type> as_c(const std::vector<double>& re, con
   for (size_t i = 0; i < re.size(); i++) o[i] = {(T)re[i], (T)im[i]};
   return o;
 }
+// The split · multiplier · unsplit map of each pair of bins (split_bridge):
+// for k ≥ 1, with ω = exp(−2πik/n), c1 = 1 + i·conj ω, c2 = 1 − i·conj ω,
+// a1 = (1 − iω)/2, a2 = (1 + iω)/2 and j = m − k:
+//   A = c1·a1·M[k] + c2·conj(c2)/2·conj M[j],  B = c1·a2·M[k] + c2·conj(c1)/2·conj M[j],
+//   A' = i·conj(A)/n,  B' = i·conj(B)/n;
+// bin 0 holds (Re M[0]/n, Re M[m]/n). Computed in float64, rounded to T.
+template <class T>
+static std::vector<Quad<T>> bridge_table(const FftTables& f, const std::vector<double>& mre, const std::vector<double>& mim) {
+  typedef std::complex<double> cd;
+  const int64_t m = f.m;
+  const double scale = 1.0 / (double)f.n;
+  if ((int64_t)mre.size() < m + 1 || (int64_t)mim.size() < m + 1) throw InvalidArg("a bin multiplier shorter than m + 1");
+  std::vector<Quad<T>> ab((size_t)m);
+  ab[0] = Quad<T>{(T)(mre[0] * scale), (T)(mre[m] * scale), (T)0, (T)0};
+  const cd I(0, 1);
+  for (int64_t k = 1; k < m; k++) {
+    const int64_t j = m - k;
+    const cd w(f.split_re[k], f.split_im[k]);
+    const cd c1 = 1.0 + I * std::conj(w), c2 = 1.0 - I * std::conj(w);
+    const cd a1 = (1.0 - I * w) / 2.0, a2 = (1.0 + I * w) / 2.0;
+    const cd Mk(mre[k], mim[k]), Mj(mre[j], mim[j]);
+    const cd A = c1 * a1 * Mk + c2 * std::conj(c2) / 2.0 * std::conj(Mj);
+    const cd B = c1 * a2 * Mk + c2 * std::conj(c1) / 2.0 * std::conj(Mj);
+    const cd Ap = I * std::conj(A) * scale, Bp = I * std::conj(B) * scale;
+    ab[k] = Quad<T>{(T)Ap.real(), (T)Ap.imag(), (T)Bp.real(), (T)Bp.imag()};
+  }
+  return ab;
+}
+
 static FftDesc fft_desc(const FftTables& t) {
   FftDesc d{};
   d.m = (int)t.m;
   d.npass = (int)t.radices.size();
   if (d.npass > 24) throw InvalidArg("an FFT of more than 24 passes");
-  int64_t cur = t.m, off = 0;
+  unsigned long long st = 1;  // the product of the earlier radices
   for (int i = 0; i < d.npass; i++) {
     d.radix[i] = t.radices[i];
-    d.twoff[i] = (int)off;
-    int64_t sub = cur / t.radices[i];
-    off += sub * (t.radices[i] - 1);
-    cur = sub;
+    d.magic[i] = st == 1 ? 0u : (unsigned)((1ull << 32) / st + ((1ull << 32) % st != 0));  // ⌈2^32 / s⌉
+    st *= (unsigned long long)t.radices[i];
   }
   return d;
 }
@@ -1270,6 +486,7 @@ struct psg_plan {
   int device = 0;
   int threads = 256;
   int max_radix = 12;  // the largest FFT radix compiled into the plan's kernel
+  std::vector<int> recipe;  // per part: the recipe kernel that runs it (RC_GENERIC: the step switch)
   int x_elems = 0, work_off = 0, x_bytes = 0;
   bool prefetch = false;
   size_t smem = 0;
@@ -1292,9 +509,8 @@ struct psg_corr_plan {
   CorrHost host;
   int dtype = 0;
   std::vector<std::unique_ptr<DeviceBuf>> keep;
-  void* mul = nullptr;
+  void* bridge = nullptr;
   void* tw = nullptr;
-  void* split = nullptr;
   void* gwork = nullptr;
   size_t smem = 0;
   int grid = 1;
@@ -1370,16 +586,31 @@ static int64_t ws_host_bytes(bool needs_panel, int64_t rows, int32_t cols, int d
   return ws_device_bytes(rows) + align256(rows * 4) + align256(rows * 8) + align256(stage_rows * (int64_t)cols * esz);
 }
 
-// The pipeline kernel of a sample type and largest radix.
-template <class T> static void (*pipe_kernel_for(int max_radix, bool pf))(PipeArgs) {
-  if (sizeof(T) == 8 || max_radix <= 8)
-    return pf ? pipeline_kernel<T, 8, true, false> : pipeline_kernel<T, 8, false, false>;
-  return pf ? pipeline_kernel<T, 12, true, false> : pipeline_kernel<T, 12, false, false>;
+// The pipeline kernel of a sample type and largest radix (psg_pipe_f32.cu,
+// psg_pipe_f64.cu).
+template <class T> static const void* pipe_kernel_for(int recipe, bool pf) {
+  return sizeof(T) == 4 ? pipe_kernel_f32(recipe, pf, false) : pipe_kernel_f64(recipe, pf);
 }
-// The batched form (float32 plans of one largest radix).
-static void (*batch_kernel_for(int max_radix, bool pf))(PipeArgs) {
-  if (max_radix <= 8) return pf ? pipeline_kernel<float, 8, true, true> : pipeline_kernel<float, 8, false, true>;
-  return pf ? pipeline_kernel<float, 12, true, true> : pipeline_kernel<float, 12, false, true>;
+// The batched form (float32 plans, any step sequence).
+static const void* batch_kernel_for(bool pf) { return pipe_kernel_f32(RC_GENERIC, pf, true); }
+
+// The recipe that runs steps [first, last) of a plan, by their kinds;
+// PSG_RECIPES=0 in the environment (read at compile time) keeps every plan on
+// the step switch.
+static int recipe_of(const PlanHost& h, int first, int last) {
+  if (const char* e = getenv("PSG_RECIPES"))
+    if (atoi(e) == 0) return RC_GENERIC;
+  std::vector<int> k;
+  for (int i = first; i < last; i++) k.push_back(h.steps[i].kind);
+  if (k == std::vector<int>{ST_DEMEAN, ST_FILTER, ST_AGC}) return RC_DFA;
+  if (k == std::vector<int>{ST_DEMEAN, ST_FILTER, ST_AGC, ST_NORM_TRACE}) return RC_DFAN;
+  if (k == std::vector<int>{ST_FILTER, ST_NORM_TRACE}) return RC_FN;
+  if (k == std::vector<int>{ST_FILTER, ST_GAIN_CURVE}) return RC_FG;
+  return RC_GENERIC;
+}
+static void launch_pipe(const void* kernel, int grid, int threads, size_t smem, cudaStream_t stream, PipeArgs& a) {
+  void* args[] = {&a};
+  CUDA_OK(cudaLaunchKernel(kernel, dim3(grid), dim3(threads), args, smem, stream));
 }
 
 template <class T> static void build_device_steps(psg_plan* p) {
@@ -1403,10 +634,9 @@ template <class T> static void build_device_steps(psg_plan* p) {
       d.nfft = (int)f.nfft;
       d.dc_gain = f.dc_gain;
       d.fft = fft_desc(f.fft);
-      d.gain = upload(p->keep, as_t<T>(f.gain));
+      d.bridge = upload(p->keep, bridge_table<T>(f.fft, f.gain, std::vector<double>(f.gain.size(), 0.0)));
       d.fall = upload(p->keep, as_t<T>(f.fall));
       d.tw = upload(p->keep, as_c<T>(f.fft.tw_re, f.fft.tw_im));
-      d.split = upload(p->keep, as_c<T>(f.fft.split_re, f.fft.split_im));
       work = std::max<int64_t>(work, 2 * f.fft.m * (int64_t)sizeof(V));
     } else if (s.kind == ST_AGC) {
       d.half = (int)s.half;
@@ -1451,7 +681,7 @@ template <class T> static void build_device_steps(psg_plan* p) {
   p->x_bytes = (int)align256((p->host.samples + 8) * (int64_t)sizeof(T));
   auto occupancy = [&](bool pf) {
     size_t sm = (size_t)((pf ? 2 : 1) * p->x_bytes + work);
-    auto k = pipe_kernel_for<T>(p->max_radix, pf);
+    auto k = pipe_kernel_for<T>(RC_GENERIC, pf);
     allow_smem(k);
     int per_sm = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, p->threads, sm));
@@ -1473,7 +703,7 @@ template <class T> static void build_device_steps(psg_plan* p) {
     CUDA_OK(cudaMemcpy(b->p, ds.data(), ds.size() * sizeof(DevStep), cudaMemcpyHostToDevice));
     p->d_steps = (DevStep*)b->p;
   }
-  auto kern = pipe_kernel_for<T>(p->max_radix, p->prefetch);
+  auto kern = pipe_kernel_for<T>(RC_GENERIC, p->prefetch);
   allow_smem(kern);
   int per_sm = 0;
   CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p->threads, p->smem));
@@ -1535,8 +765,9 @@ static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void*
   bool nothing = a.job.first >= a.job.last && !factor && (src == nullptr || src == dst);
   if (nothing || rows == 0) return;
   int grid = (int)std::min<int64_t>(rows, p->grid);
-  pipe_kernel_for<T>(p->max_radix, p->prefetch)<<<grid, p->threads, p->smem, stream>>>(a);
-  CUDA_OK(cudaGetLastError());
+  const void* kern = pipe_kernel_for<T>(p->recipe[part], p->prefetch);
+  allow_smem(kern);
+  launch_pipe(kern, grid, p->threads, p->smem, stream, a);
 }
 
 template <class T>
@@ -1550,13 +781,12 @@ static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const vo
 
 template <class T> static void corr_upload(psg_corr_plan* p) {
   typedef typename C2<T>::type V;
-  p->mul = upload(p->keep, as_c<T>(p->host.mul_re, p->host.mul_im));
+  p->bridge = upload(p->keep, bridge_table<T>(p->host.fft, p->host.mul_re, p->host.mul_im));
   p->tw = upload(p->keep, as_c<T>(p->host.fft.tw_re, p->host.fft.tw_im));
-  p->split = upload(p->keep, as_c<T>(p->host.fft.split_re, p->host.fft.split_im));
   p->fft = fft_desc(p->host.fft);
   size_t need = (size_t)(2 * p->host.fft.m * sizeof(V));
   int limit = g_max_smem - (int)sizeof(Shared) - 1024;
-  allow_smem(corr_kernel<T>);
+  allow_smem((const void*)corr_kernel<T>);
   if ((int64_t)need <= limit) {
     p->smem = need;
     int per_sm = 0;
@@ -1620,8 +850,11 @@ int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_
     *out = nullptr;
     std::unique_ptr<psg_plan> p(new psg_plan());
     p->max_radix = dtype == PSG_F32 ? 12 : 8;
-    if (const char* e = getenv("PSG_MAX_RADIX")) p->max_radix = std::min(p->max_radix, std::max(2, atoi(e)));
     p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples, p->max_radix);
+    for (auto& r : p->host.parts) {
+      const bool panel = r.first < r.second && p->host.steps[r.first].kind == ST_NORM_PANEL;
+      p->recipe.push_back(recipe_of(p->host, panel ? r.first + 1 : r.first, r.second));
+    }
     ensure_device();
     CUDA_OK(cudaGetDevice(&p->device));
     if (dtype == PSG_F32) build_device_steps<float>(p.get());
@@ -2108,9 +1341,8 @@ static int corr_launch(const psg_corr_plan* plan, psg_stack* st, const void* src
     a.pilot_len = (int)plan->host.pilot_len;
     a.record = (int)plan->host.record;
     a.live = live;
-    a.mul = plan->mul;
+    a.bridge = plan->bridge;
     a.tw = plan->tw;
-    a.split = plan->split;
     a.fft = plan->fft;
     a.gwork = plan->gwork;
     if (st) {
@@ -2422,7 +1654,7 @@ void launch_batch(psg_server* S) {
   Job* jh = S->jobs_h + slot * psg_server::kMaxJobs;
   long long* bh = S->begin_h + slot * psg_server::kMaxJobs;
   long long total = 0;
-  int xb = 0, maxr = 12;
+  int xb = 0;
   size_t work = 0;
   for (size_t i = 0; i < take; i++) {
     Req* r = b->reqs[i];
@@ -2444,7 +1676,6 @@ void launch_batch(psg_server* S) {
     total += r->rows;
     xb = std::max(xb, p->x_bytes);
     work = std::max(work, p->smem - (size_t)p->work_off);
-    maxr = std::min(maxr, p->max_radix);
   }
   CUDA_OK(cudaMemcpyAsync(S->jobs_d + slot * psg_server::kMaxJobs, jh, take * sizeof(Job), cudaMemcpyHostToDevice, S->s_comp));
   CUDA_OK(cudaMemcpyAsync(S->begin_d + slot * psg_server::kMaxJobs, bh, take * sizeof(long long), cudaMemcpyHostToDevice, S->s_comp));
@@ -2458,7 +1689,7 @@ void launch_batch(psg_server* S) {
   // one row buffer, or two when the prefetch costs no occupancy
   auto occ = [&](bool pf, size_t& sm) {
     sm = (size_t)((pf ? 2 : 1) * xb) + work;
-    auto k = batch_kernel_for(maxr, pf);
+    auto k = batch_kernel_for(pf);
     allow_smem(k);
     int per = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, sm));
@@ -2471,7 +1702,7 @@ void launch_batch(psg_server* S) {
   int per = pf ? o2 : o1;
   if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
   int grid = (int)std::min<long long>(total, (long long)per * g_sm_count);
-  if (total > 0) batch_kernel_for(maxr, pf)<<<grid, 256, pf ? sm2 : sm1, S->s_comp>>>(a);
+  if (total > 0) launch_pipe(batch_kernel_for(pf), grid, 256, pf ? sm2 : sm1, S->s_comp, a);
   CUDA_OK(cudaGetLastError());
   b->kern = get_event(S);
   CUDA_OK(cudaEventRecord(b->kern, S->s_comp));

@@ -47,7 +47,7 @@ __device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
   }
   return v;
 }
-__device__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
+__device__ inline unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
   v = warp_max_u64(v);
   int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
   __syncthreads();
@@ -208,32 +208,32 @@ struct InGlobal {
 // One decimation-in-frequency Stockham pass of radix R over `s · sub`
 // butterflies (fft/plan.nim:187-190):
 //   y[q + s·(R·p + k)] = (Σ_j x[q + s·(p + j·sub)]·ω_R^{jk})·ω_cur^{pk}
-// with the pass's twiddles tw[p·(R − 1) + k − 1] = ω_cur^{pk}; x and y are
-// element offsets into the buffer memory.
+// with cur = R·sub = m / s, so ω_cur^{pk} = tw[p·k·s] from the one table
+// tw[e] = ω_m^e of the transform; x and y are element offsets into the
+// buffer memory. Butterfly b = p·s + q: p = ⌊b / s⌋ from a multiply-high by
+// magic = ⌈2^32 / s⌉ — ⌊b / s⌋ or one more for b < 2^31 — and one correction
+// (magic = 0 marks s = 1).
 template <int R, class T, class M>
-__device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, int sub,
+__device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, int sub, unsigned magic,
                                          const typename C2<T>::type* __restrict__ tw) {
   typedef typename C2<T>::type V;
   V* buf = reinterpret_cast<V*>(mem.base());
-  const int total = s * sub;
-  const float inv_s = 1.0f / (float)s;
-  const int step = total;  // s · sub: the distance between a butterfly's inputs
+  const int total = s * sub;  // also the distance between a butterfly's inputs
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
-    int p = (int)((float)b * inv_s);
+    int p = magic ? (int)__umulhi((unsigned)b, magic) : b;
     if (p * s > b) p--;
-    else if ((p + 1) * s <= b) p++;
     const int q = b - p * s;
     V v[R];
-    const int xi = xo + q + s * p;
+    const V* x = buf + (xo + q + s * p);
 #pragma unroll
-    for (int j = 0; j < R; j++) v[j] = buf[xi + j * step];
+    for (int j = 0; j < R; j++) v[j] = x[j * total];
     Dft<V, T, R>::run(v);
-    const V* t = tw + p * (R - 1);
+    const int ps = p * s;
 #pragma unroll
-    for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&t[k - 1]));
-    const int yi = yo + q + s * R * p;
+    for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&tw[ps * k]));
+    V* y = buf + (yo + q + s * R * p);
 #pragma unroll
-    for (int k = 0; k < R; k++) buf[yi + s * k] = v[k];
+    for (int k = 0; k < R; k++) y[s * k] = v[k];
   }
 }
 
@@ -242,7 +242,7 @@ struct FftDesc {
   int m;          // complex length
   int npass;
   int radix[24];
-  int twoff[24];  // offset of each pass's twiddles
+  unsigned magic[24];  // ⌈2^32 / s⌉ of each pass, 0 for s = 1
 };
 
 // Forward complex FFT of the m points at offset `ao`, `bo` the second
@@ -251,26 +251,25 @@ struct FftDesc {
 // registers a pass needs); the plan's factorization never uses a larger one.
 template <class T, int MAXR, class M>
 __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const FftDesc& d,
-                                            const typename C2<T>::type* tw) {
-  typedef typename C2<T>::type V;
+                                         const typename C2<T>::type* tw) {
   int x = ao, y = bo;
   int cur = d.m, s = 1;
   for (int i = 0; i < d.npass; i++) {
     const int r = d.radix[i];
     const int sub = cur / r;
-    const V* t = tw + d.twoff[i];
+    const unsigned mg = d.magic[i];
     switch (r) {
-      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T>(mem, x, y, s, sub, t); break;
-      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T>(mem, x, y, s, sub, t); break;
-      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T>(mem, x, y, s, sub, t); break;
-      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T>(mem, x, y, s, sub, t); break;
-      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T>(mem, x, y, s, sub, t); break;
-      case 8: fft_pass<8, T>(mem, x, y, s, sub, t); break;
-      case 6: fft_pass<6, T>(mem, x, y, s, sub, t); break;
-      case 5: fft_pass<5, T>(mem, x, y, s, sub, t); break;
-      case 4: fft_pass<4, T>(mem, x, y, s, sub, t); break;
-      case 3: fft_pass<3, T>(mem, x, y, s, sub, t); break;
-      default: fft_pass<2, T>(mem, x, y, s, sub, t); break;
+      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T>(mem, x, y, s, sub, mg, tw); break;
+      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T>(mem, x, y, s, sub, mg, tw); break;
+      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T>(mem, x, y, s, sub, mg, tw); break;
+      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T>(mem, x, y, s, sub, mg, tw); break;
+      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T>(mem, x, y, s, sub, mg, tw); break;
+      case 8: fft_pass<8, T>(mem, x, y, s, sub, mg, tw); break;
+      case 6: fft_pass<6, T>(mem, x, y, s, sub, mg, tw); break;
+      case 5: fft_pass<5, T>(mem, x, y, s, sub, mg, tw); break;
+      case 4: fft_pass<4, T>(mem, x, y, s, sub, mg, tw); break;
+      case 3: fft_pass<3, T>(mem, x, y, s, sub, mg, tw); break;
+      default: fft_pass<2, T>(mem, x, y, s, sub, mg, tw); break;
     }
     __syncthreads();
     cur = sub;
@@ -282,59 +281,39 @@ __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const 
   return x;
 }
 
+// Four values of T: a bin's pair of complex coefficients.
+template <class T> struct alignas(4 * sizeof(T)) Quad { T x, y, z, w; };
+
 // The real-FFT bridge between the forward and inverse complex transforms of
 // a real trace of n = 2m samples packed as z[k] = x[2k] + i·x[2k+1]
-// (fft/plan.nim:470-499), fused into one in-place pass over the pairs
-// (k, m − k): split into the spectrum X[k], multiply by the bin's complex
-// factor (a real gain: im = 0), and un-split into swap(Z'), scaled by 1/n,
-// ready for the forward transform that inverts it.
-template <class T, class M, class MulFn>
-__device__ __forceinline__ void split_mul_unsplit(const M& mem, int zo, int m, const typename C2<T>::type* split,
-                                                  T scale, MulFn mul) {
+// (fft/plan.nim:470-499): split into the spectrum X[k], multiply by the
+// bin's factor M[k], un-split, scale by 1/n and swap re/im for the forward
+// transform that inverts it. All of it is linear in (z[k], conj z[m − k]),
+// so for each pair of bins it is one 2×2 map,
+//   z'[k] = A'_k·conj(z[k]) + B'_k·z[m − k],
+// with A'_k, B'_k computed on the host in float64 from ω^k = exp(−2πik/n),
+// M[k], M[m − k] and 1/n (bridge_table). Bin 0 keeps the reference's real
+// forms of the DC and Nyquist bins (the imaginary parts of M·X there are
+// dropped): ab[0] = (Re M[0]/n, Re M[m]/n).
+template <class T, class M>
+__device__ __forceinline__ void split_bridge(const M& mem, int zo, int m, const Quad<T>* __restrict__ ab) {
   typedef typename C2<T>::type V;
   V* z = reinterpret_cast<V*>(mem.base()) + zo;
-  const T half = (T)0.5;
   for (int k = threadIdx.x; k <= m / 2; k += blockDim.x) {
     if (k == 0) {
-      V z0 = z[0];
-      V x0 = {z0.x + z0.y, (T)0}, xm = {z0.x - z0.y, (T)0};
-      x0 = mul(x0, 0);
-      xm = mul(xm, m);
-      // ai[0] = (x0 + xm)·scale = Re Z'0, ar[0] = (x0 − xm)·scale = Im Z'0; stored swapped.
-      z[0] = {(x0.x - xm.x) * scale, (x0.x + xm.x) * scale};
+      const V z0 = z[0];
+      const Quad<T> c = ab[0];
+      const T x0 = (z0.x + z0.y) * c.x, xm = (z0.x - z0.y) * c.y;
+      z[0] = {x0 - xm, x0 + xm};
       continue;
     }
     const int j = m - k;
-    V a = z[k], b = z[j];
-    V wk = __ldg(&split[k]), wj = __ldg(&split[j]);
-    // forward split at k (a = Z[k], b = Z[m−k]) and at m − k (roles swapped)
-    V Xk, Xj;
-    {
-      T er = half * (a.x + b.x), ei = half * (a.y - b.y), orr = half * (a.y + b.y), oi = half * (b.x - a.x);
-      Xk = {er + wk.x * orr - wk.y * oi, ei + wk.x * oi + wk.y * orr};
-    }
-    {
-      T er = half * (b.x + a.x), ei = half * (b.y - a.y), orr = half * (b.y + a.y), oi = half * (a.x - b.x);
-      Xj = {er + wj.x * orr - wj.y * oi, ei + wj.x * oi + wj.y * orr};
-    }
-    Xk = mul(Xk, k);
-    Xj = mul(Xj, j);
-    // inverse split at k (ar = X[k], br = X[m−k], ω = (wr, −wi)), stored as swap(Z')
-    V Zk, Zj;
-    {
-      T wr = wk.x, wi = -wk.y;
-      T er = Xk.x + Xj.x, ei = Xk.y - Xj.y, dr = Xk.x - Xj.x, di = Xk.y + Xj.y;
-      T orr = dr * wr - di * wi, oi = dr * wi + di * wr;
-      Zk = {(ei + orr) * scale, (er - oi) * scale};
-    }
-    {
-      T wr = wj.x, wi = -wj.y;
-      T er = Xj.x + Xk.x, ei = Xj.y - Xk.y, dr = Xj.x - Xk.x, di = Xj.y + Xk.y;
-      T orr = dr * wr - di * wi, oi = dr * wi + di * wr;
-      Zj = {(ei + orr) * scale, (er - oi) * scale};
-    }
-    z[k] = Zk;
-    if (j != k) z[j] = Zj;
+    const V a = z[k], b = z[j];
+    const Quad<T> ck = ab[k], cj = ab[j];
+    // A·conj(a) + B·b
+    z[k] = {ck.x * a.x + ck.y * a.y + ck.z * b.x - ck.w * b.y, ck.y * a.x - ck.x * a.y + ck.z * b.y + ck.w * b.x};
+    if (j != k)
+      z[j] = {cj.x * b.x + cj.y * b.y + cj.z * a.x - cj.w * a.y, cj.y * b.x - cj.x * b.y + cj.z * a.y + cj.w * a.x};
   }
   __syncthreads();
 }

@@ -40,7 +40,7 @@ int64_t next_fast(int64_t n, bool even = true);
 struct FftTables {
   int64_t n = 0, m = 0;
   std::vector<int> radices;
-  std::vector<double> tw_re, tw_im;       // per pass: sub·(r − 1) values
+  std::vector<double> tw_re, tw_im;       // exp(−2πi·e/m), e < m
   std::vector<double> split_re, split_im; // exp(−2πik/n), k = 0 .. m
 };
 FftTables fft_tables(int64_t n, int max_radix = 16);

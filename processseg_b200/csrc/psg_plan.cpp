@@ -99,7 +99,8 @@ int64_t next_fast(int64_t n, bool even) {
 // threads) rounds of R elements each, at the small DFT's arithmetic per
 // element plus the pass's shared-memory traffic and twiddle multiply.
 // The twiddle of output k of butterfly p in a pass of `cur` points is
-// exp(−2πi·(p·k mod cur)/cur), as fft/plan.nim:146-155 builds them.
+// exp(−2πi·p·k/cur) (fft/plan.nim:146-155), read from one table of
+// exp(−2πi·e/m).
 namespace {
 double radix_cost(int r) {
   switch (r) {
@@ -165,16 +166,13 @@ FftTables fft_tables(int64_t n, int max_radix) {
   t.n = n;
   t.m = n / 2;
   t.radices = plan_radices(t.m, 256, max_radix);
-  int64_t cur = t.m;
-  for (int r : t.radices) {
-    int64_t sub = cur / r;
-    for (int64_t p = 0; p < sub; p++)
-      for (int q = 1; q < r; q++) {
-        double a = -2 * kPi * (double)((p * q) % cur) / (double)cur;
-        t.tw_re.push_back(std::cos(a));
-        t.tw_im.push_back(std::sin(a));
-      }
-    cur = sub;
+  // One table for every pass: the twiddle of output k of butterfly p in the
+  // pass after radices of product s (cur = m / s points) is
+  // ω_cur^{p·k} = ω_m^{p·k·s}, and p·k·s < m.
+  for (int64_t e = 0; e < t.m; e++) {
+    double a = -2 * kPi * (double)e / (double)t.m;
+    t.tw_re.push_back(std::cos(a));
+    t.tw_im.push_back(std::sin(a));
   }
   for (int64_t j = 0; j <= t.m; j++) {
     double a = -2 * kPi * (double)j / (double)n;

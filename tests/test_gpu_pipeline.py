@@ -274,3 +274,47 @@ def test_panel_factor_matches_oracle():
     f = plan.panelFactorOf(b, meta, 1, ws)
     st = O.panel_stats(g.data, meta.flat(800)[0], 99.0)
     assert abs(f - 2 / st["clip"]) <= 1e-12 * abs(f)
+
+
+@pytest.mark.parametrize("window_ms", [100, 300, 500, 700])
+@pytest.mark.parametrize("dtype", [P.F32, P.F64])
+def test_agc_window_edges_match_oracle(window_ms, dtype):
+    """AGC at live lengths around the half window h, the whole window
+    w = 2h + 1 and its multiples (head, whole-trace, whole-window and tail
+    forms of gain/gain.nim:433-461), in both modes, with a row whose second
+    half is 120 dB quieter than its first (tests/tgain.nim:187-212)."""
+    h = int(round(window_ms / 2.0 / 2))
+    w = 2 * h + 1
+    cols = 1201
+    lens = sorted({n for n in (1, 2, 3, h - 1, h, h + 1, 2 * h - 1, 2 * h, w, w + 1, 2 * w - 1, 2 * w,
+                               2 * w + 1, 3 * w + h, 4 * w - 1, cols - 1, cols) if 1 <= n <= cols})
+    npd = np.float32 if dtype == P.F32 else np.float64
+    g = synth.shot_gather(len(lens) + 1, cols, 2.0, seed=21, dtype=npd, workload="agc_edges")
+    g.numSamples[:len(lens)] = lens
+    g.numSamples[-1] = cols
+    g.data[-1, cols // 2:] *= 1e-6
+    for r, n in enumerate(g.numSamples):
+        g.data[r, n:] = 0
+    meta = g.meta()
+    for mode in (P.agcRms, P.agcMeanAbs):
+        flow = [P.agcOp(window_ms, mode)]
+        got = run_gpu(flow, g.data, meta, dtype, 2.0)
+        assert_parity(got, flow, g.data, meta, dtype, 2.0)
+
+
+@pytest.mark.parametrize("flow", [C2_FLOW, C2_FLOW + [P.normalizeOp(P.normPercentile, percentile=99.0)],
+                                  [P.bandPassOp(P.Corners(4, 8, 60, 80)), P.normalizeOp(P.normRms)],
+                                  [P.filterOp(P.butterBandPass(5, 100, 24)), P.gainCurveOp(P.powerGain(2))]],
+                         ids=["dfa", "dfan", "fn", "fg"])
+def test_recipe_kernels_and_step_switch_match_oracle(flow, monkeypatch):
+    """The fixed-sequence kernels (demean fused into the filter's pack) and
+    the generic step switch (PSG_RECIPES=0 at compile time) each match the
+    oracle on the same uneven panel."""
+    g = synth.c2(rows=160)
+    g.status[[4]] = P.tsDead
+    meta = g.meta()
+    fast = run_gpu(flow, g.data, meta, P.float32, 2.0)
+    monkeypatch.setenv("PSG_RECIPES", "0")
+    generic = run_gpu(flow, g.data, meta, P.float32, 2.0)
+    for got in (fast, generic):
+        assert_parity(got, flow, g.data, meta, P.F32, 2.0)
