@@ -308,13 +308,21 @@ def test_agc_window_edges_match_oracle(window_ms, dtype):
                          ids=["dfa", "dfan", "fn", "fg"])
 def test_recipe_kernels_and_step_switch_match_oracle(flow, monkeypatch):
     """The fixed-sequence kernels (demean fused into the filter's pack) and
-    the generic step switch (PSG_RECIPES=0 at compile time) each match the
-    oracle on the same uneven panel."""
-    g = synth.c2(rows=160)
+    the generic step switch (PSG_RECIPES=0, read at compile time) both match
+    the oracle on the same uneven panel of an odd number of rows, with a dead
+    row and a row holding a NaN that stays in its row."""
+    g = synth.c2(rows=161)
     g.status[[4]] = P.tsDead
+    g.data[17, 40] = np.nan
     meta = g.meta()
-    fast = run_gpu(flow, g.data, meta, P.float32, 2.0)
+    outs = [run_gpu(flow, g.data, meta, P.float32, 2.0)]
     monkeypatch.setenv("PSG_RECIPES", "0")
-    generic = run_gpu(flow, g.data, meta, P.float32, 2.0)
-    for got in (fast, generic):
-        assert_parity(got, flow, g.data, meta, P.F32, 2.0)
+    outs.append(run_gpu(flow, g.data, meta, P.float32, 2.0))
+    ok = np.ones(g.data.shape[0], bool)
+    ok[17] = False
+    live = meta.flat(3001)[0]
+    for got in outs:
+        assert np.isnan(got[17, :live[17]]).any()
+        assert np.all(np.isfinite(got[ok]))
+        assert_parity(got[ok], flow, g.data[ok], P.initChunkMeta(g.status[ok], g.numSamples[ok], 2.0,
+                                                                  g.t0Ms[ok], 0), P.F32, 2.0)
