@@ -217,6 +217,83 @@ def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
                           "requests_per_launch": sat_launch}}
 
 
+def workloads_leg(peak):
+    """The other configurations, device-resident, each timed with CUDA events
+    after a warm-up: C1 (48×2001, demean → band-pass 4-8-60-80 → AGC 500 ms),
+    C3 (4 sweeps × 240 channels × 10001 samples correlated with a 12 s
+    8–80 Hz pilot to 6 s, stacked), C5 (50000×6001 at 1 ms, demean →
+    band-pass 2/5/120/150 → AGC 250 ms → per-trace p99 normalization).
+    HBM fraction: algorithmic bytes (each input sample read once, each output
+    written once) over the time, against the measured copy bandwidth."""
+    import numpy as np
+    import torch
+    import processseg_b200 as P
+    from processseg_b200 import synth
+
+    def timed(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps * 1e-3
+
+    out = {}
+    g = synth.c1()
+    meta = g.meta()
+    plan = P.initPipeline([P.demeanOp(), P.bandPassOp(P.Corners(4, 8, 60, 80)), P.agcOp(500)]).compile(P.float32, 2.0, 2001)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=48, cols=2001)
+    src = torch.from_numpy(g.data).cuda()
+    dst = torch.empty_like(src)
+    t = timed(lambda: plan.apply(src, dst, meta, ws), 200)
+    out["c1"] = {"workload": "48x2001 f32 @2ms: demean -> bandpass 4-8-60-80 -> AGC 500 ms", "us_per_panel": t * 1e6,
+                 "msamples_per_s": 48 * 2001 / t / 1e6, "hbm_frac": 2 * 48 * 2001 * 4 / t / 1e9 / peak}
+
+    spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
+    pilot = P.generatePilot(spec, np.float64)
+    recs = synth.vibroseis_records(pilot.samples, channels=240, sweeps=4)
+    sweeps, ch, ns = recs.shape
+    cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=3000)
+    stack = P.initRecordStack(ch, 3000, 2.0)
+    cmeta = P.initChunkMeta(np.full(ch, P.tsLive, np.int32), np.full(ch, ns, np.int32), 2.0)
+    xs = [torch.from_numpy(recs[s]).cuda() for s in range(sweeps)]
+    d = torch.empty(ch, 3000, device="cuda")
+    so = torch.empty(ch, 3000, device="cuda")
+
+    def c3():
+        stack.clear()
+        for x in xs:
+            cplan.correlateInto(x, d, cmeta, stack=stack)
+        stack.stackInto(so)
+    t = timed(c3, 20)
+    inb = sweeps * ch * ns * 4
+    outb = sweeps * ch * 3000 * 4 + ch * 3000 * 4
+    out["c3"] = {"workload": "4 sweeps x 240 channels x 10001 f32 @2ms, 12 s 8-80 Hz pilot, nfft 16200, 6 s out, vertical stack",
+                 "ms_per_gather": t * 1e3, "msamples_per_s": sweeps * ch * ns / t / 1e6,
+                 "hbm_frac": (inb + outb) / t / 1e9 / peak}
+
+    g = synth.c5()
+    meta = g.meta()
+    flow = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(2, 5, 120, 150))), P.agcOp(250),
+            P.normalizeOp(P.normPercentile, P.perTrace, percentile=99.0)]
+    plan = P.initPipeline(flow).compile(P.float32, 1.0, 6001)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=50000, cols=6001)
+    src = torch.from_numpy(g.data).cuda()
+    dst = torch.empty_like(src)
+    t = timed(lambda: plan.apply(src, dst, meta, ws), 3)
+    out["c5"] = {"workload": "50000x6001 f32 @1ms (1.2 GB), live U{4000..6001}: demean -> bandpass 2/5/120/150 -> AGC 250 ms -> per-trace p99",
+                 "ms_per_panel": t * 1e3, "msamples_per_s": 50000 * 6001 / t / 1e6,
+                 "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak}
+    del src, dst
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -343,6 +420,8 @@ def run_ours(args):
         }
         if not args.no_serving:
             line["serving"] = serving_leg()
+        if not args.no_workloads:
+            line["workloads"] = workloads_leg(peak)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(steps=3, warmup=1)
         print(json.dumps(line), flush=True)
@@ -359,6 +438,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-load leg")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the C1/C3/C5 legs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -22,6 +22,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <type_traits>
 
 #include "psg_device.cuh"
 #include "psg_internal.h"
@@ -286,7 +287,21 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
     if (n > 0) {
       const T* x = src + r * (long long)a.cols;
       T* Ar = reinterpret_cast<T*>(buf);
-      for (int j = threadIdx.x; j < a.nfft; j += blockDim.x) Ar[j] = j < n ? x[j] : (T)0;
+      // the record: 16-byte loads over its aligned body, element loads at the
+      // ends, zeros to nfft
+      constexpr int per = 16 / (int)sizeof(T);
+      const int head = min((int)(((16 - ((uintptr_t)x & 15)) & 15) / sizeof(T)), n);
+      const int nv = (n - head) / per, tail0 = head + nv * per;
+      typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type Q;
+      const Q* xv = reinterpret_cast<const Q*>(x + head);
+      for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        const Q q = __ldg(xv + v);
+        const T* e = reinterpret_cast<const T*>(&q);
+#pragma unroll
+        for (int u = 0; u < per; u++) Ar[head + per * v + u] = e[u];
+      }
+      for (int j = threadIdx.x; j < head; j += blockDim.x) Ar[j] = x[j];
+      for (int j = tail0 + threadIdx.x; j < a.nfft; j += blockDim.x) Ar[j] = j < n ? x[j] : (T)0;
       __syncthreads();
       constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
       const int zo = cfft_forward<T, MAXR>(mem, 0, m, a.fft, tw);
@@ -330,9 +345,13 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
 }
 
 // correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
-// pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
+// pass, with the vertical-stack add (vstack.nim:186-202) fused after it. A
+// record's two transform buffers fill most of an SM's shared memory (one CTA
+// per SM at nfft 16200), so the CTA is 512 threads wide: 16 warps per SM to
+// hide the latency of the record's loads and of the passes.
+constexpr int kCorrThreads = 512;
 template <class T>
-__global__ void __launch_bounds__(256) corr_kernel(CorrArgs a) {
+__global__ void __launch_bounds__(kCorrThreads) corr_kernel(CorrArgs a) {
   __shared__ Shared S;
   if (a.gwork) {
     typedef typename C2<T>::type V;
@@ -790,7 +809,7 @@ template <class T> static void corr_upload(psg_corr_plan* p) {
   if ((int64_t)need <= limit) {
     p->smem = need;
     int per_sm = 0;
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, corr_kernel<T>, 256, p->smem));
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, corr_kernel<T>, kCorrThreads, p->smem));
     p->grid = std::max(1, per_sm) * g_sm_count;
   } else {
     // Too long for shared memory: each CTA works in its own slice of global
@@ -1356,8 +1375,8 @@ static int corr_launch(const psg_corr_plan* plan, psg_stack* st, const void* src
     }
     int grid = (int)std::min<int64_t>(rows, plan->grid);
     cudaStream_t s = (cudaStream_t)stream;
-    if (plan->dtype == PSG_F32) corr_kernel<float><<<grid, 256, plan->smem, s>>>(a);
-    else corr_kernel<double><<<grid, 256, plan->smem, s>>>(a);
+    if (plan->dtype == PSG_F32) corr_kernel<float><<<grid, kCorrThreads, plan->smem, s>>>(a);
+    else corr_kernel<double><<<grid, kCorrThreads, plan->smem, s>>>(a);
     CUDA_OK(cudaGetLastError());
   });
 }
