@@ -54,7 +54,7 @@ template <class T>
 __global__ void __launch_bounds__(256) row_stats_kernel(const T* __restrict__ b, long long rows, int cols,
                                                         const int* __restrict__ live, double* __restrict__ ss,
                                                         double* __restrict__ mx) {
-  __shared__ Shared S;
+  __shared__ SharedMem S;
   for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
     int n = min(max(live[r], 0), cols);
     const T* x = b + r * (long long)cols;
@@ -66,8 +66,8 @@ __global__ void __launch_bounds__(256) row_stats_kernel(const T* __restrict__ b,
       unsigned long long bb = abs_bits(x[i]);
       m = bb > m ? bb : m;
     }
-    s = block_sum(s, S.red[0]);
-    m = block_max_u64(m, S.redu);
+    s = block_sum(s, S.red[0][0]);
+    m = block_max_u64(m, S.redu[0]);
     if (threadIdx.x == 0) {
       ss[r] = s;
       mx[r] = n > 0 ? bits_value(m, (T)0) : (double)NAN;
@@ -91,7 +91,7 @@ __device__ __forceinline__ bool usable_d(double ssr, double mxr, int n) {
 __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int cols, const int* __restrict__ live,
                                                           const double* __restrict__ ss, const double* __restrict__ mx,
                                                           PanelOut* out) {
-  __shared__ Shared S;
+  __shared__ SharedMem S;
   double sum = 0, cnt = 0, nr = 0;
   unsigned long long mb = 0;
   for (long long r = threadIdx.x; r < rows; r += blockDim.x) {
@@ -103,10 +103,10 @@ __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int co
     unsigned long long b = (unsigned long long)__double_as_longlong(mx[r]);
     mb = b > mb ? b : mb;
   }
-  sum = block_sum(sum, S.red[0]);
-  cnt = block_sum(cnt, S.red[0]);
-  nr = block_sum(nr, S.red[0]);
-  mb = block_max_u64(mb, S.redu);
+  sum = block_sum(sum, S.red[0][0]);
+  cnt = block_sum(cnt, S.red[0][0]);
+  nr = block_sum(nr, S.red[0][0]);
+  mb = block_max_u64(mb, S.redu[0]);
   if (threadIdx.x == 0) {
     out->rows = nr;
     out->samples = cnt;
@@ -271,7 +271,7 @@ struct CorrArgs {
 // correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
 // pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
 template <class T, class M>
-__device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Shared& S) {
+__device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, SharedMem& S) {
   typedef typename C2<T>::type V;
   const int m = a.nfft / 2;
   V* buf = reinterpret_cast<V*>(mem.base());
@@ -329,7 +329,7 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
           double v = (double)value(c);
           bad += v - v;  // allFinite: x − x is 0 for finite x
         }
-        bad = block_sum(bad, S.red[0]);
+        bad = block_sum(bad, S.red[0][0]);
         if (bad == 0) {
           double* nm = a.num + (long long)o * a.stack_samples;
           int* ct = a.cnt + (long long)o * a.stack_samples;
@@ -352,7 +352,7 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
 constexpr int kCorrThreads = 512;
 template <class T>
 __global__ void __launch_bounds__(kCorrThreads) corr_kernel(CorrArgs a) {
-  __shared__ Shared S;
+  __shared__ SharedMem S;
   if (a.gwork) {
     typedef typename C2<T>::type V;
     InGlobal g{reinterpret_cast<unsigned char*>(a.gwork) + (size_t)blockIdx.x * a.nfft * sizeof(V)};
@@ -367,7 +367,7 @@ template <class T>
 __global__ void __launch_bounds__(256) stack_add_kernel(const T* __restrict__ b, long long rows, int cols,
                                                         const int* __restrict__ live, const int* __restrict__ row_map,
                                                         double* num, int* cnt, int samples, long long out_rows) {
-  __shared__ Shared S;
+  __shared__ SharedMem S;
   for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
     int o = row_map ? row_map[r] : (int)r;
     int n = min(max(live[r], 0), min(cols, samples));
@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(256) stack_add_kernel(const T* __restrict__ b,
       double v = (double)x[c];
       bad += v - v;
     }
-    bad = block_sum(bad, S.red[0]);
+    bad = block_sum(bad, S.red[0][0]);
     if (bad == 0) {
       for (int c = threadIdx.x; c < n; c += blockDim.x) {
         num[(long long)o * samples + c] += (double)x[c];
@@ -420,7 +420,7 @@ static void ensure_device() {
 }
 
 static void allow_smem(const void* kernel) {
-  CUDA_OK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_max_smem - (int)sizeof(Shared) - 1024));
+  CUDA_OK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_max_smem - (int)sizeof(SharedMem) - 1024));
 }
 
 struct DeviceBuf {
@@ -711,7 +711,7 @@ template <class T> static void build_device_steps(psg_plan* p) {
   if (const char* e = getenv("PSG_PREFETCH")) p->prefetch = atoi(e) != 0 && two > 0;
   p->work_off = (p->prefetch ? 2 : 1) * p->x_bytes;
   p->smem = (size_t)(p->work_off + work);
-  int limit = g_max_smem - (int)sizeof(Shared) - 1024;
+  int limit = g_max_smem - (int)sizeof(SharedMem) - 1024;
   if ((int64_t)p->smem > limit)
     throw InvalidArg("the plan's traces (" + std::to_string(p->host.samples) + " samples) and FFTs need " +
                      std::to_string(p->smem) + " bytes of shared memory; the device gives " + std::to_string(limit));
@@ -804,7 +804,7 @@ template <class T> static void corr_upload(psg_corr_plan* p) {
   p->tw = upload(p->keep, as_c<T>(p->host.fft.tw_re, p->host.fft.tw_im));
   p->fft = fft_desc(p->host.fft);
   size_t need = (size_t)(2 * p->host.fft.m * sizeof(V));
-  int limit = g_max_smem - (int)sizeof(Shared) - 1024;
+  int limit = g_max_smem - (int)sizeof(SharedMem) - 1024;
   allow_smem((const void*)corr_kernel<T>);
   if ((int64_t)need <= limit) {
     p->smem = need;

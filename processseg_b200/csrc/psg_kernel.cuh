@@ -161,15 +161,21 @@ __device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* his
 // makes a pass of its own for them.
 enum { NEED_S1 = 1, NEED_SI = 2, NEED_S2 = 4, NEED_MX = 8 };
 
-struct Shared {
-  double red[4][32];
-  unsigned long long redu[32];
-  double sv[32];
-  int sf[32];
-  double pv[32];
+// The CTA's static shared memory: two sets of per-warp reduction slots (a
+// reduction fills one set while threads may still read the other set of the
+// reduction before it), and the radix selection's histogram.
+struct SharedMem {
+  double red[2][4][32];
+  unsigned long long redu[2][32];
   unsigned hist[256];
   int sh[4];
-  double out[4];
+};
+// A thread's handle on its CTA's SharedMem: `flip` picks the reduction slot
+// set, and every thread flips it at every reduction (all threads run the
+// same reductions in the same order, so they agree on it).
+struct Shared {
+  SharedMem* m;
+  int flip;
 };
 
 struct Stats {
@@ -226,15 +232,17 @@ template <int NEED, class F> __device__ __forceinline__ auto with_need_k(int nee
   }
 }
 
-// Folds the partial sums over the block. Always ends with a __syncthreads(),
-// so the loop's writes to the trace are visible to the next step.
+// Folds the partial sums over the block with one barrier: each warp's lane 0
+// writes its warp's sums, and after the barrier every thread adds the warps'
+// sums itself, in warp order (the same order, so the same result, in every
+// thread). The barrier also orders the loop's writes to the trace before the
+// next step reads them. Consecutive reductions use alternate slot sets
+// (Shared::flip), so a warp that runs ahead into the next reduction never
+// writes slots another thread is still reading: the reduction after that
+// reuses them only past the next reduction's barrier.
 template <class T> __device__ __forceinline__ Stats reduce_stats(const Acc<T>& a, int need, Shared& S) {
   Stats r{0, 0, 0, 0};
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if (need == 0) {
-    __syncthreads();
-    return r;
-  }
   double v0 = (double)a.s1, v1 = (double)a.si, v2 = (double)a.s2;
   unsigned long long m = a.mx;
 #pragma unroll
@@ -247,38 +255,32 @@ template <class T> __device__ __forceinline__ Stats reduce_stats(const Acc<T>& a
       m = u > m ? u : m;
     }
   }
-  if (lane == 0) {
-    S.red[0][warp] = v0;
-    S.red[1][warp] = v1;
-    S.red[2][warp] = v2;
-    S.redu[warp] = m;
+  double(*red)[32] = S.m->red[S.flip];
+  unsigned long long* redu = S.m->redu[S.flip];
+  S.flip ^= 1;
+  if (need && lane == 0) {
+    if (need & NEED_S1) red[0][warp] = v0;
+    if (need & NEED_SI) red[1][warp] = v1;
+    if (need & NEED_S2) red[2][warp] = v2;
+    if (need & NEED_MX) redu[warp] = m;
   }
   __syncthreads();
-  if (warp == 0) {
-    v0 = lane < nw ? S.red[0][lane] : 0.0;
-    v1 = lane < nw ? S.red[1][lane] : 0.0;
-    v2 = lane < nw ? S.red[2][lane] : 0.0;
-    m = lane < nw ? S.redu[lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-      v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-      v2 += __shfl_xor_sync(0xffffffffu, v2, o);
-      unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
+  if (need == 0) return r;
+  v0 = v1 = v2 = 0;
+  m = 0;
+  for (int w = 0; w < nw; w++) {
+    if (need & NEED_S1) v0 += red[0][w];
+    if (need & NEED_SI) v1 += red[1][w];
+    if (need & NEED_S2) v2 += red[2][w];
+    if (need & NEED_MX) {
+      const unsigned long long u = redu[w];
       m = u > m ? u : m;
     }
-    if (lane == 0) {
-      S.out[0] = v0;
-      S.out[1] = v1;
-      S.out[2] = v2;
-      S.out[3] = bits_value(m, (T)0);
-    }
   }
-  __syncthreads();
-  r.s1 = S.out[0];
-  r.si = S.out[1];
-  r.s2 = S.out[2];
-  r.mx = S.out[3];
+  r.s1 = v0;
+  r.si = v1;
+  r.s2 = v2;
+  r.mx = bits_value(m, (T)0);
   return r;
 }
 
@@ -393,14 +395,9 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
 // below the float32 range of squares, the float64 sum of a pass of its own.
 template <class T> __device__ __forceinline__ double trace_s2(const Stats& in, const T* X, int n, Shared& S) {
   if (sizeof(T) == 8 || (isfinite(in.s2) && in.s2 >= 1e-30)) return in.s2;
-  double v = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double d = (double)X[i];
-    v += d * d;
-  }
-  v = block_sum(v, S.red[0]);
-  __syncthreads();  // every warp has read the sum before S.red is written again
-  return v;
+  Acc<double> acc;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc.template add_t<NEED_S2>((double)X[i], 0.0);
+  return reduce_stats(acc, NEED_S2, S).s2;
 }
 
 // Warp scans of one value per lane: the sum over the lanes below (or above)
@@ -594,11 +591,11 @@ __device__ __forceinline__ Stats step_norm_trace(const DevStep& st, const Stats&
   } else {
     double hr = (double)(n - 1) * st.percentile / 100;
     int k = min((int)floor(hr), n - 1);
-    double lower = bits_value(select_kth(X, n, k, S.hist, S.sh), (T)0);
+    double lower = bits_value(select_kth(X, n, k, S.m->hist, S.m->sh), (T)0);
     if (k + 1 >= n) {
       level = lower;
     } else {
-      double upper = bits_value(select_kth(X, n, k + 1, S.hist, S.sh), (T)0);
+      double upper = bits_value(select_kth(X, n, k + 1, S.m->hist, S.m->sh), (T)0);
       double f = hr - (double)k;
       level = f == 0 ? lower : lower + f * (upper - lower);
     }
@@ -783,7 +780,8 @@ __device__ __forceinline__ void run_recipe(const DevStep* d, Stats st, T* X, int
 // plans, widths and blocks) in one launch.
 template <class T, int MAXR, bool PF, bool BATCH, int RECIPE>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
-  __shared__ Shared S;
+  __shared__ SharedMem smem;
+  Shared S{&smem, 0};
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ RowSlot slot[2];
   __shared__ int s_ok;
@@ -863,7 +861,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
     T* X = reinterpret_cast<T*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
     for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = c.from[i];
     for (int i = sl.tail + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = c.from[i];
-    __syncthreads();  // the ragged ends are read by other threads below
+    if (sl.head > 0 || sl.tail < sl.len) __syncthreads();  // the ragged ends are read by other threads below
     const int n = c.n;
     if constexpr (RECIPE != RC_GENERIC) {
       if (n > 0) {
