@@ -503,7 +503,7 @@ struct psg_plan {
   std::vector<std::unique_ptr<DeviceBuf>> keep;
   DevStep* d_steps = nullptr;
   int device = 0;
-  int threads = 256;
+  int threads = kNT;
   int max_radix = 12;  // the largest FFT radix compiled into the plan's kernel
   std::vector<int> recipe;  // per part: the recipe kernel that runs it (RC_GENERIC: the step switch)
   int x_elems = 0, work_off = 0, x_bytes = 0;
@@ -1711,7 +1711,7 @@ void launch_batch(psg_server* S) {
     auto k = batch_kernel_for(pf);
     allow_smem(k);
     int per = 0;
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, sm));
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kNT, sm));
     return per;
   };
   size_t sm1, sm2;
@@ -1721,7 +1721,7 @@ void launch_batch(psg_server* S) {
   int per = pf ? o2 : o1;
   if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
   int grid = (int)std::min<long long>(total, (long long)per * g_sm_count);
-  if (total > 0) launch_pipe(batch_kernel_for(pf), grid, 256, pf ? sm2 : sm1, S->s_comp, a);
+  if (total > 0) launch_pipe(batch_kernel_for(pf), grid, kNT, pf ? sm2 : sm1, S->s_comp, a);
   CUDA_OK(cudaGetLastError());
   b->kern = get_event(S);
   CUDA_OK(cudaEventRecord(b->kern, S->s_comp));

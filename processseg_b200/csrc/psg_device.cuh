@@ -213,13 +213,14 @@ struct InGlobal {
 // buffer memory. Butterfly b = p·s + q: p = ⌊b / s⌋ from a multiply-high by
 // magic = ⌈2^32 / s⌉ — ⌊b / s⌋ or one more for b < 2^31 — and one correction
 // (magic = 0 marks s = 1).
-template <int R, class T, class M>
+template <int R, class T, int NT, class M>
 __device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, int sub, unsigned magic,
                                          const typename C2<T>::type* __restrict__ tw) {
+  const int nt = NT ? NT : (int)blockDim.x;
   typedef typename C2<T>::type V;
   V* buf = reinterpret_cast<V*>(mem.base());
   const int total = s * sub;  // also the distance between a butterfly's inputs
-  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+  for (int b = threadIdx.x; b < total; b += nt) {
     int p = magic ? (int)__umulhi((unsigned)b, magic) : b;
     if (p * s > b) p--;
     const int q = b - p * s;
@@ -249,7 +250,8 @@ struct FftDesc {
 // buffer. Returns the offset holding the result; ends with a
 // __syncthreads(). MAXR bounds the radices compiled in (and with them the
 // registers a pass needs); the plan's factorization never uses a larger one.
-template <class T, int MAXR, class M>
+// NT: the CTA's thread count when known at compile time (0: blockDim.x).
+template <class T, int MAXR, int NT = 0, class M>
 __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const FftDesc& d,
                                          const typename C2<T>::type* tw) {
   int x = ao, y = bo;
@@ -259,17 +261,17 @@ __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const 
     const int sub = cur / r;
     const unsigned mg = d.magic[i];
     switch (r) {
-      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T>(mem, x, y, s, sub, mg, tw); break;
-      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T>(mem, x, y, s, sub, mg, tw); break;
-      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T>(mem, x, y, s, sub, mg, tw); break;
-      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T>(mem, x, y, s, sub, mg, tw); break;
-      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T>(mem, x, y, s, sub, mg, tw); break;
-      case 8: fft_pass<8, T>(mem, x, y, s, sub, mg, tw); break;
-      case 6: fft_pass<6, T>(mem, x, y, s, sub, mg, tw); break;
-      case 5: fft_pass<5, T>(mem, x, y, s, sub, mg, tw); break;
-      case 4: fft_pass<4, T>(mem, x, y, s, sub, mg, tw); break;
-      case 3: fft_pass<3, T>(mem, x, y, s, sub, mg, tw); break;
-      default: fft_pass<2, T>(mem, x, y, s, sub, mg, tw); break;
+      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 8: fft_pass<8, T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 6: fft_pass<6, T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 5: fft_pass<5, T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 4: fft_pass<4, T, NT>(mem, x, y, s, sub, mg, tw); break;
+      case 3: fft_pass<3, T, NT>(mem, x, y, s, sub, mg, tw); break;
+      default: fft_pass<2, T, NT>(mem, x, y, s, sub, mg, tw); break;
     }
     __syncthreads();
     cur = sub;
@@ -295,11 +297,12 @@ template <class T> struct alignas(4 * sizeof(T)) Quad { T x, y, z, w; };
 // M[k], M[m − k] and 1/n (bridge_table). Bin 0 keeps the reference's real
 // forms of the DC and Nyquist bins (the imaginary parts of M·X there are
 // dropped): ab[0] = (Re M[0]/n, Re M[m]/n).
-template <class T, class M>
+template <class T, int NT = 0, class M>
 __device__ __forceinline__ void split_bridge(const M& mem, int zo, int m, const Quad<T>* __restrict__ ab) {
   typedef typename C2<T>::type V;
   V* z = reinterpret_cast<V*>(mem.base()) + zo;
-  for (int k = threadIdx.x; k <= m / 2; k += blockDim.x) {
+  const int nt = NT ? NT : (int)blockDim.x;
+  for (int k = threadIdx.x; k <= m / 2; k += nt) {
     if (k == 0) {
       const V z0 = z[0];
       const Quad<T> c = ab[0];

@@ -24,6 +24,10 @@
 namespace psg {
 using namespace psgd;
 
+// The pipeline kernels' CTA width (every launch of them uses it), a
+// compile-time constant so that the trace loops' strides and offsets are too.
+constexpr int kNT = 256;
+
 // ============================================================ device plan
 struct DevStep {
   int kind, trend, reflect, zero_dc;
@@ -72,38 +76,38 @@ template <class T> __device__ __forceinline__ bool fits_d(double x) {
 // Row copies between global buffers and shared memory, 16-byte vectors where
 // the addresses allow it.
 template <class T> __device__ void load_row(const T* __restrict__ g, T* s, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+  for (int i = threadIdx.x; i < n; i += kNT) s[i] = g[i];
 }
 template <> __device__ inline void load_row<float>(const float* __restrict__ g, float* s, int n) {
   int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
   if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += blockDim.x) s[i] = g[i];
+  for (int i = threadIdx.x; i < head; i += kNT) s[i] = g[i];
   int nv = (n - head) >> 2;
   const float4* gv = reinterpret_cast<const float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+  for (int v = threadIdx.x; v < nv; v += kNT) {
     float4 q = __ldcs(gv + v);
     int i = head + 4 * v;
     s[i] = q.x; s[i + 1] = q.y; s[i + 2] = q.z; s[i + 3] = q.w;
   }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+  for (int i = head + 4 * nv + threadIdx.x; i < n; i += kNT) s[i] = g[i];
 }
 template <class T> __device__ void store_row(const T* s, T* __restrict__ g, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+  for (int i = threadIdx.x; i < n; i += kNT) g[i] = s[i];
 }
 template <> __device__ inline void store_row<float>(const float* s, float* __restrict__ g, int n) {
   int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
   if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
+  for (int i = threadIdx.x; i < head; i += kNT) g[i] = s[i];
   int nv = (n - head) >> 2;
   float4* gv = reinterpret_cast<float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+  for (int v = threadIdx.x; v < nv; v += kNT) {
     int i = head + 4 * v;
     __stcs(gv + v, make_float4(s[i], s[i + 1], s[i + 2], s[i + 3]));
   }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+  for (int i = head + 4 * nv + threadIdx.x; i < n; i += kNT) g[i] = s[i];
 }
 template <class T> __device__ void copy_global(const T* __restrict__ a, T* __restrict__ b, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
+  for (int i = threadIdx.x; i < n; i += kNT) b[i] = a[i];
 }
 
 // The k-th smallest |x| (0-based) as its bits, by an 8-bit radix selection
@@ -113,9 +117,9 @@ __device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* his
   unsigned long long prefix = 0, mask = 0;
   int kk = k;
   for (int shift = (int)sizeof(T) * 8 - 8; shift >= 0; shift -= 8) {
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    for (int i = threadIdx.x; i < 256; i += kNT) hist[i] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = threadIdx.x; i < n; i += kNT) {
       unsigned long long key = abs_bits(X[i]);
       if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
     }
@@ -242,7 +246,7 @@ template <int NEED, class F> __device__ __forceinline__ auto with_need_k(int nee
 // reuses them only past the next reduction's barrier.
 template <class T> __device__ __forceinline__ Stats reduce_stats(const Acc<T>& a, int need, Shared& S) {
   Stats r{0, 0, 0, 0};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (kNT + 31) >> 5;
   double v0 = (double)a.s1, v1 = (double)a.si, v2 = (double)a.s2;
   unsigned long long m = a.mx;
 #pragma unroll
@@ -292,8 +296,8 @@ __device__ __forceinline__ Stats map_trace(T* X, int n, int need, Shared& S, Op 
     constexpr int NEED = decltype(K)::value;
     Acc<T> acc;
     T ti = (T)threadIdx.x;
-    const T tstep = (T)blockDim.x;
-    for (int i = threadIdx.x; i < n; i += blockDim.x, ti += tstep) {
+    const T tstep = (T)kNT;
+    for (int i = threadIdx.x; i < n; i += kNT, ti += tstep) {
       const T o = op(X[i], i);
       X[i] = o;
       acc.template add_t<NEED>(o, ti);
@@ -310,8 +314,8 @@ __device__ __forceinline__ Stats stats_pass(const T* X, int n, int need, Shared&
     Acc<T> acc;
     if (NEED) {
       T ti = (T)threadIdx.x;
-      const T tstep = (T)blockDim.x;
-      for (int i = threadIdx.x; i < n; i += blockDim.x, ti += tstep) acc.template add_t<NEED>(X[i], ti);
+      const T tstep = (T)kNT;
+      for (int i = threadIdx.x; i < n; i += kNT, ti += tstep) acc.template add_t<NEED>(X[i], ti);
     }
     return reduce_stats(acc, NEED, S);
   });
@@ -353,12 +357,12 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
   // packInto: the detrended samples at p .. p+n (a loop of its own, so that
   // the pads' arithmetic is not evaluated for them), then the pads — odd
   // reflections tapered by `fall`, or zeros — and zeros to nfft.
-  for (int i = threadIdx.x; i < n; i += blockDim.x) Ar[p + i] = (T)((double)(X[i] - pre) - (a + b * (double)i));
+  for (int i = threadIdx.x; i < n; i += kNT) Ar[p + i] = (T)((double)(X[i] - pre) - (a + b * (double)i));
   const int rest = nfft - n;  // [0, p) and [p + n, nfft)
   if (st.reflect) {
     const T d0 = (T)((double)(X[0] - pre) - a);
     const T dn = (T)((double)(X[n - 1] - pre) - (a + b * (double)(n - 1)));
-    for (int t = threadIdx.x; t < rest; t += blockDim.x) {
+    for (int t = threadIdx.x; t < rest; t += kNT) {
       const int j = t < p ? t : t + n, i = j - p;
       T v = (T)0;
       if (i < 0) {
@@ -373,13 +377,13 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
       Ar[j] = v;
     }
   } else {
-    for (int t = threadIdx.x; t < rest; t += blockDim.x) Ar[t < p ? t : t + n] = (T)0;
+    for (int t = threadIdx.x; t < rest; t += kNT) Ar[t < p ? t : t + n] = (T)0;
   }
   __syncthreads();
   const V* tw = reinterpret_cast<const V*>(st.tw);
-  const int zo = cfft_forward<T, MAXR>(mem, ao, bo, st.fft, tw);
-  split_bridge<T>(mem, zo, m, reinterpret_cast<const Quad<T>*>(st.bridge));
-  const int yo = cfft_forward<T, MAXR>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
+  const int zo = cfft_forward<T, MAXR, kNT>(mem, ao, bo, st.fft, tw);
+  split_bridge<T, kNT>(mem, zo, m, reinterpret_cast<const Quad<T>*>(st.bridge));
+  const int yo = cfft_forward<T, MAXR, kNT>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
   // unpackFrom: the output is swap(y): sample 2k is y[k].im and 2k + 1 is
   // y[k].re, so sample j of the real view is Yr[j ^ 1].
   const T* Yr = reinterpret_cast<const T*>(reinterpret_cast<const V*>(psg_dyn_smem) + yo);
@@ -396,7 +400,7 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
 template <class T> __device__ __forceinline__ double trace_s2(const Stats& in, const T* X, int n, Shared& S) {
   if (sizeof(T) == 8 || (isfinite(in.s2) && in.s2 >= 1e-30)) return in.s2;
   Acc<double> acc;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc.template add_t<NEED_S2>((double)X[i], 0.0);
+  for (int i = threadIdx.x; i < n; i += kNT) acc.template add_t<NEED_S2>((double)X[i], 0.0);
   return reduce_stats(acc, NEED_S2, S).s2;
 }
 
@@ -439,7 +443,7 @@ template <class A> __device__ __forceinline__ A warp_excl_suffix(A v) {
 template <class T, int E>
 __device__ __forceinline__ void agc_block_sums(const T* X, int n, int w, bool rms_mode, T r, T* P, T* Sx) {
   constexpr int CH = 32 * E;
-  const int lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
+  const int lane = threadIdx.x & 31, nw = (int)(kNT >> 5);
   const int j0 = lane * E;
   const int nb = (n + w - 1) / w;
   auto term = [&](int g) {
@@ -567,12 +571,12 @@ __device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T*
       X[i] = y;
       acc.template add<NEED>(y, i);
     };
-    for (int i = first + (int)threadIdx.x; i < last; i += blockDim.x) put(i, (Sx[i - h] + P[i + h + 1]) * invW);
-    for (int i = threadIdx.x; i < headCut; i += blockDim.x) put(i, P[i + h + 1] * recip((T)(i + h + 1)));
-    for (int i = headCut + (int)threadIdx.x; i < first; i += blockDim.x) put(i, headWhole);
-    for (int i = last + (int)threadIdx.x; i < tailCut; i += blockDim.x)
+    for (int i = first + (int)threadIdx.x; i < last; i += kNT) put(i, (Sx[i - h] + P[i + h + 1]) * invW);
+    for (int i = threadIdx.x; i < headCut; i += kNT) put(i, P[i + h + 1] * recip((T)(i + h + 1)));
+    for (int i = headCut + (int)threadIdx.x; i < first; i += kNT) put(i, headWhole);
+    for (int i = last + (int)threadIdx.x; i < tailCut; i += kNT)
       put(i, (Sx[i - h] + pn) * recip((T)(n - (i - h))));
-    for (int i = tailCut + (int)threadIdx.x; i < n; i += blockDim.x) put(i, Sx[i - h] * recip((T)(n - (i - h))));
+    for (int i = tailCut + (int)threadIdx.x; i < n; i += kNT) put(i, Sx[i - h] * recip((T)(n - (i - h))));
     return reduce_stats(acc, NEED, S);
   });
 }
@@ -667,14 +671,14 @@ template <class T> __device__ __forceinline__ void store_out(const T* s, T* __re
   if (sizeof(T) == 4) {
     const int head = min((int)((4 - (((uintptr_t)g >> 2) & 3)) & 3), n);
     const int nv = (n - head) >> 2;
-    for (int i = threadIdx.x; i < head; i += blockDim.x) g[i] = s[i];
+    for (int i = threadIdx.x; i < head; i += kNT) g[i] = s[i];
     float4* gv = reinterpret_cast<float4*>(g + head);
     const float* sf = reinterpret_cast<const float*>(s) + head;
-    for (int v = threadIdx.x; v < nv; v += blockDim.x)
+    for (int v = threadIdx.x; v < nv; v += kNT)
       __stcs(gv + v, make_float4(sf[4 * v], sf[4 * v + 1], sf[4 * v + 2], sf[4 * v + 3]));
-    for (int i = head + 4 * nv + threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+    for (int i = head + 4 * nv + threadIdx.x; i < n; i += kNT) g[i] = s[i];
   } else {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = s[i];
+    for (int i = threadIdx.x; i < n; i += kNT) g[i] = s[i];
   }
 }
 
@@ -779,7 +783,7 @@ __device__ __forceinline__ void run_recipe(const DevStep* d, Stats st, T* X, int
 // loaded at the top of each row. BATCH: the rows of several jobs (several
 // plans, widths and blocks) in one launch.
 template <class T, int MAXR, bool PF, bool BATCH, int RECIPE>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
+__global__ void __launch_bounds__(kNT, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
   __shared__ SharedMem smem;
   Shared S{&smem, 0};
   __shared__ __align__(8) uint64_t bars[2];
@@ -859,8 +863,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
     const RowCtx<T> c = row_ctx<T, BATCH>(a, t);
     const RowSlot sl = slot[cur];
     T* X = reinterpret_cast<T*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
-    for (int i = threadIdx.x; i < sl.head; i += blockDim.x) X[i] = c.from[i];
-    for (int i = sl.tail + threadIdx.x; i < sl.len; i += blockDim.x) X[i] = c.from[i];
+    for (int i = threadIdx.x; i < sl.head; i += kNT) X[i] = c.from[i];
+    for (int i = sl.tail + threadIdx.x; i < sl.len; i += kNT) X[i] = c.from[i];
     if (sl.head > 0 || sl.tail < sl.len) __syncthreads();  // the ragged ends are read by other threads below
     const int n = c.n;
     if constexpr (RECIPE != RC_GENERIC) {
