@@ -133,7 +133,8 @@ class CorrelationPlan:
     def correlateInto(self, src, dst, meta: ChunkMeta, stack: "RecordStack" = None, rowMap=None):
         """correlate.nim:421-464 on CUDA tensors; with ``stack`` the
         correlated live rows are also added to it (vstack.nim:357-380) in the
-        same launch."""
+        same launch, row r to stack row ``rowMap[r]`` (−1: not stacked; a host
+        sequence, or a CUDA int32 tensor used as it is)."""
         import torch
         rows, cols = int(src.shape[0]), int(src.shape[1])
         meta.checkShape(rows)
@@ -153,8 +154,14 @@ class CorrelationPlan:
         else:
             slive, _ = meta.device(self.outSamples, 0, src.device.index)
             rm = None
-            if rowMap is not None:
+            if isinstance(rowMap, torch.Tensor) and rowMap.is_cuda:
+                if rowMap.dtype != torch.int32 or rowMap.numel() != rows or not rowMap.is_contiguous():
+                    raise ValueError(f"a device rowMap is {rows} contiguous int32 values")
+                rm = rowMap
+            elif rowMap is not None:
                 rm = torch.as_tensor(np.asarray(rowMap, np.int32), device=src.device)
+                if rm.numel() != rows:
+                    raise ValueError(f"rowMap has {rm.numel()} entries for {rows} rows")
                 self._rm = rm
             A.check(A.lib().psg_correlate_stack(self.h, stack.h, src.data_ptr(), dptr, rows, cols,
                                                 live.data_ptr(), slive.data_ptr(),

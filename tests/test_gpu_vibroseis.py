@@ -90,3 +90,31 @@ def test_stack_skips_non_finite_rows():
     f = fold.cpu().numpy()
     assert f[0, 0] == 2 and f[1, 0] == 0 and f[2, 0] == 1 and f[3, 0] == 2
     assert np.all(out.cpu().numpy()[[0, 2, 3]] == 1)
+
+
+def test_sweeps_in_one_block_stack_as_sweep_by_sweep():
+    """The gather's sweeps correlated as one block of records, each mapped to
+    its channel's stack row (a device rowMap), give the stack of the
+    sweep-by-sweep calls (float64 sums, added in another order)."""
+    pilot, recs = c3_inputs(channels=48, sweeps=3)
+    sweeps, ch, ns = recs.shape
+    plan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=3000)
+    meta1 = P.initChunkMeta(np.full(ch, P.tsLive, np.int32), np.full(ch, ns, np.int32), 2.0)
+    a = P.initRecordStack(ch, 3000, 2.0)
+    for s in range(sweeps):
+        plan.correlateInto(torch.from_numpy(recs[s]).cuda(), None, meta1, stack=a)
+    b = P.initRecordStack(ch, 3000, 2.0)
+    metan = P.initChunkMeta(np.full(sweeps * ch, P.tsLive, np.int32), np.full(sweeps * ch, ns, np.int32), 2.0)
+    rmap = (torch.arange(sweeps * ch, dtype=torch.int32, device="cuda") % ch).contiguous()
+    plan.correlateInto(torch.from_numpy(recs.reshape(sweeps * ch, ns)).cuda(), None, metan, stack=b, rowMap=rmap)
+    oa, ob = torch.zeros(ch, 3000, device="cuda"), torch.zeros(ch, 3000, device="cuda")
+    a.stackInto(oa)
+    b.stackInto(ob)
+    fa = torch.zeros(ch, 3000, dtype=torch.int32, device="cuda")
+    fb = torch.zeros_like(fa)
+    a.foldInto(fa)
+    b.foldInto(fb)
+    torch.cuda.synchronize()
+    assert torch.equal(fa, fb) and int(fa.max()) == sweeps
+    ref = float(oa.abs().max())
+    assert float((oa - ob).abs().max()) <= 1e-6 * ref
