@@ -213,7 +213,8 @@ struct InGlobal {
 // buffer memory. Butterfly b = p·s + q: p = ⌊b / s⌋ from a multiply-high by
 // magic = ⌈2^32 / s⌉ — ⌊b / s⌋ or one more for b < 2^31 — and one correction
 // (magic = 0 marks s = 1).
-template <int R, class T, int NT, class M>
+// LAST: the transform's last pass (sub = 1, so p = 0 and every twiddle is 1).
+template <int R, class T, int NT, bool LAST, class M>
 __device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, int sub, unsigned magic,
                                          const typename C2<T>::type* __restrict__ tw) {
   const int nt = NT ? NT : (int)blockDim.x;
@@ -221,17 +222,19 @@ __device__ __forceinline__ void fft_pass(const M& mem, int xo, int yo, int s, in
   V* buf = reinterpret_cast<V*>(mem.base());
   const int total = s * sub;  // also the distance between a butterfly's inputs
   for (int b = threadIdx.x; b < total; b += nt) {
-    int p = magic ? (int)__umulhi((unsigned)b, magic) : b;
-    if (p * s > b) p--;
+    int p = LAST ? 0 : (magic ? (int)__umulhi((unsigned)b, magic) : b);
+    if (!LAST && p * s > b) p--;
     const int q = b - p * s;
     V v[R];
     const V* x = buf + (xo + q + s * p);
 #pragma unroll
     for (int j = 0; j < R; j++) v[j] = x[j * total];
     Dft<V, T, R>::run(v);
-    const int ps = p * s;
+    if (!LAST) {
+      const int ps = p * s;
 #pragma unroll
-    for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&tw[ps * k]));
+      for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&tw[ps * k]));
+    }
     V* y = buf + (yo + q + s * R * p);
 #pragma unroll
     for (int k = 0; k < R; k++) y[s * k] = v[k];
@@ -260,18 +263,34 @@ __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const 
     const int r = d.radix[i];
     const int sub = cur / r;
     const unsigned mg = d.magic[i];
-    switch (r) {
-      case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 8: fft_pass<8, T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 6: fft_pass<6, T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 5: fft_pass<5, T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 4: fft_pass<4, T, NT>(mem, x, y, s, sub, mg, tw); break;
-      case 3: fft_pass<3, T, NT>(mem, x, y, s, sub, mg, tw); break;
-      default: fft_pass<2, T, NT>(mem, x, y, s, sub, mg, tw); break;
+    if (sub == 1) {
+      switch (r) {
+        case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 8: fft_pass<8, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 6: fft_pass<6, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 5: fft_pass<5, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 4: fft_pass<4, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        case 3: fft_pass<3, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+        default: fft_pass<2, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
+      }
+    } else {
+      switch (r) {
+        case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 8: fft_pass<8, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 6: fft_pass<6, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 5: fft_pass<5, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 4: fft_pass<4, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        case 3: fft_pass<3, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+        default: fft_pass<2, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
+      }
     }
     __syncthreads();
     cur = sub;

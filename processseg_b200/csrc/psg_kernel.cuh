@@ -73,43 +73,6 @@ template <class T> __device__ __forceinline__ bool fits_d(double x) {
   return isfinite(y) && y > 0;
 }
 
-// Row copies between global buffers and shared memory, 16-byte vectors where
-// the addresses allow it.
-template <class T> __device__ void load_row(const T* __restrict__ g, T* s, int n) {
-  for (int i = threadIdx.x; i < n; i += kNT) s[i] = g[i];
-}
-template <> __device__ inline void load_row<float>(const float* __restrict__ g, float* s, int n) {
-  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
-  if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += kNT) s[i] = g[i];
-  int nv = (n - head) >> 2;
-  const float4* gv = reinterpret_cast<const float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += kNT) {
-    float4 q = __ldcs(gv + v);
-    int i = head + 4 * v;
-    s[i] = q.x; s[i + 1] = q.y; s[i + 2] = q.z; s[i + 3] = q.w;
-  }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += kNT) s[i] = g[i];
-}
-template <class T> __device__ void store_row(const T* s, T* __restrict__ g, int n) {
-  for (int i = threadIdx.x; i < n; i += kNT) g[i] = s[i];
-}
-template <> __device__ inline void store_row<float>(const float* s, float* __restrict__ g, int n) {
-  int head = (int)((4 - (((uintptr_t)g >> 2) & 3)) & 3);
-  if (head > n) head = n;
-  for (int i = threadIdx.x; i < head; i += kNT) g[i] = s[i];
-  int nv = (n - head) >> 2;
-  float4* gv = reinterpret_cast<float4*>(g + head);
-  for (int v = threadIdx.x; v < nv; v += kNT) {
-    int i = head + 4 * v;
-    __stcs(gv + v, make_float4(s[i], s[i + 1], s[i + 2], s[i + 3]));
-  }
-  for (int i = head + 4 * nv + threadIdx.x; i < n; i += kNT) g[i] = s[i];
-}
-template <class T> __device__ void copy_global(const T* __restrict__ a, T* __restrict__ b, int n) {
-  for (int i = threadIdx.x; i < n; i += kNT) b[i] = a[i];
-}
-
 // The k-th smallest |x| (0-based) as its bits, by an 8-bit radix selection
 // over the bit patterns in shared memory.
 template <class T>
