@@ -419,11 +419,14 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }
-        if not args.no_serving:
+        # the one-GPU legs: the served load, the other configurations and the
+        # CPU baseline run at N = 1 only (under torchrun the other ranks wait
+        # for rank 0 at the final barrier)
+        if world == 1 and not args.no_serving:
             line["serving"] = serving_leg()
-        if not args.no_workloads:
+        if world == 1 and not args.no_workloads:
             line["workloads"] = workloads_leg(peak)
-        if not args.no_cpu:
+        if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(steps=3, warmup=1)
         print(json.dumps(line), flush=True)
     if dist:
