@@ -140,7 +140,12 @@ void psg_decode_window(int64_t shown_first, int64_t shown_last, int64_t margin,
 
 /* --------------------------------------------------------------- plans */
 /* compile, src/processSEG/pipeline.nim:466-523. Uploads the plan's tables to
- * the current device once. */
+ * the current device once. A trace is processed in one CTA's shared memory;
+ * when its FFT or AGC work areas do not fit beside it there, they go to
+ * per-CTA slices of global memory held by the workspace (the plan's
+ * psg_plan_workspace_bytes counts them). A trace itself longer than shared
+ * memory holds (about 56,000 float32 or 28,000 float64 samples) is
+ * PSG_EINVAL. PSG_WIDE=1 in the environment lays out any plan that way. */
 int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms,
                      int32_t samples, int32_t record_samples, psg_plan** out);
 void psg_plan_destroy(psg_plan* plan);
@@ -160,7 +165,8 @@ int32_t psg_plan_len(const psg_plan* plan);
 int32_t psg_plan_step_nfft(const psg_plan* plan, int32_t step);
 int32_t psg_plan_step_margin(const psg_plan* plan, int32_t step);
 /* Scratch bytes of device memory the plan needs for `rows` rows
- * (WorkspaceSize, src/processSEG/pipeline.nim:599-602). */
+ * (WorkspaceSize, src/processSEG/pipeline.nim:599-602), with the global
+ * work areas of a plan with long traces. */
 int64_t psg_plan_workspace_bytes(const psg_plan* plan, int64_t rows, int32_t cols);
 
 /* --------------------------------------------------------------- workspace */
@@ -240,6 +246,20 @@ int psg_panel_partials(const psg_plan* plan, psg_workspace* ws, int32_t part,
                        double* partial, void* stream);
 int psg_panel_factor_from(const psg_plan* plan, psg_workspace* ws, int32_t part,
                           const double* partial, double* factor_out, void* stream);
+
+/* appliedResponseInto, src/processSEG/pipeline.nim:840-880 (responseModuli,
+ * pipeline.nim:774-838): the response of the flow `ops` as applied. A unit
+ * impulse at sample samples / 2 of one live row (t0 = 0) runs through the
+ * compiled plan on the device, with every filter's trend removal set to
+ * PSG_TR_NONE (the caller's ops are not changed); gain[i] (host) receives
+ * |sum_j x[j] exp(-2 pi i hz[i] j dt)| of that output, in float64 on the
+ * device. hz and gain are host arrays of n_hz doubles. Compiles a plan and
+ * allocates the impulse row on every call; ws is grown to the plan when it
+ * does not already hold it. PSG_EINVAL when the flow does not compile.
+ * Synchronous (the legacy default stream). */
+int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms,
+                         int32_t samples, const double* hz, int32_t n_hz, double* gain,
+                         psg_workspace* ws);
 
 /* ----------------------------------------------------------- statistics */
 /* traceStatsInto, src/processSEG/gain/stats.nim:186-199: rms and maxAbs per

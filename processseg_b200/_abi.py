@@ -127,6 +127,7 @@ def _declare(lib):
         "psg_rows_flatten": (C.c_int, [P, P, P, I64, I32, DBL, P, I64, I32, I32, P, P]),
         "psg_apply": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
         "psg_apply_host": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
+        "psg_applied_response": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, P, I32, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),
         "psg_panel_partials": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),

@@ -511,12 +511,19 @@ struct psg_plan {
   size_t smem = 0;
   int grid = 1;
   bool needs_panel = false;
+  // Traces whose FFT and AGC work does not fit beside the row in shared
+  // memory: the work areas are per-CTA slices of the workspace's global
+  // scratch (gwork_stride bytes each, gwork_bytes for the plan's grid).
+  bool wide = false;
+  int64_t gwork_stride = 0, gwork_bytes = 0;
 };
 
 struct psg_workspace {
   int device = -1;
   void* d = nullptr;
   int64_t bytes = 0;
+  void* g = nullptr;  // the work areas of plans with long traces (psg_plan::wide)
+  int64_t g_bytes = 0;
   // Streams and events of the chunked host-memory apply (created on first use).
   static const int kLanes = 4;
   cudaStream_t lane[kLanes] = {};
@@ -610,6 +617,7 @@ static int64_t ws_host_bytes(bool needs_panel, int64_t rows, int32_t cols, int d
 template <class T> static const void* pipe_kernel_for(int recipe, bool pf) {
   return sizeof(T) == 4 ? pipe_kernel_f32(recipe, pf, false) : pipe_kernel_f64(recipe, pf);
 }
+template <class T> static const void* wide_kernel_for() { return sizeof(T) == 4 ? wide_kernel_f32() : wide_kernel_f64(); }
 // The batched form (float32 plans, any step sequence).
 static const void* batch_kernel_for(bool pf) { return pipe_kernel_f32(RC_GENERIC, pf, true); }
 
@@ -706,15 +714,29 @@ template <class T> static void build_device_steps(psg_plan* p) {
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, p->threads, sm));
     return per_sm;
   };
-  int one = occupancy(false), two = occupancy(true);
-  p->prefetch = two > 0 && two >= one;
-  if (const char* e = getenv("PSG_PREFETCH")) p->prefetch = atoi(e) != 0 && two > 0;
-  p->work_off = (p->prefetch ? 2 : 1) * p->x_bytes;
-  p->smem = (size_t)(p->work_off + work);
   int limit = g_max_smem - (int)sizeof(SharedMem) - 1024;
-  if ((int64_t)p->smem > limit)
-    throw InvalidArg("the plan's traces (" + std::to_string(p->host.samples) + " samples) and FFTs need " +
-                     std::to_string(p->smem) + " bytes of shared memory; the device gives " + std::to_string(limit));
+  // PSG_WIDE=1 in the environment (read at compile time) puts every plan's
+  // work areas in global memory: the layout of long traces, for any plan.
+  const char* wide_env = getenv("PSG_WIDE");
+  const bool force_wide = wide_env && atoi(wide_env) != 0;
+  if (!force_wide && (int64_t)p->x_bytes + work <= limit) {
+    int one = occupancy(false), two = occupancy(true);
+    p->prefetch = two > 0 && two >= one;
+    if (const char* e = getenv("PSG_PREFETCH")) p->prefetch = atoi(e) != 0 && two > 0;
+    p->work_off = (p->prefetch ? 2 : 1) * p->x_bytes;
+    p->smem = (size_t)(p->work_off + work);
+  } else {
+    // The row alone in shared memory; the FFT and AGC work areas in global
+    // memory, one slice per CTA of the grid.
+    if (p->x_bytes > limit)
+      throw InvalidArg("a trace of " + std::to_string(p->host.samples) + " samples needs " +
+                       std::to_string(p->x_bytes) + " bytes of shared memory; the device gives " + std::to_string(limit));
+    p->wide = true;
+    p->prefetch = false;
+    p->work_off = p->x_bytes;
+    p->smem = (size_t)p->x_bytes;
+    p->gwork_stride = align256(work);
+  }
   if (!ds.empty()) {
     DeviceBuf* b = new DeviceBuf();
     p->keep.emplace_back(b);
@@ -722,11 +744,12 @@ template <class T> static void build_device_steps(psg_plan* p) {
     CUDA_OK(cudaMemcpy(b->p, ds.data(), ds.size() * sizeof(DevStep), cudaMemcpyHostToDevice));
     p->d_steps = (DevStep*)b->p;
   }
-  auto kern = pipe_kernel_for<T>(RC_GENERIC, p->prefetch);
+  auto kern = p->wide ? wide_kernel_for<T>() : pipe_kernel_for<T>(RC_GENERIC, p->prefetch);
   allow_smem(kern);
   int per_sm = 0;
   CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p->threads, p->smem));
   p->grid = std::max(1, per_sm) * g_sm_count;
+  if (p->wide) p->gwork_bytes = p->gwork_stride * p->grid;
 }
 
 // The per-panel factor of part `part` (which starts with a per-panel
@@ -784,7 +807,12 @@ static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void*
   bool nothing = a.job.first >= a.job.last && !factor && (src == nullptr || src == dst);
   if (nothing || rows == 0) return;
   int grid = (int)std::min<int64_t>(rows, p->grid);
-  const void* kern = pipe_kernel_for<T>(p->recipe[part], p->prefetch);
+  if (p->wide) {
+    if (ws->g_bytes < p->gwork_bytes) throw WorkspaceError("reserve the workspace for the plan first");
+    a.gwork = (unsigned char*)ws->g;
+    a.gwork_stride = p->gwork_stride;
+  }
+  const void* kern = p->wide ? wide_kernel_for<T>() : pipe_kernel_for<T>(p->recipe[part], p->prefetch);
   allow_smem(kern);
   launch_pipe(kern, grid, p->threads, p->smem, stream, a);
 }
@@ -862,23 +890,34 @@ void psg_decode_window(int64_t a, int64_t b, int64_t margin, int64_t trace_len, 
   out[1] = std::min(trace_len - 1, b + m);
 }
 
+}  // extern "C"
+
+// compile (pipeline.nim:466-523): the host plan, its recipes, its device tables.
+static std::unique_ptr<psg_plan> make_plan(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms,
+                                           int32_t samples, int32_t record_samples) {
+  std::unique_ptr<psg_plan> p(new psg_plan());
+  p->max_radix = dtype == PSG_F32 ? 12 : 8;
+  p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples, p->max_radix);
+  for (auto& r : p->host.parts) {
+    const bool panel = r.first < r.second && p->host.steps[r.first].kind == ST_NORM_PANEL;
+    p->recipe.push_back(recipe_of(p->host, panel ? r.first + 1 : r.first, r.second));
+  }
+  ensure_device();
+  CUDA_OK(cudaGetDevice(&p->device));
+  if (dtype == PSG_F32) build_device_steps<float>(p.get());
+  else build_device_steps<double>(p.get());
+  if (p->wide) std::fill(p->recipe.begin(), p->recipe.end(), (int)RC_GENERIC);
+  return p;
+}
+
+extern "C" {
+
 int psg_plan_compile(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms, int32_t samples,
                      int32_t record_samples, psg_plan** out) {
   return guarded([&] {
     if (!out) throw InvalidArg("null argument");
     *out = nullptr;
-    std::unique_ptr<psg_plan> p(new psg_plan());
-    p->max_radix = dtype == PSG_F32 ? 12 : 8;
-    p->host = compile_plan(ops, n_ops, dtype, dt_ms, samples, record_samples, p->max_radix);
-    for (auto& r : p->host.parts) {
-      const bool panel = r.first < r.second && p->host.steps[r.first].kind == ST_NORM_PANEL;
-      p->recipe.push_back(recipe_of(p->host, panel ? r.first + 1 : r.first, r.second));
-    }
-    ensure_device();
-    CUDA_OK(cudaGetDevice(&p->device));
-    if (dtype == PSG_F32) build_device_steps<float>(p.get());
-    else build_device_steps<double>(p.get());
-    *out = p.release();
+    *out = make_plan(ops, n_ops, dtype, dt_ms, samples, record_samples).release();
   });
 }
 void psg_plan_destroy(psg_plan* plan) { delete plan; }
@@ -902,7 +941,7 @@ int32_t psg_plan_step_margin(const psg_plan* p, int32_t i) {
   return (int32_t)p->host.steps[i].margin();
 }
 int64_t psg_plan_workspace_bytes(const psg_plan* p, int64_t rows, int32_t cols) {
-  return p ? ws_host_bytes(p->needs_panel, rows, cols, p->host.dtype) : 0;
+  return p ? ws_host_bytes(p->needs_panel, rows, cols, p->host.dtype) + p->gwork_bytes : 0;
 }
 
 int psg_workspace_create(psg_workspace** out) {
@@ -921,6 +960,7 @@ void psg_workspace_destroy(psg_workspace* ws) {
     cudaEventDestroy(ws->start_ev);
   }
   if (ws->d) cudaFree(ws->d);
+  if (ws->g) cudaFree(ws->g);
   delete ws;
 }
 static void ws_grow(psg_workspace* ws, int64_t need) {
@@ -939,14 +979,27 @@ static void ws_grow(psg_workspace* ws, int64_t need) {
   ws->bytes = need;
   ws->device = dev;
 }
+// The arena and, for a plan with long traces, its global work areas.
+static void ws_grow_for(psg_workspace* ws, const psg_plan* p, int64_t rows, int32_t cols) {
+  ws_grow(ws, ws_host_bytes(p->needs_panel, rows, cols, p->host.dtype));
+  if (ws->g_bytes >= p->gwork_bytes) return;
+  if (ws->g) {
+    CUDA_OK(cudaDeviceSynchronize());
+    CUDA_OK(cudaFree(ws->g));
+    ws->g = nullptr;
+    ws->g_bytes = 0;
+  }
+  CUDA_OK(cudaMalloc(&ws->g, (size_t)p->gwork_bytes));
+  ws->g_bytes = p->gwork_bytes;
+}
 int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows, int32_t cols) {
   return guarded([&] {
     if (!ws || !plan) throw InvalidArg("null argument");
     if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
-    ws_grow(ws, ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype));
+    ws_grow_for(ws, plan, rows, cols);
   });
 }
-int64_t psg_workspace_bytes(const psg_workspace* ws) { return ws ? ws->bytes : 0; }
+int64_t psg_workspace_bytes(const psg_workspace* ws) { return ws ? ws->bytes + ws->g_bytes : 0; }
 
 int psg_rows_flatten(const int32_t* status, const int32_t* num_samples, const double* t0_ms, int64_t rows,
                      int32_t first_sample, double dt_ms, const int64_t* failed, int64_t n_failed, int32_t cols,
@@ -992,7 +1045,7 @@ static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src
   if (need_ws) {
     if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
     int64_t need = plan->needs_panel ? ws_device_bytes(rows) : 512;
-    if (ws->bytes < need) throw WorkspaceError("reserve the workspace for the plan first");
+    if (ws->bytes < need || ws->g_bytes < plan->gwork_bytes) throw WorkspaceError("reserve the workspace for the plan first");
   }
 }
 
@@ -1022,7 +1075,8 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
   return guarded([&] {
     check_apply(plan, ws, src_host, dst_host, rows, cols, live_host, dt_ms, false);
     if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
-    if (ws->bytes < ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype)) throw WorkspaceError("reserve the workspace for the plan first");
+    if (ws->bytes < ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype) || ws->g_bytes < plan->gwork_bytes)
+      throw WorkspaceError("reserve the workspace for the plan first");
     if (rows == 0) return;
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -1178,6 +1232,85 @@ int psg_panel_factor_from(const psg_plan* plan, psg_workspace* ws, int32_t part,
                                                  ns.norm_target, plan->host.dtype);
     CUDA_OK(cudaMemcpyAsync(factor_out, &out->factor, 8, cudaMemcpyDeviceToDevice, s));
     CUDA_OK(cudaGetLastError());
+  });
+}
+
+}  // extern "C"
+
+// responseModuli (pipeline.nim:774-838): |Σ_j x[j]·exp(−2πi·f·j·dt)| at each
+// frequency, one warp per frequency. Each lane sums every 32nd sample in
+// float64 at the angle ((−2π·f)·j)·dt, rounded as the reference forms it
+// (its phasor is snapped onto that angle every sample); the sine and cosine
+// are taken at each sample instead of stepping a phasor, and the lanes' sums
+// fold by shuffles.
+template <class T>
+__global__ void __launch_bounds__(256) response_moduli_kernel(const T* __restrict__ x, int n,
+                                                              const double* __restrict__ hz, int m, double dt_s,
+                                                              double* __restrict__ gain) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < m; k += warps) {
+    const double a = (-2.0 * 3.141592653589793) * hz[k];
+    double re = 0, im = 0;
+    for (int j = lane; j < n; j += 32) {
+      const double v = (double)x[j];
+      double sn, cs;
+      sincos(__dmul_rn(a, (double)j) * dt_s, &sn, &cs);
+      re += v * cs;
+      im += v * sn;
+    }
+    re = warp_sum(re);
+    im = warp_sum(im);
+    if (lane == 0) gain[k] = hypot(re, im);
+  }
+}
+
+template <class T>
+static void applied_response(const psg_plan* p, psg_workspace* ws, int32_t samples, const double* hz, int32_t n_hz,
+                             double* gain) {
+  const size_t xb = align256((int64_t)samples * (int64_t)sizeof(T));
+  DeviceBuf buf;
+  CUDA_OK(cudaMalloc(&buf.p, xb + 256 + 256 + align256((int64_t)n_hz * 16)));
+  char* base = (char*)buf.p;
+  T* x = reinterpret_cast<T*>(base);
+  int* live = reinterpret_cast<int*>(base + xb);
+  double* start = reinterpret_cast<double*>(base + xb + 256);
+  double* dhz = reinterpret_cast<double*>(base + xb + 512);
+  double* dg = dhz + n_hz;
+  // a unit impulse at samples / 2 on one live row at t0 = 0
+  const T one = (T)1;
+  const double zero = 0;
+  CUDA_OK(cudaMemset(x, 0, (size_t)samples * sizeof(T)));
+  CUDA_OK(cudaMemcpy(x + samples / 2, &one, sizeof(T), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(live, &samples, sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(start, &zero, sizeof(double), cudaMemcpyHostToDevice));
+  if (n_hz > 0) CUDA_OK(cudaMemcpy(dhz, hz, (size_t)n_hz * sizeof(double), cudaMemcpyHostToDevice));
+  for (int part = 0; part < (int)p->host.parts.size(); part++)
+    launch_part<T>(p, ws, part, nullptr, x, 1, samples, live, start, 0);
+  if (n_hz > 0) {
+    const int grid = (int)std::min<int64_t>(((int64_t)n_hz + 7) / 8, (int64_t)g_sm_count * 8);
+    response_moduli_kernel<T><<<grid, 256>>>(x, samples, dhz, n_hz, p->host.dt_ms / 1000, dg);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemcpy(gain, dg, (size_t)n_hz * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  CUDA_OK(cudaDeviceSynchronize());
+}
+
+extern "C" {
+
+int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms, int32_t samples,
+                         const double* hz, int32_t n_hz, double* gain, psg_workspace* ws) {
+  return guarded([&] {
+    if (n_ops < 0 || (n_ops > 0 && !ops) || n_hz < 0 || (n_hz > 0 && (!hz || !gain)) || !ws)
+      throw InvalidArg("null argument");
+    // the filters without their trend removal, so that it does not bend the impulse
+    std::vector<psg_op> copy(ops, ops + n_ops);
+    for (auto& o : copy)
+      if (o.kind == PSG_OP_FILTER || o.kind == PSG_OP_IIR) o.trend = PSG_TR_NONE;
+    std::unique_ptr<psg_plan> p = make_plan(copy.data(), n_ops, dtype, dt_ms, samples, 0);
+    ws_grow_for(ws, p.get(), 1, samples);
+    if (dtype == PSG_F32) applied_response<float>(p.get(), ws, samples, hz, n_hz, gain);
+    else applied_response<double>(p.get(), ws, samples, hz, n_hz, gain);
   });
 }
 
@@ -1859,6 +1992,7 @@ int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* 
     check_apply(plan, nullptr, src_host, dst_host, rows, cols, live_host, dt_ms, false);
     if (plan->host.dtype != PSG_F32) throw InvalidArg("the request loop serves float32 plans");
     if (plan->host.parts.size() != 1) throw InvalidArg("the request loop serves plans without a per-panel normalization");
+    if (plan->wide) throw InvalidArg("the request loop serves plans whose traces and FFTs fit the device's shared memory");
     if (!src_host) throw InvalidArg("src is required");
     std::unique_ptr<Req> r(new Req());
     r->plan = plan;

@@ -63,6 +63,11 @@ struct PipeArgs {
   int work_off;          // byte offset of the work area
   int x_bytes;           // bytes of one row buffer (two of them with the bulk prefetch)
   int* status;           // set to 1 when a bounded wait gives up
+  // Traces whose FFT buffers do not fit beside the row in shared memory:
+  // each CTA's work area is its own slice of global memory (mostly
+  // L2-resident), gwork + blockIdx.x · gwork_stride.
+  unsigned char* gwork;
+  long long gwork_stride;
 };
 
 // ----------------------------------------------------------- device helpers
@@ -304,15 +309,16 @@ __device__ __forceinline__ void trend_from(int trend, const Stats& st, int n, do
 // (filter/apply.nim:194-231, 340-363) on the trace in shared memory.
 // `pre` is subtracted (in T) from every sample as it is read: a demean fused
 // into the filter (the caller passes the statistics of the demeaned samples).
-// NEED_K: the next step's statistics when known at compile time.
-template <class T, int MAXR, int NEED_K = -1>
+// NEED_K: the next step's statistics when known at compile time. The two
+// transform buffers are at byte `work_off` of `mem` (shared memory, or a
+// CTA's slice of global memory for traces too long for it).
+template <class T, int MAXR, int NEED_K = -1, class M = InShared>
 __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S,
-                                             T pre = (T)0) {
+                                             T pre = (T)0, const M& mem = M()) {
   typedef typename C2<T>::type V;
   const int p = st.pad, nfft = st.nfft, m = nfft / 2;
-  const InShared mem;
   const int ao = work_off / (int)sizeof(V), bo = ao + m;  // offsets of the two buffers
-  V* A = reinterpret_cast<V*>(psg_dyn_smem) + ao;
+  V* A = reinterpret_cast<V*>(mem.base()) + ao;
   double a, b;
   trend_from(st.trend, in, n, a, b);
   const T* fall = reinterpret_cast<const T*>(st.fall);
@@ -349,7 +355,7 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
   const int yo = cfft_forward<T, MAXR, kNT>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
   // unpackFrom: the output is swap(y): sample 2k is y[k].im and 2k + 1 is
   // y[k].re, so sample j of the real view is Yr[j ^ 1].
-  const T* Yr = reinterpret_cast<const T*>(reinterpret_cast<const V*>(psg_dyn_smem) + yo);
+  const T* Yr = reinterpret_cast<const T*>(reinterpret_cast<const V*>(mem.base()) + yo);
   const double gb = b * st.dc_gain;
   const double ga = st.zero_dc ? -gb * (double)(n - 1) / 2 : a * st.dc_gain;
   if (ga == 0 && gb == 0) return map_trace<NEED_K>(X, n, st.need_next, S, [&](T, int i) { return Yr[(p + i) ^ 1]; });
@@ -501,14 +507,15 @@ __device__ __forceinline__ double recip(double c) { return __drcp_rn(c); }
 // pass forms each window mean — s[i − h] + p[i + h + 1] over w for whole
 // windows, the head, whole-trace and tail forms at the ends — and scales the
 // sample by the gain, all in T.
-template <class T, int NEED_K = -1>
-__device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S) {
+template <class T, int NEED_K = -1, class M = InShared>
+__device__ __forceinline__ Stats step_agc(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S,
+                                          const M& mem = M()) {
   const int need = st.need_next;
   const bool rms_mode = st.agc_mode == PSG_AGC_RMS;
   const double rms = sqrt(trace_s2(in, X, n, S) / (double)n);
   if (rms == 0 || !fits_d<T>(st.target / rms / st.epsilon)) return stats_pass<NEED_K>(X, n, need, S);
   const int h = st.half, w = 2 * h + 1;
-  T* P = reinterpret_cast<T*>(psg_dyn_smem + work_off);  // n + 1 values
+  T* P = reinterpret_cast<T*>(mem.base() + work_off);  // n + 1 values
   T* Sx = P + ((n + 1 + 3) & ~3);                          // n values
   const T r = (T)(1 / rms);
   if (w <= 32) agc_block_sums<T, 1>(X, n, w, rms_mode, r, P, Sx);
@@ -744,9 +751,11 @@ __device__ __forceinline__ void run_recipe(const DevStep* d, Stats st, T* X, int
 // PF: prefetch the next row into the second buffer while this one is
 // processed (when the second buffer costs no occupancy); otherwise one buffer,
 // loaded at the top of each row. BATCH: the rows of several jobs (several
-// plans, widths and blocks) in one launch.
-template <class T, int MAXR, bool PF, bool BATCH, int RECIPE>
-__global__ void __launch_bounds__(kNT, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel(PipeArgs a) {
+// plans, widths and blocks) in one launch. GW: the FFT and AGC work areas in
+// global memory (a.gwork), for traces whose work does not fit beside the row
+// in shared memory.
+template <class T, int MAXR, bool PF, bool BATCH, int RECIPE, bool GW = false>
+__global__ void __launch_bounds__(kNT, (GW || sizeof(T) == 8 ? 2 : 4)) pipeline_kernel(PipeArgs a) {
   __shared__ SharedMem smem;
   Shared S{&smem, 0};
   __shared__ __align__(8) uint64_t bars[2];
@@ -877,8 +886,19 @@ __global__ void __launch_bounds__(kNT, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
           case ST_POLARITY:
             st = map_trace(X, n, need, S, [&](T x, int) { return -x; });
             break;
-          case ST_FILTER: st = step_filter<T, MAXR>(d, st, X, n, a.work_off, S); break;
-          case ST_AGC: st = step_agc(d, st, X, n, a.work_off, S); break;
+          case ST_FILTER:
+            if constexpr (GW)
+              st = step_filter<T, MAXR, -1, InGlobal>(d, st, X, n, 0, S, (T)0,
+                                                      InGlobal{a.gwork + (size_t)blockIdx.x * a.gwork_stride});
+            else
+              st = step_filter<T, MAXR>(d, st, X, n, a.work_off, S);
+            break;
+          case ST_AGC:
+            if constexpr (GW)
+              st = step_agc<T, -1, InGlobal>(d, st, X, n, 0, S, InGlobal{a.gwork + (size_t)blockIdx.x * a.gwork_stride});
+            else
+              st = step_agc(d, st, X, n, a.work_off, S);
+            break;
           case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
           case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, c.start, S); break;
           default: break;
@@ -894,6 +914,9 @@ __global__ void __launch_bounds__(kNT, (sizeof(T) == 4 ? 4 : 2)) pipeline_kernel
 // query and the shared-memory attribute. BATCH is float32 only.
 const void* pipe_kernel_f32(int recipe, bool pf, bool batch);
 const void* pipe_kernel_f64(int recipe, bool pf);
+// GW: the step switch with its work areas in global memory (single job, no prefetch)
+const void* wide_kernel_f32();
+const void* wide_kernel_f64();
 const void* recipe_kernel_f32(int recipe, bool pf);
 const void* recipe_kernel_f64(int recipe, bool pf);
 

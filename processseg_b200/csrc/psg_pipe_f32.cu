@@ -1,6 +1,7 @@
 // psg_pipe_f32.cu — the float32 instantiations of the generic pipeline_kernel
 // (any step sequence): with and without the next-row bulk prefetch,
-// single-job and batched (several plans and blocks per launch).
+// single-job and batched (several plans and blocks per launch), and the
+// single-job form whose work areas are in global memory (long traces).
 #include "psg_kernel.cuh"
 
 namespace psg {
@@ -13,5 +14,7 @@ const void* pipe_kernel_f32(int recipe, bool pf, bool batch) {
   return pf ? (const void*)pipeline_kernel<float, 12, true, false, RC_GENERIC>
             : (const void*)pipeline_kernel<float, 12, false, false, RC_GENERIC>;
 }
+
+const void* wide_kernel_f32() { return (const void*)pipeline_kernel<float, 12, false, false, RC_GENERIC, true>; }
 
 }  // namespace psg

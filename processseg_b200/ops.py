@@ -231,6 +231,25 @@ class Pipeline:
         A.check(A.lib().psg_required_margin(arr, len(self._ops), dtMs, C.byref(out)))
         return out.value
 
+    def appliedResponseInto(self, T, dtMs: float, samples: int, hz, gain, ws) -> None:
+        """The response of the flow as applied (pipeline.nim:840-880): a
+        unit impulse at sample ``samples // 2`` of one live row at t0 = 0
+        runs through the compiled plan on the device, with every filter's
+        trend removal off (this pipeline is not changed), and ``gain[i]``
+        receives ``|Σ x[j] exp(−2πi·hz[i]·j·dt)|`` of the output, in float64.
+        ``ValueError`` when the flow does not compile; ``AssertionError``
+        when ``hz`` and ``gain`` differ in length. Compiles a plan on every
+        call; ``ws`` (a ``Workspace``) is grown to it when needed."""
+        import numpy as np
+        from .plan import _dtype_code
+        hz_a = np.ascontiguousarray(np.asarray(hz, dtype=np.float64).reshape(-1))
+        assert len(gain) == len(hz_a), "hz and gain need the same length"
+        out = np.zeros(len(hz_a), dtype=np.float64)
+        A.check(A.lib().psg_applied_response(self.c_ops(), len(self._ops), _dtype_code(T), float(dtMs),
+                                             int(samples), hz_a.ctypes.data, len(hz_a), out.ctypes.data, ws.h))
+        for i in range(len(out)):
+            gain[i] = float(out[i])
+
 
 def initPipeline(ops: Iterable[Op] = ()) -> Pipeline:
     return Pipeline(ops)

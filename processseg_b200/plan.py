@@ -124,6 +124,13 @@ class PipelinePlan:
     def stepMargin(self, i: int) -> int:
         return A.lib().psg_plan_step_margin(self.h, i)
 
+    def workspaceSize(self, rows: int = 65536, cols: int = 0) -> int:
+        """The device bytes ``Workspace.reserve(plan, rows, cols)`` holds
+        for this plan (pipeline.nim ``workspaceSize``): the arena, plus the
+        global work areas of a plan whose traces are too long for their FFT
+        buffers to sit beside them in shared memory."""
+        return A.lib().psg_plan_workspace_bytes(self.h, int(rows), int(cols))
+
     # ---------------------------------------------------------------- apply
     def _check_block(self, x, name):
         if x.ndim != 2:

@@ -326,3 +326,68 @@ def test_recipe_kernels_and_step_switch_match_oracle(flow, monkeypatch):
         assert np.all(np.isfinite(got[ok]))
         assert_parity(got[ok], flow, g.data[ok], P.initChunkMeta(g.status[ok], g.numSamples[ok], 2.0,
                                                                   g.t0Ms[ok], 0), P.F32, 2.0)
+
+
+def long_gather(rows, cols, dtMs, dtype, seed):
+    g = synth.shot_gather(rows, cols, dtMs, seed, dtype, live_range=(cols // 2, cols), sine_hz=50.0,
+                          workload="long")
+    g.status[[2]] = P.tsDead
+    return g
+
+
+@pytest.mark.parametrize("dtype,cols,dtMs,flow", [
+    (P.F64, 16384, 0.5, [P.demeanOp(), P.bandPassOp(P.Corners(8, 12, 40, 50)), P.agcOp(200)]),
+    (P.F32, 30000, 1.0, [P.demeanOp(), P.bandPassOp(P.Corners(2, 5, 120, 150)), P.agcOp(250),
+                         P.normalizeOp(P.normPercentile, percentile=99.0)]),
+    (P.F64, 20000, 1.0, [P.agcOp(500), P.scaleOp(2)]),
+], ids=["f64-16384-filter-agc", "f32-30000-filter-agc-p99", "f64-20000-agc"])
+def test_long_traces_match_oracle(dtype, cols, dtMs, flow):
+    """Traces whose FFT (or AGC) work areas do not fit beside the row in
+    shared memory run with those areas in global memory; the same bar
+    against the oracle, on ragged live lengths with a dead row."""
+    npdt = np.float32 if dtype == P.F32 else np.float64
+    g = long_gather(7, cols, dtMs, npdt, seed=11)
+    meta = g.meta()
+    got = run_gpu(flow, g.data, meta, dtype, dtMs)
+    assert_parity(got, flow, g.data, meta, dtype, dtMs)
+    assert np.array_equal(got[2], g.data[2])
+
+
+@pytest.mark.parametrize("dtype", [P.F32, P.F64])
+def test_global_work_layout_matches_shared_bit_for_bit(dtype, monkeypatch):
+    """PSG_WIDE=1 (read at compile time) puts any plan's work areas in global
+    memory: the step switch then gives the same bits as with them in shared
+    memory."""
+    npdt = np.float32 if dtype == P.F32 else np.float64
+    g = synth.c2(rows=97, dtype=npdt)
+    g.data[9, 100] = np.inf
+    meta = g.meta()
+    flow = C2_FLOW + [P.normalizeOp(P.normRms)]
+    monkeypatch.setenv("PSG_RECIPES", "0")
+    shared = run_gpu(flow, g.data, meta, dtype, 2.0)
+    monkeypatch.setenv("PSG_WIDE", "1")
+    wide = run_gpu(flow, g.data, meta, dtype, 2.0)
+    wide_host = run_gpu(flow, g.data, meta, dtype, 2.0, host=True)
+    np.testing.assert_array_equal(wide, shared)
+    np.testing.assert_array_equal(wide_host, shared)
+
+
+def test_long_trace_workspace_and_limits():
+    """A plan with long traces needs its workspace reserved for it (the
+    reference's AssertionDefect otherwise); a trace too long for one CTA's
+    shared memory is refused at compile time."""
+    flow = P.initPipeline([P.bandPassOp(P.Corners(8, 12, 40, 50))])
+    long_plan = flow.compile(P.float64, 0.5, 16384)
+    short_plan = flow.compile(P.float64, 0.5, 2000)
+    ws = P.initWorkspace()
+    ws.reserve(short_plan, rows=4, cols=2000)
+    src = torch.zeros(4, 16384, dtype=torch.float64, device="cuda")
+    meta = P.liveMeta(4, 16384, 0.5)
+    with pytest.raises(AssertionError):
+        long_plan.apply(src, meta, ws)
+    ws.reserve(long_plan, rows=4, cols=16384)
+    long_plan.apply(src, meta, ws)
+    torch.cuda.synchronize()
+    assert ws.bytes >= long_plan.workspaceSize(4, 16384) > short_plan.workspaceSize(4, 16384)
+    with pytest.raises(ValueError, match="shared memory"):
+        flow.compile(P.float64, 0.5, 40000)
