@@ -93,11 +93,29 @@ typedef struct psg_gain_curve {
   psg_gain_knot knots[PSG_MAX_KNOTS];
 } psg_gain_curve;
 
+/* MuteCurve, src/processSEG/core/mute.nim:37-49 (table knots inline). A
+ * time mute: t_ms on every trace. A table: |offset| knots (finite, ≥ 0,
+ * strictly ascending) and their times, linear between and flat beyond. An
+ * LMO mute: t0_ms + |offset|·1000/velocity + pad_ms. */
+typedef enum psg_mute_kind { PSG_MK_TIME = 0, PSG_MK_TABLE = 1, PSG_MK_LMO = 2 } psg_mute_kind;
+#define PSG_MAX_MUTE_KNOTS 64
+typedef struct psg_mute_curve {
+  int32_t kind;       /* psg_mute_kind */
+  int32_t n_knots;
+  double t_ms;                          /* time */
+  double velocity, t0_ms, pad_ms;       /* LMO */
+  double offsets[PSG_MAX_MUTE_KNOTS];   /* table */
+  double times_ms[PSG_MAX_MUTE_KNOTS];
+} psg_mute_curve;
+
+/* IirPhase, src/processSEG/filter/iir.nim:76-80 */
+typedef enum psg_iir_phase { PSG_IP_ZERO = 0, PSG_IP_MINIMUM = 1 } psg_iir_phase;
+
 /* Op, src/processSEG/pipeline.nim:117-174, as one plain struct: the fields a
  * kind does not use are ignored. */
 typedef struct psg_op {
   int32_t kind;        /* psg_op_kind */
-  int32_t trend;       /* filter: psg_trend */
+  int32_t trend;       /* filter and IIR filter: psg_trend */
   double factor;       /* scale: factor; gain dB: dB */
   double lo, hi;       /* clip */
   psg_filter_spec filter;
@@ -105,11 +123,25 @@ typedef struct psg_op {
   int32_t agc_mode;    /* psg_agc_mode */
   int32_t norm_stat;   /* psg_norm_stat */
   int32_t norm_scope;  /* psg_norm_scope */
-  int32_t _pad;
+  int32_t iir_phase;   /* IIR filter: psg_iir_phase */
   double norm_target, percentile;     /* normalize */
   psg_gain_curve curve;
   double t_min_ms, t_max_ms;          /* gain curve table span (NaN: record end) */
+  psg_mute_curve mute;                /* top and bottom mutes */
+  double taper_ms;                    /* mute taper on the muted side */
 } psg_op;
+
+/* The trace keys a mute reads (ChunkMeta.keys, src/processSEG/core/types.nim:
+ * 206-214, with the window origin): per row its offset and t0Ms (arrays of
+ * `rows` doubles; NaN: unknown, and a mute that needs it leaves the row
+ * alone; a NULL array reads as all NaN) and the block's first sample of the
+ * trace (ChunkMeta.firstSample). */
+typedef struct psg_keys {
+  const double* offset;
+  const double* t0_ms;
+  int32_t first_sample;
+  int32_t _pad;
+} psg_keys;
 
 /* ------------------------------------------------------------------ handles */
 typedef struct psg_plan psg_plan;           /* PipelinePlan[T]                 */
@@ -159,6 +191,9 @@ int32_t psg_plan_part_count(const psg_plan* plan);
 /* partNeedsPanel, src/processSEG/pipeline.nim:649-654: 1 when part `part`
  * starts with a per-panel normalization, else 0 (also for no such part). */
 int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part);
+/* 1 when the plan mutes: it is applied with its rows' keys (the _keyed
+ * entry points; the others refuse it with PSG_EINVAL). */
+int32_t psg_plan_needs_keys(const psg_plan* plan);
 int32_t psg_plan_len(const psg_plan* plan);
 /* For step i of the plan: its FFT length (0 for steps without one) and the
  * pad laid out each side (FilterPlan.nfft / pad, filter/apply.nim:161-164). */
@@ -204,12 +239,23 @@ int psg_rows_flatten(const int32_t* status, const int32_t* num_samples,
 int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst,
               int64_t rows, int32_t cols, const int32_t* live, const double* start_ms,
               double dt_ms, void* stream);
+/* psg_apply with the rows' trace keys (device arrays), which a plan with
+ * mutes needs: the mute column of row r is (t − t0_ms[r])/dt_ms −
+ * first_sample, t the curve's time at offset[r] (core/mute.nim:209-214). */
+int psg_apply_keyed(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst,
+                    int64_t rows, int32_t cols, const int32_t* live, const double* start_ms,
+                    const psg_keys* keys, double dt_ms, void* stream);
 /* The same from and to host memory (pinned memory overlaps best): the
  * host→device copy of src, live and start_ms, the apply, and the
  * device→host copy of dst, all on `stream`; returns after dst is written. */
 int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host,
                    void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
                    const double* start_ms_host, double dt_ms, void* stream);
+/* psg_apply_host with the rows' trace keys (host arrays). */
+int psg_apply_host_keyed(const psg_plan* plan, psg_workspace* ws, const void* src_host,
+                         void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
+                         const double* start_ms_host, const psg_keys* keys_host, double dt_ms,
+                         void* stream);
 
 /* Parts API, src/processSEG/pipeline.nim:643-723: the per-panel factor of a
  * part (NaN: the block is left alone) over the whole block, on the device;
@@ -226,6 +272,11 @@ int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part,
 int psg_run_part(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src,
                  void* dst, int64_t rows, int32_t cols, const int32_t* live,
                  const double* start_ms, double dt_ms, const double* factor, void* stream);
+/* psg_run_part with the rows' trace keys (device arrays). */
+int psg_run_part_keyed(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src,
+                       void* dst, int64_t rows, int32_t cols, const int32_t* live,
+                       const double* start_ms, const psg_keys* keys, double dt_ms,
+                       const double* factor, void* stream);
 
 /* A panel split by traces over several devices (or calls): the per-panel
  * factor of panelFactor (src/processSEG/gain/gain.nim:221-240, over

@@ -57,6 +57,7 @@ def lib():
             "orc_plan_step_nfft": (I64, [P, C.c_int]),
             "orc_rows_flatten": (C.c_int, [P, P, P, I64, I32, DBL, P, I64, I32, I32, P, P]),
             "orc_plan_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int]),
+            "orc_plan_apply_keyed": (C.c_int, [P, P, P, I64, I64, P, P, P, P, I64, C.c_double, C.c_int]),
             "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int,
                                           C.POINTER(DBL), C.POINTER(DBL)]),
             "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
@@ -178,13 +179,23 @@ class OraclePlan:
     def step_nfft(self, i):
         return lib().orc_plan_step_nfft(self.h, i)
 
-    def apply(self, src, live, startMs=None, threads=1, inplace=False):
+    def apply(self, src, live, startMs=None, threads=1, inplace=False, keys=None):
         """Runs the plan on ``src`` ([rows, cols], the plan's dtype): returns
-        dst (src → dst form; the copy fused per row as the reference)."""
+        dst (src → dst form; the copy fused per row as the reference).
+        ``keys`` = (offsets, t0Ms, firstSample, dtMs): the rows' trace keys,
+        which mutes read."""
         src = np.ascontiguousarray(src)
         rows, cols = src.shape
         live = np.ascontiguousarray(live, dtype=np.int32)
         st = None if startMs is None else np.ascontiguousarray(startMs, dtype=np.float64)
+        if keys is not None:
+            off = None if keys[0] is None else np.ascontiguousarray(keys[0], dtype=np.float64)
+            t0 = None if keys[1] is None else np.ascontiguousarray(keys[1], dtype=np.float64)
+            dst = src.copy() if inplace else np.zeros_like(src)
+            _check(lib().orc_plan_apply_keyed(self.h, None if inplace else _ptr(src), _ptr(dst), rows, cols,
+                                              _ptr(live), _ptr(st), _ptr(off), _ptr(t0), int(keys[2]),
+                                              float(keys[3]), threads))
+            return dst
         if inplace:
             dst = src.copy()
             _check(lib().orc_plan_apply(self.h, None, _ptr(dst), rows, cols, _ptr(live), _ptr(st),

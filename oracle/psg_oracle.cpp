@@ -1025,10 +1025,80 @@ template <class T> void applyGainCurve(const CurvePlan<T>& plan, T* x, int64_t n
   }
 }
 
+// ------------------------------------------------------------ core/mute --
+// MuteCurve.muteTimeMs, core/mute.nim:103-123
+double muteTimeMs(const psg_mute_curve& c, double msPerDist, double offset) {
+  switch (c.kind) {
+    case PSG_MK_TIME: return c.t_ms;
+    case PSG_MK_LMO: return c.t0_ms + std::fabs(offset) * msPerDist + c.pad_ms;
+    default: {
+      double x = std::fabs(offset);
+      if (std::isnan(x)) return NaN;
+      int last = c.n_knots - 1;
+      if (x <= c.offsets[0]) return c.times_ms[0];
+      if (x >= c.offsets[last]) return c.times_ms[last];
+      int lo = 0, hi = last;
+      while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (c.offsets[mid] <= x) lo = mid; else hi = mid;
+      }
+      double u = (x - c.offsets[lo]) / (c.offsets[hi] - c.offsets[lo]);
+      return c.times_ms[lo] + u * (c.times_ms[hi] - c.times_ms[lo]);
+    }
+  }
+}
+// core/mute.nim:127-137
+int64_t firstAtOrAfter(double c, int64_t n) {
+  if (!(c > 0)) return 0;
+  if (c >= (double)n) return n;
+  return (int64_t)std::ceil(c);
+}
+int64_t firstAfter(double c, int64_t n) {
+  if (!(c >= 0)) return 0;
+  if (c >= (double)n) return n;
+  return (int64_t)std::floor(c) + 1;
+}
+// muteTop, core/mute.nim:139-159
+template <class T> void muteTop(T* x, int64_t n, double startCol, double taperCols) {
+  if (std::isnan(startCol)) return;
+  if (!(taperCols < INF)) taperCols = 0.0;
+  double rampStart = startCol - taperCols;
+  int64_t zeroEnd = firstAtOrAfter(rampStart, n);
+  for (int64_t j = 0; j < zeroEnd; j++) x[j] = T(0);
+  if (taperCols > 0)
+    for (int64_t j = zeroEnd; j < firstAtOrAfter(startCol, n); j++) {
+      double w = std::sin(PI / 2 * ((double)j - rampStart) / taperCols);
+      x[j] = T((double)x[j] * (w * w));
+    }
+}
+// muteBottom, core/mute.nim:161-180
+template <class T> void muteBottom(T* x, int64_t n, double endCol, double taperCols) {
+  if (std::isnan(endCol)) return;
+  if (!(taperCols < INF)) taperCols = 0.0;
+  double rampEnd = endCol + taperCols;
+  int64_t zeroStart = firstAfter(rampEnd, n);
+  if (taperCols > 0)
+    for (int64_t j = firstAfter(endCol, n); j < zeroStart; j++) {
+      double w = std::sin(PI / 2 * (rampEnd - (double)j) / taperCols);
+      x[j] = T((double)x[j] * (w * w));
+    }
+  for (int64_t j = zeroStart; j < n; j++) x[j] = T(0);
+}
+// The keys a mute reads per row (ChunkMeta.keys, core/types.nim:206-214).
+struct RowKeys {
+  const double* offset = nullptr;  // NULL: NaN
+  const double* t0 = nullptr;      // NULL: NaN
+  int64_t firstSample = 0;
+  double dtMs = 0;
+};
+
 // -------------------------------------------------------------- pipeline --
-enum StepKind { stDemean, stDetrend, stScale, stClip, stPolarity, stFilter, stAgc, stNormTrace, stNormPanel, stGainCurve };
+enum StepKind { stDemean, stDetrend, stScale, stClip, stPolarity, stFilter, stAgc, stNormTrace, stNormPanel, stGainCurve,
+                stMuteTop, stMuteBottom };
 template <class T> struct Step {
   StepKind kind;
+  psg_mute_curve mute{};
+  double msPerDist = 0, taperMs = 0;
   double factor = 0, lo = 0, hi = 0;
   FilterPlan<T> filter;
   AgcPlan agc;
@@ -1078,6 +1148,32 @@ template <class T> Step<T> compileOp(const psg_op& op, double dtMs, int64_t samp
       s.kind = op.norm_scope == PSG_PER_PANEL ? stNormPanel : stNormTrace; break;
     case PSG_OP_GAIN_CURVE:
       s.kind = stGainCurve; s.curve = initGainCurvePlan<T>(op.curve, dtMs, record, op.t_min_ms, op.t_max_ms); break;
+    case PSG_OP_MUTE_TOP:
+    case PSG_OP_MUTE_BOTTOM: {
+      // pipeline.nim:417-424 and the builders' checks, core/mute.nim:55-97
+      const psg_mute_curve& c = op.mute;
+      if (c.kind == PSG_MK_TIME) {
+        if (!isFin(c.t_ms)) throw ValueError("a mute time must be finite, got " + fmt(c.t_ms));
+      } else if (c.kind == PSG_MK_TABLE) {
+        if (c.n_knots < 1 || c.n_knots > PSG_MAX_MUTE_KNOTS) throw ValueError("a mute table needs 1 .. 64 knots");
+        for (int i = 0; i < c.n_knots; i++) {
+          if (!isFin(c.offsets[i]) || c.offsets[i] < 0) throw ValueError("mute table offsets must be finite and >= 0");
+          if (i > 0 && c.offsets[i] <= c.offsets[i - 1]) throw ValueError("mute table offsets must be strictly ascending");
+          if (!isFin(c.times_ms[i])) throw ValueError("mute table times must be finite");
+        }
+      } else if (c.kind == PSG_MK_LMO) {
+        if (!isFin(c.velocity) || c.velocity <= 0) throw ValueError("an LMO mute velocity must be finite and positive");
+        if (!isFin(c.t0_ms) || !isFin(c.pad_ms)) throw ValueError("LMO mute times must be finite");
+      } else {
+        throw ValueError("unknown mute kind");
+      }
+      if (!isFin(op.taper_ms) || op.taper_ms < 0) throw ValueError("a mute taper must be finite and >= 0 ms, got " + fmt(op.taper_ms));
+      s.kind = op.kind == PSG_OP_MUTE_TOP ? stMuteTop : stMuteBottom;
+      s.mute = c;
+      s.msPerDist = c.kind == PSG_MK_LMO ? 1000 / c.velocity : 0;
+      s.taperMs = op.taper_ms;
+      break;
+    }
     default:
       throw ValueError("this op is not supported by the oracle");
   }
@@ -1109,9 +1205,20 @@ template <class T> Plan<T> compile(const psg_op* ops, int nops, double dtMs, int
   p.parts.push_back({start, (int)p.steps.size()});
   return p;
 }
-// pipeline.nim:671-688 on one row
-template <class T> void runStep(const Step<T>& s, T* x, int64_t n, double startMs, int64_t cols) {
+// pipeline.nim:671-688 on one row; `k` holds the row's keys (r: its index).
+template <class T> void runStep(const Step<T>& s, T* x, int64_t n, double startMs, int64_t cols, const RowKeys& k,
+                                int64_t r) {
   switch (s.kind) {
+    case stMuteTop:
+    case stMuteBottom: {
+      // muteCol, core/mute.nim:209-214, and the block forms :216-240
+      double off = k.offset ? k.offset[r] : NaN, t0 = k.t0 ? k.t0[r] : NaN;
+      double col = (muteTimeMs(s.mute, s.msPerDist, off) - t0) / k.dtMs - (double)k.firstSample;
+      double taperCols = s.taperMs / k.dtMs;
+      if (s.kind == stMuteTop) muteTop(x, n, col, taperCols);
+      else muteBottom(x, n, col, taperCols);
+      break;
+    }
     case stDemean: demean(x, n); break;
     case stDetrend: detrend(x, n); break;
     case stPolarity: polarity(x, n); break;
@@ -1128,7 +1235,7 @@ template <class T> void runStep(const Step<T>& s, T* x, int64_t n, double startM
 // (rows are independent, so the reference's 256 KB tiles give the same values).
 template <class T>
 void runPart(const Plan<T>& plan, int part, const T* src, T* dst, int64_t r0, int64_t r1, int64_t cols,
-             const int32_t* live, const double* startMs, double factor) {
+             const int32_t* live, const double* startMs, double factor, const RowKeys& keys) {
   auto range = plan.parts[part];
   int first = (range.first < range.second && plan.steps[range.first].kind == stNormPanel) ? range.first + 1 : range.first;
   if (src && src != dst) std::memcpy(dst + r0 * cols, src + r0 * cols, (size_t)(r1 - r0) * cols * sizeof(T));
@@ -1137,7 +1244,7 @@ void runPart(const Plan<T>& plan, int part, const T* src, T* dst, int64_t r0, in
     if (n <= 0) continue;
     T* x = dst + r * cols;
     if (!std::isnan(factor)) scale(x, n, factor);
-    for (int i = first; i < range.second; i++) runStep(plan.steps[i], x, n, startMs ? startMs[r] : NaN, cols);
+    for (int i = first; i < range.second; i++) runStep(plan.steps[i], x, n, startMs ? startMs[r] : NaN, cols, keys, r);
   }
 }
 
@@ -1203,7 +1310,8 @@ class Pool {
 // pipeline.nim:725-734 with the pool's part/panel jobs, pool.nim:239-308.
 template <class T>
 void applyPool(Pool* pool, const Plan<T>& plan, const T* src, T* dst, int64_t rows, int64_t cols,
-               const int32_t* live, const double* startMs) {
+               const int32_t* live, const double* startMs, RowKeys keys = RowKeys()) {
+  if (!(keys.dtMs > 0)) keys.dtMs = plan.dtMs;
   int64_t grain = std::max<int64_t>(8, (256 * 1024 / std::max<int64_t>(1, cols * (int64_t)sizeof(T))) / 8 * 8);
   for (int part = 0; part < (int)plan.parts.size(); part++) {
     bool from0 = part == 0 && src && src != dst;
@@ -1213,7 +1321,7 @@ void applyPool(Pool* pool, const Plan<T>& plan, const T* src, T* dst, int64_t ro
       factor = panelFactor(plan.steps[rg.first].norm, from0 ? src : dst, rows, cols, live);
     const T* s = from0 ? src : nullptr;
     if (!pool) {
-      runPart(plan, part, s, dst, 0, rows, cols, live, startMs, factor);
+      runPart(plan, part, s, dst, 0, rows, cols, live, startMs, factor, keys);
       continue;
     }
     std::atomic<int64_t> next{0};
@@ -1221,7 +1329,7 @@ void applyPool(Pool* pool, const Plan<T>& plan, const T* src, T* dst, int64_t ro
       while (true) {
         int64_t a = next.fetch_add(grain);
         if (a >= rows) break;
-        runPart(plan, part, s, dst, a, std::min(rows, a + grain), cols, live, startMs, factor);
+        runPart(plan, part, s, dst, a, std::min(rows, a + grain), cols, live, startMs, factor, keys);
       }
     };
     pool->run(job);
@@ -1524,6 +1632,25 @@ int orc_plan_apply(void* h, const void* src, void* dst, int64_t rows, int64_t co
       applyPool(pool.get(), *(Plan<float>*)op->p, (const float*)src, (float*)dst, rows, cols, live, startMs);
     else
       applyPool(pool.get(), *(Plan<double>*)op->p, (const double*)src, (double*)dst, rows, cols, live, startMs);
+  });
+}
+// The same with the rows' keys, which a plan with mutes reads: offset and
+// t0Ms per row (NULL: NaN), the block's first sample and the rows' interval.
+int orc_plan_apply_keyed(void* h, const void* src, void* dst, int64_t rows, int64_t cols, const int32_t* live,
+                         const double* startMs, const double* offset, const double* t0, int64_t firstSample,
+                         double dtMs, int threads) {
+  return guard([&] {
+    OrcPlan* op = (OrcPlan*)h;
+    std::unique_ptr<Pool> pool(threads > 1 ? new Pool(threads) : nullptr);
+    RowKeys k;
+    k.offset = offset;
+    k.t0 = t0;
+    k.firstSample = firstSample;
+    k.dtMs = dtMs;
+    if (op->dtype == PSG_F32)
+      applyPool(pool.get(), *(Plan<float>*)op->p, (const float*)src, (float*)dst, rows, cols, live, startMs, k);
+    else
+      applyPool(pool.get(), *(Plan<double>*)op->p, (const double*)src, (double*)dst, rows, cols, live, startMs, k);
   });
 }
 // The CPU baseline: `iters` applies of the plan through one pool of

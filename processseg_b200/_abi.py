@@ -16,6 +16,7 @@ import os
 
 MAX_NOTCHES = 8
 MAX_KNOTS = 64
+MAX_MUTE_KNOTS = 64
 
 # psg_status
 OK, EINVAL, EWORKSPACE, ENOMEM, ETIMEOUT, ECUDA, ENODEV = range(7)
@@ -44,6 +45,9 @@ PANEL_PARTIAL_DOUBLES = PANEL_PARTIAL_HEAD + 65536
 GC_KNOTS, GC_POWER, GC_EXPONENTIAL = 0, 1, 2
 # psg_trace_status
 TS_UNKNOWN, TS_LIVE, TS_DEAD, TS_AUX = 0, 1, 2, 3
+# psg_mute_kind (MuteKind) / psg_iir_phase (IirPhase)
+MK_TIME, MK_TABLE, MK_LMO = 0, 1, 2
+IP_ZERO, IP_MINIMUM = 0, 1
 # psg_corr_mode / psg_fold_norm
 CM_CORRELATE, CM_DECONVOLVE = 0, 1
 FN_NONE, FN_FOLD, FN_SQRT_FOLD = 0, 1, 2
@@ -72,13 +76,25 @@ class GainCurveC(C.Structure):
                 ("db_per_s", C.c_double), ("knots", GainKnotC * MAX_KNOTS)]
 
 
+class MuteCurveC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_knots", C.c_int32), ("t_ms", C.c_double),
+                ("velocity", C.c_double), ("t0_ms", C.c_double), ("pad_ms", C.c_double),
+                ("offsets", C.c_double * MAX_MUTE_KNOTS), ("times_ms", C.c_double * MAX_MUTE_KNOTS)]
+
+
+class KeysC(C.Structure):
+    _fields_ = [("offset", C.c_void_p), ("t0_ms", C.c_void_p), ("first_sample", C.c_int32),
+                ("_pad", C.c_int32)]
+
+
 class OpC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("trend", C.c_int32), ("factor", C.c_double),
                 ("lo", C.c_double), ("hi", C.c_double), ("filter", FilterSpecC),
                 ("window_ms", C.c_double), ("target", C.c_double), ("epsilon", C.c_double),
                 ("agc_mode", C.c_int32), ("norm_stat", C.c_int32), ("norm_scope", C.c_int32),
-                ("_pad", C.c_int32), ("norm_target", C.c_double), ("percentile", C.c_double),
-                ("curve", GainCurveC), ("t_min_ms", C.c_double), ("t_max_ms", C.c_double)]
+                ("iir_phase", C.c_int32), ("norm_target", C.c_double), ("percentile", C.c_double),
+                ("curve", GainCurveC), ("t_min_ms", C.c_double), ("t_max_ms", C.c_double),
+                ("mute", MuteCurveC), ("taper_ms", C.c_double)]
 
 
 def ops_array(ops) -> C.Array:
@@ -127,9 +143,13 @@ def _declare(lib):
         "psg_rows_flatten": (C.c_int, [P, P, P, I64, I32, DBL, P, I64, I32, I32, P, P]),
         "psg_apply": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
         "psg_apply_host": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, P]),
+        "psg_apply_keyed": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P]),
+        "psg_apply_host_keyed": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P]),
+        "psg_plan_needs_keys": (I32, [P]),
         "psg_applied_response": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, P, I32, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),
+        "psg_run_part_keyed": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P, P]),
         "psg_panel_partials": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_panel_factor_from": (C.c_int, [P, P, I32, P, P, P]),
         "psg_trace_stats": (C.c_int, [P, I32, I64, I32, P, P, P, P]),

@@ -516,6 +516,7 @@ struct psg_plan {
   // scratch (gwork_stride bytes each, gwork_bytes for the plan's grid).
   bool wide = false;
   int64_t gwork_stride = 0, gwork_bytes = 0;
+  bool needs_keys = false;  // a mute reads each row's offset and t0Ms
 };
 
 struct psg_workspace {
@@ -609,7 +610,7 @@ static int64_t ws_host_bytes(bool needs_panel, int64_t rows, int32_t cols, int d
   int64_t stage_rows = host_whole_block(needs_panel, rows, cols, esz)
                            ? rows
                            : psg_workspace::kLanes * host_chunk_rows(rows, cols, esz);
-  return ws_device_bytes(rows) + align256(rows * 4) + align256(rows * 8) + align256(stage_rows * (int64_t)cols * esz);
+  return ws_device_bytes(rows) + align256(rows * 4) + 3 * align256(rows * 8) + align256(stage_rows * (int64_t)cols * esz);
 }
 
 // The pipeline kernel of a sample type and largest radix (psg_pipe_f32.cu,
@@ -681,6 +682,20 @@ template <class T> static void build_device_steps(psg_plan* p) {
       d.t_min_ms = s.t_min_ms;
       d.table_len = (int)s.table.size();
       d.table = upload(p->keep, as_t<T>(s.table));
+    } else if (s.kind == ST_MUTE_TOP || s.kind == ST_MUTE_BOTTOM) {
+      d.mute_kind = s.mute.kind;
+      d.mute_t = s.mute.t_ms;
+      d.ms_per_dist = s.ms_per_dist;
+      d.mute_t0 = s.mute.t0_ms;
+      d.mute_pad = s.mute.pad_ms;
+      d.taper_ms = s.taper_ms;
+      if (s.mute.kind == PSG_MK_TABLE) {
+        d.n_knots = s.mute.n_knots;
+        std::vector<double> k(s.mute.offsets, s.mute.offsets + s.mute.n_knots);
+        k.insert(k.end(), s.mute.times_ms, s.mute.times_ms + s.mute.n_knots);
+        d.knots = (const double*)upload(p->keep, k);
+      }
+      p->needs_keys = true;
     }
     if (s.kind == ST_NORM_PANEL) p->needs_panel = true;
     // what the step needs of its input (accumulated by the loop before it)
@@ -787,10 +802,15 @@ static bool part_needs_panel(const psg_plan* p, int part) {
 // is copied in.
 template <class T>
 static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
-                     int32_t cols, const int* live, const double* start, const double* factor, cudaStream_t stream) {
+                     int32_t cols, const int* live, const double* start, const double* factor, cudaStream_t stream,
+                     const psg_keys* keys = nullptr, double dt_ms = 0) {
   auto range = p->host.parts[part];
   bool panel = part_needs_panel(p, part);
   PipeArgs a{};
+  a.job.offset = keys ? keys->offset : nullptr;
+  a.job.t0_ms = keys ? keys->t0_ms : nullptr;
+  a.job.first_sample = keys ? keys->first_sample : 0;
+  a.job.dt_ms = dt_ms > 0 ? dt_ms : p->host.dt_ms;
   a.job.src = src;
   a.job.dst = dst;
   a.job.rows = rows;
@@ -819,11 +839,12 @@ static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void*
 
 template <class T>
 static void launch_part(const psg_plan* p, psg_workspace* ws, int part, const void* src, void* dst, int64_t rows,
-                        int32_t cols, const int* live, const double* start, cudaStream_t stream) {
+                        int32_t cols, const int* live, const double* start, cudaStream_t stream,
+                        const psg_keys* keys = nullptr, double dt_ms = 0) {
   const double* factor = nullptr;
   if (part_needs_panel(p, part))
     factor = panel_factor_dev<T>(p, ws, part, reinterpret_cast<const T*>(src ? src : dst), rows, cols, live, stream);
-  run_part<T>(p, ws, part, src, dst, rows, cols, live, start, factor, stream);
+  run_part<T>(p, ws, part, src, dst, rows, cols, live, start, factor, stream, keys, dt_ms);
 }
 
 template <class T> static void corr_upload(psg_corr_plan* p) {
@@ -932,6 +953,7 @@ int32_t psg_plan_step_nfft(const psg_plan* p, int32_t i) {
   return p->host.steps[i].kind == ST_FILTER ? (int32_t)p->host.steps[i].filter.nfft : 0;
 }
 
+int32_t psg_plan_needs_keys(const psg_plan* plan) { return plan && plan->needs_keys ? 1 : 0; }
 int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part) {
   if (!plan || part < 0 || part >= (int)plan->host.parts.size()) return 0;
   return part_needs_panel(plan, part) ? 1 : 0;
@@ -1029,8 +1051,11 @@ int psg_rows_flatten(const int32_t* status, const int32_t* num_samples, const do
 }
 
 static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
-                        const int32_t* live, double dt_ms, bool need_ws) {
+                        const int32_t* live, double dt_ms, bool need_ws, const psg_keys* keys = nullptr) {
   if (!plan) throw InvalidArg("a PipelinePlan must come from compile");
+  if (plan->needs_keys && !keys)
+    throw InvalidArg("the plan mutes: each row's offset and t0Ms are needed (apply it with its keys, psg_apply_keyed)");
+  if (keys && keys->first_sample < 0) throw InvalidArg("firstSample must be ≥ 0");
   if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
   if (rows > 0 && (!dst || !live)) throw InvalidArg("dst and live are required");
   int64_t esz = plan->host.dtype == PSG_F32 ? 4 : 8;
@@ -1051,14 +1076,19 @@ static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src
 
 int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
               const int32_t* live, const double* start_ms, double dt_ms, void* stream) {
+  return psg_apply_keyed(plan, ws, src, dst, rows, cols, live, start_ms, nullptr, dt_ms, stream);
+}
+
+int psg_apply_keyed(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
+                    const int32_t* live, const double* start_ms, const psg_keys* keys, double dt_ms, void* stream) {
   return guarded([&] {
-    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, true);
+    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, true, keys);
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
     for (int part = 0; part < (int)plan->host.parts.size(); part++) {
       const void* from = part == 0 ? src : nullptr;
-      if (plan->host.dtype == PSG_F32) launch_part<float>(plan, ws, part, from, dst, rows, cols, live, start_ms, s);
-      else launch_part<double>(plan, ws, part, from, dst, rows, cols, live, start_ms, s);
+      if (plan->host.dtype == PSG_F32) launch_part<float>(plan, ws, part, from, dst, rows, cols, live, start_ms, s, keys, dt_ms);
+      else launch_part<double>(plan, ws, part, from, dst, rows, cols, live, start_ms, s, keys, dt_ms);
     }
     CUDA_OK(cudaGetLastError());
   });
@@ -1072,8 +1102,14 @@ int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* ds
 // copy out.
 int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host, void* dst_host, int64_t rows,
                    int32_t cols, const int32_t* live_host, const double* start_ms_host, double dt_ms, void* stream) {
+  return psg_apply_host_keyed(plan, ws, src_host, dst_host, rows, cols, live_host, start_ms_host, nullptr, dt_ms, stream);
+}
+
+int psg_apply_host_keyed(const psg_plan* plan, psg_workspace* ws, const void* src_host, void* dst_host, int64_t rows,
+                         int32_t cols, const int32_t* live_host, const double* start_ms_host, const psg_keys* keys_host,
+                         double dt_ms, void* stream) {
   return guarded([&] {
-    check_apply(plan, ws, src_host, dst_host, rows, cols, live_host, dt_ms, false);
+    check_apply(plan, ws, src_host, dst_host, rows, cols, live_host, dt_ms, false, keys_host);
     if (!ws) throw WorkspaceError("reserve the workspace for the plan first");
     if (ws->bytes < ws_host_bytes(plan->needs_panel, rows, cols, plan->host.dtype) || ws->g_bytes < plan->gwork_bytes)
       throw WorkspaceError("reserve the workspace for the plan first");
@@ -1084,22 +1120,39 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
     char* base = (char*)ws->d + ws_device_bytes(rows);
     int32_t* d_live = (int32_t*)base;
     double* d_start = (double*)(base + align256(rows * 4));
-    char* d_data = base + align256(rows * 4) + align256(rows * 8);
+    double* d_offset = (double*)(base + align256(rows * 4) + align256(rows * 8));
+    double* d_t0 = (double*)(base + align256(rows * 4) + 2 * align256(rows * 8));
+    char* d_data = base + align256(rows * 4) + 3 * align256(rows * 8);
     const char* from = (const char*)(src_host ? src_host : dst_host);
     const double* dstart = start_ms_host ? d_start : nullptr;
+    const bool koff = keys_host && keys_host->offset, kt0 = keys_host && keys_host->t0_ms;
     auto run_parts = [&](void* blk, int64_t r0, int64_t nr, cudaStream_t st) {
+      psg_keys k{};
+      if (keys_host) {
+        k.offset = koff ? d_offset + r0 : nullptr;
+        k.t0_ms = kt0 ? d_t0 + r0 : nullptr;
+        k.first_sample = keys_host->first_sample;
+      }
+      const psg_keys* kp = keys_host ? &k : nullptr;
       for (int part = 0; part < (int)plan->host.parts.size(); part++) {
         if (plan->host.dtype == PSG_F32)
-          launch_part<float>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st);
+          launch_part<float>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st, kp,
+                             dt_ms);
         else
-          launch_part<double>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st);
+          launch_part<double>(plan, ws, part, nullptr, blk, nr, cols, d_live + r0, dstart ? dstart + r0 : nullptr, st, kp,
+                              dt_ms);
       }
+    };
+    auto copy_keys = [&](cudaStream_t st) {
+      if (koff) CUDA_OK(cudaMemcpyAsync(d_offset, keys_host->offset, rows * 8, cudaMemcpyHostToDevice, st));
+      if (kt0) CUDA_OK(cudaMemcpyAsync(d_t0, keys_host->t0_ms, rows * 8, cudaMemcpyHostToDevice, st));
     };
     const int64_t row_bytes = (int64_t)cols * esz;
     const int64_t chunk = host_chunk_rows(rows, cols, esz);
     if (host_whole_block(plan->needs_panel, rows, cols, esz)) {
       CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, s));
       if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, s));
+      copy_keys(s);
       CUDA_OK(cudaMemcpyAsync(d_data, from, (size_t)(rows * row_bytes), cudaMemcpyHostToDevice, s));
       run_parts(d_data, 0, rows, s);
       CUDA_OK(cudaMemcpyAsync(dst_host, d_data, (size_t)(rows * row_bytes), cudaMemcpyDeviceToHost, s));
@@ -1119,6 +1172,7 @@ int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host
     for (int i = 0; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamWaitEvent(ws->lane[i], ws->start_ev, 0));
     CUDA_OK(cudaMemcpyAsync(d_live, live_host, rows * 4, cudaMemcpyHostToDevice, ws->lane[0]));
     if (start_ms_host) CUDA_OK(cudaMemcpyAsync(d_start, start_ms_host, rows * 8, cudaMemcpyHostToDevice, ws->lane[0]));
+    copy_keys(ws->lane[0]);
     CUDA_OK(cudaEventRecord(ws->done_ev[0], ws->lane[0]));
     for (int i = 1; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamWaitEvent(ws->lane[i], ws->done_ev[0], 0));
     int k = 0;
@@ -1168,15 +1222,21 @@ int psg_panel_factor(const psg_plan* plan, psg_workspace* ws, int32_t part, cons
 int psg_run_part(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src, void* dst, int64_t rows,
                  int32_t cols, const int32_t* live, const double* start_ms, double dt_ms, const double* factor,
                  void* stream) {
+  return psg_run_part_keyed(plan, ws, part, src, dst, rows, cols, live, start_ms, nullptr, dt_ms, factor, stream);
+}
+
+int psg_run_part_keyed(const psg_plan* plan, psg_workspace* ws, int32_t part, const void* src, void* dst, int64_t rows,
+                       int32_t cols, const int32_t* live, const double* start_ms, const psg_keys* keys, double dt_ms,
+                       const double* factor, void* stream) {
   return guarded([&] {
-    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, false);
+    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, false, keys);
     if (part < 0 || part >= (int)plan->host.parts.size()) throw WorkspaceError("no part " + std::to_string(part));
     if (!ws || ws->bytes < 512) throw WorkspaceError("reserve the workspace for the plan first");
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
     const double* f = part_needs_panel(plan, part) ? factor : nullptr;
-    if (plan->host.dtype == PSG_F32) run_part<float>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s);
-    else run_part<double>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s);
+    if (plan->host.dtype == PSG_F32) run_part<float>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s, keys, dt_ms);
+    else run_part<double>(plan, ws, part, src, dst, rows, cols, live, start_ms, f, s, keys, dt_ms);
   });
 }
 
@@ -1274,19 +1334,20 @@ static void applied_response(const psg_plan* p, psg_workspace* ws, int32_t sampl
   char* base = (char*)buf.p;
   T* x = reinterpret_cast<T*>(base);
   int* live = reinterpret_cast<int*>(base + xb);
-  double* start = reinterpret_cast<double*>(base + xb + 256);
+  double* start = reinterpret_cast<double*>(base + xb + 256);  // startMs, t0Ms, offset: all 0
   double* dhz = reinterpret_cast<double*>(base + xb + 512);
   double* dg = dhz + n_hz;
-  // a unit impulse at samples / 2 on one live row at t0 = 0
+  // a unit impulse at samples / 2 on one live row at t0 = 0 and offset 0
   const T one = (T)1;
-  const double zero = 0;
+  const double zeros[3] = {0, 0, 0};
   CUDA_OK(cudaMemset(x, 0, (size_t)samples * sizeof(T)));
   CUDA_OK(cudaMemcpy(x + samples / 2, &one, sizeof(T), cudaMemcpyHostToDevice));
   CUDA_OK(cudaMemcpy(live, &samples, sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_OK(cudaMemcpy(start, &zero, sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(start, zeros, sizeof(zeros), cudaMemcpyHostToDevice));
   if (n_hz > 0) CUDA_OK(cudaMemcpy(dhz, hz, (size_t)n_hz * sizeof(double), cudaMemcpyHostToDevice));
+  const psg_keys keys{start + 2, start + 1, 0, 0};
   for (int part = 0; part < (int)p->host.parts.size(); part++)
-    launch_part<T>(p, ws, part, nullptr, x, 1, samples, live, start, 0);
+    launch_part<T>(p, ws, part, nullptr, x, 1, samples, live, start, 0, &keys, p->host.dt_ms);
   if (n_hz > 0) {
     const int grid = (int)std::min<int64_t>(((int64_t)n_hz + 7) / 8, (int64_t)g_sm_count * 8);
     response_moduli_kernel<T><<<grid, 256>>>(x, samples, dhz, n_hz, p->host.dt_ms / 1000, dg);
@@ -1993,6 +2054,7 @@ int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* 
     if (plan->host.dtype != PSG_F32) throw InvalidArg("the request loop serves float32 plans");
     if (plan->host.parts.size() != 1) throw InvalidArg("the request loop serves plans without a per-panel normalization");
     if (plan->wide) throw InvalidArg("the request loop serves plans whose traces and FFTs fit the device's shared memory");
+    if (plan->needs_keys) throw InvalidArg("the request loop serves plans without mutes");
     if (!src_host) throw InvalidArg("src is required");
     std::unique_ptr<Req> r(new Req());
     r->plan = plan;

@@ -64,7 +64,7 @@ FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, 
 // ---------------------------------------------------------------- the plan
 enum StepKind {
   ST_DEMEAN = 0, ST_DETREND, ST_SCALE, ST_CLIP, ST_POLARITY, ST_FILTER, ST_AGC,
-  ST_NORM_TRACE, ST_NORM_PANEL, ST_GAIN_CURVE
+  ST_NORM_TRACE, ST_NORM_PANEL, ST_GAIN_CURVE, ST_MUTE_TOP, ST_MUTE_BOTTOM, ST_IIR
 };
 
 struct StepHost {
@@ -82,6 +82,9 @@ struct StepHost {
   psg_gain_curve curve{};
   std::vector<double> table;
   double t_min_ms = 0;
+  // mutes (core/mute.nim): the curve, 1000/velocity of an LMO mute, the taper
+  psg_mute_curve mute{};
+  double ms_per_dist = 0, taper_ms = 0;
   int64_t margin() const { return kind == ST_FILTER ? filter.margin : (kind == ST_AGC ? half : 0); }
 };
 

@@ -40,6 +40,10 @@ struct DevStep {
   const void* tw;
   const void* table;
   psg_gain_curve curve;
+  // mutes: the curve (knots: |offset| knots then their times) and the taper
+  int mute_kind, n_knots;
+  double mute_t, ms_per_dist, mute_t0, mute_pad, taper_ms;
+  const double* knots;
 };
 
 // One apply: a block of rows and the plan steps of one part.
@@ -50,7 +54,11 @@ struct Job {
   const double* start_ms;
   const DevStep* steps;
   long long rows;
-  int cols, first, last, _pad;
+  int cols, first, last;
+  int first_sample;        // the block's first sample of the trace (mutes)
+  const double* offset;    // per row: the trace's offset (mutes; NULL: NaN)
+  const double* t0_ms;     // per row: the trace's t0Ms (mutes; NULL: NaN)
+  double dt_ms;            // the rows' sample interval
 };
 
 struct PipeArgs {
@@ -635,6 +643,80 @@ __device__ __forceinline__ Stats step_gain_curve(const DevStep& st, T* X, int n,
   });
 }
 
+// ------------------------------------------------------------ mutes
+// muteTimeMs (core/mute.nim:103-123) in the reference's order of operations
+// (no contraction into fused multiply-adds).
+__device__ __forceinline__ double mute_time_d(const DevStep& st, double offset) {
+  if (st.mute_kind == PSG_MK_TIME) return st.mute_t;
+  const double x = fabs(offset);
+  if (st.mute_kind == PSG_MK_LMO) return __dadd_rn(__dadd_rn(st.mute_t0, __dmul_rn(x, st.ms_per_dist)), st.mute_pad);
+  if (isnan(x)) return x;
+  const double* off = st.knots;
+  const double* tm = st.knots + st.n_knots;
+  const int last = st.n_knots - 1;
+  if (x <= off[0]) return tm[0];
+  if (x >= off[last]) return tm[last];
+  int lo = 0, hi = last;  // the last knot ≤ x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  const double u = __ddiv_rn(__dsub_rn(x, off[lo]), __dsub_rn(off[hi], off[lo]));
+  return __dadd_rn(tm[lo], __dmul_rn(u, __dsub_rn(tm[hi], tm[lo])));
+}
+// firstAtOrAfter / firstAfter (core/mute.nim:127-137): the first column ≥ c
+// (> c), clamped to 0 .. n, 0 for NaN.
+__device__ __forceinline__ int first_at_or_after(double c, int n) {
+  if (!(c > 0)) return 0;
+  if (c >= (double)n) return n;
+  return (int)ceil(c);
+}
+__device__ __forceinline__ int first_after(double c, int n) {
+  if (!(c >= 0)) return 0;
+  if (c >= (double)n) return n;
+  return (int)floor(c) + 1;
+}
+// muteTop / muteBottom of one row (core/mute.nim:139-200) at the column of
+// the row's keys, (t − t0Ms)/dtMs − firstSample (core/mute.nim:209-214),
+// with a taper of taperMs/dtMs columns on the muted side: sin² weights in
+// float64, zeros beyond. A NaN column leaves the row alone.
+template <class T, int NEED_K = -1>
+__device__ __forceinline__ Stats step_mute(const DevStep& st, const Job* J, long long r, T* X, int n, Shared& S) {
+  const int need = st.need_next;
+  const double offset = J->offset ? J->offset[r] : (double)NAN;
+  const double t0 = J->t0_ms ? J->t0_ms[r] : (double)NAN;
+  const double c = __dsub_rn(__ddiv_rn(__dsub_rn(mute_time_d(st, offset), t0), J->dt_ms), (double)J->first_sample);
+  if (isnan(c)) return stats_pass<NEED_K>(X, n, need, S);
+  double taper = __ddiv_rn(st.taper_ms, J->dt_ms);
+  if (!(taper < INFINITY)) taper = 0;
+  const double half_pi = 3.141592653589793 / 2;
+  if (st.kind == ST_MUTE_TOP) {
+    const double ramp = __dsub_rn(c, taper);
+    const int zero_end = first_at_or_after(ramp, n);
+    const int keep = taper > 0 ? first_at_or_after(c, n) : zero_end;
+    return map_trace<NEED_K>(X, n, need, S, [&](T v, int j) {
+      if (j < zero_end) return (T)0;
+      if (j < keep) {
+        const double w = sin(__ddiv_rn(__dmul_rn(half_pi, __dsub_rn((double)j, ramp)), taper));
+        return (T)((double)v * __dmul_rn(w, w));
+      }
+      return v;
+    });
+  }
+  const double ramp = __dadd_rn(c, taper);
+  const int zero_start = first_after(ramp, n);
+  const int keep = taper > 0 ? first_after(c, n) : zero_start;
+  return map_trace<NEED_K>(X, n, need, S, [&](T v, int j) {
+    if (j >= zero_start) return (T)0;
+    if (j >= keep) {
+      const double w = sin(__ddiv_rn(__dmul_rn(half_pi, __dsub_rn(ramp, (double)j)), taper));
+      return (T)((double)v * __dmul_rn(w, w));
+    }
+    return v;
+  });
+}
+
 // ------------------------------------------------------------ the kernel
 // Stores a row from shared memory, 16-byte vectors where the row allows.
 template <class T> __device__ __forceinline__ void store_out(const T* s, T* __restrict__ g, int n) {
@@ -667,6 +749,8 @@ template <class T> struct RowCtx {
   const T* blk_lo;  // the block `from` lies in: [blk_lo, blk_hi)
   const T* blk_hi;
   const DevStep* steps;
+  const Job* job;
+  long long r;  // the row within its job
   double start;
   int n, cols, first, last;
   bool copy;
@@ -697,6 +781,8 @@ __device__ __forceinline__ RowCtx<T> row_ctx(const PipeArgs& a, long long t) {
   c.n = min(max(J->live[r], 0), c.cols);
   c.start = J->start_ms ? J->start_ms[r] : (double)NAN;
   c.steps = J->steps;
+  c.job = J;
+  c.r = r;
   c.first = J->first;
   c.last = J->last;
   return c;
@@ -901,6 +987,8 @@ __global__ void __launch_bounds__(kNT, (GW || sizeof(T) == 8 ? 2 : 4)) pipeline_
             break;
           case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
           case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, c.start, S); break;
+          case ST_MUTE_TOP:
+          case ST_MUTE_BOTTOM: st = step_mute(d, c.job, c.r, X, n, S); break;
           default: break;
         }
       }

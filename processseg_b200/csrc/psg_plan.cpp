@@ -438,6 +438,32 @@ int64_t agc_half(double window_ms, double dt_ms, int64_t samples, double target,
   return (int64_t)h;
 }
 
+// timeMute / tableMute / lmoMute (core/mute.nim:55-97): what the builders
+// check, for curves that come through the C ABI.
+void check_mute(const psg_mute_curve& c) {
+  switch (c.kind) {
+    case PSG_MK_TIME:
+      need(fin(c.t_ms), "a mute time must be finite, got " + num(c.t_ms));
+      break;
+    case PSG_MK_TABLE:
+      need(c.n_knots >= 1, "a mute table needs at least one knot");
+      need(c.n_knots <= PSG_MAX_MUTE_KNOTS, "a mute table takes at most " + std::to_string(PSG_MAX_MUTE_KNOTS) + " knots");
+      for (int i = 0; i < c.n_knots; i++) {
+        need(fin(c.offsets[i]) && c.offsets[i] >= 0, "mute table offsets must be finite and ≥ 0, got " + num(c.offsets[i]));
+        need(i == 0 || c.offsets[i] > c.offsets[i - 1], "mute table offsets must be strictly ascending: " +
+                                                           num(c.offsets[i > 0 ? i - 1 : 0]) + " is followed by " + num(c.offsets[i]));
+        need(fin(c.times_ms[i]), "mute table times must be finite, got " + num(c.times_ms[i]));
+      }
+      break;
+    case PSG_MK_LMO:
+      need(fin(c.velocity) && c.velocity > 0, "an LMO mute velocity must be finite and positive, got " + num(c.velocity));
+      need(fin(c.t0_ms) && fin(c.pad_ms), "LMO mute times must be finite, got t0Ms " + num(c.t0_ms) + ", padMs " + num(c.pad_ms));
+      break;
+    default:
+      throw InvalidArg("unknown mute kind " + std::to_string(c.kind));
+  }
+}
+
 // pipeline.nim:392-447
 StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, int64_t record, int max_radix) {
   StepHost s;
@@ -513,6 +539,13 @@ StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, 
     }
     case PSG_OP_MUTE_TOP:
     case PSG_OP_MUTE_BOTTOM:
+      check_mute(op.mute);
+      need(fin(op.taper_ms) && op.taper_ms >= 0, "a mute taper must be finite and ≥ 0 ms, got " + num(op.taper_ms));
+      s.kind = op.kind == PSG_OP_MUTE_TOP ? ST_MUTE_TOP : ST_MUTE_BOTTOM;
+      s.mute = op.mute;
+      s.ms_per_dist = op.mute.kind == PSG_MK_LMO ? 1000 / op.mute.velocity : 0;
+      s.taper_ms = op.taper_ms;
+      break;
     case PSG_OP_IIR:
     case PSG_OP_CALIBRATE:
     case PSG_OP_UNCALIBRATE:

@@ -3,9 +3,10 @@ samples (src/processSEG/core/types.nim:69-288).
 
 The reference wraps parseSEG's ``TraceRows`` view; parseSEG is not part of
 this build, so a meta here holds the same facts as arrays: each row's trace
-status, its trace length (``numSamples``) and start time (``t0Ms``), the
-block's interval, its window origin (``firstSample``) and the rows that
-could not be decoded (``failed``, ascending).
+status, its trace length (``numSamples``), start time (``t0Ms``) and
+source-receiver offset (``offset``, which mutes read; NaN when the headers
+cannot give it), the block's interval, its window origin (``firstSample``)
+and the rows that could not be decoded (``failed``, ascending).
 
 For the device it is flattened once per block width into two arrays
 (``isLive``/``liveSamples``/``sampleTimeMs`` per row) by the library's
@@ -32,11 +33,13 @@ class ChunkMeta:
     """The metadata of a block of rows (types.nim:69-78); build it with
     ``initChunkMeta``."""
 
-    def __init__(self, status, numSamples, t0Ms, dtMs, firstSample=0, failed=()):
+    def __init__(self, status, numSamples, t0Ms, dtMs, firstSample=0, failed=(), offsets=None):
         self.status = np.ascontiguousarray(status, dtype=np.int32)
         self.numSamples = np.ascontiguousarray(numSamples, dtype=np.int32)
         self.t0 = (np.full(self.status.size, math.nan) if t0Ms is None
                    else np.ascontiguousarray(t0Ms, dtype=np.float64))
+        self.offsets = (np.full(self.status.size, math.nan) if offsets is None
+                        else np.ascontiguousarray(offsets, dtype=np.float64))
         self.dtMs = float(dtMs)
         self.firstSample = int(firstSample)
         self.failed = np.ascontiguousarray(failed, dtype=np.int64)
@@ -66,6 +69,9 @@ class ChunkMeta:
     def t0Ms(self, row: int) -> float:
         return float(self.t0[row])
 
+    def offset(self, row: int) -> float:
+        return float(self.offsets[row])
+
     def sampleTimeMs(self, row: int, col: int) -> float:
         """types.nim:237-240."""
         return float(self.t0[row]) + (self.firstSample + col) * self.dtMs
@@ -78,7 +84,7 @@ class ChunkMeta:
         sl = slice(first, last + 1)
         f = self.failed[(self.failed >= first) & (self.failed <= last)] - first
         return ChunkMeta(self.status[sl], self.numSamples[sl], self.t0[sl], self.dtMs,
-                         self.firstSample, f)
+                         self.firstSample, f, self.offsets[sl])
 
     def checkShape(self, rows: int):
         if rows != len(self):
@@ -100,6 +106,19 @@ class ChunkMeta:
             self._flat[key] = (live, start)
         return self._flat[key]
 
+    def keys(self):
+        """(offset, t0Ms) host arrays: the trace keys a mute reads."""
+        return self.offsets, self.t0
+
+    def device_keys(self, device=None):
+        """(offset, t0Ms) as CUDA tensors (cached per device)."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        key = ("keys", dev.index)
+        if key not in self._dev:
+            self._dev[key] = (torch.from_numpy(self.offsets).to(dev), torch.from_numpy(self.t0).to(dev))
+        return self._dev[key]
+
     def device(self, cols: int, mode: int = 0, device=None):
         """The flattened arrays as CUDA tensors (cached per device)."""
         import torch
@@ -113,7 +132,7 @@ class ChunkMeta:
 
 def initChunkMeta(status: Sequence[int], numSamples: Sequence[int], dtMs: float,
                   t0Ms: Optional[Sequence[float]] = None, firstSample: int = 0,
-                  failed: Sequence[int] = ()) -> ChunkMeta:
+                  failed: Sequence[int] = (), offsets: Optional[Sequence[float]] = None) -> ChunkMeta:
     """types.nim:80-122: validates once; raises ``ValueError``."""
     if not (math.isfinite(dtMs) and dtMs > 0) or (dtMs != 0 and abs(dtMs) < 2.2250738585072014e-308):
         raise ValueError(f"dtMs must be finite and positive, got {dtMs}")
@@ -122,6 +141,8 @@ def initChunkMeta(status: Sequence[int], numSamples: Sequence[int], dtMs: float,
     rows = len(status)
     if len(numSamples) != rows:
         raise ValueError("need one numSamples per row")
+    if offsets is not None and len(offsets) != rows:
+        raise ValueError("need one offset per row")
     prev = None
     for r in failed:
         if r < 0 or r >= rows:
@@ -129,7 +150,7 @@ def initChunkMeta(status: Sequence[int], numSamples: Sequence[int], dtMs: float,
         if prev is not None and r <= prev:
             raise ValueError(f"failed rows must be ascending and unique: {prev} is followed by {r}")
         prev = r
-    return ChunkMeta(status, numSamples, t0Ms, dtMs, firstSample, failed)
+    return ChunkMeta(status, numSamples, t0Ms, dtMs, firstSample, failed, offsets)
 
 
 def liveMeta(rows: int, samples: int, dtMs: float, t0Ms: float = 0.0) -> ChunkMeta:

@@ -16,6 +16,7 @@ from typing import Iterable, List, Optional
 
 from . import _abi as A
 from .design import Corners, FilterSpec, GainCurve, bandPass
+from .mute import MuteCurve
 
 
 @dataclass
@@ -44,6 +45,14 @@ class NormalizeParams:
 class ClipParams:
     lo: float
     hi: float
+
+
+@dataclass
+class MuteParams:
+    """An ``opMuteTop`` / ``opMuteBottom``: the mute time per offset and the
+    taper on the muted side (pipeline.nim:121-125)."""
+    curve: MuteCurve
+    taperMs: float = 0.0
 
 
 @dataclass
@@ -100,6 +109,10 @@ class Op:
     def gainCurve(self) -> GainCurveParams:
         return self._get((A.OP_GAIN_CURVE,), "gain curve")
 
+    @property
+    def mute(self) -> MuteParams:
+        return self._get((A.OP_MUTE_TOP, A.OP_MUTE_BOTTOM), "mute")
+
     def __repr__(self):
         return f"Op({A.OP_NAMES[self._kind]}, {self._p!r})"
 
@@ -128,6 +141,9 @@ class Op:
         elif k == A.OP_GAIN_CURVE:
             o.curve = p.curve.to_c()
             o.t_min_ms, o.t_max_ms = p.tMinMs, p.tMaxMs
+        elif k in (A.OP_MUTE_TOP, A.OP_MUTE_BOTTOM):
+            o.mute = p.curve.to_c()
+            o.taper_ms = p.taperMs
         return o
 
 
@@ -154,6 +170,17 @@ def clipOp(lo: float, hi: float) -> Op:
 
 def polarityOp() -> Op:
     return Op(A.OP_POLARITY)
+
+
+def muteTopOp(curve: MuteCurve, taperMs: float = 0.0) -> Op:
+    """Zeroes each trace before its ``curve`` time, with a taper of
+    ``taperMs`` on the muted side (pipeline.nim:282-285)."""
+    return Op(A.OP_MUTE_TOP, MuteParams(curve, float(taperMs)))
+
+
+def muteBottomOp(curve: MuteCurve, taperMs: float = 0.0) -> Op:
+    """Zeroes each trace after its ``curve`` time (pipeline.nim:287-289)."""
+    return Op(A.OP_MUTE_BOTTOM, MuteParams(curve, float(taperMs)))
 
 
 def filterOp(spec: FilterSpec, trend: int = A.TR_LINEAR) -> Op:

@@ -175,15 +175,37 @@ class PipelinePlan:
             import torch
             live, start = meta.device(cols, 0, dst.device.index)
             st = stream if stream is not None else torch.cuda.current_stream(dst.device).cuda_stream
-            A.check(A.lib().psg_apply(self.h, ws.h, None if src is None else src.data_ptr(),
-                                      dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
-                                      meta.dtMs, st))
+            keys = self._keys(meta, dst.device.index)
+            A.check(A.lib().psg_apply_keyed(self.h, ws.h, None if src is None else src.data_ptr(),
+                                            dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
+                                            keys, meta.dtMs, st))
         else:
             live, start = meta.flat(cols, 0)
             p = lambda a: a.ctypes.data_as(C.c_void_p)
-            A.check(A.lib().psg_apply_host(self.h, ws.h, None if src is None else p(src), p(dst), rows,
-                                           cols, p(live), p(start), meta.dtMs,
-                                           stream if stream is not None else None))
+            keys = self._keys(meta, None)
+            A.check(A.lib().psg_apply_host_keyed(self.h, ws.h, None if src is None else p(src), p(dst), rows,
+                                                 cols, p(live), p(start), keys, meta.dtMs,
+                                                 stream if stream is not None else None))
+
+    @property
+    def needsKeys(self) -> bool:
+        """The plan mutes: it reads each row's offset and t0Ms."""
+        return bool(A.lib().psg_plan_needs_keys(self.h))
+
+    def _keys(self, meta: ChunkMeta, device):
+        """A ``psg_keys`` for a plan that mutes (device arrays for a device
+        index, else the meta's host arrays); None for one that does not."""
+        if not self.needsKeys:
+            return None
+        k = A.KeysC()
+        if device is None:
+            off, t0 = meta.keys()
+            k.offset, k.t0_ms = off.ctypes.data, t0.ctypes.data
+        else:
+            off, t0 = meta.device_keys(device)
+            k.offset, k.t0_ms = off.data_ptr(), t0.data_ptr()
+        k.first_sample = meta.firstSample
+        return C.pointer(k)
 
     def partNeedsPanel(self, part: int) -> bool:
         """Part ``part`` starts with a per-panel normalization
@@ -209,9 +231,10 @@ class PipelinePlan:
                 raise ValueError(f"src is {src.shape[0]} × {src.shape[1]}, dst {rows} × {cols}")
         meta.checkShape(rows)
         live, start, st = self._device_call(dst, meta, cols)
-        A.check(A.lib().psg_run_part(self.h, ws.h, int(part), None if src is None else src.data_ptr(),
-                                     dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
-                                     meta.dtMs, None if factor is None else factor.data_ptr(), st))
+        A.check(A.lib().psg_run_part_keyed(self.h, ws.h, int(part), None if src is None else src.data_ptr(),
+                                           dst.data_ptr(), rows, cols, live.data_ptr(), start.data_ptr(),
+                                           self._keys(meta, dst.device.index), meta.dtMs,
+                                           None if factor is None else factor.data_ptr(), st))
 
     def panelPartials(self, b, meta: ChunkMeta, part: int, ws: Workspace):
         """The mergeable statistics of part ``part``'s per-panel

@@ -12,6 +12,7 @@ baseline and the GPU runs of one process.
 from __future__ import annotations
 
 import math
+from typing import Optional
 from dataclasses import dataclass
 
 import numpy as np
@@ -56,11 +57,12 @@ class Gather:
     t0Ms: np.ndarray        # float64 per row
     dtMs: float
     failed: np.ndarray      # ascending int64
+    offsets: Optional[np.ndarray] = None  # float64 per row (NaN: unknown)
 
     def meta(self, firstSample=0):
         from .meta import initChunkMeta
         return initChunkMeta(self.status, self.numSamples, self.dtMs, self.t0Ms, firstSample,
-                             self.failed)
+                             self.failed, self.offsets)
 
 
 def shot_gather(rows, cols, dtMs, seed, dtype=np.float32, live_range=None, sine_hz=None,
@@ -87,7 +89,8 @@ def shot_gather(rows, cols, dtMs, seed, dtype=np.float32, live_range=None, sine_
     mask = np.arange(cols)[None, :] < live[:, None]
     x = np.where(mask, x, 0.0).astype(dtype)
     return Gather(np.ascontiguousarray(x), np.full(rows, A.TS_LIVE, np.int32),
-                  live.astype(np.int32), np.zeros(rows), float(dtMs), np.zeros(0, np.int64))
+                  live.astype(np.int32), np.zeros(rows), float(dtMs), np.zeros(0, np.int64),
+                  offsets.astype(np.float64))
 
 
 def c1(seed=1, dtype=np.float32):

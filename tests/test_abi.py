@@ -6,6 +6,8 @@ import ctypes as C
 import math
 import os
 import re
+import subprocess
+import tempfile
 
 import numpy as np
 import pytest
@@ -38,7 +40,29 @@ def test_struct_layout_matches_header():
     # psg_op is shared by ctypes callers: its size is fixed by the header.
     assert C.sizeof(A.FilterSpecC) == 16 + 8 * 8 + 16 * 8
     assert C.sizeof(A.GainCurveC) == 8 + 4 * 8 + 16 * 64
-    assert C.sizeof(A.OpC) == 8 + 8 * 3 + C.sizeof(A.FilterSpecC) + 8 * 3 + 16 + 16 + C.sizeof(A.GainCurveC) + 16
+    assert C.sizeof(A.MuteCurveC) == 8 + 4 * 8 + 16 * 64
+    assert C.sizeof(A.OpC) == (8 + 8 * 3 + C.sizeof(A.FilterSpecC) + 8 * 3 + 16 + 16 + C.sizeof(A.GainCurveC) + 16
+                               + C.sizeof(A.MuteCurveC) + 8)
+    # and as the C compiler lays the header out
+    prog = r'''
+#include <stddef.h>
+#include <stdio.h>
+#include "psg.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(psg_op), offsetof(psg_op, iir_phase), offsetof(psg_op, curve),
+         offsetof(psg_op, mute), offsetof(psg_op, taper_ms), sizeof(psg_keys));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
+        with open(src, "w") as f:
+            f.write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", exe, src], check=True)
+        got = [int(v) for v in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()]
+    want = [C.sizeof(A.OpC), A.OpC.iir_phase.offset, A.OpC.curve.offset, A.OpC.mute.offset, A.OpC.taper_ms.offset,
+            C.sizeof(A.KeysC)]
+    assert got == want
 
 
 def test_fast_lengths_match_oracle():
