@@ -164,6 +164,16 @@ int64_t psg_next_fast_len(int64_t n, int even);
 int psg_impulse_length(const psg_filter_spec* spec, double dt_ms, int32_t* out);
 /* response, src/processSEG/filter/design.nim:236-255 */
 int psg_response(const psg_filter_spec* spec, double f_hz, double dt_ms, double* out);
+/* initIirPlan, src/processSEG/filter/iir.nim:193-239, on the host: the
+ * cascade's order (poles of one pass), requiredMargin and gain at 0 Hz
+ * (G(1), or G(1)² for zero phase) of a Butterworth spec (any pointer may be
+ * NULL). PSG_EINVAL for what initIirPlan rejects. */
+int psg_iir_design(const psg_filter_spec* spec, double dt_ms, int32_t samples, int32_t phase,
+                   int32_t trend, int32_t* order, int32_t* margin, double* dc_gain);
+/* IirPlan.magnitudeAt, src/processSEG/filter/iir.nim:268-278: |H| (minimum
+ * phase) or |H|² (zero phase) at n frequencies (host arrays). */
+int psg_iir_magnitude(const psg_filter_spec* spec, double dt_ms, int32_t phase,
+                      const double* f_hz, int32_t n, double* out);
 /* Pipeline.requiredMargin, src/processSEG/pipeline.nim:525-548 */
 int psg_required_margin(const psg_op* ops, int32_t n_ops, double dt_ms, int32_t* out);
 /* decodeWindow, src/processSEG/pipeline.nim:550-560: out[0..1] = first, last */

@@ -58,6 +58,9 @@ def lib():
             "orc_rows_flatten": (C.c_int, [P, P, P, I64, I32, DBL, P, I64, I32, I32, P, P]),
             "orc_plan_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int]),
             "orc_plan_apply_keyed": (C.c_int, [P, P, P, I64, I64, P, P, P, P, I64, C.c_double, C.c_int]),
+            "orc_iir_info": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_double, I64, C.c_int, C.c_int,
+                                       C.POINTER(C.c_int), C.POINTER(I64), C.POINTER(C.c_double), P, I64, P]),
+            "orc_iir_apply": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_double, I64, C.c_int, C.c_int, P, I64]),
             "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int,
                                           C.POINTER(DBL), C.POINTER(DBL)]),
             "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
@@ -218,6 +221,26 @@ class OraclePlan:
         _check(lib().orc_bench_apply(self.h, _ptr(src), _ptr(dst), rows, cols, _ptr(live), _ptr(st),
                                      threads, warm, iters, C.byref(med), C.byref(mn)))
         return med.value, mn.value
+
+
+def iir_info(spec, dtMs, samples, phase=A.IP_ZERO, trend=A.TR_LINEAR, freqs=()):
+    """(order, requiredMargin, dcGain, magnitudeAt(freqs)) of an IIR plan."""
+    c = spec.to_c()
+    f = np.ascontiguousarray(freqs, dtype=np.float64)
+    mag = np.zeros(f.size)
+    order, pad, g = C.c_int(), C.c_int64(), C.c_double()
+    _check(lib().orc_iir_info(C.byref(c), dtMs, samples, phase, trend, C.byref(order), C.byref(pad), C.byref(g),
+                              _ptr(f), f.size, _ptr(mag)))
+    return order.value, pad.value, g.value, mag
+
+
+def iir_apply(spec, dtMs, x, phase=A.IP_ZERO, trend=A.TR_LINEAR, samples=None):
+    """One trace (float64) through an IIR plan of ``samples`` (default: its
+    length), as the reference's single-trace applyFilter."""
+    c = spec.to_c()
+    y = np.ascontiguousarray(x, dtype=np.float64).copy()
+    _check(lib().orc_iir_apply(C.byref(c), dtMs, samples or y.size, phase, trend, _ptr(y), y.size))
+    return y
 
 
 def rows_flatten(status, numSamples, t0Ms, firstSample, dtMs, failed, cols, mode=0):

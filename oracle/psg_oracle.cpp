@@ -1025,6 +1025,199 @@ template <class T> void applyGainCurve(const CurvePlan<T>& plan, T* x, int64_t n
   }
 }
 
+// ------------------------------------------------------------- filter/iir --
+// A biquad, a0 = 1, with its 0 Hz gain (filter/iir.nim:82-111).
+struct Sos {
+  double b0, b1, b2, a1, a2, g;
+};
+static Sos mkSos(double b0, double b1, double b2, double a1, double a2) {
+  return Sos{b0, b1, b2, a1, a2, (b0 + b1 + b2) / (1 + a1 + a2)};
+}
+// Complex division as Nim's std/complex `/` (Smith's method).
+static void cdivNim(double xr, double xi, double yr, double yi, double& r_re, double& r_im) {
+  double r, den;
+  if (std::fabs(yr) < std::fabs(yi)) {
+    r = yr / yi;
+    den = yi + r * yr;
+    r_re = (xr * r + xi) / den;
+    r_im = (xi * r - xr) / den;
+  } else {
+    r = yi / yr;
+    den = yr + r * yi;
+    r_re = (xr + r * xi) / den;
+    r_im = (xi - r * xr) / den;
+  }
+}
+// butterSections, filter/iir.nim:113-148
+static std::vector<Sos> butterSections(double fc, double dtMs, int order, bool high) {
+  std::vector<Sos> res;
+  double fs = 1000 / dtMs;
+  double wc = 2 * fs * std::tan(PI * fc / fs);
+  double k2 = 2 * fs;
+  for (int k = 0; k < order / 2; k++) {
+    double th = PI * (double)(2 * k + 1) / (double)(2 * order);
+    double sr = -wc * std::sin(th), si = wc * std::cos(th);
+    double zr, zi;
+    cdivNim(k2 + sr, 0.0 + si, k2 - sr, 0.0 - si, zr, zi);
+    double a1 = -2 * zr, a2 = zr * zr + zi * zi;
+    if (high) {
+      double g = (1 - a1 + a2) / 4;
+      res.push_back(mkSos(g, -2 * g, g, a1, a2));
+    } else {
+      double g = (1 + a1 + a2) / 4;
+      res.push_back(mkSos(g, 2 * g, g, a1, a2));
+    }
+  }
+  if (order % 2 == 1) {
+    double z = (k2 - wc) / (k2 + wc);
+    double a1 = -z;
+    if (high) {
+      double g = (1 - a1) / 2;
+      res.push_back(mkSos(g, -g, 0, a1, 0));
+    } else {
+      double g = (1 + a1) / 2;
+      res.push_back(mkSos(g, g, 0, a1, 0));
+    }
+  }
+  return res;
+}
+// causalLength, filter/iir.nim:150-182
+static int64_t causalLength(const std::vector<Sos>& sections) {
+  int64_t n = 1024;
+  while (true) {
+    std::vector<double> h(n, 0.0);
+    h[0] = 1;
+    for (const Sos& c : sections) {
+      double s1 = 0, s2 = 0;
+      for (int64_t j = 0; j < n; j++) {
+        double x = h[j];
+        double y = c.b0 * x + s1;
+        s1 = c.b1 * x - c.a1 * y + s2;
+        s2 = c.b2 * x - c.a2 * y;
+        h[j] = y;
+      }
+    }
+    double rest = 0, tail = 0;
+    for (int64_t j = 1; j < n; j++) {
+      rest += h[j] * h[j];
+      if (j >= n - n / 4) tail += h[j] * h[j];
+    }
+    if (tail <= 1e-12 * std::max(rest, 1e-300) || n >= (int64_t(1) << 24)) {
+      int64_t result = 0;
+      for (double c0 : {h[0], 1 - h[0]}) {
+        double total = c0 * c0 + rest, e = c0 * c0;
+        int64_t L = 0;
+        while (e < 0.9999 * total && L < n - 1) {
+          L++;
+          e += h[L] * h[L];
+        }
+        result = std::max(result, L);
+      }
+      return result;
+    }
+    n *= 2;
+  }
+}
+static int iirPoles(double slope, double perPole, const char* side) {
+  double n = slope / perPole;
+  if (!(n >= 1 && n <= 32 && n == std::round(n)))
+    throw ValueError(std::string("the ") + side + " slope of an IIR filter must be a multiple of " + fmt(perPole) +
+                     " dB/octave, 1 .. 32 poles; got " + fmt(slope));
+  return (int)n;
+}
+struct IirPlan {
+  Spec spec;
+  std::vector<Sos> sections;
+  int phase = PSG_IP_ZERO, trend = PSG_TR_LINEAR;
+  int64_t pad = 0, lead = 0, tail = 0, samples = 0;
+  bool reflect = false;
+  double dtMs = 0, dcGain = 1, dcSlope = 0;
+};
+// initIirPlan, filter/iir.nim:193-239
+static IirPlan initIirPlan(const Spec& spec, double dtMs, int64_t samples, int phase, int trend) {
+  if (samples < 1) throw ValueError("an IIR plan needs samples >= 1, got " + std::to_string(samples));
+  validate(spec, dtMs);
+  if (spec.kind != PSG_RK_BUTTERWORTH) throw ValueError("an IIR filter needs a Butterworth spec");
+  if (spec.n_notches > 0 || spec.zero_dc) throw ValueError("an IIR filter takes no notches and no 0 Hz suppression");
+  double perPole = phase == PSG_IP_ZERO ? 12.0 : 6.0;
+  std::vector<Sos> lowSecs, highSecs;
+  if (spec.low_hz > 0) lowSecs = butterSections(spec.low_hz, dtMs, iirPoles(spec.low_slope, perPole, "low-cut"), true);
+  if (spec.high_hz < INF)
+    highSecs = butterSections(spec.high_hz, dtMs, iirPoles(spec.high_slope, perPole, "high-cut"), false);
+  IirPlan p;
+  p.sections = lowSecs;
+  p.sections.insert(p.sections.end(), highSecs.begin(), highSecs.end());
+  p.spec = spec;
+  p.phase = phase;
+  p.pad = phase == PSG_IP_ZERO ? impulseLength(spec, dtMs) : std::max(causalLength(lowSecs), causalLength(highSecs));
+  p.samples = samples;
+  p.dtMs = dtMs;
+  double g = 1.0, dg = 0.0;
+  for (const Sos& c : p.sections) {
+    double n1 = c.b0 + c.b1 + c.b2, d1 = 1 + c.a1 + c.a2;
+    double gi = n1 / d1;
+    double dgi = ((c.b1 + 2 * c.b2) * d1 - n1 * (c.a1 + 2 * c.a2)) / (d1 * d1);
+    dg = dg * gi + g * dgi;
+    g *= gi;
+  }
+  p.dcGain = phase == PSG_IP_ZERO ? g * g : g;
+  p.dcSlope = phase == PSG_IP_ZERO ? 0.0 : dg;
+  p.trend = trend;
+  p.reflect = std::fabs(p.dcGain) >= 0.5 || trend != PSG_TR_LINEAR;
+  p.lead = p.reflect ? p.pad : 0;
+  p.tail = phase == PSG_IP_ZERO ? p.pad : 0;
+  return p;
+}
+// sosKernel for one trace, filter/iir.nim:303-351: from rest or from the
+// steady state of the first input, the state flushed to 0 below 1e-250
+// every 256 steps.
+static void sosSingle(double* buf, int64_t m, const Sos& c, bool steady, bool backward) {
+  double s1 = 0, s2 = 0;
+  if (steady && m > 0) {
+    double u = buf[backward ? m - 1 : 0];
+    double y = c.g * u;
+    s2 = c.b2 * u - c.a2 * y;
+    s1 = y - c.b0 * u;
+  }
+  int64_t done = 0;
+  while (done < m) {
+    int64_t run = std::min<int64_t>(256, m - done);
+    for (int64_t k = 0; k < run; k++) {
+      int64_t j = backward ? m - 1 - done - k : done + k;
+      double x = buf[j];
+      double y = c.b0 * x + s1;
+      s1 = c.b1 * x - c.a1 * y + s2;
+      s2 = c.b2 * x - c.a2 * y;
+      buf[j] = y;
+    }
+    s1 = std::fabs(s1) < 1e-250 ? 0.0 : s1;
+    s2 = std::fabs(s2) < 1e-250 ? 0.0 : s2;
+    done += run;
+  }
+}
+// applyFilter on one trace, filter/iir.nim:363-433 (packInto, runSingle, unpackFrom)
+template <class T> void applyIir(const IirPlan& plan, T* x, int64_t n) {
+  if (n <= 0) return;
+  int64_t p = plan.lead, m = plan.lead + n + plan.tail;
+  std::vector<double> buf(m, 0.0);
+  double a, b;
+  trendOf(plan.trend, x, n, a, b);
+  for (int64_t i = 0; i < n; i++) buf[p + i] = (double)x[i] - (a + b * (double)i);
+  if (plan.reflect) {
+    double d0 = buf[p];
+    for (int64_t k = 1; k <= p; k++) buf[p - k] = 2 * d0 - buf[p + std::min(k, n - 1)];
+    double dn = buf[p + n - 1];
+    for (int64_t k = 1; k <= plan.tail; k++) buf[p + n - 1 + k] = 2 * dn - buf[p + n - 1 - std::min(k, n - 1)];
+  } else {
+    for (int64_t k = 1; k <= plan.tail; k++) buf[p + n - 1 + k] = 0;
+  }
+  for (const Sos& c : plan.sections) sosSingle(buf.data(), m, c, plan.reflect, false);
+  if (plan.phase == PSG_IP_ZERO)
+    for (const Sos& c : plan.sections) sosSingle(buf.data(), m, c, plan.reflect, true);
+  double ga = a * plan.dcGain - b * plan.dcSlope, gb = b * plan.dcGain;
+  for (int64_t i = 0; i < n; i++) x[i] = (T)(buf[p + i] + (ga + gb * (double)i));
+}
+
 // ------------------------------------------------------------ core/mute --
 // MuteCurve.muteTimeMs, core/mute.nim:103-123
 double muteTimeMs(const psg_mute_curve& c, double msPerDist, double offset) {
@@ -1094,9 +1287,10 @@ struct RowKeys {
 
 // -------------------------------------------------------------- pipeline --
 enum StepKind { stDemean, stDetrend, stScale, stClip, stPolarity, stFilter, stAgc, stNormTrace, stNormPanel, stGainCurve,
-                stMuteTop, stMuteBottom };
+                stMuteTop, stMuteBottom, stIir };
 template <class T> struct Step {
   StepKind kind;
+  IirPlan iir;
   psg_mute_curve mute{};
   double msPerDist = 0, taperMs = 0;
   double factor = 0, lo = 0, hi = 0;
@@ -1104,7 +1298,9 @@ template <class T> struct Step {
   AgcPlan agc;
   NormPlan norm;
   CurvePlan<T> curve;
-  int64_t margin() const { return kind == stFilter ? filter.margin : (kind == stAgc ? agc.half : 0); }
+  int64_t margin() const {
+    return kind == stFilter ? filter.margin : (kind == stAgc ? agc.half : (kind == stIir ? iir.pad : 0));
+  }
 };
 static const char* opName(int k) {
   static const char* names[] = {"opDemean", "opDetrend", "opScale", "opGainDb", "opClip", "opPolarity",
@@ -1148,6 +1344,8 @@ template <class T> Step<T> compileOp(const psg_op& op, double dtMs, int64_t samp
       s.kind = op.norm_scope == PSG_PER_PANEL ? stNormPanel : stNormTrace; break;
     case PSG_OP_GAIN_CURVE:
       s.kind = stGainCurve; s.curve = initGainCurvePlan<T>(op.curve, dtMs, record, op.t_min_ms, op.t_max_ms); break;
+    case PSG_OP_IIR:
+      s.kind = stIir; s.iir = initIirPlan(op.filter, dtMs, samples, op.iir_phase, op.trend); break;
     case PSG_OP_MUTE_TOP:
     case PSG_OP_MUTE_BOTTOM: {
       // pipeline.nim:417-424 and the builders' checks, core/mute.nim:55-97
@@ -1209,6 +1407,7 @@ template <class T> Plan<T> compile(const psg_op* ops, int nops, double dtMs, int
 template <class T> void runStep(const Step<T>& s, T* x, int64_t n, double startMs, int64_t cols, const RowKeys& k,
                                 int64_t r) {
   switch (s.kind) {
+    case stIir: applyIir(s.iir, x, n); break;
     case stMuteTop:
     case stMuteBottom: {
       // muteCol, core/mute.nim:209-214, and the block forms :216-240
@@ -1557,12 +1756,53 @@ int orc_required_margin(const psg_op* ops, int nops, double dtMs, int64_t* out) 
           m += impulseLength(ops[i].filter, dtMs);
         } else if (ops[i].kind == PSG_OP_AGC) {
           m += initAgcPlan(ops[i].window_ms, dtMs, 1, ops[i].agc_mode, ops[i].target, ops[i].epsilon).half;
+        } else if (ops[i].kind == PSG_OP_IIR) {
+          m += initIirPlan(ops[i].filter, dtMs, 1, ops[i].iir_phase, ops[i].trend).pad;
         }
       } catch (const ValueError& e) {
         throw ValueError("op " + std::to_string(i) + " (" + opName(ops[i].kind) + "): " + e.what());
       }
     }
     *out = m;
+  });
+}
+// IirPlan's order, requiredMargin, dcGain and magnitudeAt (filter/iir.nim:
+// 241-278) at the frequencies f[0 .. nf).
+int orc_iir_info(const psg_filter_spec* spec, double dtMs, int64_t samples, int phase, int trend, int* order,
+                 int64_t* pad, double* dcGain, const double* f, int64_t nf, double* mag) {
+  return guard([&] {
+    IirPlan p = initIirPlan(*spec, dtMs, samples, phase, trend);
+    int o = 0;
+    for (const Sos& c : p.sections) o += c.a2 == 0 ? 1 : 2;
+    *order = o;
+    *pad = p.pad;
+    *dcGain = p.dcGain;
+    for (int64_t i = 0; i < nf; i++) {
+      double w = 2 * PI * f[i] * dtMs / 1000;
+      double zr = std::cos(w), zi = -std::sin(w);
+      double z2r = zr * zr - zi * zi, z2i = zr * zi + zi * zr;
+      double hr = 1, hi = 0;
+      for (const Sos& c : p.sections) {
+        double nr = c.b0 + c.b1 * zr + c.b2 * z2r, ni = c.b1 * zi + c.b2 * z2i;
+        double dr = 1.0 + c.a1 * zr + c.a2 * z2r, di = c.a1 * zi + c.a2 * z2i;
+        double qr, qi;
+        cdivNim(nr, ni, dr, di, qr, qi);
+        double tr = hr * qr - hi * qi, ti = hr * qi + hi * qr;
+        hr = tr;
+        hi = ti;
+      }
+      double a = std::hypot(hr, hi);
+      mag[i] = phase == PSG_IP_ZERO ? a * a : a;
+    }
+  });
+}
+// applyFilter of an IIR plan on one trace of n samples, in place (float64).
+int orc_iir_apply(const psg_filter_spec* spec, double dtMs, int64_t samples, int phase, int trend, double* x,
+                  int64_t n) {
+  return guard([&] {
+    IirPlan p = initIirPlan(*spec, dtMs, samples, phase, trend);
+    if (n > samples) throw ValueError("a trace longer than the plan's samples");
+    applyIir(p, x, n);
   });
 }
 int orc_plan_compile(const psg_op* ops, int nops, int dtype, double dtMs, int64_t samples, int64_t record,

@@ -13,9 +13,10 @@ from .design import (Corners, FilterSpec, GainCurve, GainKnot, bandPass, butterB
                      butterHighCut, butterLowCut, exponentialGain, highCut, knotGain, lowCut,
                      powerGain)
 from .ops import (Op, Pipeline, agcOp, bandPassOp, clipOp, decodeWindow, demeanOp, detrendOp,
-                  filterOp, gainCurveOp, gainDbOp, initPipeline, muteBottomOp, muteTopOp, normalizeOp,
-                  polarityOp, scaleOp)
+                  filterOp, gainCurveOp, gainDbOp, iirOp, initPipeline, muteBottomOp, muteTopOp,
+                  normalizeOp, polarityOp, scaleOp)
 from .mute import MuteCurve, lmoMute, tableMute, timeMute
+from .iir import IirPlan, initIirPlan
 
 # Reference enum names (pipeline.nim / gain.nim / edges.nim)
 trNone, trMean, trLinear = TR_NONE, TR_MEAN, TR_LINEAR
@@ -27,6 +28,7 @@ cmCorrelate, cmDeconvolve = CM_CORRELATE, CM_DECONVOLVE
 fnNone, fnFold, fnSqrtFold = FN_NONE, FN_FOLD, FN_SQRT_FOLD
 float32, float64 = F32, F64
 mkTime, mkTable, mkLmo = _abi.MK_TIME, _abi.MK_TABLE, _abi.MK_LMO
+ipZero, ipMinimum = _abi.IP_ZERO, _abi.IP_MINIMUM
 from .meta import ChunkMeta, initChunkMeta, liveMeta
 from .plan import PipelinePlan, Workspace, compile, initWorkspace
 from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepSpec, SweepTaper, generatePilot,

@@ -123,6 +123,9 @@ def _declare(lib):
         "psg_impulse_length": (C.c_int, [C.POINTER(FilterSpecC), DBL, C.POINTER(I32)]),
         "psg_response": (C.c_int, [C.POINTER(FilterSpecC), DBL, DBL, C.POINTER(DBL)]),
         "psg_required_margin": (C.c_int, [C.POINTER(OpC), I32, DBL, C.POINTER(I32)]),
+        "psg_iir_design": (C.c_int, [C.POINTER(FilterSpecC), DBL, I32, I32, I32, C.POINTER(I32), C.POINTER(I32),
+                                     C.POINTER(DBL)]),
+        "psg_iir_magnitude": (C.c_int, [C.POINTER(FilterSpecC), DBL, I32, P, I32, P]),
         "psg_decode_window": (None, [I64, I64, I64, I64, C.POINTER(I64)]),
         "psg_plan_compile": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, I32, C.POINTER(P)]),
         "psg_plan_destroy": (None, [P]),

@@ -641,6 +641,55 @@ static void launch_pipe(const void* kernel, int grid, int threads, size_t smem, 
   CUDA_OK(cudaLaunchKernel(kernel, dim3(grid), dim3(threads), args, smem, stream));
 }
 
+// Double-double on the host (Dekker's and Knuth's error-free sums and
+// products), for the IIR scan tables.
+namespace hdd {
+struct DD {
+  double hi, lo;
+};
+static DD quick(double a, double b) {
+  double s = a + b;
+  return DD{s, b - (s - a)};
+}
+static DD two_sum(double a, double b) {
+  double s = a + b, bb = s - a;
+  return DD{s, (a - (s - bb)) + (b - bb)};
+}
+static DD add(DD x, DD y) {
+  DD s = two_sum(x.hi, y.hi), t = two_sum(x.lo, y.lo);
+  s = quick(s.hi, s.lo + t.hi);
+  return quick(s.hi, s.lo + t.lo);
+}
+static DD mul(DD x, DD y) {
+  double p = x.hi * y.hi;
+  double e = std::fma(x.hi, y.hi, -p) + (x.hi * y.lo + x.lo * y.hi);
+  return quick(p, e);
+}
+struct M2 {
+  DD a, b, c, d;
+};
+static M2 mul(const M2& x, const M2& y) {
+  return M2{add(mul(x.a, y.a), mul(x.b, y.c)), add(mul(x.a, y.b), mul(x.b, y.d)), add(mul(x.c, y.a), mul(x.d, y.c)),
+            add(mul(x.c, y.b), mul(x.d, y.d))};
+}
+}  // namespace hdd
+
+// The IIR scan table of a section: for each chunk length L = 1 .. lmax the
+// powers (M^L)^(2^i), i = 0 .. 5, of its state map M = [[−a1, 1], [−a2, 0]],
+// as 2×2 double-double matrices (48 doubles per L).
+static void iir_scan_table(const Biquad& q, int lmax, std::vector<double>& out) {
+  const hdd::M2 m{hdd::DD{-q.a1, 0}, hdd::DD{1, 0}, hdd::DD{-q.a2, 0}, hdd::DD{0, 0}};
+  hdd::M2 pl{hdd::DD{1, 0}, hdd::DD{0, 0}, hdd::DD{0, 0}, hdd::DD{1, 0}};
+  for (int L = 1; L <= lmax; L++) {
+    pl = hdd::mul(pl, m);
+    hdd::M2 w = pl;
+    for (int i = 0; i < 6; i++) {
+      out.insert(out.end(), {w.a.hi, w.a.lo, w.b.hi, w.b.lo, w.c.hi, w.c.lo, w.d.hi, w.d.lo});
+      w = hdd::mul(w, w);
+    }
+  }
+}
+
 template <class T> static void build_device_steps(psg_plan* p) {
   typedef typename C2<T>::type V;
   std::vector<DevStep> ds;
@@ -696,6 +745,29 @@ template <class T> static void build_device_steps(psg_plan* p) {
         d.knots = (const double*)upload(p->keep, k);
       }
       p->needs_keys = true;
+    } else if (s.kind == ST_IIR) {
+      const IirHost& f = s.iir;
+      d.trend = f.trend;
+      d.reflect = f.reflect;
+      d.dc_gain = f.dc_gain;
+      d.dc_slope = f.dc_slope;
+      d.n_sec = (int)f.sections.size();
+      d.iir_zero = f.phase == PSG_IP_ZERO;
+      d.lead = (int)f.lead;
+      d.tail = (int)f.tail;
+      if (f.lead + f.tail > (1 << 24)) throw InvalidArg("the IIR filter's pads are too long for the device");
+      std::vector<double> sec, pw;
+      const int lmax = (int)((f.lead + p->host.samples + f.tail + kNT - 1) / kNT);
+      for (const Biquad& b : f.sections) {
+        sec.insert(sec.end(), {b.b0, b.b1, b.b2, b.a1, b.a2, b.g});
+        iir_scan_table(b, lmax, pw);
+      }
+      d.pw_len = lmax;
+      if (!sec.empty()) {
+        d.sec = (const double*)upload(p->keep, sec);
+        d.pw = (const double*)upload(p->keep, pw);
+      }
+      work = std::max<int64_t>(work, (f.lead + p->host.samples + f.tail) * 8);
     }
     if (s.kind == ST_NORM_PANEL) p->needs_panel = true;
     // what the step needs of its input (accumulated by the loop before it)
@@ -704,6 +776,9 @@ template <class T> static void build_device_steps(psg_plan* p) {
       case ST_DETREND: d.need = NEED_S1 | NEED_SI; break;
       case ST_FILTER:
         d.need = s.filter.trend == PSG_TR_LINEAR ? (NEED_S1 | NEED_SI) : (s.filter.trend == PSG_TR_MEAN ? NEED_S1 : 0);
+        break;
+      case ST_IIR:
+        d.need = s.iir.trend == PSG_TR_LINEAR ? (NEED_S1 | NEED_SI) : (s.iir.trend == PSG_TR_MEAN ? NEED_S1 : 0);
         break;
       case ST_AGC: d.need = NEED_S2; break;
       case ST_NORM_TRACE: d.need = s.stat == PSG_NORM_RMS ? NEED_S2 : NEED_MX; break;
@@ -897,6 +972,24 @@ int psg_response(const psg_filter_spec* spec, double f_hz, double dt_ms, double*
   return guarded([&] {
     if (!spec || !out) throw InvalidArg("null argument");
     *out = spec_response(*spec, f_hz, dt_ms);
+  });
+}
+int psg_iir_design(const psg_filter_spec* spec, double dt_ms, int32_t samples, int32_t phase, int32_t trend,
+                   int32_t* order, int32_t* margin, double* dc_gain) {
+  return guarded([&] {
+    if (!spec) throw InvalidArg("null argument");
+    IirHost p = iir_plan(*spec, dt_ms, samples, phase, trend);
+    if (order) *order = iir_order(p);
+    if (margin) *margin = (int32_t)p.pad;
+    if (dc_gain) *dc_gain = p.dc_gain;
+  });
+}
+int psg_iir_magnitude(const psg_filter_spec* spec, double dt_ms, int32_t phase, const double* f_hz, int32_t n,
+                      double* out) {
+  return guarded([&] {
+    if (!spec || (n > 0 && (!f_hz || !out)) || n < 0) throw InvalidArg("null argument");
+    IirHost p = iir_plan(*spec, dt_ms, 1, phase, PSG_TR_NONE);
+    for (int32_t i = 0; i < n; i++) out[i] = iir_magnitude(p, f_hz[i], dt_ms);
   });
 }
 int psg_required_margin(const psg_op* ops, int32_t n_ops, double dt_ms, int32_t* out) {
@@ -2055,6 +2148,8 @@ int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* 
     if (plan->host.parts.size() != 1) throw InvalidArg("the request loop serves plans without a per-panel normalization");
     if (plan->wide) throw InvalidArg("the request loop serves plans whose traces and FFTs fit the device's shared memory");
     if (plan->needs_keys) throw InvalidArg("the request loop serves plans without mutes");
+    for (const StepHost& st : plan->host.steps)
+      if (st.kind == ST_IIR) throw InvalidArg("the request loop serves plans without IIR filters");
     if (!src_host) throw InvalidArg("src is required");
     std::unique_ptr<Req> r(new Req());
     r->plan = plan;

@@ -61,6 +61,24 @@ double spec_response(const psg_filter_spec& s, double f_hz, double dt_ms);
 int64_t spec_impulse_length(const psg_filter_spec& s, double dt_ms);
 FilterHost filter_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int trend, int max_radix = 16);
 
+// ------------------------------------------------------------- IIR filters
+// A second-order section in transposed direct form II (a0 = 1) and its gain
+// at 0 Hz, g = (b0 + b1 + b2)/(1 + a1 + a2).
+struct Biquad {
+  double b0, b1, b2, a1, a2, g;
+};
+struct IirHost {
+  psg_filter_spec spec{};
+  std::vector<Biquad> sections;  // low-cut (high-pass) sections, then high-cut
+  int phase = PSG_IP_ZERO, trend = PSG_TR_LINEAR;
+  int64_t pad = 0, lead = 0, tail = 0;  // requiredMargin; padded samples before and after
+  bool reflect = false;  // odd-reflection pads and steady-state starts (else zeros, from rest)
+  double dc_gain = 1, dc_slope = 0;
+};
+IirHost iir_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int phase, int trend);
+double iir_magnitude(const IirHost& p, double f_hz, double dt_ms);
+int iir_order(const IirHost& p);
+
 // ---------------------------------------------------------------- the plan
 enum StepKind {
   ST_DEMEAN = 0, ST_DETREND, ST_SCALE, ST_CLIP, ST_POLARITY, ST_FILTER, ST_AGC,
@@ -85,7 +103,11 @@ struct StepHost {
   // mutes (core/mute.nim): the curve, 1000/velocity of an LMO mute, the taper
   psg_mute_curve mute{};
   double ms_per_dist = 0, taper_ms = 0;
-  int64_t margin() const { return kind == ST_FILTER ? filter.margin : (kind == ST_AGC ? half : 0); }
+  // IIR filter
+  IirHost iir;
+  int64_t margin() const {
+    return kind == ST_FILTER ? filter.margin : (kind == ST_AGC ? half : (kind == ST_IIR ? iir.pad : 0));
+  }
 };
 
 struct PlanHost {

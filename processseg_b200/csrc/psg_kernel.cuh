@@ -44,6 +44,16 @@ struct DevStep {
   int mute_kind, n_knots;
   double mute_t, ms_per_dist, mute_t0, mute_pad, taper_ms;
   const double* knots;
+  // IIR filter: sections (b0, b1, b2, a1, a2, g each), zero phase or
+  // minimum, the pads before and after the data, G'(1) (trend, reflect and
+  // dc_gain as the FFT filter's)
+  int n_sec, iir_zero, lead, tail;
+  double dc_slope;
+  const double* sec;
+  // per section and chunk length L = 1 .. pw_len: (M^L)^(2^i), i = 0 .. 5,
+  // 2×2 in double-double (48 doubles)
+  const double* pw;
+  int pw_len, _pad2;
 };
 
 // One apply: a block of rows and the plan steps of one part.
@@ -643,6 +653,177 @@ __device__ __forceinline__ Stats step_gain_curve(const DevStep& st, T* X, int n,
   });
 }
 
+// ------------------------------------------------------------ IIR filters
+// Double-double numbers (an unevaluated sum hi + lo, |lo| ≤ ulp(hi)/2) by
+// the error-free transformations of Dekker and Knuth: the carried states of
+// the chunked recurrence below keep about 106 bits, so that its result is
+// as close to the exact recurrence as the serial float64 one is.
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_quick(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  return DD{s, __dsub_rn(b, __dsub_rn(s, a))};
+}
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b), bb = __dsub_rn(s, a);
+  return DD{s, __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb))};
+}
+__device__ __forceinline__ DD dd_add(DD x, DD y) {
+  DD s = dd_two_sum(x.hi, y.hi);
+  const DD t = dd_two_sum(x.lo, y.lo);
+  s = dd_quick(s.hi, __dadd_rn(s.lo, t.hi));
+  return dd_quick(s.hi, __dadd_rn(s.lo, t.lo));
+}
+__device__ __forceinline__ DD dd_mul(DD x, DD y) {
+  const double p = __dmul_rn(x.hi, y.hi);
+  double e = __fma_rn(x.hi, y.hi, -p);
+  e = __dadd_rn(e, __dadd_rn(__dmul_rn(x.hi, y.lo), __dmul_rn(x.lo, y.hi)));
+  return dd_quick(p, e);
+}
+// A 2×2 matrix of the biquad state map, row-major, in double-double.
+struct M2 {
+  DD a, b, c, d;
+};
+__device__ __forceinline__ M2 m2_mul(const M2& x, const M2& y) {
+  return M2{dd_add(dd_mul(x.a, y.a), dd_mul(x.b, y.c)), dd_add(dd_mul(x.a, y.b), dd_mul(x.b, y.d)),
+            dd_add(dd_mul(x.c, y.a), dd_mul(x.d, y.c)), dd_add(dd_mul(x.c, y.b), dd_mul(x.d, y.d))};
+}
+__device__ __forceinline__ M2 m2_load(const double* t) {
+  return M2{DD{t[0], t[1]}, DD{t[2], t[3]}, DD{t[4], t[5]}, DD{t[6], t[7]}};
+}
+// y += Q·u
+__device__ __forceinline__ void m2_madd(const M2& Q, DD u1, DD u2, DD& y1, DD& y2) {
+  y1 = dd_add(y1, dd_add(dd_mul(Q.a, u1), dd_mul(Q.b, u2)));
+  y2 = dd_add(y2, dd_add(dd_mul(Q.c, u1), dd_mul(Q.d, u2)));
+}
+__device__ __forceinline__ DD dd_shfl_up(DD v, int d) {
+  return DD{__shfl_up_sync(0xffffffffu, v.hi, d), __shfl_up_sync(0xffffffffu, v.lo, d)};
+}
+
+// One pass of one section (filter/iir.nim:319-351) over the m padded samples
+// of B (float64, in place), forwards or backwards, from rest or from the
+// steady state of its first input sample. A section in transposed direct
+// form II is a linear map of its state (s1, s2) per sample,
+//   y = b0·x + s1,  s1' = b1·x − a1·y + s2,  s2' = b2·x − a2·y,
+// so the pass runs in parallel over the CTA: thread t takes the L = ⌈m/256⌉
+// samples of chunk t, (1) runs them from a zero state (thread 0 from the
+// pass's start state) to the chunk's end state Z_t, (2) a scan over the
+// threads gives each chunk's true start state, E_t = P·E_{t−1} + Z_t with
+// P = M^L the state map over L zero samples (warp scans with the powers
+// P^(2^i), read from the host's double-double table `pw` for this L, then
+// across the warps), and (3) each thread reruns its chunk from its start
+// state and writes the outputs. A start state below 1e-250 is set to 0, so a
+// decay after the input stops ends in exact zeros (filter/iir.nim:311-317).
+__device__ __forceinline__ void iir_pass(double* B, int m, const double* c, const double* pw, bool steady,
+                                         bool backward) {
+  __shared__ double w_end[kNT / 32][4];
+  const double b0 = c[0], b1 = c[1], b2 = c[2], a1 = c[3], a2 = c[4], g = c[5];
+  const int L = (m + kNT - 1) / kNT;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int j0 = min(t * L, m), j1 = min(j0 + L, m);
+  const double* tab = pw + (size_t)(L - 1) * 48;  // P^(2^i), i = 0 .. 5, for this L
+  auto at = [&](int j) -> double& { return B[backward ? m - 1 - j : j]; };
+  __syncthreads();  // the previous pass's outputs
+  double i1 = 0, i2 = 0;  // the pass's start state
+  if (steady && m > 0) {
+    const double u = at(0);
+    const double y = __dmul_rn(g, u);
+    i2 = __dsub_rn(__dmul_rn(b2, u), __dmul_rn(a2, y));
+    i1 = __dsub_rn(y, __dmul_rn(b0, u));
+  }
+  auto step = [&](double x, double& s1, double& s2) {
+    const double y = __dadd_rn(__dmul_rn(b0, x), s1);
+    s1 = __dadd_rn(__dsub_rn(__dmul_rn(b1, x), __dmul_rn(a1, y)), s2);
+    s2 = __dsub_rn(__dmul_rn(b2, x), __dmul_rn(a2, y));
+    return y;
+  };
+  // (1) the chunk from rest (chunk 0 from the start state)
+  double z1 = t == 0 ? i1 : 0.0, z2 = t == 0 ? i2 : 0.0;
+  for (int j = j0; j < j1; j++) step(at(j), z1, z2);
+  // (2) warp scan: e_t = Σ_k P^(t−k)·Z_k over the warp's lanes
+  DD e1{z1, 0}, e2{z2, 0};
+  for (int i = 0; i < 5; i++) {
+    const DD u1 = dd_shfl_up(e1, 1 << i), u2 = dd_shfl_up(e2, 1 << i);
+    if (lane >= (1 << i)) m2_madd(m2_load(tab + 8 * i), u1, u2, e1, e2);
+  }
+  if (lane == 31) {
+    w_end[warp][0] = e1.hi;
+    w_end[warp][1] = e1.lo;
+    w_end[warp][2] = e2.hi;
+    w_end[warp][3] = e2.lo;
+  }
+  __syncthreads();
+  // the carry into this warp: the true end state of the previous warp's last chunk
+  DD c1{0, 0}, c2{0, 0};
+  if (warp > 0) {
+    const M2 Q32 = m2_load(tab + 40);
+    for (int v = 0; v < warp; v++) {
+      DD n1{w_end[v][0], w_end[v][1]}, n2{w_end[v][2], w_end[v][3]};
+      m2_madd(Q32, c1, c2, n1, n2);
+      c1 = n1;
+      c2 = n2;
+    }
+    // E_t = e_t + P^(lane+1)·carry
+    const int k = lane + 1;
+    M2 R = m2_load(tab + 8 * (31 - __clz(k)));
+    for (int i = 0; i < 31 - __clz(k); i++)
+      if ((k >> i) & 1) R = m2_mul(R, m2_load(tab + 8 * i));
+    m2_madd(R, c1, c2, e1, e2);
+  }
+  // this chunk starts from the previous chunk's end
+  const DD p1 = dd_shfl_up(e1, 1), p2 = dd_shfl_up(e2, 1);
+  double s1 = __dadd_rn(p1.hi, p1.lo), s2 = __dadd_rn(p2.hi, p2.lo);
+  if (lane == 0) {
+    s1 = __dadd_rn(c1.hi, c1.lo);
+    s2 = __dadd_rn(c2.hi, c2.lo);
+  }
+  if (t == 0) {
+    s1 = i1;
+    s2 = i2;
+  }
+  if (fabs(s1) < 1e-250) s1 = 0;
+  if (fabs(s2) < 1e-250) s2 = 0;
+  // (3) the chunk from its true start
+  for (int j = j0; j < j1; j++) {
+    double& x = at(j);
+    x = step(x, s1, s2);
+  }
+}
+
+// The IIR filter (filter/iir.nim:363-433) on one trace: the detrended live
+// samples with their pads (odd reflections, or zeros after the data) in a
+// float64 work area of lead + n + tail values, every section forwards (then
+// backwards for zero phase), and the trend added back as the cascade's
+// steady-state response to it, G(1)·(a + b·i) − b·G'(1).
+template <class T, int NEED_K = -1, class M = InShared>
+__device__ __noinline__ Stats step_iir(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S,
+                                          const M& mem = M()) {
+  double* B = reinterpret_cast<double*>(mem.base() + work_off);
+  double a, b;
+  trend_from(st.trend, in, n, a, b);
+  const int p = st.lead, tail = st.tail, m = p + n + tail;
+  for (int i = threadIdx.x; i < n; i += kNT)
+    B[p + i] = __dsub_rn((double)X[i], __dadd_rn(a, __dmul_rn(b, (double)i)));
+  __syncthreads();
+  if (st.reflect) {
+    const double d0 = B[p], dn = B[p + n - 1];
+    for (int k = threadIdx.x + 1; k <= p; k += kNT) B[p - k] = __dsub_rn(2 * d0, B[p + min(k, n - 1)]);
+    for (int k = threadIdx.x + 1; k <= tail; k += kNT) B[p + n - 1 + k] = __dsub_rn(2 * dn, B[p + n - 1 - min(k, n - 1)]);
+  } else {
+    for (int k = threadIdx.x + 1; k <= tail; k += kNT) B[p + n - 1 + k] = 0;
+  }
+  const int lmax = st.pw_len;
+  for (int i = 0; i < st.n_sec; i++) iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * 48, st.reflect, false);
+  if (st.iir_zero)
+    for (int i = 0; i < st.n_sec; i++)
+      iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * 48, st.reflect, true);
+  __syncthreads();
+  const double ga = __dsub_rn(__dmul_rn(a, st.dc_gain), __dmul_rn(b, st.dc_slope)), gb = __dmul_rn(b, st.dc_gain);
+  return map_trace<NEED_K>(X, n, st.need_next, S,
+                           [&](T, int i) { return (T)__dadd_rn(B[p + i], __dadd_rn(ga, __dmul_rn(gb, (double)i))); });
+}
+
 // ------------------------------------------------------------ mutes
 // muteTimeMs (core/mute.nim:103-123) in the reference's order of operations
 // (no contraction into fused multiply-adds).
@@ -987,8 +1168,18 @@ __global__ void __launch_bounds__(kNT, (GW || sizeof(T) == 8 ? 2 : 4)) pipeline_
             break;
           case ST_NORM_TRACE: st = step_norm_trace(d, st, X, n, S); break;
           case ST_GAIN_CURVE: st = step_gain_curve(d, X, n, c.start, S); break;
+          // mutes and IIR filters: single-job launches only (the request
+          // loop, which batches, refuses plans with them)
           case ST_MUTE_TOP:
-          case ST_MUTE_BOTTOM: st = step_mute(d, c.job, c.r, X, n, S); break;
+          case ST_MUTE_BOTTOM:
+            if constexpr (!BATCH) st = step_mute(d, c.job, c.r, X, n, S);
+            break;
+          case ST_IIR:
+            if constexpr (GW)
+              st = step_iir<T, -1, InGlobal>(d, st, X, n, 0, S, InGlobal{a.gwork + (size_t)blockIdx.x * a.gwork_stride});
+            else if constexpr (!BATCH)
+              st = step_iir(d, st, X, n, a.work_off, S);
+            break;
           default: break;
         }
       }

@@ -547,6 +547,9 @@ StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, 
       s.taper_ms = op.taper_ms;
       break;
     case PSG_OP_IIR:
+      s.kind = ST_IIR;
+      s.iir = iir_plan(op.filter, dt_ms, samples, op.iir_phase, op.trend);
+      break;
     case PSG_OP_CALIBRATE:
     case PSG_OP_UNCALIBRATE:
       throw InvalidArg("this op is not part of the GPU hot path yet");
@@ -603,11 +606,173 @@ int64_t required_margin(const psg_op* ops, int n_ops, double dt_ms) {
     try {
       if (ops[i].kind == PSG_OP_FILTER) m += spec_impulse_length(ops[i].filter, dt_ms);
       else if (ops[i].kind == PSG_OP_AGC) m += agc_half(ops[i].window_ms, dt_ms, 1, ops[i].target, ops[i].epsilon);
+      else if (ops[i].kind == PSG_OP_IIR) m += iir_plan(ops[i].filter, dt_ms, 1, ops[i].iir_phase, ops[i].trend).pad;
     } catch (const InvalidArg& e) {
       throw InvalidArg(std::string("op ") + std::to_string(i) + " (" + op_name(ops[i].kind) + "): " + e.what());
     }
   }
   return m;
+}
+
+// ------------------------------------------------------------- IIR filters
+namespace {
+// Complex a/b by Smith's method (scaled by the larger part of b).
+void cdiv(double ar, double ai, double br, double bi, double& qr, double& qi) {
+  if (std::fabs(br) < std::fabs(bi)) {
+    double r = br / bi, den = bi + r * br;
+    qr = (ar * r + ai) / den;
+    qi = (ai * r - ar) / den;
+  } else {
+    double r = bi / br, den = br + r * bi;
+    qr = (ar + r * ai) / den;
+    qi = (ai - r * ar) / den;
+  }
+}
+Biquad biquad(double b0, double b1, double b2, double a1, double a2) {
+  return Biquad{b0, b1, b2, a1, a2, (b0 + b1 + b2) / (1 + a1 + a2)};
+}
+// butterSections (filter/iir.nim:113-148): a digital Butterworth low-pass or
+// high-pass of `order` poles, −3 dB at fc, by the bilinear transform
+// prewarped at fc. The analog prototype's poles are wc·(−sin θ ± i cos θ),
+// θ = π(2k + 1)/(2N); each conjugate pair maps to z = (2fs + s)/(2fs − s).
+std::vector<Biquad> butter_sections(double fc, double dt_ms, int order, bool high) {
+  std::vector<Biquad> out;
+  double fs = 1000 / dt_ms;
+  double wc = 2 * fs * std::tan(kPi * fc / fs);
+  double k2 = 2 * fs;
+  for (int k = 0; k < order / 2; k++) {
+    double th = kPi * (double)(2 * k + 1) / (double)(2 * order);
+    double sr = -wc * std::sin(th), si = wc * std::cos(th);
+    double zr, zi;
+    cdiv(k2 + sr, si, k2 - sr, -si, zr, zi);
+    double a1 = -2 * zr, a2 = zr * zr + zi * zi;
+    if (high) {
+      double g = (1 - a1 + a2) / 4;  // gain 1 at Nyquist
+      out.push_back(biquad(g, -2 * g, g, a1, a2));
+    } else {
+      double g = (1 + a1 + a2) / 4;  // gain 1 at 0 Hz
+      out.push_back(biquad(g, 2 * g, g, a1, a2));
+    }
+  }
+  if (order % 2 == 1) {
+    double z = (k2 - wc) / (k2 + wc), a1 = -z;
+    if (high) {
+      double g = (1 - a1) / 2;
+      out.push_back(biquad(g, -g, 0, a1, 0));
+    } else {
+      double g = (1 + a1) / 2;
+      out.push_back(biquad(g, g, 0, a1, 0));
+    }
+  }
+  return out;
+}
+// causalLength (filter/iir.nim:150-182): the samples after a spike holding
+// 99.99 % of the energy of the cascade's causal impulse response h (or of
+// δ − h, whichever is longer), h run from rest until its last quarter holds
+// under 1e-12 of the energy.
+int64_t causal_length(const std::vector<Biquad>& secs) {
+  const double frac = 0.9999;
+  for (int64_t n = 1024;; n *= 2) {
+    std::vector<double> h(n, 0.0);
+    h[0] = 1;
+    for (const Biquad& c : secs) {
+      double s1 = 0, s2 = 0;
+      for (int64_t j = 0; j < n; j++) {
+        double x = h[j];
+        double y = c.b0 * x + s1;
+        s1 = c.b1 * x - c.a1 * y + s2;
+        s2 = c.b2 * x - c.a2 * y;
+        h[j] = y;
+      }
+    }
+    double rest = 0, tail = 0;
+    for (int64_t j = 1; j < n; j++) {
+      rest += h[j] * h[j];
+      if (j >= n - n / 4) tail += h[j] * h[j];
+    }
+    if (tail <= 1e-12 * std::max(rest, 1e-300) || n >= (1 << 24)) {
+      int64_t best = 0;
+      for (double c0 : {h[0], 1 - h[0]}) {
+        double total = c0 * c0 + rest, e = c0 * c0;
+        int64_t L = 0;
+        while (e < frac * total && L < n - 1) {
+          L++;
+          e += h[L] * h[L];
+        }
+        best = std::max(best, L);
+      }
+      return best;
+    }
+  }
+}
+int poles(double slope, double per_pole, const char* side) {
+  double n = slope / per_pole;
+  need(n >= 1 && n <= 32 && n == std::round(n),
+       std::string("the ") + side + " slope of an IIR filter must be a multiple of " + num(per_pole) +
+           " dB/octave (" + std::to_string((int)per_pole) + " per pole), 1 .. 32 poles; got " + num(slope));
+  return (int)n;
+}
+}  // namespace
+
+// initIirPlan (filter/iir.nim:193-239)
+IirHost iir_plan(const psg_filter_spec& s, double dt_ms, int64_t samples, int phase, int trend) {
+  need(samples >= 1, "an IIR plan needs samples ≥ 1, got " + std::to_string(samples));
+  need(phase == PSG_IP_ZERO || phase == PSG_IP_MINIMUM, "unknown IIR phase " + std::to_string(phase));
+  need(trend >= PSG_TR_NONE && trend <= PSG_TR_LINEAR, "unknown trend removal " + std::to_string(trend));
+  validate_spec(s, dt_ms);
+  need(s.kind == PSG_RK_BUTTERWORTH,
+       "an IIR filter needs a Butterworth spec (butterLowCut, butterHighCut, butterBandPass)");
+  need(s.n_notches == 0 && !s.zero_dc, "an IIR filter takes no notches and no 0 Hz suppression");
+  IirHost p;
+  p.spec = s;
+  p.phase = phase;
+  p.trend = trend;
+  double per_pole = phase == PSG_IP_ZERO ? 12.0 : 6.0;
+  std::vector<Biquad> low, high;
+  if (s.low_hz > 0) low = butter_sections(s.low_hz, dt_ms, poles(s.low_slope, per_pole, "low-cut"), true);
+  if (s.high_hz < kInf) high = butter_sections(s.high_hz, dt_ms, poles(s.high_slope, per_pole, "high-cut"), false);
+  p.sections = low;
+  p.sections.insert(p.sections.end(), high.begin(), high.end());
+  p.pad = phase == PSG_IP_ZERO ? spec_impulse_length(s, dt_ms) : std::max(causal_length(low), causal_length(high));
+  // G(1) and G'(1) of the cascade from each section's N(q)/D(q), q = 1/z
+  double g = 1, dg = 0;
+  for (const Biquad& c : p.sections) {
+    double n1 = c.b0 + c.b1 + c.b2, d1 = 1 + c.a1 + c.a2;
+    double gi = n1 / d1;
+    double dgi = ((c.b1 + 2 * c.b2) * d1 - n1 * (c.a1 + 2 * c.a2)) / (d1 * d1);
+    dg = dg * gi + g * dgi;
+    g *= gi;
+  }
+  p.dc_gain = phase == PSG_IP_ZERO ? g * g : g;
+  p.dc_slope = phase == PSG_IP_ZERO ? 0.0 : dg;
+  p.reflect = std::fabs(p.dc_gain) >= 0.5 || trend != PSG_TR_LINEAR;
+  p.lead = p.reflect ? p.pad : 0;
+  p.tail = phase == PSG_IP_ZERO ? p.pad : 0;
+  return p;
+}
+// magnitudeAt (filter/iir.nim:268-278): |H| (minimum phase) or |H|² (zero
+// phase) at f Hz from the sections.
+double iir_magnitude(const IirHost& p, double f, double dt_ms) {
+  double w = 2 * kPi * f * dt_ms / 1000;
+  double zr = std::cos(w), zi = -std::sin(w);       // z^-1
+  double z2r = zr * zr - zi * zi, z2i = 2 * zr * zi;  // z^-2
+  double hr = 1, hi = 0;
+  for (const Biquad& c : p.sections) {
+    double nr = c.b0 + c.b1 * zr + c.b2 * z2r, ni = c.b1 * zi + c.b2 * z2i;
+    double dr = 1 + c.a1 * zr + c.a2 * z2r, di = c.a1 * zi + c.a2 * z2i;
+    double qr, qi;
+    cdiv(nr, ni, dr, di, qr, qi);
+    double tr = hr * qr - hi * qi;
+    hi = hr * qi + hi * qr;
+    hr = tr;
+  }
+  double a = std::hypot(hr, hi);
+  return p.phase == PSG_IP_ZERO ? a * a : a;
+}
+int iir_order(const IirHost& p) {
+  int o = 0;
+  for (const Biquad& c : p.sections) o += c.a2 == 0 ? 1 : 2;
+  return o;
 }
 
 // --------------------------------------------------------------- vibroseis

@@ -26,6 +26,15 @@ class FilterParams:
 
 
 @dataclass
+class IirParams:
+    """An ``opIir``: a Butterworth spec, the phase and the trend removal
+    (pipeline.nim:133-137)."""
+    spec: FilterSpec
+    phase: int = A.IP_ZERO
+    trend: int = A.TR_LINEAR
+
+
+@dataclass
 class AgcParams:
     windowMs: float
     mode: int = A.AGC_RMS
@@ -98,6 +107,10 @@ class Op:
         return self._get((A.OP_FILTER,), "FFT filter")
 
     @property
+    def iir(self) -> IirParams:
+        return self._get((A.OP_IIR,), "IIR filter")
+
+    @property
     def agc(self) -> AgcParams:
         return self._get((A.OP_AGC,), "AGC")
 
@@ -133,6 +146,10 @@ class Op:
         elif k == A.OP_FILTER:
             o.filter = p.spec.to_c()
             o.trend = int(p.trend)
+        elif k == A.OP_IIR:
+            o.filter = p.spec.to_c()
+            o.trend = int(p.trend)
+            o.iir_phase = int(p.phase)
         elif k == A.OP_AGC:
             o.window_ms, o.agc_mode, o.target, o.epsilon = p.windowMs, int(p.mode), p.target, p.epsilon
         elif k == A.OP_NORMALIZE:
@@ -191,6 +208,13 @@ def bandPassOp(corners: Corners, trend: int = A.TR_LINEAR) -> Op:
     """``filterOp(bandPass(corners))``; ``ValueError`` for bad corners
     (pipeline.nim:295-298)."""
     return filterOp(bandPass(corners), trend)
+
+
+def iirOp(spec: FilterSpec, phase: int = A.IP_ZERO, trend: int = A.TR_LINEAR) -> Op:
+    """A Butterworth biquad cascade (``IirPlan``, filter/iir.nim): zero phase
+    (forward-backward) or minimum phase (one causal pass), with the edge
+    handling of the FFT filters (pipeline.nim:300-303)."""
+    return Op(A.OP_IIR, IirParams(spec, phase, trend))
 
 
 def agcOp(windowMs: float, mode: int = A.AGC_RMS, target: float = 1.0,

@@ -33,6 +33,8 @@ def without_trend(flow):
     for o in ops:
         if o.kind == A.OP_FILTER:
             o.filter.trend = A.TR_NONE
+        elif o.kind == A.OP_IIR:
+            o.iir.trend = A.TR_NONE
     return ops
 
 
@@ -98,6 +100,7 @@ def test_applied_response_matches_sine_cosine(T):
     T = getattr(P, T)
     flows = [
         P.initPipeline([P.bandPassOp(P.Corners(8, 12, 40, 50))]),
+        P.initPipeline([P.iirOp(P.butterBandPass(4, 60, 24))]),
         P.initPipeline([P.gainDbOp(12), P.filterOp(P.lowCut(4, 8))]),
     ]
     ws = P.initWorkspace()
