@@ -354,6 +354,41 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
                            const int32_t* live, double clip_percentile, double* out,
                            void* stream);
 
+/* ------------------------------------------------------------- spectra */
+/* SpectrumPlan, src/processSEG/fft/spectrum.nim:79-107: windows of
+ * window_len samples at dt_ms, demeaned (demean != 0) and tapered over
+ * taper_fraction of each end (a sin² ramp), zero-padded to nfft (0: the
+ * next power of two of the window). PSG_EINVAL for what initSpectrumPlan
+ * rejects. */
+typedef struct psg_spectrum_plan psg_spectrum_plan;
+int psg_spectrum_plan_create(int32_t dtype, double dt_ms, int32_t window_len, double taper_fraction,
+                             int32_t nfft, int32_t demean, psg_spectrum_plan** out);
+void psg_spectrum_plan_destroy(psg_spectrum_plan* plan);
+/* nfft, bins (nfft/2 + 1), the window length and Σ of its taper weights. */
+int psg_spectrum_plan_info(const psg_spectrum_plan* plan, int32_t* nfft, int32_t* bins,
+                           int32_t* window_len, double* taper_sum);
+/* averageAmplitudeInto, fft/spectrum.nim:267-416: the power-averaged
+ * amplitude spectrum of the window first_col ..< first_col + window_len of
+ * the live rows row0 .. row1 (clipped to the block) of a device block:
+ * sqrt(mean over the rows of |X[k]|²/Σw²)·(2, or 1 at 0 Hz and Nyquist).
+ * Rows with no live sample past first_col, or a NaN or infinite sample in
+ * the window, are left out. amp: device, bins doubles (zeros when no row
+ * counts); used (device int64, may be NULL): the rows averaged. The
+ * workspace's spectrum scratch grows on the first call that needs it.
+ * Asynchronous on `stream`. */
+int psg_spectrum_average(const psg_spectrum_plan* plan, psg_workspace* ws, const void* block,
+                         int64_t rows, int32_t cols, const int32_t* live, double dt_ms,
+                         int32_t first_col, int64_t row0, int64_t row1, double* amp,
+                         int64_t* used, void* stream);
+/* amplitudeInto, fft/spectrum.nim:283-300, for every row of a device
+ * block: its window (up to its live end) to the scaled amplitude
+ * |X[k]|·sides/Σw and the phase atan2(Im, Re) from the window's first
+ * sample, into device arrays of rows × bins values of the plan's dtype (a
+ * row without samples in the window gets NaN amplitudes). */
+int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, const void* block,
+                           int64_t rows, int32_t cols, const int32_t* live, double dt_ms,
+                           int32_t first_col, void* amp, void* phase, void* stream);
+
 /* ----------------------------------------------------------- vibroseis */
 /* linearSweep + sweepInto + generatePilot (taper shapes tpLinear, tpCosine,
  * tpCos2, tpHamming, tpBlackman), src/processSEG/vibroseis/sweep.nim:185-342,

@@ -61,6 +61,8 @@ def lib():
             "orc_iir_info": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_double, I64, C.c_int, C.c_int,
                                        C.POINTER(C.c_int), C.POINTER(I64), C.POINTER(C.c_double), P, I64, P]),
             "orc_iir_apply": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_double, I64, C.c_int, C.c_int, P, I64]),
+            "orc_spectrum": (C.c_int, [C.c_int, C.c_double, I64, C.c_double, I64, C.c_int, P, I64, I64, P, I64,
+                                       I64, I64, P, P, P, P, P, P]),
             "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int,
                                           C.POINTER(DBL), C.POINTER(DBL)]),
             "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
@@ -241,6 +243,42 @@ def iir_apply(spec, dtMs, x, phase=A.IP_ZERO, trend=A.TR_LINEAR, samples=None):
     y = np.ascontiguousarray(x, dtype=np.float64).copy()
     _check(lib().orc_iir_apply(C.byref(c), dtMs, samples or y.size, phase, trend, _ptr(y), y.size))
     return y
+
+
+def spectrum_plan(dtype, dtMs, windowLen, taperFraction=0.1, nfft=0, demean=True):
+    """(nfft, Σw) of a SpectrumPlan."""
+    n, sw = C.c_int64(), C.c_double()
+    _check(lib().orc_spectrum(dtype, dtMs, windowLen, taperFraction, nfft, int(demean), None, 0, 0, None, 0, 0, -1,
+                              None, None, None, None, C.byref(n), C.byref(sw)))
+    return n.value, sw.value
+
+
+def spectrum_average(b, live, dtMs, windowLen, firstCol, taperFraction=0.1, nfft=0, demean=True, rows=(0, 2 ** 62)):
+    """(amp, used): averageAmplitudeInto over the rows ``rows`` (inclusive)."""
+    b = np.ascontiguousarray(b)
+    dtype = A.F32 if b.dtype == np.float32 else A.F64
+    n, _ = spectrum_plan(dtype, dtMs, windowLen, taperFraction, nfft, demean)
+    amp = np.zeros(n // 2 + 1)
+    used = C.c_int64()
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    _check(lib().orc_spectrum(dtype, dtMs, windowLen, taperFraction, nfft, int(demean), _ptr(b), b.shape[0],
+                              b.shape[1], _ptr(live), firstCol, rows[0], rows[1], _ptr(amp), C.byref(used), None,
+                              None, None, None))
+    return amp, used.value
+
+
+def spectrum_amplitudes(b, live, dtMs, windowLen, firstCol, taperFraction=0.1, nfft=0, demean=True):
+    """(amp, phase), rows × bins of the block's dtype: amplitudeInto per row."""
+    b = np.ascontiguousarray(b)
+    dtype = A.F32 if b.dtype == np.float32 else A.F64
+    n, _ = spectrum_plan(dtype, dtMs, windowLen, taperFraction, nfft, demean)
+    amp = np.zeros((b.shape[0], n // 2 + 1), b.dtype)
+    phase = np.zeros_like(amp)
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    _check(lib().orc_spectrum(dtype, dtMs, windowLen, taperFraction, nfft, int(demean), _ptr(b), b.shape[0],
+                              b.shape[1], _ptr(live), firstCol, 0, -1, None, None, _ptr(amp), _ptr(phase), None,
+                              None))
+    return amp, phase
 
 
 def rows_flatten(status, numSamples, t0Ms, firstSample, dtMs, failed, cols, mode=0):

@@ -1025,6 +1025,100 @@ template <class T> void applyGainCurve(const CurvePlan<T>& plan, T* x, int64_t n
   }
 }
 
+// ---------------------------------------------------------- fft/spectrum --
+template <class T> struct SpectrumPlan {
+  FftPlan<T> fft;
+  std::vector<T> taper;
+  double taperSum = 0, dtMs = 0;
+  bool demean = true;
+};
+// initSpectrumPlan, fft/spectrum.nim:79-107
+template <class T> SpectrumPlan<T> initSpectrumPlan(double dtMs, int64_t windowLen, double taperFraction, int64_t nfft,
+                                                   bool demean) {
+  if (windowLen < 1) throw ValueError("a spectrum window needs >= 1 sample, got " + std::to_string(windowLen));
+  if (!(dtMs > 0 && dtMs < INF)) throw ValueError("dtMs must be finite and > 0");
+  if (!(taperFraction >= 0 && taperFraction <= 0.5)) throw ValueError("taperFraction must be in 0 .. 0.5");
+  int64_t n = nfft;
+  if (n == 0) {
+    n = 1;
+    while (n < windowLen) n <<= 1;
+  }
+  if (n < windowLen) throw ValueError("nfft is shorter than the window");
+  SpectrumPlan<T> sp;
+  sp.fft = initFftPlan<T>(n);
+  sp.dtMs = dtMs;
+  sp.demean = demean;
+  sp.taper.resize(windowLen);
+  int64_t ramp = (int64_t)std::round(taperFraction * (double)windowLen);
+  for (int64_t i = 0; i < windowLen; i++) {
+    int64_t d = std::min(i, windowLen - 1 - i);
+    double w = 1.0;
+    if (d < ramp) {
+      double sv = std::sin(PI / 2 * (double)(d + 1) / (double)(ramp + 1));
+      w = sv * sv;
+    }
+    sp.taper[i] = (T)w;
+    sp.taperSum += (double)sp.taper[i];
+  }
+  return sp;
+}
+// windowInto, fft/spectrum.nim:261-281: returns Σw, NaN for a non-finite window
+template <class T> double windowInto(const SpectrumPlan<T>& sp, const T* x, int64_t len, T* dst) {
+  int64_t n = std::min<int64_t>(len, (int64_t)sp.taper.size());
+  double sum = n > 0 ? sum64(x, n) : 0.0;
+  bool finite = sum - sum == 0;
+  T m = (sp.demean && n > 0 && finite) ? (T)(sum / (double)n) : (T)0;
+  double sw = 0;
+  if (n == (int64_t)sp.taper.size()) {
+    for (int64_t j = 0; j < n; j++) dst[j] = (x[j] - m) * sp.taper[j];
+    sw = sp.taperSum;
+  } else {
+    for (int64_t j = 0; j < n; j++) {
+      T w = std::min(sp.taper[j], sp.taper[n - 1 - j]);
+      dst[j] = (x[j] - m) * w;
+      sw += (double)w;
+    }
+  }
+  for (int64_t j = n; j < sp.fft.n; j++) dst[j] = (T)0;
+  return finite ? sw : NaN;
+}
+template <class T> double sides(const SpectrumPlan<T>& sp, int64_t k) { return (k == 0 || 2 * k == sp.fft.n) ? 1.0 : 2.0; }
+// amplitudeInto, fft/spectrum.nim:283-300
+template <class T> void amplitudeInto(const SpectrumPlan<T>& sp, const T* x, int64_t len, T* amp, T* phase) {
+  int64_t nb = sp.fft.bins();
+  std::vector<T> xw(sp.fft.n), re(nb), im(nb);
+  double sw = windowInto(sp, x, len, xw.data());
+  fftForward(sp.fft, xw.data(), re.data(), im.data());
+  for (int64_t k = 0; k < nb; k++) {
+    amp[k] = (T)(std::hypot((double)re[k], (double)im[k]) * sides(sp, k) / sw);
+    phase[k] = (T)std::atan2((double)im[k], (double)re[k]);
+  }
+}
+// averageAmplitudeInto, fft/spectrum.nim:302-416 (rows in order, one at a time)
+template <class T> int64_t averageAmplitude(const SpectrumPlan<T>& sp, const T* b, int64_t rows, int64_t cols,
+                                            const int32_t* live, int64_t firstCol, int64_t r0, int64_t r1, double* amp) {
+  int64_t nb = sp.fft.bins();
+  std::vector<double> acc(nb, 0.0);
+  std::vector<T> xw(sp.fft.n), re(nb), im(nb);
+  int64_t used = 0;
+  for (int64_t r = std::max<int64_t>(r0, 0); r <= std::min(r1, rows - 1); r++) {
+    int64_t lv = std::min<int64_t>(std::max<int32_t>(live[r], 0), cols);
+    if (lv <= firstCol) continue;
+    int64_t last = std::min<int64_t>(lv, firstCol + (int64_t)sp.taper.size());
+    double sw = windowInto(sp, b + r * cols + firstCol, last - firstCol, xw.data());
+    if (!(sw > 0)) continue;
+    fftForward(sp.fft, xw.data(), re.data(), im.data());
+    double scale = 1 / (sw * sw);
+    for (int64_t k = 0; k < nb; k++) {
+      double rr = (double)re[k], ii = (double)im[k];
+      acc[k] += (rr * rr + ii * ii) * scale;
+    }
+    used++;
+  }
+  for (int64_t k = 0; k < nb; k++) amp[k] = used > 0 ? std::sqrt(acc[k] / (double)used) * sides(sp, k) : 0.0;
+  return used;
+}
+
 // ------------------------------------------------------------- filter/iir --
 // A biquad, a0 = 1, with its 0 Hz gain (filter/iir.nim:82-111).
 struct Sos {
@@ -1764,6 +1858,32 @@ int orc_required_margin(const psg_op* ops, int nops, double dtMs, int64_t* out) 
       }
     }
     *out = m;
+  });
+}
+// SpectrumPlan's nfft and Σw; averageAmplitudeInto over rows r0 .. r1
+// (returns the rows averaged in *used); amplitudeInto per row (windows up to
+// each row's live end; rows × bins of amp and phase).
+int orc_spectrum(int dtype, double dtMs, int64_t windowLen, double taperFraction, int64_t nfft, int demean,
+                 const void* b, int64_t rows, int64_t cols, const int32_t* live, int64_t firstCol, int64_t r0,
+                 int64_t r1, double* avg, int64_t* used, void* amp, void* phase, int64_t* nfftOut, double* taperSum) {
+  return guard([&] {
+    auto run = [&](auto tag) {
+      typedef decltype(tag) T;
+      SpectrumPlan<T> sp = initSpectrumPlan<T>(dtMs, windowLen, taperFraction, nfft, demean != 0);
+      if (nfftOut) *nfftOut = sp.fft.n;
+      if (taperSum) *taperSum = sp.taperSum;
+      if (avg) *used = averageAmplitude(sp, (const T*)b, rows, cols, live, firstCol, r0, r1, avg);
+      if (amp) {
+        int64_t nb = sp.fft.bins();
+        for (int64_t r = 0; r < rows; r++) {
+          int64_t lv = std::min<int64_t>(std::max<int32_t>(live[r], 0), cols);
+          int64_t n = std::max<int64_t>(0, std::min<int64_t>(lv, firstCol + windowLen) - firstCol);
+          amplitudeInto(sp, (const T*)b + r * cols + firstCol, n, (T*)amp + r * nb, (T*)phase + r * nb);
+        }
+      }
+    };
+    if (dtype == PSG_F32) run(float());
+    else run(double());
   });
 }
 // IirPlan's order, requiredMargin, dcGain and magnitudeAt (filter/iir.nim:

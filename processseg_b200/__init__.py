@@ -17,6 +17,8 @@ from .ops import (Op, Pipeline, agcOp, bandPassOp, clipOp, decodeWindow, demeanO
                   normalizeOp, polarityOp, scaleOp)
 from .mute import MuteCurve, lmoMute, tableMute, timeMute
 from .iir import IirPlan, initIirPlan
+from .spectrum import (SpectrumPlan, amplitudePhaseInto, circularMeanDeg, dbAbsolute, dbPeak, initSpectrumPlan,
+                       removeDelayInto, toDbInto, unwrapPhaseInto)
 
 # Reference enum names (pipeline.nim / gain.nim / edges.nim)
 trNone, trMean, trLinear = TR_NONE, TR_MEAN, TR_LINEAR

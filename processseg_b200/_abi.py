@@ -150,6 +150,11 @@ def _declare(lib):
         "psg_apply_host_keyed": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P]),
         "psg_plan_needs_keys": (I32, [P]),
         "psg_applied_response": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, P, I32, P, P]),
+        "psg_spectrum_plan_create": (C.c_int, [I32, DBL, I32, DBL, I32, I32, C.POINTER(P)]),
+        "psg_spectrum_plan_destroy": (None, [P]),
+        "psg_spectrum_plan_info": (C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(DBL)]),
+        "psg_spectrum_average": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, I64, I64, P, P, P]),
+        "psg_spectrum_amplitude": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, P, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),
         "psg_run_part_keyed": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P, P]),

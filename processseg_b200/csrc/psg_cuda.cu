@@ -403,6 +403,133 @@ __global__ void stack_result_kernel(const double* __restrict__ num, const int* _
   }
 }
 
+// ============================================================ spectra
+struct SpecArgs {
+  const void* src;
+  long long row0, row1;  // the rows taken (inclusive)
+  int cols, first_col;
+  const int* live;
+  int window, nfft, bins, odd, demean;
+  const void* taper;  // T[window]
+  double taper_sum;
+  const void* tw;     // ω_m^e of the complex FFT
+  const void* split;  // exp(−2πik/nfft), k = 0 .. nfft/2 (even nfft)
+  FftDesc fft;
+  void* gwork;        // per-CTA transform buffers in global memory (else NULL)
+  long long gstride;
+  double* acc;        // average: per CTA, Σ over its rows of |X[k]|²/Σw²
+  int* used;          // average: per CTA, its rows
+  void* amp;          // amplitude: rows × bins of T (the block's rows)
+  void* phase;
+};
+
+// The windowed spectrum of rows row0 .. row1 (fft/spectrum.nim:232-416), one
+// CTA per row: the window's samples (up to its live end) demeaned in T and
+// tapered (a short window with its own end ramp and Σw), the forward
+// transform in the CTA's buffers, and per bin either the scaled power added
+// to this CTA's accumulator (AVG; rows in order, so the sums are the same on
+// every run) or the scaled amplitude and the phase of the row.
+template <class T, bool AVG, class M>
+__device__ __forceinline__ void spectrum_rows(const SpecArgs& a, const M& mem, SharedMem& S) {
+  typedef typename C2<T>::type V;
+  const T* src = reinterpret_cast<const T*>(a.src);
+  const T* taper = reinterpret_cast<const T*>(a.taper);
+  const V* tw = reinterpret_cast<const V*>(a.tw);
+  const V* split = reinterpret_cast<const V*>(a.split);
+  const int W = a.window, n2 = a.nfft, mc = a.odd ? n2 : n2 / 2;  // complex points
+  V* buf = reinterpret_cast<V*>(mem.base());
+  double* acc = AVG ? a.acc + (size_t)blockIdx.x * a.bins : nullptr;
+  int used = 0;
+  for (long long r = a.row0 + blockIdx.x; r <= a.row1; r += gridDim.x) {
+    const int live = min(max(a.live[r], 0), a.cols);
+    if (AVG && live <= a.first_col) continue;
+    const int n = max(0, min(live, a.first_col + W) - a.first_col);
+    const T* x = src + r * (long long)a.cols + a.first_col;
+    double sum = 0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) sum += (double)x[j];
+    sum = block_sum(sum, S.red[0][0]);
+    const bool finite = sum - sum == 0;
+    const T mean = a.demean && n > 0 && finite ? (T)(sum / (double)n) : (T)0;
+    double sw = 0;
+    T* Ar = reinterpret_cast<T*>(buf);
+    for (int j = threadIdx.x; j < n2; j += blockDim.x) {
+      T v = (T)0;
+      if (j < n) {
+        const T w = n == W ? taper[j] : min(taper[j], taper[n - 1 - j]);
+        v = (x[j] - mean) * w;
+        if (n != W) sw += (double)w;
+      }
+      if (a.odd) buf[j] = V{v, (T)0};
+      else Ar[j] = v;
+    }
+    sw = n == W ? a.taper_sum : block_sum(sw, S.red[1][0]);
+    if (!finite) sw = NAN;
+    if (AVG && !(sw > 0)) continue;  // a NaN or infinite sample: the row is left out
+    __syncthreads();
+    constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
+    const V* z = buf + cfft_forward<T, MAXR>(mem, 0, mc, a.fft, tw);
+    const double sc = AVG ? 1 / (sw * sw) : 0.0;
+    for (int k = threadIdx.x; k < a.bins; k += blockDim.x) {
+      T re, im;
+      if (a.odd) {
+        re = z[k].x;
+        im = z[k].y;
+      } else if (k == 0 || k == mc) {
+        // the real DC and Nyquist bins: Re z0 ± Im z0
+        re = k == 0 ? z[0].x + z[0].y : z[0].x - z[0].y;
+        im = (T)0;
+      } else {
+        // X[k] = E − i·ω^k·O, E = (z[k] + conj z[m−k])/2, O = (z[k] − conj z[m−k])/2
+        const V p = z[k], q = z[mc - k], w = split[k];
+        const T er = (p.x + q.x) * (T)0.5, ei = (p.y - q.y) * (T)0.5;
+        const T orr = (p.x - q.x) * (T)0.5, oi = (p.y + q.y) * (T)0.5;
+        const T tr = w.x * orr - w.y * oi, ti = w.x * oi + w.y * orr;  // ω^k·O
+        re = er + ti;
+        im = ei - tr;
+      }
+      if (AVG) {
+        const double dr = (double)re, di = (double)im;
+        acc[k] += (dr * dr + di * di) * sc;
+      } else {
+        const double side = (k == 0 || 2 * k == n2) ? 1.0 : 2.0;
+        reinterpret_cast<T*>(a.amp)[r * (long long)a.bins + k] = (T)(hypot((double)re, (double)im) * side / sw);
+        reinterpret_cast<T*>(a.phase)[r * (long long)a.bins + k] = (T)atan2((double)im, (double)re);
+      }
+    }
+    used++;
+    __syncthreads();  // the buffers are refilled for the next row
+  }
+  if (AVG && threadIdx.x == 0) a.used[blockIdx.x] = used;
+}
+
+template <class T, bool AVG>
+__global__ void __launch_bounds__(256) spectrum_kernel(SpecArgs a) {
+  __shared__ SharedMem S;
+  if (AVG)
+    for (int k = threadIdx.x; k < a.bins; k += blockDim.x) a.acc[(size_t)blockIdx.x * a.bins + k] = 0;
+  __syncthreads();
+  if (a.gwork) {
+    spectrum_rows<T, AVG>(a, InGlobal{reinterpret_cast<unsigned char*>(a.gwork) + (size_t)blockIdx.x * a.gstride}, S);
+  } else {
+    spectrum_rows<T, AVG>(a, InShared(), S);
+  }
+}
+
+// averageAmplitudeInto's last step: sqrt(mean power)·sides per bin over the
+// CTAs' sums (in CTA order), and the rows averaged.
+__global__ void spectrum_finish(const double* __restrict__ acc, const int* __restrict__ used, int ctas, int bins,
+                                int nfft, double* __restrict__ amp, long long* __restrict__ used_out) {
+  long long u = 0;
+  for (int b = 0; b < ctas; b++) u += used[b];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bins; k += gridDim.x * blockDim.x) {
+    double t = 0;
+    for (int b = 0; b < ctas; b++) t += acc[(size_t)b * bins + k];
+    const double side = (k == 0 || 2 * k == nfft) ? 1.0 : 2.0;
+    amp[k] = u > 0 ? sqrt(t / (double)u) * side : 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && used_out) *used_out = u;
+}
+
 // ======================================================== host plumbing
 static int g_sm_count = 0, g_max_smem = 0, g_device = -1;
 
@@ -525,6 +652,8 @@ struct psg_workspace {
   int64_t bytes = 0;
   void* g = nullptr;  // the work areas of plans with long traces (psg_plan::wide)
   int64_t g_bytes = 0;
+  void* sp = nullptr;  // spectra: per-CTA sums and transform buffers
+  int64_t sp_bytes = 0;
   // Streams and events of the chunked host-memory apply (created on first use).
   static const int kLanes = 4;
   cudaStream_t lane[kLanes] = {};
@@ -542,6 +671,18 @@ struct psg_corr_plan {
   size_t smem = 0;
   int grid = 1;
   FftDesc fft{};
+};
+
+struct psg_spectrum_plan {
+  SpectrumHost host;
+  std::vector<std::unique_ptr<DeviceBuf>> keep;
+  void* taper = nullptr;
+  void* tw = nullptr;
+  void* split = nullptr;
+  FftDesc fft{};
+  size_t smem = 0;   // dynamic shared memory per CTA (0: global buffers)
+  int grid = 1;
+  int64_t gstride = 0;
 };
 
 struct psg_stack {
@@ -1076,6 +1217,7 @@ void psg_workspace_destroy(psg_workspace* ws) {
   }
   if (ws->d) cudaFree(ws->d);
   if (ws->g) cudaFree(ws->g);
+  if (ws->sp) cudaFree(ws->sp);
   delete ws;
 }
 static void ws_grow(psg_workspace* ws, int64_t need) {
@@ -1735,6 +1877,142 @@ int psg_correlate_stack(const psg_corr_plan* plan, psg_stack* st, const void* sr
     return PSG_EINVAL;
   }
   return corr_launch(plan, st, src, dst, rows, cols, live, stack_live, row_map, dt_ms, stream);
+}
+
+// ------------------------------------------------------------- spectra
+int psg_spectrum_plan_create(int32_t dtype, double dt_ms, int32_t window_len, double taper_fraction, int32_t nfft,
+                             int32_t demean, psg_spectrum_plan** out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    *out = nullptr;
+    std::unique_ptr<psg_spectrum_plan> p(new psg_spectrum_plan());
+    p->host = spectrum_plan(dtype, dt_ms, window_len, taper_fraction, nfft, demean != 0, dtype == PSG_F32 ? 12 : 8);
+    ensure_device();
+    const SpectrumHost& h = p->host;
+    const int limit = g_max_smem - (int)sizeof(SharedMem) - 1024;
+    auto setup = [&](auto tag) {
+      typedef decltype(tag) T;
+      typedef typename C2<T>::type V;
+      p->taper = upload(p->keep, as_t<T>(h.taper));
+      p->tw = upload(p->keep, as_c<T>(h.fft.tw_re, h.fft.tw_im));
+      p->split = upload(p->keep, as_c<T>(h.fft.split_re, h.fft.split_im));
+      p->fft = fft_desc(h.fft);
+      const int64_t need = 2 * h.fft.m * (int64_t)sizeof(V);
+      const void* k0 = (const void*)spectrum_kernel<T, true>;
+      const void* k1 = (const void*)spectrum_kernel<T, false>;
+      if (need <= limit) {
+        p->smem = (size_t)need;
+        allow_smem(k0);
+        allow_smem(k1);
+        int per_sm = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k0, 256, p->smem));
+        p->grid = std::max(1, per_sm) * g_sm_count;
+      } else {
+        p->smem = 0;
+        p->gstride = align256(need);
+        p->grid = 2 * g_sm_count;
+      }
+    };
+    if (dtype == PSG_F32) setup(float());
+    else setup(double());
+    *out = p.release();
+  });
+}
+void psg_spectrum_plan_destroy(psg_spectrum_plan* p) { delete p; }
+int psg_spectrum_plan_info(const psg_spectrum_plan* p, int32_t* nfft, int32_t* bins, int32_t* window_len,
+                           double* taper_sum) {
+  return guarded([&] {
+    if (!p) throw InvalidArg("a SpectrumPlan must come from initSpectrumPlan");
+    if (nfft) *nfft = (int32_t)p->host.nfft;
+    if (bins) *bins = (int32_t)p->host.bins;
+    if (window_len) *window_len = (int32_t)p->host.window;
+    if (taper_sum) *taper_sum = p->host.taper_sum;
+  });
+}
+
+static void sp_grow(psg_workspace* ws, int64_t need) {
+  int dev;
+  CUDA_OK(cudaGetDevice(&dev));
+  if ((ws->d || ws->sp) && ws->device >= 0 && ws->device != dev) throw InvalidArg("the workspace belongs to another device");
+  ws->device = dev;
+  if (ws->sp_bytes >= need) return;
+  if (ws->sp) {
+    CUDA_OK(cudaDeviceSynchronize());
+    CUDA_OK(cudaFree(ws->sp));
+    ws->sp = nullptr;
+    ws->sp_bytes = 0;
+  }
+  CUDA_OK(cudaMalloc(&ws->sp, (size_t)need));
+  ws->sp_bytes = need;
+}
+
+static void spectrum_launch(const psg_spectrum_plan* p, psg_workspace* ws, const void* block, int64_t rows, int32_t cols,
+                            const int32_t* live, double dt_ms, int32_t first_col, int64_t row0, int64_t row1, bool avg,
+                            double* amp, int64_t* used, void* amp_t, void* phase_t, cudaStream_t stream) {
+  if (!p) throw InvalidArg("a SpectrumPlan must come from initSpectrumPlan");
+  if (!ws) throw InvalidArg("a workspace is required");
+  if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+  if (rows > 0 && (!block || !live)) throw InvalidArg("block and live are required");
+  if (!same_interval(dt_ms, p->host.dt_ms))
+    throw InvalidArg("the rows' interval " + std::to_string(dt_ms) + " ms is not the plan's " + std::to_string(p->host.dt_ms) + " ms");
+  if (first_col < 0) throw InvalidArg("firstCol must be ≥ 0, got " + std::to_string(first_col));
+  if (avg && !amp) throw InvalidArg("amp is required");
+  if (!avg && rows > 0 && (!amp_t || !phase_t)) throw InvalidArg("amp and phase are required");
+  ensure_device();
+  const int64_t lo = std::max<int64_t>(row0, 0), hi = std::min<int64_t>(row1, rows - 1);
+  const int64_t nr = hi >= lo ? hi - lo + 1 : 0;
+  const int bins = (int)p->host.bins;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nr, p->grid));
+  const int64_t acc_b = avg ? align256((int64_t)grid * bins * 8) + align256((int64_t)grid * 4) : 0;
+  sp_grow(ws, acc_b + p->gstride * grid + 256);
+  SpecArgs a{};
+  a.src = block;
+  a.row0 = lo;
+  a.row1 = hi;
+  a.cols = cols;
+  a.first_col = first_col;
+  a.live = live;
+  a.window = (int)p->host.window;
+  a.nfft = (int)p->host.nfft;
+  a.bins = bins;
+  a.odd = p->host.odd;
+  a.demean = p->host.demean;
+  a.taper = p->taper;
+  a.taper_sum = p->host.taper_sum;
+  a.tw = p->tw;
+  a.split = p->split;
+  a.fft = p->fft;
+  char* base = (char*)ws->sp;
+  a.acc = avg ? (double*)base : nullptr;
+  a.used = avg ? (int*)(base + align256((int64_t)grid * bins * 8)) : nullptr;
+  a.gwork = p->smem ? nullptr : base + acc_b;
+  a.gstride = p->gstride;
+  a.amp = amp_t;
+  a.phase = phase_t;
+  void* args[] = {&a};
+  const bool f32 = p->host.dtype == PSG_F32;
+  const void* k = avg ? (f32 ? (const void*)spectrum_kernel<float, true> : (const void*)spectrum_kernel<double, true>)
+                      : (f32 ? (const void*)spectrum_kernel<float, false> : (const void*)spectrum_kernel<double, false>);
+  if (nr > 0 || avg) CUDA_OK(cudaLaunchKernel(k, dim3(grid), dim3(256), args, p->smem, stream));
+  if (avg) spectrum_finish<<<(bins + 255) / 256, 256, 0, stream>>>(a.acc, a.used, grid, bins, a.nfft, amp, (long long*)used);
+  CUDA_OK(cudaGetLastError());
+}
+
+int psg_spectrum_average(const psg_spectrum_plan* plan, psg_workspace* ws, const void* block, int64_t rows, int32_t cols,
+                         const int32_t* live, double dt_ms, int32_t first_col, int64_t row0, int64_t row1, double* amp,
+                         int64_t* used, void* stream) {
+  return guarded([&] {
+    spectrum_launch(plan, ws, block, rows, cols, live, dt_ms, first_col, row0, row1, true, amp, used, nullptr, nullptr,
+                    (cudaStream_t)stream);
+  });
+}
+int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, const void* block, int64_t rows,
+                           int32_t cols, const int32_t* live, double dt_ms, int32_t first_col, void* amp, void* phase,
+                           void* stream) {
+  return guarded([&] {
+    spectrum_launch(plan, ws, block, rows, cols, live, dt_ms, first_col, 0, rows - 1, false, nullptr, nullptr, amp,
+                    phase, (cudaStream_t)stream);
+  });
 }
 int psg_stack_result(const psg_stack* st, void* dst, int32_t dtype, int32_t norm, void* stream) {
   return guarded([&] {

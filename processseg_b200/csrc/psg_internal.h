@@ -125,6 +125,23 @@ int64_t required_margin(const psg_op* ops, int n_ops, double dt_ms);
 double gain_factor_at(const psg_gain_curve& c, double t_ms);
 bool same_interval(double dt, double plan_dt);
 
+// --------------------------------------------------------------- spectra
+// SpectrumPlan (fft/spectrum.nim:79-107): a window of `window` samples,
+// tapered and zero-padded to nfft. The device FFT is complex: of nfft/2
+// points over sample pairs for an even nfft (then the real-FFT split), of
+// nfft points over the samples for an odd one.
+struct SpectrumHost {
+  int dtype = PSG_F32;
+  double dt_ms = 0;
+  int64_t window = 0, nfft = 0, bins = 0;
+  bool demean = true, odd = false;
+  std::vector<double> taper;  // the weights, rounded to T
+  double taper_sum = 0;       // Σ of the T weights, in float64
+  FftTables fft;
+};
+SpectrumHost spectrum_plan(int dtype, double dt_ms, int64_t window, double taper_fraction, int64_t nfft,
+                           bool demean, int max_radix);
+
 // ----------------------------------------------------------- correlation
 struct CorrHost {
   int64_t n = 0, shift = 0, record = 0, out = 0, pilot_len = 0;

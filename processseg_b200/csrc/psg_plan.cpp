@@ -775,6 +775,46 @@ int iir_order(const IirHost& p) {
   return o;
 }
 
+// ---------------------------------------------------------------- spectra
+// initSpectrumPlan (fft/spectrum.nim:79-107)
+SpectrumHost spectrum_plan(int dtype, double dt_ms, int64_t window, double taper_fraction, int64_t nfft,
+                           bool demean, int max_radix) {
+  need(dtype == PSG_F32 || dtype == PSG_F64, "dtype must be float32 or float64");
+  need(window >= 1, "a spectrum window needs ≥ 1 sample, got " + std::to_string(window));
+  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and > 0, got " + num(dt_ms));
+  need(taper_fraction >= 0 && taper_fraction <= 0.5, "taperFraction must be in 0 .. 0.5, got " + num(taper_fraction));
+  int64_t n = nfft;
+  if (n == 0) {
+    n = 1;
+    while (n < window) n *= 2;  // nextPowerOfTwo
+  }
+  need(n >= window, "nfft " + std::to_string(n) + " is shorter than the window (" + std::to_string(window) + ")");
+  need(fast_len(n), "an FFT length must be 2·3·5-smooth, got " + std::to_string(n));
+  need(n <= (1 << 22), "a spectrum FFT of " + std::to_string(n) + " points is too long for the device");
+  SpectrumHost p;
+  p.dtype = dtype;
+  p.dt_ms = dt_ms;
+  p.window = window;
+  p.nfft = n;
+  p.bins = n / 2 + 1;
+  p.demean = demean;
+  p.odd = (n & 1) != 0;
+  p.fft = fft_tables(p.odd ? 2 * n : n, max_radix);
+  const int64_t ramp = (int64_t)std::round(taper_fraction * (double)window);
+  p.taper.resize(window);
+  for (int64_t i = 0; i < window; i++) {
+    const int64_t d = std::min(i, window - 1 - i);  // from the nearer end
+    double w = 1.0;
+    if (d < ramp) {
+      double s = std::sin(kPi / 2 * (double)(d + 1) / (double)(ramp + 1));
+      w = s * s;
+    }
+    p.taper[i] = as_dtype(dtype, w);
+    p.taper_sum += p.taper[i];
+  }
+  return p;
+}
+
 // --------------------------------------------------------------- vibroseis
 namespace {
 // vibroseis/taper.nim:125-145 for the shapes that need no special function.
