@@ -17,6 +17,7 @@ from .ops import (Op, Pipeline, agcOp, bandPassOp, clipOp, decodeWindow, demeanO
                   normalizeOp, polarityOp, scaleOp)
 from .mute import MuteCurve, lmoMute, tableMute, timeMute
 from .iir import IirPlan, initIirPlan
+from .pool import ProcessPool, newProcessPool
 from .spectrum import (SpectrumPlan, amplitudePhaseInto, circularMeanDeg, dbAbsolute, dbPeak, initSpectrumPlan,
                        removeDelayInto, toDbInto, unwrapPhaseInto)
 

@@ -391,3 +391,23 @@ def test_long_trace_workspace_and_limits():
     assert ws.bytes >= long_plan.workspaceSize(4, 16384) > short_plan.workspaceSize(4, 16384)
     with pytest.raises(ValueError, match="shared memory"):
         flow.compile(P.float64, 0.5, 40000)
+
+
+def test_process_pool_apply_matches_plan_apply():
+    """newProcessPool / ProcessPool.apply (pool.nim:145-302): the same rows
+    as PipelinePlan.apply, on device tensors and host arrays, blocking."""
+    g = synth.c2(rows=64)
+    meta = g.meta()
+    plan = P.initPipeline(C2_FLOW).compile(P.float32, 2.0, 3001)
+    want = run_gpu(C2_FLOW, g.data, meta, P.F32, 2.0)
+    pool = P.newProcessPool(8)
+    assert pool.workers == 8
+    dst = np.zeros_like(g.data)
+    pool.apply(plan, g.data, dst, meta)
+    assert np.array_equal(dst, want)
+    x = torch.from_numpy(g.data).cuda()
+    pool.apply(plan, x, meta)
+    assert np.array_equal(x.cpu().numpy(), want)
+    pool.ping()
+    with pytest.raises(ValueError):
+        P.newProcessPool(0)
