@@ -389,6 +389,29 @@ int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, con
                            int64_t rows, int32_t cols, const int32_t* live, double dt_ms,
                            int32_t first_col, void* amp, void* phase, void* stream);
 
+/* --------------------------------------------------------------- SEG-Y */
+/* The decode a reader does before the path (parseSEG's trace reading, which
+ * the reference does not vendor), on the device: `rows` raw trace records
+ * of record_bytes each (device memory), a header of header_bytes (240 for
+ * SEG-Y) and then `samples` samples of data sample format `format` (SEG-Y
+ * rev 2 codes 1 IBM float, 2 int32, 3 int16, 5 IEEE float32, 6 IEEE
+ * float64, 7 int24, 8 int8, 10 uint32, 11 uint16, 15 uint24, 16 uint8),
+ * big-endian unless little_endian, into a device block of out_cols columns
+ * of dtype (zeros past `samples`). Each value converts exactly to float64
+ * first, then rounds to dtype. Asynchronous on `stream`. */
+int psg_segy_decode(const void* records, int64_t rows, int64_t record_bytes, int32_t header_bytes,
+                    int32_t samples, int32_t format, int32_t little_endian, int32_t dtype,
+                    void* out, int32_t out_cols, void* stream);
+/* The trace-header keys of the same records (SEG-Y rev 2 trace header):
+ * status from the trace identification code (bytes 29-30: 1 live, 2 dead,
+ * 0 unknown, others auxiliary), offset (37-40), t0 = the delay recording
+ * time in ms (109-110), the number of samples (115-116) and the sample
+ * interval in µs (117-118). Device arrays of `rows` values; any may be
+ * NULL. */
+int psg_segy_keys(const void* records, int64_t rows, int64_t record_bytes, int32_t little_endian,
+                  int32_t* status, int32_t* num_samples, double* interval_us, double* offset,
+                  double* t0_ms, void* stream);
+
 /* ----------------------------------------------------------- vibroseis */
 /* linearSweep + sweepInto + generatePilot (taper shapes tpLinear, tpCosine,
  * tpCos2, tpHamming, tpBlackman), src/processSEG/vibroseis/sweep.nim:185-342,

@@ -281,6 +281,57 @@ def spectrum_amplitudes(b, live, dtMs, windowLen, firstCol, taperFraction=0.1, n
     return amp, phase
 
 
+def segy_decode(records, samples, format, dtype=np.float32, little=False, header=240, out_cols=0):
+    """SEG-Y rev 2 data samples of each record (numpy, exact float64 first,
+    then rounded to dtype). IBM float: (−1)^s · 0.f · 16^(e − 64), a 24-bit
+    fraction f and a 7-bit excess-64 exponent e."""
+    sz = {1: 4, 2: 4, 3: 2, 5: 4, 6: 8, 7: 3, 8: 1, 10: 4, 11: 2, 15: 3, 16: 1}[format]
+    rec = np.ascontiguousarray(records, dtype=np.uint8)
+    raw = rec[:, header:header + samples * sz].reshape(rec.shape[0], samples, sz).astype(np.uint64)
+    if little:
+        raw = raw[:, :, ::-1]
+    u = np.zeros(raw.shape[:2], np.uint64)
+    for i in range(sz):
+        u = (u << np.uint64(8)) | raw[:, :, i]
+    if format == 1:
+        frac = (u & np.uint64(0xFFFFFF)).astype(np.float64)
+        e = ((u >> np.uint64(24)) & np.uint64(0x7F)).astype(np.int64)
+        v = np.ldexp(frac, 4 * e - 280)
+        v = np.where((u >> np.uint64(31)) & np.uint64(1), -v, v)
+    elif format == 2:
+        v = u.astype(np.uint32).view(np.int32).astype(np.float64)
+    elif format == 3:
+        v = u.astype(np.uint16).view(np.int16).astype(np.float64)
+    elif format == 5:
+        v = u.astype(np.uint32).view(np.float32).astype(np.float64)
+    elif format == 6:
+        v = u.view(np.float64).copy()
+    elif format == 7:
+        v = ((u.astype(np.int64) ^ 0x800000) - 0x800000).astype(np.float64)
+    elif format == 8:
+        v = u.astype(np.uint8).view(np.int8).astype(np.float64)
+    else:
+        v = u.astype(np.float64)
+    cols = out_cols or samples
+    out = np.zeros((rec.shape[0], cols), dtype)
+    with np.errstate(over="ignore"):
+        out[:, :min(cols, samples)] = v[:, :min(cols, samples)].astype(dtype)
+    return out
+
+
+def segy_keys(records, little=False):
+    """(status, numSamples, intervalUs, offset, t0Ms) from the trace headers."""
+    rec = np.ascontiguousarray(records, dtype=np.uint8)
+    o = "<" if little else ">"
+    def field(at, t):
+        return np.frombuffer(rec[:, at:at + np.dtype(t).itemsize].tobytes(), dtype=np.dtype(o + t))
+    code = field(28, "i2")
+    status = np.where(code == 1, A.TS_LIVE, np.where(code == 2, A.TS_DEAD, np.where(code == 0, A.TS_UNKNOWN,
+                                                                                     A.TS_AUX)))
+    return (status.astype(np.int32), field(114, "u2").astype(np.int32), field(116, "u2").astype(np.float64),
+            field(36, "i4").astype(np.float64), field(108, "i2").astype(np.float64))
+
+
 def rows_flatten(status, numSamples, t0Ms, firstSample, dtMs, failed, cols, mode=0):
     status = np.ascontiguousarray(status, dtype=np.int32)
     ns = np.ascontiguousarray(numSamples, dtype=np.int32)

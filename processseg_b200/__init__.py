@@ -18,6 +18,7 @@ from .ops import (Op, Pipeline, agcOp, bandPassOp, clipOp, decodeWindow, demeanO
 from .mute import MuteCurve, lmoMute, tableMute, timeMute
 from .iir import IirPlan, initIirPlan
 from .pool import ProcessPool, newProcessPool
+from . import segy
 from .spectrum import (SpectrumPlan, amplitudePhaseInto, circularMeanDeg, dbAbsolute, dbPeak, initSpectrumPlan,
                        removeDelayInto, toDbInto, unwrapPhaseInto)
 

@@ -155,6 +155,8 @@ def _declare(lib):
         "psg_spectrum_plan_info": (C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(DBL)]),
         "psg_spectrum_average": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, I64, I64, P, P, P]),
         "psg_spectrum_amplitude": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, P, P, P]),
+        "psg_segy_decode": (C.c_int, [P, I64, I64, I32, I32, I32, I32, I32, P, I32, P]),
+        "psg_segy_keys": (C.c_int, [P, I64, I64, I32, P, P, P, P, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),
         "psg_run_part_keyed": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P, P]),

@@ -530,6 +530,80 @@ __global__ void spectrum_finish(const double* __restrict__ acc, const int* __res
   if (blockIdx.x == 0 && threadIdx.x == 0 && used_out) *used_out = u;
 }
 
+// ============================================================ SEG-Y decode
+// The sample formats of SEG-Y rev 2 (data sample format code, binary header
+// bytes 3225-3226): 1 IBM hexadecimal float, 2 int32, 3 int16, 5 IEEE
+// float32, 6 IEEE float64, 7 int24, 8 int8, 10 uint32, 11 uint16, 15
+// uint24, 16 uint8; big-endian unless the file is little-endian.
+__host__ __device__ inline int segy_sample_bytes(int format) {
+  switch (format) {
+    case 1: case 2: case 5: case 10: return 4;
+    case 3: case 11: return 2;
+    case 6: return 8;
+    case 7: case 15: return 3;
+    case 8: case 16: return 1;
+    default: return 0;
+  }
+}
+// An unsigned big- (or little-) endian integer of `n` bytes at p.
+__device__ __forceinline__ unsigned long long segy_uint(const unsigned char* __restrict__ p, int n, bool little) {
+  unsigned long long v = 0;
+  for (int i = 0; i < n; i++) v = (v << 8) | (unsigned long long)__ldg(p + (little ? n - 1 - i : i));
+  return v;
+}
+// One sample as a double: exact for every format (an IBM float's 24-bit
+// fraction times 16^(e − 64) is a double).
+__device__ __forceinline__ double segy_value(unsigned long long u, int format) {
+  switch (format) {
+    case 1: {  // IBM: sign, 7-bit excess-64 base-16 exponent, 24-bit fraction
+      const double f = ldexp((double)(u & 0xffffffull), 4 * (int)((u >> 24) & 0x7f) - 280);
+      return (u >> 31) ? -f : f;
+    }
+    case 2: return (double)(int)(unsigned)u;
+    case 3: return (double)(short)(unsigned short)u;
+    case 5: return (double)__uint_as_float((unsigned)u);
+    case 6: return __longlong_as_double((long long)u);
+    case 7: return (double)((int)((unsigned)u << 8) >> 8);
+    case 8: return (double)(signed char)(unsigned char)u;
+    default: return (double)u;  // 10, 11, 15, 16: unsigned
+  }
+}
+// Rows of raw trace records (a header of `header_bytes`, then `samples`
+// samples) into a block of T, `out_cols` wide (zeros past the record's
+// samples). One CTA per row; a warp reads consecutive samples.
+template <class T>
+__global__ void __launch_bounds__(256) segy_decode_kernel(const unsigned char* __restrict__ rec, long long rows,
+                                                          long long record_bytes, int header_bytes, int samples,
+                                                          int format, int little, T* __restrict__ out, int out_cols) {
+  const int sz = segy_sample_bytes(format);
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const unsigned char* p = rec + r * record_bytes + header_bytes;
+    T* o = out + r * (long long)out_cols;
+    for (int j = threadIdx.x; j < out_cols; j += blockDim.x)
+      o[j] = j < samples ? (T)segy_value(segy_uint(p + (long long)j * sz, sz, little != 0), format) : (T)0;
+  }
+}
+// The trace-header keys a meta needs, one thread per row (SEG-Y rev 2 trace
+// header, 1-based byte positions): the trace identification code (29-30:
+// 1 live, 2 dead, 0 unknown, others auxiliary), the offset (37-40, int32),
+// the delay recording time (109-110, int16 ms), the number of samples
+// (115-116, uint16) and the sample interval (117-118, uint16 µs).
+__global__ void segy_keys_kernel(const unsigned char* __restrict__ rec, long long rows, long long record_bytes,
+                                 int little, int* __restrict__ status, int* __restrict__ num_samples,
+                                 double* __restrict__ interval_us, double* __restrict__ offset,
+                                 double* __restrict__ t0_ms) {
+  const bool le = little != 0;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows; r += (long long)gridDim.x * blockDim.x) {
+    const unsigned char* h = rec + r * record_bytes;
+    const int code = (short)(unsigned short)segy_uint(h + 28, 2, le);
+    if (status) status[r] = code == 1 ? PSG_TS_LIVE : (code == 2 ? PSG_TS_DEAD : (code == 0 ? PSG_TS_UNKNOWN : PSG_TS_AUX));
+    if (offset) offset[r] = (double)(int)(unsigned)segy_uint(h + 36, 4, le);
+    if (t0_ms) t0_ms[r] = (double)(short)(unsigned short)segy_uint(h + 108, 2, le);
+    if (num_samples) num_samples[r] = (int)segy_uint(h + 114, 2, le);
+    if (interval_us) interval_us[r] = (double)segy_uint(h + 116, 2, le);
+  }
+}
+
 // ======================================================== host plumbing
 static int g_sm_count = 0, g_max_smem = 0, g_device = -1;
 
@@ -2012,6 +2086,48 @@ int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, con
   return guarded([&] {
     spectrum_launch(plan, ws, block, rows, cols, live, dt_ms, first_col, 0, rows - 1, false, nullptr, nullptr, amp,
                     phase, (cudaStream_t)stream);
+  });
+}
+
+// ------------------------------------------------------------- SEG-Y
+int psg_segy_decode(const void* records, int64_t rows, int64_t record_bytes, int32_t header_bytes, int32_t samples,
+                    int32_t format, int32_t little_endian, int32_t dtype, void* out, int32_t out_cols, void* stream) {
+  return guarded([&] {
+    const int sz = segy_sample_bytes(format);
+    if (sz == 0) throw InvalidArg("SEG-Y data sample format " + std::to_string(format) + " is not supported");
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    if (rows < 0 || header_bytes < 0 || samples < 0 || out_cols < 0) throw InvalidArg("negative size");
+    if ((int64_t)header_bytes + (int64_t)samples * sz > record_bytes)
+      throw InvalidArg("a record of " + std::to_string(record_bytes) + " bytes holds no " + std::to_string(samples) +
+                       " samples of " + std::to_string(sz) + " bytes after a " + std::to_string(header_bytes) +
+                       "-byte header");
+    if (rows > 0 && (!records || (!out && out_cols > 0))) throw InvalidArg("null argument");
+    if (rows == 0 || out_cols == 0) return;
+    ensure_device();
+    const int grid = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == PSG_F32)
+      segy_decode_kernel<float><<<grid, 256, 0, st>>>((const unsigned char*)records, rows, record_bytes, header_bytes,
+                                                      samples, format, little_endian, (float*)out, out_cols);
+    else
+      segy_decode_kernel<double><<<grid, 256, 0, st>>>((const unsigned char*)records, rows, record_bytes, header_bytes,
+                                                       samples, format, little_endian, (double*)out, out_cols);
+    CUDA_OK(cudaGetLastError());
+  });
+}
+int psg_segy_keys(const void* records, int64_t rows, int64_t record_bytes, int32_t little_endian, int32_t* status,
+                  int32_t* num_samples, double* interval_us, double* offset, double* t0_ms, void* stream) {
+  return guarded([&] {
+    if (rows < 0) throw InvalidArg("negative size");
+    if (record_bytes < 240) throw InvalidArg("a SEG-Y trace record holds a 240-byte header");
+    if (rows > 0 && !records) throw InvalidArg("null argument");
+    if (rows == 0) return;
+    ensure_device();
+    const int grid = (int)std::min<int64_t>((rows + 255) / 256, (int64_t)g_sm_count * 8);
+    segy_keys_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const unsigned char*)records, rows, record_bytes,
+                                                             little_endian, status, num_samples, interval_us, offset,
+                                                             t0_ms);
+    CUDA_OK(cudaGetLastError());
   });
 }
 int psg_stack_result(const psg_stack* st, void* dst, int32_t dtype, int32_t norm, void* stream) {
