@@ -303,7 +303,8 @@ def segy_decode(records, samples, format, dtype=np.float32, little=False, header
     elif format == 3:
         v = u.astype(np.uint16).view(np.int16).astype(np.float64)
     elif format == 5:
-        v = u.astype(np.uint32).view(np.float32).astype(np.float64)
+        with np.errstate(invalid="ignore"):
+            v = u.astype(np.uint32).view(np.float32).astype(np.float64)
     elif format == 6:
         v = u.view(np.float64).copy()
     elif format == 7:
@@ -314,7 +315,7 @@ def segy_decode(records, samples, format, dtype=np.float32, little=False, header
         v = u.astype(np.float64)
     cols = out_cols or samples
     out = np.zeros((rec.shape[0], cols), dtype)
-    with np.errstate(over="ignore"):
+    with np.errstate(over="ignore", invalid="ignore"):
         out[:, :min(cols, samples)] = v[:, :min(cols, samples)].astype(dtype)
     return out
 
