@@ -556,7 +556,10 @@ __device__ __forceinline__ unsigned long long segy_uint(const unsigned char* __r
 __device__ __forceinline__ double segy_value(unsigned long long u, int format) {
   switch (format) {
     case 1: {  // IBM: sign, 7-bit excess-64 base-16 exponent, 24-bit fraction
-      const double f = ldexp((double)(u & 0xffffffull), 4 * (int)((u >> 24) & 0x7f) - 280);
+      // fraction · 2^(4e − 280), the power of two built as a double (exact:
+      // 4e − 280 lies in −280 .. 228)
+      const int e2 = 4 * (int)((u >> 24) & 0x7f) - 280;
+      const double f = (double)(unsigned)(u & 0xffffffu) * __hiloint2double((e2 + 1023) << 20, 0);
       return (u >> 31) ? -f : f;
     }
     case 2: return (double)(int)(unsigned)u;
@@ -571,16 +574,50 @@ __device__ __forceinline__ double segy_value(unsigned long long u, int format) {
 // Rows of raw trace records (a header of `header_bytes`, then `samples`
 // samples) into a block of T, `out_cols` wide (zeros past the record's
 // samples). One CTA per row; a warp reads consecutive samples.
+// 4- and 2-byte samples on their own alignment (every row's samples start
+// aligned when the records' base, header and length are) are read one word
+// per sample, four words in flight per thread, and byte-swapped with a
+// permute; other layouts byte by byte.
+template <class T, class W>
+__device__ __forceinline__ void segy_words(const W* __restrict__ w, T* __restrict__ o, int samples, int out_cols,
+                                           int format, bool le) {
+  constexpr int U = 4;
+  for (int j0 = threadIdx.x; j0 < out_cols; j0 += U * blockDim.x) {
+    unsigned u[U];
+#pragma unroll
+    for (int q = 0; q < U; q++) {
+      const int j = j0 + q * (int)blockDim.x;
+      u[q] = j < samples ? (unsigned)__ldg(w + j) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < U; q++) {
+      const int j = j0 + q * (int)blockDim.x;
+      if (j < out_cols) {
+        unsigned v = u[q];
+        if (!le) v = sizeof(W) == 4 ? __byte_perm(v, 0, 0x0123) : (__byte_perm(v, 0, 0x3201) & 0xffffu);
+        o[j] = j < samples ? (T)segy_value(v, format) : (T)0;
+      }
+    }
+  }
+}
 template <class T>
 __global__ void __launch_bounds__(256) segy_decode_kernel(const unsigned char* __restrict__ rec, long long rows,
                                                           long long record_bytes, int header_bytes, int samples,
                                                           int format, int little, T* __restrict__ out, int out_cols) {
   const int sz = segy_sample_bytes(format);
+  const bool le = little != 0;
+  const bool words = (sz == 4 || sz == 2) && (((uintptr_t)rec | (uintptr_t)header_bytes | (uintptr_t)record_bytes) % sz) == 0;
   for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
     const unsigned char* p = rec + r * record_bytes + header_bytes;
     T* o = out + r * (long long)out_cols;
-    for (int j = threadIdx.x; j < out_cols; j += blockDim.x)
-      o[j] = j < samples ? (T)segy_value(segy_uint(p + (long long)j * sz, sz, little != 0), format) : (T)0;
+    if (words && sz == 4) {
+      segy_words<T>(reinterpret_cast<const unsigned*>(p), o, samples, out_cols, format, le);
+    } else if (words) {
+      segy_words<T>(reinterpret_cast<const unsigned short*>(p), o, samples, out_cols, format, le);
+    } else {
+      for (int j = threadIdx.x; j < out_cols; j += blockDim.x)
+        o[j] = j < samples ? (T)segy_value(segy_uint(p + (long long)j * sz, sz, le), format) : (T)0;
+    }
   }
 }
 // The trace-header keys a meta needs, one thread per row (SEG-Y rev 2 trace

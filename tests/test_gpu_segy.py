@@ -15,12 +15,15 @@ torch = pytest.importorskip("torch")
 pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("built")]
 
 
+@pytest.mark.parametrize("slack", [0, 6])
 @pytest.mark.parametrize("little", [False, True])
 @pytest.mark.parametrize("fmt", [1, 2, 3, 5, 6, 7, 8, 10, 11, 15, 16])
-def test_decode_matches_oracle_bit_for_bit(fmt, little):
+def test_decode_matches_oracle_bit_for_bit(fmt, little, slack):
+    """Records packed back to back (the word-wide reads of 2- and 4-byte
+    samples) and with 6 bytes of slack after each (the byte-wise reads)."""
     sz = segy.SAMPLE_BYTES[fmt]
     rng = np.random.default_rng(fmt * 2 + little)
-    rec = rng.integers(0, 256, (37, 240 + 501 * sz + 6), dtype=np.uint8)  # 6 bytes of slack after each
+    rec = rng.integers(0, 256, (37, 240 + 501 * sz + slack), dtype=np.uint8)
     for T, npdt in ((P.float32, np.float32), (P.float64, np.float64)):
         got = segy.decodeTraces(rec, 501, fmt, T, little, outCols=520).cpu().numpy()
         want = O.segy_decode(rec, 501, fmt, npdt, little, out_cols=520)
