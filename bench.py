@@ -292,6 +292,35 @@ def workloads_leg(peak):
                  "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak}
     del src, dst
     torch.cuda.empty_cache()
+
+    # SEG-Y decode: 20000 records of 3001 IBM-float samples (random words)
+    # to a float32 block, and a viewer's spectrum panel (501-sample windows
+    # of the C2 panel, power-averaged)
+    from processseg_b200 import _abi as A
+    rows, n = 20000, 3001
+    rec = torch.randint(0, 256, (rows, 240 + 4 * n), dtype=torch.uint8, device="cuda")
+    blk = torch.empty(rows, n, dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    t = timed(lambda: A.check(A.lib().psg_segy_decode(rec.data_ptr(), rows, 240 + 4 * n, 240, n, 1, 0, A.F32,
+                                                      blk.data_ptr(), n, st)), 10)
+    nbytes = rec.numel() + blk.numel() * 4
+    out["segy"] = {"workload": "20000 SEG-Y records x 3001 IBM float samples -> f32 block", "us_per_block": t * 1e6,
+                   "gb_per_s": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / peak}
+    del rec, blk
+    g = synth.c2()
+    meta = g.meta()
+    sp = P.initSpectrumPlan(P.float32, 2.0, 501)
+    ws = P.initWorkspace()
+    src = torch.from_numpy(g.data).cuda()
+    amp = [0.0] * sp.bins
+    live, _ = meta.device(3001)
+    avg = torch.empty(sp.bins, dtype=torch.float64, device="cuda")
+    t = timed(lambda: A.check(A.lib().psg_spectrum_average(sp.h, ws.h, src.data_ptr(), 2000, 3001, live.data_ptr(), 2.0,
+                                                           500, 0, 1999, avg.data_ptr(), None, st)), 20)
+    out["spectrum"] = {"workload": "spectrum panel: 2000 traces x 501-sample windows from sample 500, nfft 512",
+                       "us_per_panel": t * 1e6, "msamples_per_s": 2000 * 501 / t / 1e6}
+    del src
+    torch.cuda.empty_cache()
     return out
 
 

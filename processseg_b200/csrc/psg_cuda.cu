@@ -515,19 +515,26 @@ __global__ void __launch_bounds__(256) spectrum_kernel(SpecArgs a) {
   }
 }
 
-// averageAmplitudeInto's last step: sqrt(mean power)·sides per bin over the
-// CTAs' sums (in CTA order), and the rows averaged.
-__global__ void spectrum_finish(const double* __restrict__ acc, const int* __restrict__ used, int ctas, int bins,
-                                int nfft, double* __restrict__ amp, long long* __restrict__ used_out) {
-  long long u = 0;
-  for (int b = 0; b < ctas; b++) u += used[b];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < bins; k += gridDim.x * blockDim.x) {
-    double t = 0;
-    for (int b = 0; b < ctas; b++) t += acc[(size_t)b * bins + k];
-    const double side = (k == 0 || 2 * k == nfft) ? 1.0 : 2.0;
-    amp[k] = u > 0 ? sqrt(t / (double)u) * side : 0.0;
+// averageAmplitudeInto's last step, one CTA per bin: the CTAs' sums of the
+// bin (each thread a fixed set of CTAs, then a fixed reduction tree, so the
+// bits repeat), sqrt(mean power)·sides, and the rows averaged.
+__global__ void __launch_bounds__(256) spectrum_finish(const double* __restrict__ acc, const int* __restrict__ used,
+                                                       int ctas, int bins, int nfft, double* __restrict__ amp,
+                                                       long long* __restrict__ used_out) {
+  __shared__ double red_t[32], red_u[32];
+  const int k = blockIdx.x;
+  double t = 0, u = 0;
+  for (int b = threadIdx.x; b < ctas; b += blockDim.x) {
+    t += acc[(size_t)b * bins + k];
+    u += (double)used[b];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && used_out) *used_out = u;
+  t = block_sum(t, red_t);
+  u = block_sum(u, red_u);
+  if (threadIdx.x == 0) {
+    const double side = (k == 0 || 2 * k == nfft) ? 1.0 : 2.0;
+    amp[k] = u > 0 ? sqrt(t / u) * side : 0.0;
+    if (k == 0 && used_out) *used_out = (long long)u;
+  }
 }
 
 // ============================================================ SEG-Y decode
@@ -2105,7 +2112,7 @@ static void spectrum_launch(const psg_spectrum_plan* p, psg_workspace* ws, const
   const void* k = avg ? (f32 ? (const void*)spectrum_kernel<float, true> : (const void*)spectrum_kernel<double, true>)
                       : (f32 ? (const void*)spectrum_kernel<float, false> : (const void*)spectrum_kernel<double, false>);
   if (nr > 0 || avg) CUDA_OK(cudaLaunchKernel(k, dim3(grid), dim3(256), args, p->smem, stream));
-  if (avg) spectrum_finish<<<(bins + 255) / 256, 256, 0, stream>>>(a.acc, a.used, grid, bins, a.nfft, amp, (long long*)used);
+  if (avg) spectrum_finish<<<bins, 256, 0, stream>>>(a.acc, a.used, grid, bins, a.nfft, amp, (long long*)used);
   CUDA_OK(cudaGetLastError());
 }
 
