@@ -298,15 +298,17 @@ def workloads_leg(peak):
     # of the C2 panel, power-averaged)
     from processseg_b200 import _abi as A
     rows, n = 20000, 3001
-    rec = torch.randint(0, 256, (rows, 240 + 4 * n), dtype=torch.uint8, device="cuda")
-    blk = torch.empty(rows, n, dtype=torch.float32, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
-    t = timed(lambda: A.check(A.lib().psg_segy_decode(rec.data_ptr(), rows, 240 + 4 * n, 240, n, 1, 0, A.F32,
-                                                      blk.data_ptr(), n, st)), 10)
-    nbytes = rec.numel() + blk.numel() * 4
-    out["segy"] = {"workload": "20000 SEG-Y records x 3001 IBM float samples -> f32 block", "us_per_block": t * 1e6,
-                   "gb_per_s": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / peak}
-    del rec, blk
+    blk = torch.empty(rows, n, dtype=torch.float32, device="cuda")
+    out["segy"] = {"workload": "20000 SEG-Y records x 3001 samples (random words) -> f32 block"}
+    for fmt, name, sz in ((1, "ibm", 4), (3, "int16", 2), (5, "ieee32", 4)):
+        rec = torch.randint(0, 256, (rows, 240 + sz * n), dtype=torch.uint8, device="cuda")
+        t = timed(lambda: A.check(A.lib().psg_segy_decode(rec.data_ptr(), rows, 240 + sz * n, 240, n, fmt, 0, A.F32,
+                                                          blk.data_ptr(), n, st)), 10)
+        nbytes = rec.numel() + blk.numel() * 4
+        out["segy"][name] = {"us_per_block": t * 1e6, "gb_per_s": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / peak}
+        del rec
+    del blk
     g = synth.c2()
     meta = g.meta()
     sp = P.initSpectrumPlan(P.float32, 2.0, 501)
