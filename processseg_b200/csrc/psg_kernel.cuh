@@ -134,6 +134,7 @@ __device__ unsigned long long select_kth(const T* X, int n, int k, unsigned* his
         }
         sh[0] = lane * 8 + d;
         sh[1] = kk - (int)below;
+        sh[2] = (int)(c[d] - (unsigned)(kk - (int)below));  // this bucket's keys at rank k and above
       }
     }
     __syncthreads();
@@ -583,11 +584,26 @@ __device__ __forceinline__ Stats step_norm_trace(const DevStep& st, const Stats&
   } else {
     double hr = (double)(n - 1) * st.percentile / 100;
     int k = min((int)floor(hr), n - 1);
-    double lower = bits_value(select_kth(X, n, k, S.m->hist, S.m->sh), (T)0);
+    const unsigned long long lb = select_kth(X, n, k, S.m->hist, S.m->sh);
+    const int same = S.m->sh[2];  // keys equal to the k-th at ranks k and above
+    double lower = bits_value(lb, (T)0);
     if (k + 1 >= n) {
       level = lower;
     } else {
-      double upper = bits_value(select_kth(X, n, k + 1, S.m->hist, S.m->sh), (T)0);
+      // the (k+1)-th: the k-th again when it repeats, else the least key
+      // above it (the largest complement), one pass instead of a selection
+      unsigned long long ub = lb;
+      if (same < 2) {
+        unsigned long long best = 0;
+        for (int i = threadIdx.x; i < n; i += kNT) {
+          const unsigned long long key = abs_bits(X[i]);
+          if (key > lb && ~key > best) best = ~key;
+        }
+        best = block_max_u64(best, S.m->redu[S.flip]);
+        S.flip ^= 1;
+        ub = ~best;
+      }
+      double upper = bits_value(ub, (T)0);
       double f = hr - (double)k;
       level = f == 0 ? lower : lower + f * (upper - lower);
     }
