@@ -428,10 +428,12 @@ def run_ours(args):
         kavg = statistics.mean(kernel_ms)
         alg_bytes = 2 * ROWS * COLS * 4
         achieved = alg_bytes / (kavg * 1e-3) / 1e9
-        traffic = None
+        traffic, insts = None, None
         try:
             with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-                traffic = json.load(f).get("pipeline_kernel_c2_bytes")
+                tj = json.load(f)
+            traffic = tj.get("pipeline_kernel_c2_bytes")
+            insts = tj.get("pipeline_kernel_c2_warp_instructions")
         except Exception:
             pass
         line = {
@@ -444,12 +446,22 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "pipeline_kernel<float>", "algorithmic_bytes": alg_bytes},
+            # the bound that sets the time: warp-instruction issue, with the
+            # launch's instruction count from its ncu capture over the measured
+            # kernel time, against 4 schedulers x SMs x the clock seen
+            "issue": None if not insts else {
+                "achieved": insts / (kavg * 1e-3) / 1e12, "unit": "T warp-instructions/s",
+                "peak": 4 * torch.cuda.get_device_properties(0).multi_processor_count
+                * (clk.summary().get("sm_mhz") or 1965.0) * 1e6 / 1e12,
+                "warp_instructions_per_launch": insts},
             "e2e": {"value": e2e, "unit": "Msamples/s",
                     "h2d_bytes_per_step": ROWS * COLS * 4 + ROWS * 12,
                     "d2h_bytes_per_step": ROWS * COLS * 4},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }
+        if line["issue"]:
+            line["issue"]["frac"] = line["issue"]["achieved"] / line["issue"]["peak"]
         # the one-GPU legs: the served load, the other configurations and the
         # CPU baseline run at N = 1 only (under torchrun the other ranks wait
         # for rank 0 at the final barrier)
