@@ -231,7 +231,9 @@ int64_t psg_workspace_bytes(const psg_workspace* ws);
  * start_ms[r] = the time of column 0 (NaN when unknown). mode 0 is the
  * processing rule (live or unknown status, not failed); mode 1 the
  * correlation rule (not dead, not failed: auxiliary rows are correlated,
- * src/processSEG/vibroseis/correlate.nim:442-443). `t0_ms` may be NULL (NaN). */
+ * src/processSEG/vibroseis/correlate.nim:442-443); mode 2 every row that is
+ * not failed (scaleRows, core/calibrate.nim:575-581). `t0_ms` may be NULL
+ * (NaN). */
 int psg_rows_flatten(const int32_t* status, const int32_t* num_samples,
                      const double* t0_ms, int64_t rows, int32_t first_sample,
                      double dt_ms, const int64_t* failed, int64_t n_failed,
@@ -388,6 +390,18 @@ int psg_spectrum_average(const psg_spectrum_plan* plan, psg_workspace* ws, const
 int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, const void* block,
                            int64_t rows, int32_t cols, const int32_t* live, double dt_ms,
                            int32_t first_col, void* amp, void* phase, void* stream);
+
+/* ------------------------------------------------------- per-row scale */
+/* scaleRows / scaleRowsInto, src/processSEG/core/calibrate.nim:562-612 (the
+ * scaling `calibrate` does with its resolved per-row factors): row r of src
+ * times T(factors_host[r]) over its first live[r] samples into dst (src NULL
+ * or dst: in place), the rest of dst copied from src. live from
+ * psg_rows_flatten mode 2 (every row but the failed ones, to its live
+ * length). A NaN factor fills the row's live samples with NaN; an infinite
+ * one (also in float32) is PSG_EINVAL before any sample changes. Device
+ * blocks; returns when the factors' staging in the workspace is free. */
+int psg_scale_rows(psg_workspace* ws, int32_t dtype, const void* src, void* dst, int64_t rows,
+                   int32_t cols, const int32_t* live, const double* factors_host, void* stream);
 
 /* --------------------------------------------------------------- SEG-Y */
 /* The decode a reader does before the path (parseSEG's trace reading, which

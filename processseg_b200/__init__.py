@@ -19,6 +19,7 @@ from .mute import MuteCurve, lmoMute, tableMute, timeMute
 from .iir import IirPlan, initIirPlan
 from .pool import ProcessPool, newProcessPool
 from . import segy
+from .calibrate import scaleRows, scaleRowsInto
 from .spectrum import (SpectrumPlan, amplitudePhaseInto, circularMeanDeg, dbAbsolute, dbPeak, initSpectrumPlan,
                        removeDelayInto, toDbInto, unwrapPhaseInto)
 

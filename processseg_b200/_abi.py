@@ -156,6 +156,7 @@ def _declare(lib):
         "psg_spectrum_average": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, I64, I64, P, P, P]),
         "psg_spectrum_amplitude": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, P, P, P]),
         "psg_segy_decode": (C.c_int, [P, I64, I64, I32, I32, I32, I32, I32, P, I32, P]),
+        "psg_scale_rows": (C.c_int, [P, I32, P, P, I64, I32, P, P, P]),
         "psg_segy_keys": (C.c_int, [P, I64, I64, I32, P, P, P, P, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),
         "psg_run_part": (C.c_int, [P, P, I32, P, P, I64, I32, P, P, DBL, P, P]),

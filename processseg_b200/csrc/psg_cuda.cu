@@ -648,6 +648,39 @@ __global__ void segy_keys_kernel(const unsigned char* __restrict__ rec, long lon
   }
 }
 
+// ============================================================ per-row scale
+// scaleRows / scaleRowsInto (core/calibrate.nim:562-612): row r times T(k[r])
+// over its first n[r] samples, the rest (and rows with n = 0) copied from
+// src when it is another block. One CTA per row, four samples in flight per
+// thread.
+template <class T>
+__global__ void __launch_bounds__(256) scale_rows_kernel(const T* __restrict__ src, T* __restrict__ dst, long long rows,
+                                                         int cols, const int* __restrict__ live,
+                                                         const double* __restrict__ k) {
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int n = min(max(live[r], 0), cols);
+    const T f = (T)k[r];
+    const T* x = src + r * (long long)cols;
+    T* y = dst + r * (long long)cols;
+    const bool copy = src != dst;
+    if (!copy && n == 0) continue;
+    const int end = copy ? cols : n;
+    for (int j0 = threadIdx.x; j0 < end; j0 += 4 * blockDim.x) {
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int j = j0 + q * (int)blockDim.x;
+        v[q] = j < end ? x[j] : (T)0;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int j = j0 + q * (int)blockDim.x;
+        if (j < end) y[j] = j < n ? v[q] * f : v[q];
+      }
+    }
+  }
+}
+
 // ======================================================== host plumbing
 static int g_sm_count = 0, g_max_smem = 0, g_device = -1;
 
@@ -1394,8 +1427,9 @@ int psg_rows_flatten(const int32_t* status, const int32_t* num_samples, const do
       while (fi < n_failed && failed[fi] < r) fi++;
       if (fi < n_failed && failed[fi] == r) is_failed = true;
       int32_t st = status[r];
-      bool use = mode == 0 ? ((st == PSG_TS_LIVE || st == PSG_TS_UNKNOWN) && !is_failed)
-                           : (st != PSG_TS_DEAD && !is_failed);
+      bool use = mode == 0   ? ((st == PSG_TS_LIVE || st == PSG_TS_UNKNOWN) && !is_failed)
+                 : mode == 1 ? (st != PSG_TS_DEAD && !is_failed)
+                             : !is_failed;
       int64_t n = std::min<int64_t>(std::max<int64_t>((int64_t)num_samples[r] - first_sample, 0), cols);
       live_out[r] = use ? (int32_t)n : 0;
       if (start_ms_out) start_ms_out[r] = (t0_ms ? t0_ms[r] : NAN) + (double)first_sample * dt_ms;
@@ -2133,6 +2167,40 @@ int psg_spectrum_amplitude(const psg_spectrum_plan* plan, psg_workspace* ws, con
   });
 }
 
+
+// ------------------------------------------------------------- per-row scale
+int psg_scale_rows(psg_workspace* ws, int32_t dtype, const void* src, void* dst, int64_t rows, int32_t cols,
+                   const int32_t* live, const double* factors_host, void* stream) {
+  return guarded([&] {
+    if (!ws) throw InvalidArg("a workspace is required");
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if (rows > 0 && (!dst || !live || !factors_host)) throw InvalidArg("null argument");
+    const int64_t esz = dtype == PSG_F32 ? 4 : 8;
+    if (src && src != dst) {
+      uintptr_t s0 = (uintptr_t)src, d0 = (uintptr_t)dst, bytes = (uintptr_t)(rows * cols * esz);
+      if (s0 < d0 + bytes && d0 < s0 + bytes) throw InvalidArg("src and dst overlap without being the same block");
+    }
+    for (int64_t r = 0; r < rows; r++)
+      if (std::isinf(factors_host[r]) || std::isinf(dtype == PSG_F32 ? (double)(float)factors_host[r] : factors_host[r]))
+        throw InvalidArg("row " + std::to_string(r) + " has an infinite factor (" + std::to_string(factors_host[r]) + ")");
+    if (rows == 0) return;
+    ensure_device();
+    sp_grow(ws, align256(rows * 8));
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_OK(cudaMemcpyAsync(ws->sp, factors_host, (size_t)rows * 8, cudaMemcpyHostToDevice, st));
+    const int grid = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
+    if (dtype == PSG_F32)
+      scale_rows_kernel<float><<<grid, 256, 0, st>>>((const float*)(src ? src : dst), (float*)dst, rows, cols, live,
+                                                     (const double*)ws->sp);
+    else
+      scale_rows_kernel<double><<<grid, 256, 0, st>>>((const double*)(src ? src : dst), (double*)dst, rows, cols, live,
+                                                      (const double*)ws->sp);
+    CUDA_OK(cudaGetLastError());
+    // the factors' staging is reused by the next call: it must have landed
+    CUDA_OK(cudaStreamSynchronize(st));
+  });
+}
 // ------------------------------------------------------------- SEG-Y
 int psg_segy_decode(const void* records, int64_t rows, int64_t record_bytes, int32_t header_bytes, int32_t samples,
                     int32_t format, int32_t little_endian, int32_t dtype, void* out, int32_t out_cols, void* stream) {

@@ -411,3 +411,39 @@ def test_process_pool_apply_matches_plan_apply():
     pool.ping()
     with pytest.raises(ValueError):
         P.newProcessPool(0)
+
+
+def test_scale_rows_matches_reference_rules():
+    """scaleRows / scaleRowsInto (calibrate.nim:562-612): each row that is
+    not failed times T(factor) up to its live length whatever its status,
+    NaN factors fill the live part with NaN, the rest copied; an infinite
+    factor is refused before any sample changes."""
+    rng = np.random.default_rng(5)
+    for npdt in (np.float32, np.float64):
+        x = rng.standard_normal((7, 300)).astype(npdt)
+        status = np.array([P.tsLive, P.tsDead, P.tsAux, P.tsLive, P.tsLive, P.tsUnknown, P.tsLive], np.int32)
+        ns = np.array([300, 200, 100, 0, 300, 150, 299], np.int32)
+        meta = P.initChunkMeta(status, ns, 2.0, failed=[4])
+        f = np.array([2.0, -1.5, 0.5, 3.0, 7.0, np.nan, 1e-3])
+        want = x.copy()
+        for r in range(7):
+            if r == 4:
+                continue
+            n = min(ns[r], 300)
+            want[r, :n] = x[r, :n] * npdt(f[r])
+        dst = np.zeros_like(x)
+        P.scaleRowsInto(x, dst, meta, f)
+        assert np.array_equal(dst, want, equal_nan=True)
+        t = torch.from_numpy(x.copy()).cuda()
+        P.scaleRows(t, meta, f)
+        assert np.array_equal(t.cpu().numpy(), want, equal_nan=True)
+        bad = f.copy()
+        bad[2] = np.inf
+        t = torch.from_numpy(x.copy()).cuda()
+        with pytest.raises(ValueError):
+            P.scaleRows(t, meta, bad)
+        assert np.array_equal(t.cpu().numpy(), x)
+        with pytest.raises(ValueError):
+            P.scaleRows(t, meta, f[:3])
+    with pytest.raises(ValueError):  # 1e39 overflows float32
+        P.scaleRows(torch.ones(1, 4, device="cuda"), P.liveMeta(1, 4, 2.0), [1e39])
