@@ -18,11 +18,14 @@ FLOWS = {
     "max": [P.agcOp(200), P.normalizeOp(P.normMax, P.perPanel, target=2.0), P.scaleOp(0.5)],
     "rms": [P.demeanOp(), P.normalizeOp(P.normRms, P.perPanel, target=3.0),
             P.normalizeOp(P.normPercentile, P.perPanel, percentile=90.0)],
+    # mutes read each shard's own rows' offsets and t0s (psg_run_part_keyed)
+    "mutes": [P.muteTopOp(P.lmoMute(2000, t0Ms=40), taperMs=30), P.filterOp(BP),
+              P.normalizeOp(P.normMax, P.perPanel), P.muteBottomOp(P.timeMute(4500), taperMs=50)],
 }
 
 
 def _sub_meta(g, a, b):
-    return P.initChunkMeta(g.status[a:b], g.numSamples[a:b], g.dtMs, g.t0Ms[a:b])
+    return P.initChunkMeta(g.status[a:b], g.numSamples[a:b], g.dtMs, g.t0Ms[a:b], offsets=g.offsets[a:b])
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
@@ -52,7 +55,7 @@ def test_shards_reproduce_the_whole_panel(name, dtype):
             plan.runPart(srcs[i] if part == 0 else None, outs[i], metas[i], part, factor, ws)
     got = torch.cat(outs).cpu().numpy()
     w = want.cpu().numpy()
-    if name in ("pct", "max"):
+    if name in ("pct", "max", "mutes"):
         assert np.array_equal(got, w)
     else:
         # Σx² of the RMS statistic is summed in another order: the factor
