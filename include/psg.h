@@ -268,6 +268,18 @@ int psg_apply_host_keyed(const psg_plan* plan, psg_workspace* ws, const void* sr
                          void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
                          const double* start_ms_host, const psg_keys* keys_host, double dt_ms,
                          void* stream);
+/* psg_apply_host_keyed without waiting: returns once the copies and kernels
+ * are queued on the workspace's streams (after the work already queued on
+ * `stream`); psg_workspace_sync returns when they are done. Consecutive
+ * calls on one workspace overlap (one panel's copies out with the next
+ * one's copies in): the host arrays of a call (src, dst, live, start_ms,
+ * keys) must stay valid and unchanged until psg_workspace_sync, and pinned
+ * memory is what overlaps. */
+int psg_apply_host_async(const psg_plan* plan, psg_workspace* ws, const void* src_host,
+                         void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
+                         const double* start_ms_host, const psg_keys* keys_host, double dt_ms,
+                         void* stream);
+int psg_workspace_sync(psg_workspace* ws);
 
 /* Parts API, src/processSEG/pipeline.nim:643-723: the per-panel factor of a
  * part (NaN: the block is left alone) over the whole block, on the device;

@@ -62,6 +62,10 @@ class Workspace:
     def bytes(self) -> int:
         return A.lib().psg_workspace_bytes(self.h)
 
+    def synchronize(self):
+        """Waits for the host-memory applies queued with ``wait=False``."""
+        A.check(A.lib().psg_workspace_sync(self.h))
+
 
 def initWorkspace() -> Workspace:
     return Workspace()
@@ -151,9 +155,12 @@ class PipelinePlan:
             if not x.flags.c_contiguous:
                 raise ValueError(f"{name} must be C-contiguous (row-major)")
 
-    def apply(self, *args, stream=None):
+    def apply(self, *args, stream=None, wait=True):
         """``apply(b, meta, ws)`` in place, or ``apply(src, dst, meta, ws)``
-        from src into dst (pipeline.nim:736-772)."""
+        from src into dst (pipeline.nim:736-772). With host arrays and
+        ``wait=False`` the call returns once its copies and kernels are
+        queued (``ws.synchronize()`` waits); consecutive calls then overlap,
+        and the arrays must stay valid and unchanged until the wait."""
         if len(args) == 3:
             src, (dst, meta, ws) = None, args
         elif len(args) == 4:
@@ -183,9 +190,9 @@ class PipelinePlan:
             live, start = meta.flat(cols, 0)
             p = lambda a: a.ctypes.data_as(C.c_void_p)
             keys = self._keys(meta, None)
-            A.check(A.lib().psg_apply_host_keyed(self.h, ws.h, None if src is None else p(src), p(dst), rows,
-                                                 cols, p(live), p(start), keys, meta.dtMs,
-                                                 stream if stream is not None else None))
+            fn = A.lib().psg_apply_host_keyed if wait else A.lib().psg_apply_host_async
+            A.check(fn(self.h, ws.h, None if src is None else p(src), p(dst), rows, cols, p(live), p(start), keys,
+                       meta.dtMs, stream if stream is not None else None))
 
     @property
     def needsKeys(self) -> bool:

@@ -447,3 +447,61 @@ def test_scale_rows_matches_reference_rules():
             P.scaleRows(t, meta, f[:3])
     with pytest.raises(ValueError):  # 1e39 overflows float32
         P.scaleRows(torch.ones(1, 4, device="cuda"), P.liveMeta(1, 4, 2.0), [1e39])
+
+
+@pytest.mark.parametrize("flow", [C2_FLOW, C2_FLOW + [P.normalizeOp(P.normRms, P.perPanel)],
+                                  [P.muteTopOp(P.timeMute(300), taperMs=20)] + C2_FLOW],
+                         ids=["chunked", "whole-block", "keys"])
+def test_async_host_applies_overlap_and_match(flow):
+    """apply(..., wait=False) on host arrays: six panels queued back to back
+    (their copies overlap), interleaved with a waiting call, each equal to
+    the waiting apply of the same panel."""
+    plan = P.initPipeline(flow).compile(P.float32, 2.0, 3001)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=300, cols=3001)
+    gs = [synch for synch in (synth.c2(seed=40 + i, rows=300) for i in range(6))]
+    want = []
+    for g in gs:
+        d = np.zeros_like(g.data)
+        plan.apply(g.data, d, g.meta(), ws)
+        want.append(d)
+    srcs = [torch.from_numpy(g.data).pin_memory().numpy() for g in gs]
+    dsts = [torch.zeros(300, 3001).pin_memory().numpy() for _ in gs]
+    metas = [g.meta() for g in gs]
+    for i in range(6):
+        plan.apply(srcs[i], dsts[i], metas[i], ws, wait=False)
+        if i == 2:
+            extra = np.zeros_like(gs[0].data)
+            plan.apply(gs[0].data, extra, metas[0], ws)
+            assert np.array_equal(extra, want[0])
+    ws.synchronize()
+    for i in range(6):
+        assert np.array_equal(dsts[i], want[i]), i
+
+
+def test_async_host_applies_across_layouts(monkeypatch):
+    """Queued host applies whose staging is laid out differently from the
+    call before (another width, a whole block, a plan with its work areas in
+    global memory, which keeps to one lane) give the waiting results."""
+    monkeypatch.setenv("PSG_WIDE", "1")
+    wide = P.initPipeline(C2_FLOW).compile(P.float32, 2.0, 3001)
+    monkeypatch.delenv("PSG_WIDE")
+    plans = [P.initPipeline(C2_FLOW).compile(P.float32, 2.0, 3001), wide,
+             P.initPipeline(C2_FLOW).compile(P.float32, 2.0, 1500)]
+    ws = P.initWorkspace()
+    cases = []
+    for i, (plan, rows, cols) in enumerate([(0, 900, 3001), (2, 1200, 1500), (1, 900, 3001), (0, 40, 3001),
+                                            (2, 1500, 1500), (0, 900, 3001)]):
+        g = synth.shot_gather(rows, cols, 2.0, 70 + i, np.float32, live_range=(cols // 2, cols), sine_hz=50.0,
+                              workload="layouts")
+        ws.reserve(plans[plan], rows=rows, cols=cols)
+        want = np.zeros_like(g.data)
+        plans[plan].apply(g.data, want, g.meta(), ws)
+        src = torch.from_numpy(g.data).pin_memory()
+        dst = torch.zeros_like(src).pin_memory()
+        cases.append((plans[plan], src, dst, g.meta(), want))
+    for plan, src, dst, meta, _ in cases:
+        plan.apply(src.numpy(), dst.numpy(), meta, ws, wait=False)
+    ws.synchronize()
+    for i, (_, _, dst, _, want) in enumerate(cases):
+        assert np.array_equal(dst.numpy(), want), i
