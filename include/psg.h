@@ -31,7 +31,8 @@ typedef enum psg_status {
   PSG_ENOMEM = 3,     /* device memory or admission refused                  */
   PSG_ETIMEOUT = 4,   /* a bounded wait ran out                              */
   PSG_ECUDA = 5,      /* a CUDA call failed (message has the CUDA error)     */
-  PSG_ENODEV = 6      /* no usable sm_100 device                             */
+  PSG_ENODEV = 6,     /* no usable sm_100 device                             */
+  PSG_ECANCELED = 7   /* a served request was cancelled before it started    */
 } psg_status;
 
 /* ------------------------------------------------------------- enumerations
@@ -512,8 +513,17 @@ void psg_server_destroy(psg_server* server);
 int psg_submit(psg_server* server, const psg_plan* plan, const void* src_host, void* dst_host,
                int64_t rows, int32_t cols, const int32_t* live_host,
                const double* start_ms_host, double dt_ms, uint64_t* ticket);
-/* Waits for a request (PSG_ETIMEOUT after timeout_ms) and releases its ticket. */
+/* Waits for a request (PSG_ETIMEOUT after timeout_ms) and releases its ticket;
+ * PSG_ECANCELED for a request cancelled before it started. */
 int psg_wait(psg_server* server, uint64_t ticket, double timeout_ms);
+/* *done = 1 when the request has finished (or was cancelled), without
+ * waiting or releasing its ticket. */
+int psg_poll(psg_server* server, uint64_t ticket, int32_t* done);
+/* Cancels a request that has not started (not yet admitted to the arena):
+ * PSG_OK, and psg_wait then returns PSG_ECANCELED; its buffers are not
+ * touched. PSG_EINVAL for an unknown ticket or a request already started
+ * (it runs to completion: wait for it). */
+int psg_cancel(psg_server* server, uint64_t ticket);
 /* out[8]: completed, samples, launches, requests per launch, p50 and p99
  * latency (s, submit to completion), Msamples/s, refused; reset != 0 clears. */
 int psg_server_stats(psg_server* server, double* out, int reset);

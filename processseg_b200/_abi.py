@@ -19,7 +19,7 @@ MAX_KNOTS = 64
 MAX_MUTE_KNOTS = 64
 
 # psg_status
-OK, EINVAL, EWORKSPACE, ENOMEM, ETIMEOUT, ECUDA, ENODEV = range(7)
+OK, EINVAL, EWORKSPACE, ENOMEM, ETIMEOUT, ECUDA, ENODEV, ECANCELED = range(8)
 # psg_dtype
 F32, F64 = 0, 1
 # psg_op_kind (OpKind)
@@ -158,6 +158,8 @@ def _declare(lib):
         "psg_spectrum_average": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, I64, I64, P, P, P]),
         "psg_spectrum_amplitude": (C.c_int, [P, P, P, I64, I32, P, DBL, I32, P, P, P]),
         "psg_segy_decode": (C.c_int, [P, I64, I64, I32, I32, I32, I32, I32, P, I32, P]),
+        "psg_poll": (C.c_int, [P, C.c_uint64, C.POINTER(I32)]),
+        "psg_cancel": (C.c_int, [P, C.c_uint64]),
         "psg_scale_rows": (C.c_int, [P, I32, P, P, I64, I32, P, P, P]),
         "psg_segy_keys": (C.c_int, [P, I64, I64, I32, P, P, P, P, P, P]),
         "psg_panel_factor": (C.c_int, [P, P, I32, P, I64, I32, P, P, P]),

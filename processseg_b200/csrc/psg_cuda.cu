@@ -2803,8 +2803,48 @@ int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
   int st = r->status;
   S->by_ticket.erase(it);
   delete r;
-  if (st != PSG_OK) t_err = S->error.empty() ? "a CUDA call of the request loop failed" : S->error;
+  if (st == PSG_ECANCELED) t_err = "the request was cancelled";
+  else if (st != PSG_OK) t_err = S->error.empty() ? "a CUDA call of the request loop failed" : S->error;
   return st;
+}
+
+int psg_poll(psg_server* S, uint64_t ticket, int32_t* done) {
+  if (!S || !done) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->by_ticket.find(ticket);
+  if (it == S->by_ticket.end()) {
+    t_err = "unknown ticket " + std::to_string(ticket);
+    return PSG_EINVAL;
+  }
+  *done = it->second->done ? 1 : 0;
+  return PSG_OK;
+}
+
+int psg_cancel(psg_server* S, uint64_t ticket) {
+  if (!S) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::lock_guard<std::mutex> g(S->mu);
+  auto it = S->by_ticket.find(ticket);
+  if (it == S->by_ticket.end()) {
+    t_err = "unknown ticket " + std::to_string(ticket);
+    return PSG_EINVAL;
+  }
+  Req* r = it->second;
+  auto q = std::find(S->pending.begin(), S->pending.end(), r);
+  if (q == S->pending.end()) {
+    t_err = r->done ? "the request has finished" : "the request has started: wait for it";
+    return PSG_EINVAL;
+  }
+  S->pending.erase(q);
+  r->done = true;
+  r->status = PSG_ECANCELED;
+  S->cv_done.notify_all();
+  return PSG_OK;
 }
 
 // {completed, samples, launches, mean requests per launch, p50 s, p99 s,

@@ -20,6 +20,10 @@ from .meta import ChunkMeta
 from .plan import PipelinePlan
 
 
+class CancelledError(Exception):
+    """A served request cancelled before it started."""
+
+
 class Server:
     def __init__(self, device: int = 0, arena_bytes: int = 2 << 30):
         h = C.c_void_p()
@@ -55,10 +59,32 @@ class Server:
         return t.value
 
     def wait(self, ticket: int, timeout_ms: float = 10000.0):
+        """Waits for a request; ``TimeoutError`` after ``timeout_ms``,
+        ``CancelledError`` for a request cancelled before it started."""
         st = A.lib().psg_wait(self.h, ticket, timeout_ms)
         if st != A.ETIMEOUT:
             self._keep.pop(ticket, None)
+        if st == A.ECANCELED:
+            raise CancelledError(A.lib().psg_last_error().decode("utf-8", "replace"))
         A.check(st)
+
+    def poll(self, ticket: int) -> bool:
+        """True when the request has finished (or was cancelled)."""
+        done = C.c_int32()
+        A.check(A.lib().psg_poll(self.h, ticket, C.byref(done)))
+        return bool(done.value)
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a request that has not started: True; False when it has
+        started or finished (wait for it). ``ValueError`` for an unknown
+        ticket."""
+        st = A.lib().psg_cancel(self.h, ticket)
+        if st == A.OK:
+            return True
+        msg = A.lib().psg_last_error().decode("utf-8", "replace")
+        if "unknown ticket" in msg:
+            raise ValueError(msg)
+        return False
 
     def stats(self, reset: bool = False) -> dict:
         out = (C.c_double * 8)()

@@ -78,3 +78,39 @@ def test_admission_and_bounded_waits():
         with P.Server(arena_bytes=4 << 20) as srv:
             x = np.ones((10, 1000))
             srv.submit(plan64, x, np.zeros_like(x), P.liveMeta(10, 1000, 2.0))
+
+
+def test_cancel_and_poll():
+    """psg_cancel / psg_poll: requests still queued behind a small arena are
+    cancelled (their buffers untouched, wait raises CancelledError); the
+    rest complete with the plain apply's result; a started request is not
+    cancelled."""
+    from processseg_b200.server import CancelledError
+    flow = synth.viewer_flows()[0]
+    plan = P.initPipeline(flow).compile(P.float32, 2.0, 1000)
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=2000, cols=1000)
+    rng = np.random.default_rng(3)
+    srcs = [rng.standard_normal((2000, 1000)).astype(np.float32) for _ in range(12)]
+    meta = P.liveMeta(2000, 1000, 2.0)
+    # an arena of one 8 MB request at a time: the later ones stay queued
+    with P.Server(arena_bytes=9 << 20) as srv:
+        dsts = [np.full((2000, 1000), 7.0, np.float32) for _ in srcs]
+        tickets = [srv.submit(plan, s, d, meta) for s, d in zip(srcs, dsts)]
+        cancelled = {t for t in tickets[-6:] if srv.cancel(t)}
+        assert cancelled, "a one-request arena leaves requests queued"
+        for i, t in enumerate(tickets):
+            if t in cancelled:
+                assert srv.poll(t)
+                with pytest.raises(CancelledError):
+                    srv.wait(t, 10000)
+                assert np.all(dsts[i] == 7.0)
+            else:
+                srv.wait(t, 10000)
+                want = np.zeros_like(srcs[i])
+                plan.apply(srcs[i], want, meta, ws)
+                assert np.array_equal(dsts[i], want)
+        t = srv.submit(plan, srcs[0], dsts[0], meta)
+        srv.wait(t, 10000)
+        with pytest.raises(ValueError, match="unknown ticket"):
+            srv.cancel(t)
