@@ -332,7 +332,8 @@ int psg_panel_factor_from(const psg_plan* plan, psg_workspace* ws, int32_t part,
  * device. hz and gain are host arrays of n_hz doubles. Compiles a plan and
  * allocates the impulse row on every call; ws is grown to the plan when it
  * does not already hold it. PSG_EINVAL when the flow does not compile.
- * Synchronous (the legacy default stream). */
+ * Synchronous, on a stream of its own (after the workspace's queued host
+ * applies). */
 int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double dt_ms,
                          int32_t samples, const double* hz, int32_t n_hz, double* gain,
                          psg_workspace* ws);

@@ -1814,6 +1814,18 @@ __global__ void __launch_bounds__(256) response_moduli_kernel(const T* __restric
 template <class T>
 static void applied_response(const psg_plan* p, psg_workspace* ws, int32_t samples, const double* hz, int32_t n_hz,
                              double* gain) {
+  // the workspace's queued host applies finish first; then a stream of its
+  // own, so that nothing else on the device waits for this call
+  if (ws->lanes_ready)
+    for (int i = 0; i < psg_workspace::kLanes; i++) CUDA_OK(cudaStreamSynchronize(ws->lane[i]));
+  struct Stream {
+    cudaStream_t s = nullptr;
+    ~Stream() {
+      if (s) cudaStreamDestroy(s);
+    }
+  } own;
+  CUDA_OK(cudaStreamCreateWithFlags(&own.s, cudaStreamNonBlocking));
+  cudaStream_t st = own.s;
   const size_t xb = align256((int64_t)samples * (int64_t)sizeof(T));
   DeviceBuf buf;
   CUDA_OK(cudaMalloc(&buf.p, xb + 256 + 256 + align256((int64_t)n_hz * 16)));
@@ -1826,21 +1838,21 @@ static void applied_response(const psg_plan* p, psg_workspace* ws, int32_t sampl
   // a unit impulse at samples / 2 on one live row at t0 = 0 and offset 0
   const T one = (T)1;
   const double zeros[3] = {0, 0, 0};
-  CUDA_OK(cudaMemset(x, 0, (size_t)samples * sizeof(T)));
-  CUDA_OK(cudaMemcpy(x + samples / 2, &one, sizeof(T), cudaMemcpyHostToDevice));
-  CUDA_OK(cudaMemcpy(live, &samples, sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_OK(cudaMemcpy(start, zeros, sizeof(zeros), cudaMemcpyHostToDevice));
-  if (n_hz > 0) CUDA_OK(cudaMemcpy(dhz, hz, (size_t)n_hz * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemsetAsync(x, 0, (size_t)samples * sizeof(T), st));
+  CUDA_OK(cudaMemcpyAsync(x + samples / 2, &one, sizeof(T), cudaMemcpyHostToDevice, st));
+  CUDA_OK(cudaMemcpyAsync(live, &samples, sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_OK(cudaMemcpyAsync(start, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  if (n_hz > 0) CUDA_OK(cudaMemcpyAsync(dhz, hz, (size_t)n_hz * sizeof(double), cudaMemcpyHostToDevice, st));
   const psg_keys keys{start + 2, start + 1, 0, 0};
   for (int part = 0; part < (int)p->host.parts.size(); part++)
-    launch_part<T>(p, ws, part, nullptr, x, 1, samples, live, start, 0, &keys, p->host.dt_ms);
+    launch_part<T>(p, ws, part, nullptr, x, 1, samples, live, start, st, &keys, p->host.dt_ms);
   if (n_hz > 0) {
     const int grid = (int)std::min<int64_t>(((int64_t)n_hz + 7) / 8, (int64_t)g_sm_count * 8);
-    response_moduli_kernel<T><<<grid, 256>>>(x, samples, dhz, n_hz, p->host.dt_ms / 1000, dg);
+    response_moduli_kernel<T><<<grid, 256, 0, st>>>(x, samples, dhz, n_hz, p->host.dt_ms / 1000, dg);
     CUDA_OK(cudaGetLastError());
-    CUDA_OK(cudaMemcpy(gain, dg, (size_t)n_hz * sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpyAsync(gain, dg, (size_t)n_hz * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
-  CUDA_OK(cudaDeviceSynchronize());
+  CUDA_OK(cudaStreamSynchronize(st));
 }
 
 extern "C" {
