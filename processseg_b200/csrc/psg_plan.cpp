@@ -552,7 +552,8 @@ StepHost compile_op(const psg_op& op, int dtype, double dt_ms, int64_t samples, 
       break;
     case PSG_OP_CALIBRATE:
     case PSG_OP_UNCALIBRATE:
-      throw InvalidArg("this op is not part of the GPU hot path yet");
+      throw InvalidArg("calibration resolves its factors from the SEG-D keys and file scales of a reader, "
+                       "which this library does not have: apply resolved per-row factors with scaleRows");
     default:
       throw InvalidArg("unknown op kind " + std::to_string(op.kind));
   }
