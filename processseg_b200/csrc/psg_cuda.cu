@@ -987,18 +987,26 @@ static M2 mul(const M2& x, const M2& y) {
 }  // namespace hdd
 
 // The IIR scan table of a section: for each chunk length L = 1 .. lmax the
-// powers (M^L)^(2^i), i = 0 .. 5, of its state map M = [[−a1, 1], [−a2, 0]],
-// as 2×2 double-double matrices (48 doubles per L).
+// powers P^k, k = 1 .. 32, then P^64 and P^128, of P = M^L,
+// M = [[−a1, 1], [−a2, 0]] its state map, as 2×2 double-double matrices
+// (kIirTab doubles per L).
 static void iir_scan_table(const Biquad& q, int lmax, std::vector<double>& out) {
   const hdd::M2 m{hdd::DD{-q.a1, 0}, hdd::DD{1, 0}, hdd::DD{-q.a2, 0}, hdd::DD{0, 0}};
   hdd::M2 pl{hdd::DD{1, 0}, hdd::DD{0, 0}, hdd::DD{0, 0}, hdd::DD{1, 0}};
+  auto put = [&](const hdd::M2& w) {
+    out.insert(out.end(), {w.a.hi, w.a.lo, w.b.hi, w.b.lo, w.c.hi, w.c.lo, w.d.hi, w.d.lo});
+  };
   for (int L = 1; L <= lmax; L++) {
     pl = hdd::mul(pl, m);
-    hdd::M2 w = pl;
-    for (int i = 0; i < 6; i++) {
-      out.insert(out.end(), {w.a.hi, w.a.lo, w.b.hi, w.b.lo, w.c.hi, w.c.lo, w.d.hi, w.d.lo});
-      w = hdd::mul(w, w);
+    hdd::M2 w = pl, p32 = pl;
+    for (int k = 1; k <= 32; k++) {
+      put(w);
+      p32 = w;
+      w = hdd::mul(w, pl);
     }
+    const hdd::M2 p64 = hdd::mul(p32, p32);
+    put(p64);
+    put(hdd::mul(p64, p64));
   }
 }
 
@@ -1078,6 +1086,7 @@ template <class T> static void build_device_steps(psg_plan* p) {
       if (!sec.empty()) {
         d.sec = (const double*)upload(p->keep, sec);
         d.pw = (const double*)upload(p->keep, pw);
+        static_assert(kIirTab == 34 * 8, "the IIR scan table holds P^1 .. P^32, P^64, P^128 per chunk length");
       }
       work = std::max<int64_t>(work, (f.lead + p->host.samples + f.tail) * 8);
     }

@@ -50,8 +50,8 @@ struct DevStep {
   int n_sec, iir_zero, lead, tail;
   double dc_slope;
   const double* sec;
-  // per section and chunk length L = 1 .. pw_len: (M^L)^(2^i), i = 0 .. 5,
-  // 2×2 in double-double (48 doubles)
+  // per section and chunk length L = 1 .. pw_len: (M^L)^k, k = 1 .. 32,
+  // 2×2 in double-double (kIirTab doubles)
   const double* pw;
   int pw_len, _pad2;
 };
@@ -717,6 +717,10 @@ __device__ __forceinline__ DD dd_shfl_up(DD v, int d) {
   return DD{__shfl_up_sync(0xffffffffu, v.hi, d), __shfl_up_sync(0xffffffffu, v.lo, d)};
 }
 
+// Doubles per chunk length in a section's IIR scan table: P^k, k = 1 .. 32,
+// then P^64 and P^128, 2×2 in double-double.
+constexpr int kIirTab = 34 * 8;
+
 // One pass of one section (filter/iir.nim:319-351) over the m padded samples
 // of B (float64, in place), forwards or backwards, from rest or from the
 // steady state of its first input sample. A section in transposed direct
@@ -727,18 +731,20 @@ __device__ __forceinline__ DD dd_shfl_up(DD v, int d) {
 // pass's start state) to the chunk's end state Z_t, (2) a scan over the
 // threads gives each chunk's true start state, E_t = P·E_{t−1} + Z_t with
 // P = M^L the state map over L zero samples (warp scans with the powers
-// P^(2^i), read from the host's double-double table `pw` for this L, then
-// across the warps), and (3) each thread reruns its chunk from its start
+// P^(2^i); then the eight warps' totals scanned by eight lanes with P^32,
+// P^64 and P^128; every power read from the host's double-double table
+// `pw` for this L), and (3) each thread reruns its chunk from its start
 // state and writes the outputs. A start state below 1e-250 is set to 0, so a
 // decay after the input stops ends in exact zeros (filter/iir.nim:311-317).
 __device__ __forceinline__ void iir_pass(double* B, int m, const double* c, const double* pw, bool steady,
                                          bool backward) {
   __shared__ double w_end[kNT / 32][4];
+  __shared__ double w_carry[kNT / 32][4];  // the true end state of the chunk before each warp's first
   const double b0 = c[0], b1 = c[1], b2 = c[2], a1 = c[3], a2 = c[4], g = c[5];
   const int L = (m + kNT - 1) / kNT;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int j0 = min(t * L, m), j1 = min(j0 + L, m);
-  const double* tab = pw + (size_t)(L - 1) * 48;  // P^(2^i), i = 0 .. 5, for this L
+  const double* tab = pw + (size_t)(L - 1) * kIirTab;  // P^k at tab + 8·(k − 1)
   auto at = [&](int j) -> double& { return B[backward ? m - 1 - j : j]; };
   __syncthreads();  // the previous pass's outputs
   double i1 = 0, i2 = 0;  // the pass's start state
@@ -761,7 +767,7 @@ __device__ __forceinline__ void iir_pass(double* B, int m, const double* c, cons
   DD e1{z1, 0}, e2{z2, 0};
   for (int i = 0; i < 5; i++) {
     const DD u1 = dd_shfl_up(e1, 1 << i), u2 = dd_shfl_up(e2, 1 << i);
-    if (lane >= (1 << i)) m2_madd(m2_load(tab + 8 * i), u1, u2, e1, e2);
+    if (lane >= (1 << i)) m2_madd(m2_load(tab + 8 * ((1 << i) - 1)), u1, u2, e1, e2);
   }
   if (lane == 31) {
     w_end[warp][0] = e1.hi;
@@ -770,22 +776,34 @@ __device__ __forceinline__ void iir_pass(double* B, int m, const double* c, cons
     w_end[warp][3] = e2.lo;
   }
   __syncthreads();
+  // the warps' carries: an inclusive scan of the warp totals with P^32
+  // between neighbours (warp 0, eight lanes, three doubling steps)
+  constexpr int kW = kNT / 32;
+  static_assert(kW == 8, "the carry scan takes three steps over eight warps");
+  if (warp == 0) {
+    const int l = lane < kW ? lane : kW - 1;
+    DD v1{w_end[l][0], w_end[l][1]}, v2{w_end[l][2], w_end[l][3]};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int d = 1 << i;
+      const DD u1 = dd_shfl_up(v1, d), u2 = dd_shfl_up(v2, d);
+      if (lane >= d && lane < kW) m2_madd(m2_load(tab + 8 * (31 + i)), u1, u2, v1, v2);  // P^(32·d)
+    }
+    if (lane + 1 < kW) {
+      w_carry[lane + 1][0] = v1.hi;
+      w_carry[lane + 1][1] = v1.lo;
+      w_carry[lane + 1][2] = v2.hi;
+      w_carry[lane + 1][3] = v2.lo;
+    }
+  }
+  __syncthreads();
   // the carry into this warp: the true end state of the previous warp's last chunk
   DD c1{0, 0}, c2{0, 0};
   if (warp > 0) {
-    const M2 Q32 = m2_load(tab + 40);
-    for (int v = 0; v < warp; v++) {
-      DD n1{w_end[v][0], w_end[v][1]}, n2{w_end[v][2], w_end[v][3]};
-      m2_madd(Q32, c1, c2, n1, n2);
-      c1 = n1;
-      c2 = n2;
-    }
+    c1 = DD{w_carry[warp][0], w_carry[warp][1]};
+    c2 = DD{w_carry[warp][2], w_carry[warp][3]};
     // E_t = e_t + P^(lane+1)·carry
-    const int k = lane + 1;
-    M2 R = m2_load(tab + 8 * (31 - __clz(k)));
-    for (int i = 0; i < 31 - __clz(k); i++)
-      if ((k >> i) & 1) R = m2_mul(R, m2_load(tab + 8 * i));
-    m2_madd(R, c1, c2, e1, e2);
+    m2_madd(m2_load(tab + 8 * lane), c1, c2, e1, e2);
   }
   // this chunk starts from the previous chunk's end
   const DD p1 = dd_shfl_up(e1, 1), p2 = dd_shfl_up(e2, 1);
@@ -830,10 +848,11 @@ __device__ __noinline__ Stats step_iir(const DevStep& st, const Stats& in, T* X,
     for (int k = threadIdx.x + 1; k <= tail; k += kNT) B[p + n - 1 + k] = 0;
   }
   const int lmax = st.pw_len;
-  for (int i = 0; i < st.n_sec; i++) iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * 48, st.reflect, false);
+  for (int i = 0; i < st.n_sec; i++)
+    iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * kIirTab, st.reflect, false);
   if (st.iir_zero)
     for (int i = 0; i < st.n_sec; i++)
-      iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * 48, st.reflect, true);
+      iir_pass(B, m, st.sec + 6 * i, st.pw + (size_t)i * lmax * kIirTab, st.reflect, true);
   __syncthreads();
   const double ga = __dsub_rn(__dmul_rn(a, st.dc_gain), __dmul_rn(b, st.dc_slope)), gb = __dmul_rn(b, st.dc_gain);
   return map_trace<NEED_K>(X, n, st.need_next, S,
