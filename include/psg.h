@@ -441,13 +441,35 @@ int psg_segy_keys(const void* records, int64_t rows, int64_t record_bytes, int32
                   double* t0_ms, void* stream);
 
 /* ----------------------------------------------------------- vibroseis */
-/* linearSweep + sweepInto + generatePilot (taper shapes tpLinear, tpCosine,
- * tpCos2, tpHamming, tpBlackman), src/processSEG/vibroseis/sweep.nim:185-342,
- * taper.nim:125-179, pilot.nim:115-119. Phase in float64. `out` is host
- * memory of *n_out values of dtype (NULL: just report the length). */
+/* Sweep taper shapes (TaperShape, src/processSEG/vibroseis/taper.nim:46-58):
+ * 0 linear, 1 cosine, 2 cos², 3 Hamming, 4 Blackman, 5 Blackman–Harris,
+ * 6 Kaiser (param β, default 6), 7 Gaussian (σ in ramp lengths, default 0.4),
+ * 8 power (exponent p, default 2). A NaN param takes the shape's default. */
+enum psg_taper_shape {
+  PSG_TP_LINEAR = 0, PSG_TP_COSINE = 1, PSG_TP_COS2 = 2, PSG_TP_HAMMING = 3,
+  PSG_TP_BLACKMAN = 4, PSG_TP_BLACKMAN_HARRIS = 5, PSG_TP_KAISER = 6,
+  PSG_TP_GAUSSIAN = 7, PSG_TP_POWER = 8
+};
+/* taperWeight, src/processSEG/vibroseis/taper.nim:125-145: the ramp w(x) of
+ * `shape` at x clamped to [0, 1]. The parameter is not validated, as in the
+ * reference; an unknown shape is PSG_EINVAL. */
+int psg_taper_weight(int32_t shape, double x, double param, double* out);
+/* applyTaper, src/processSEG/vibroseis/taper.nim:160-179 (with validate and
+ * checkFits, :79-158): ramps of start_ms and end_ms (0 or NaN: none) applied
+ * in place to n host samples of dtype whose sample j is at j·dt_ms; each
+ * product rounds to dtype. PSG_EINVAL, with nothing written, for a dt_ms
+ * that is not finite and positive, a bad length or parameter, or ramps
+ * longer than n·dt_ms together. */
+int psg_apply_taper(int32_t dtype, void* x, int64_t n, double dt_ms, double start_ms,
+                    double end_ms, int32_t shape, double param);
+/* linearSweep + sweepInto + generatePilot, src/processSEG/vibroseis/
+ * sweep.nim:126-342, taper.nim:125-179, pilot.nim:115-119: phase in float64,
+ * each sample rounded to dtype, then the ramps of taper_shape / taper_param
+ * (as psg_apply_taper). `out` is host memory of *n_out values of dtype
+ * (NULL: just report the length). */
 int psg_linear_sweep(double f1_hz, double f2_hz, double length_ms, double dt_ms,
                      double taper_start_ms, double taper_end_ms, int32_t taper_shape,
-                     double start_phase_deg, double amplitude,
+                     double taper_param, double start_phase_deg, double amplitude,
                      double max_nyquist_fraction, int32_t dtype, void* out,
                      int64_t* n_out);
 /* initCorrelationPlan, src/processSEG/vibroseis/correlate.nim:82-160: the

@@ -12,6 +12,7 @@ tests instead (tests/test_oracle_pins.py).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -68,8 +69,9 @@ def lib():
             "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
             "orc_panel_stats": (C.c_int, [C.c_int, P, I64, I64, P, DBL, P]),
             "orc_percentile_abs": (C.c_int, [C.c_int, P, I64, DBL, C.POINTER(DBL)]),
-            "orc_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, C.c_int, DBL, DBL, C.c_int,
-                                           P, C.POINTER(I64)]),
+            "orc_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, C.c_int, DBL, DBL, DBL,
+                                           C.c_int, P, C.POINTER(I64)]),
+            "orc_taper_weight": (C.c_int, [C.c_int, DBL, DBL, C.POINTER(DBL)]),
             "orc_correlate": (C.c_int, [P, I64, DBL, DBL, C.c_int, DBL, I64, I64, C.c_int, DBL,
                                         C.c_int, P, P, I64, I64, P, C.POINTER(I64),
                                         C.POINTER(DBL)]),
@@ -369,15 +371,21 @@ def percentile_abs(x, p):
 
 
 def linear_sweep(f1, f2, lengthMs, dtMs, taperStart=0.0, taperEnd=0.0, shape=2, phaseDeg=0.0,
-                 amplitude=1.0, dtype=np.float64):
+                 amplitude=1.0, dtype=np.float64, param=math.nan):
     n = C.c_int64()
     dt = A.F32 if dtype == np.float32 else A.F64
-    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, phaseDeg,
+    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, param, phaseDeg,
                                   amplitude, dt, None, C.byref(n)))
     x = np.zeros(n.value, dtype)
-    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, phaseDeg,
+    _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, param, phaseDeg,
                                   amplitude, dt, _ptr(x), C.byref(n)))
     return x
+
+
+def taper_weight(shape, x, param=math.nan):
+    out = C.c_double()
+    _check(lib().orc_taper_weight(shape, x, param, C.byref(out)))
+    return out.value
 
 
 def correlate(pilot, pilotDt, pilotT0, src, live, dtMs, recordSamples, outSamples=0,

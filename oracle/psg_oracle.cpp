@@ -1630,8 +1630,21 @@ void applyPool(Pool* pool, const Plan<T>& plan, const T* src, T* dst, int64_t ro
 }
 
 // ---------------------------------------------------------- correlation --
-// vibroseis/taper.nim:125-145 (the shapes without a special function)
+// vibroseis/kaiser.nim:4-14: the power series of I0, stopped once a term
+// falls under 1e-17 of the running sum.
+double besselI0(double x) {
+  double term = 1.0, result = 1.0, q = x * x / 4;
+  for (int k = 1; k <= 500; k++) {
+    term *= q / (double)(k * k);
+    result += term;
+    if (term < result * 1e-17) break;
+  }
+  return result;
+}
+// vibroseis/taper.nim:69-74 (defaultParam), :125-145 (taperWeight)
+double taperDefault(int shape) { return shape == 6 ? 6.0 : shape == 7 ? 0.4 : shape == 8 ? 2.0 : NaN; }
 double taperWeight(int shape, double x, double param) {
+  double p = std::isnan(param) ? taperDefault(shape) : param;
   x = std::clamp(x, 0.0, 1.0);
   switch (shape) {
     case 0: return x;
@@ -1640,16 +1653,17 @@ double taperWeight(int shape, double x, double param) {
     case 3: return 0.54 - 0.46 * std::cos(PI * x);
     case 4: return 0.42 - 0.5 * std::cos(PI * x) + 0.08 * std::cos(2 * PI * x);
     case 5: return 0.35875 - 0.48829 * std::cos(PI * x) + 0.14128 * std::cos(2 * PI * x) - 0.01168 * std::cos(3 * PI * x);
-    case 7: { double p = std::isnan(param) ? 0.4 : param; double u = (1 - x) / p; return std::exp(-0.5 * u * u); }
-    case 8: { double p = std::isnan(param) ? 2.0 : param; return std::pow(x, p); }
-    default: throw ValueError("this taper shape is not supported by the oracle");
+    case 6: { double u = 1 - x; return besselI0(p * std::sqrt(std::max(0.0, 1 - u * u))) / besselI0(p); }
+    case 7: { double u = (1 - x) / p; return std::exp(-0.5 * u * u); }
+    case 8: return std::pow(x, p);
+    default: throw ValueError("unknown taper shape");
   }
 }
 // vibroseis/sweep.nim:292-301 (linear law), :331-342 (sweepInto),
 // taper.nim:160-179 (applyTaper)
 template <class T>
 std::vector<T> linearSweep(double f1, double f2, double lengthMs, double dtMs, double tStart, double tEnd, int shape,
-                           double phaseDeg, double amplitude) {
+                           double param, double phaseDeg, double amplitude) {
   double steps = lengthMs / dtMs;
   double r = std::round(steps);
   int64_t n = std::fabs(steps - r) <= 1e-6 ? (int64_t)r : (int64_t)std::floor(steps);
@@ -1665,10 +1679,10 @@ std::vector<T> linearSweep(double f1, double f2, double lengthMs, double dtMs, d
   double s = std::isnan(tStart) ? 0.0 : tStart, e = std::isnan(tEnd) ? 0.0 : tEnd;
   if (s > 0)
     for (int64_t j = 0; j < n && (double)j * dtMs < s; j++)
-      x[j] = (T)((double)x[j] * taperWeight(shape, (double)j * dtMs / s, NaN));
+      x[j] = (T)((double)x[j] * taperWeight(shape, (double)j * dtMs / s, param));
   if (e > 0)
     for (int64_t j = n - 1; j >= 0 && sweepMs - (double)j * dtMs < e; j--)
-      x[j] = (T)((double)x[j] * taperWeight(shape, (sweepMs - (double)j * dtMs) / e, NaN));
+      x[j] = (T)((double)x[j] * taperWeight(shape, (sweepMs - (double)j * dtMs) / e, param));
   return x;
 }
 
@@ -2057,15 +2071,18 @@ int orc_percentile_abs(int dtype, const void* x, int64_t n, double p, double* ou
     *out = dtype == PSG_F32 ? percentileAbs((const float*)x, n, p) : percentileAbs((const double*)x, n, p);
   });
 }
+int orc_taper_weight(int shape, double x, double param, double* out) {
+  return guard([&] { *out = taperWeight(shape, x, param); });
+}
 int orc_linear_sweep(double f1, double f2, double lengthMs, double dtMs, double ts, double te, int shape,
-                     double phaseDeg, double amp, int dtype, void* out, int64_t* n_out) {
+                     double param, double phaseDeg, double amp, int dtype, void* out, int64_t* n_out) {
   return guard([&] {
     if (dtype == PSG_F32) {
-      auto v = linearSweep<float>(f1, f2, lengthMs, dtMs, ts, te, shape, phaseDeg, amp);
+      auto v = linearSweep<float>(f1, f2, lengthMs, dtMs, ts, te, shape, param, phaseDeg, amp);
       if (out) std::memcpy(out, v.data(), v.size() * 4);
       *n_out = (int64_t)v.size();
     } else {
-      auto v = linearSweep<double>(f1, f2, lengthMs, dtMs, ts, te, shape, phaseDeg, amp);
+      auto v = linearSweep<double>(f1, f2, lengthMs, dtMs, ts, te, shape, param, phaseDeg, amp);
       if (out) std::memcpy(out, v.data(), v.size() * 8);
       *n_out = (int64_t)v.size();
     }

@@ -170,8 +170,10 @@ def _declare(lib):
         "psg_trace_stats": (C.c_int, [P, I32, I64, I32, P, P, P, P]),
         "psg_panel_stats": (C.c_int, [P, P, I32, I64, I32, P, DBL, P, P]),
         "psg_panel_stats_static": (C.c_int, [P, I32, I64, I32, P, DBL, P, P]),
-        "psg_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, I32, DBL, DBL, DBL, I32, P,
+        "psg_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, I32, DBL, DBL, DBL, DBL, I32, P,
                                        C.POINTER(I64)]),
+        "psg_taper_weight": (C.c_int, [I32, DBL, DBL, C.POINTER(DBL)]),
+        "psg_apply_taper": (C.c_int, [I32, P, I64, DBL, DBL, DBL, I32, DBL]),
         "psg_corr_plan_create": (C.c_int, [P, I32, I64, DBL, DBL, I32, DBL, I32, I32, I32, DBL, I32,
                                            C.POINTER(P)]),
         "psg_corr_plan_destroy": (None, [P]),

@@ -1998,16 +1998,41 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
 
 // ------------------------------------------------------------- vibroseis
 int psg_linear_sweep(double f1, double f2, double length_ms, double dt_ms, double ts, double te, int32_t shape,
-                     double phase_deg, double amplitude, double max_nyq, int32_t dtype, void* out, int64_t* n_out) {
+                     double taper_param, double phase_deg, double amplitude, double max_nyq, int32_t dtype,
+                     void* out, int64_t* n_out) {
   return guarded([&] {
     if (!n_out) throw InvalidArg("null argument");
-    std::vector<double> x = linear_sweep(f1, f2, length_ms, dt_ms, ts, te, shape, phase_deg, amplitude, max_nyq);
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    std::vector<double> x =
+        linear_sweep(f1, f2, length_ms, dt_ms, ts, te, shape, taper_param, phase_deg, amplitude, max_nyq, dtype);
     *n_out = (int64_t)x.size();
     if (out) {
       if (dtype == PSG_F32)
         for (size_t i = 0; i < x.size(); i++) ((float*)out)[i] = (float)x[i];
       else
         std::memcpy(out, x.data(), x.size() * 8);
+    }
+  });
+}
+
+int psg_taper_weight(int32_t shape, double x, double param, double* out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    *out = taper_weight(shape, x, param);
+  });
+}
+
+int psg_apply_taper(int32_t dtype, void* x, int64_t n, double dt_ms, double start_ms, double end_ms, int32_t shape,
+                    double param) {
+  return guarded([&] {
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    if (n < 0 || (n > 0 && !x)) throw InvalidArg("null argument or a negative length");
+    std::vector<double> v((size_t)n);
+    for (int64_t i = 0; i < n; i++) v[i] = dtype == PSG_F32 ? (double)((float*)x)[i] : ((double*)x)[i];
+    apply_taper(dtype, v.data(), n, dt_ms, start_ms, end_ms, shape, param);  // raises before any write
+    for (int64_t i = 0; i < n; i++) {
+      if (dtype == PSG_F32) ((float*)x)[i] = (float)v[i];
+      else ((double*)x)[i] = v[i];
     }
   });
 }

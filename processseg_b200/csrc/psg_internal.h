@@ -153,7 +153,12 @@ struct CorrHost {
 CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
                    int64_t record, int64_t out, int mode, double eps_percent, bool normalize, int max_radix = 16);
 std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
-                                 double t_end, int shape, double phase_deg, double amplitude,
-                                 double max_nyq_fraction);
+                                 double t_end, int shape, double param, double phase_deg, double amplitude,
+                                 double max_nyq_fraction, int dtype);
+double taper_default_param(int shape);
+void check_taper(double start_ms, double end_ms, int shape, double param);
+double taper_weight(int shape, double x, double param);
+void apply_taper(int dtype, double* x, int64_t n, double dt_ms, double start_ms, double end_ms, int shape,
+                 double param);
 
 }  // namespace psg

@@ -818,8 +818,45 @@ SpectrumHost spectrum_plan(int dtype, double dt_ms, int64_t window, double taper
 
 // --------------------------------------------------------------- vibroseis
 namespace {
-// vibroseis/taper.nim:125-145 for the shapes that need no special function.
-double taper_weight(int shape, double x) {
+// vibroseis/kaiser.nim:4-14: I0 by its power series Σ (x²/4)^k / (k!)²,
+// stopped once a term is below 1e-17 of the sum (about 70 terms at 50).
+double bessel_i0(double x) {
+  double term = 1, sum = 1, q = x * x / 4;
+  for (int k = 1; k <= 500; k++) {
+    term *= q / (double)(k * k);
+    sum += term;
+    if (term < sum * 1e-17) break;
+  }
+  return sum;
+}
+}  // namespace
+
+// vibroseis/taper.nim:69-74: β = 6 (Kaiser), σ = 0.4 (Gaussian), p = 2
+// (power); NaN for the shapes without a parameter.
+double taper_default_param(int shape) {
+  switch (shape) {
+    case 6: return 6.0;
+    case 7: return 0.4;
+    case 8: return 2.0;
+    default: return std::nan("");
+  }
+}
+
+// vibroseis/taper.nim:79-97 (validate): the lengths ≥ 0 and finite or NaN,
+// and the shape's parameter (NaN: its default) in range.
+void check_taper(double start_ms, double end_ms, int shape, double param) {
+  need(shape >= 0 && shape <= 8, "taper shape " + std::to_string(shape) + " is not one of 0 .. 8");
+  for (double v : {start_ms, end_ms})
+    need(std::isnan(v) || (v >= 0 && v < kInf), "a taper length must be ≥ 0 and finite (or NaN for none), got " + num(v));
+  const double p = std::isnan(param) ? taper_default_param(shape) : param;
+  if (shape == 6) need(p >= 0 && p <= 50, "a Kaiser taper needs 0 ≤ β ≤ 50, got " + num(p));
+  if (shape == 7) need(p > 0 && p < kInf, "a Gaussian taper needs σ > 0, got " + num(p));
+  if (shape == 8) need(p > 0 && p < kInf, "a power taper needs an exponent > 0, got " + num(p));
+}
+
+// vibroseis/taper.nim:125-145: w(x) on x clamped to [0, 1].
+double taper_weight(int shape, double x, double param) {
+  const double p = std::isnan(param) ? taper_default_param(shape) : param;
   x = std::min(1.0, std::max(0.0, x));
   switch (shape) {
     case 0: return x;
@@ -828,16 +865,37 @@ double taper_weight(int shape, double x) {
     case 3: return 0.54 - 0.46 * std::cos(kPi * x);
     case 4: return 0.42 - 0.5 * std::cos(kPi * x) + 0.08 * std::cos(2 * kPi * x);
     case 5: return 0.35875 - 0.48829 * std::cos(kPi * x) + 0.14128 * std::cos(2 * kPi * x) - 0.01168 * std::cos(3 * kPi * x);
-    default: throw InvalidArg("taper shape " + std::to_string(shape) + " is not supported");
+    case 6: { double u = 1 - x; return bessel_i0(p * std::sqrt(std::max(0.0, 1 - u * u))) / bessel_i0(p); }
+    case 7: { double u = (1 - x) / p; return std::exp(-0.5 * u * u); }
+    case 8: return std::pow(x, p);
+    default: throw InvalidArg("taper shape " + std::to_string(shape) + " is not one of 0 .. 8");
   }
 }
-}  // namespace
+
+// vibroseis/taper.nim:147-179 (checkFits, applyTaper) on values of dtype
+// held as doubles: each product rounds to dtype, as T(float64(x)·w).
+void apply_taper(int dtype, double* x, int64_t n, double dt_ms, double start_ms, double end_ms, int shape,
+                 double param) {
+  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and positive, got " + num(dt_ms));
+  const double sweep_ms = (double)std::max<int64_t>(n, 0) * dt_ms;
+  check_taper(start_ms, end_ms, shape, param);
+  const double s = std::isnan(start_ms) ? 0.0 : start_ms, e = std::isnan(end_ms) ? 0.0 : end_ms;
+  need(!(s + e > sweep_ms * (1 + 1e-9)), "the sweep tapers overlap: " + num(s) + " + " + num(e) +
+                                             " ms is longer than the " + num(sweep_ms) + " ms sweep");
+  if (s > 0)
+    for (int64_t j = 0; j < n && (double)j * dt_ms < s; j++)
+      x[j] = as_dtype(dtype, x[j] * taper_weight(shape, (double)j * dt_ms / s, param));
+  if (e > 0)
+    for (int64_t j = n - 1; j >= 0 && sweep_ms - (double)j * dt_ms < e; j--)
+      x[j] = as_dtype(dtype, x[j] * taper_weight(shape, (sweep_ms - (double)j * dt_ms) / e, param));
+}
 
 // vibroseis/sweep.nim:126-192 (validate, linearSweep), :292-301 (linear
-// phase, float64), :331-342 (sweepInto), taper.nim:160-179 (applyTaper).
+// phase, float64), :331-342 (sweepInto: each sample rounded to dtype),
+// taper.nim:160-179 (applyTaper).
 std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
-                                 double t_end, int shape, double phase_deg, double amplitude,
-                                 double max_nyq_fraction) {
+                                 double t_end, int shape, double param, double phase_deg, double amplitude,
+                                 double max_nyq_fraction, int dtype) {
   need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and positive, got " + num(dt_ms));
   need(length_ms >= dt_ms && length_ms < kInf, "lengthMs must be at least one sample interval, got " + num(length_ms));
   double steps = length_ms / dt_ms;
@@ -852,23 +910,16 @@ std::vector<double> linear_sweep(double f1, double f2, double length_ms, double 
     need(!(f > nyq), "a sweep frequency of " + num(f) + " Hz is above Nyquist (" + num(nyq) + " Hz)");
     need(!(f > limit * (1 + 1e-12)), "a sweep frequency of " + num(f) + " Hz is above the anti-alias limit " + num(limit) + " Hz");
   }
-  double ts = std::isnan(t_start) ? 0.0 : t_start, te = std::isnan(t_end) ? 0.0 : t_end;
-  need(ts >= 0 && ts < kInf && te >= 0 && te < kInf, "a taper length must be ≥ 0 and finite");
-  need(!(ts + te > length_ms * (1 + 1e-9)), "the sweep tapers overlap");
+  check_taper(t_start, t_end, shape, param);
   int64_t n = (int64_t)std::round(steps);
   std::vector<double> x(n);
   double dt = dt_ms / 1000, T = length_ms / 1000, rate = (f2 - f1) / T;
   double p0 = phase_deg * (kPi / 180);
   for (int64_t j = 0; j < n; j++) {
     double t = (double)j * dt;
-    x[j] = amplitude * std::sin(p0 + 2 * kPi * (f1 * t + 0.5 * rate * t * t));
+    x[j] = as_dtype(dtype, amplitude * std::sin(p0 + 2 * kPi * (f1 * t + 0.5 * rate * t * t)));
   }
-  double sweep_ms = (double)n * dt_ms;
-  if (ts > 0)
-    for (int64_t j = 0; j < n && (double)j * dt_ms < ts; j++) x[j] *= taper_weight(shape, (double)j * dt_ms / ts);
-  if (te > 0)
-    for (int64_t j = n - 1; j >= 0 && sweep_ms - (double)j * dt_ms < te; j--)
-      x[j] *= taper_weight(shape, (sweep_ms - (double)j * dt_ms) / te);
+  apply_taper(dtype, x.data(), n, dt_ms, t_start, t_end, shape, param);
   return x;
 }
 

@@ -16,26 +16,81 @@ import numpy as np
 from . import _abi as A
 from .meta import ChunkMeta
 
-tpLinear, tpCosine, tpCos2, tpHamming, tpBlackman, tpBlackmanHarris = range(6)
+tpLinear, tpCosine, tpCos2, tpHamming, tpBlackman, tpBlackmanHarris, tpKaiser, tpGaussian, tpPower = range(9)
+
+_DEFAULT_PARAM = {tpKaiser: 6.0, tpGaussian: 0.4, tpPower: 2.0}
+
+
+def defaultTaperParam(shape: int) -> float:
+    """β = 6 (Kaiser), σ = 0.4 (Gaussian), p = 2 (power); NaN for the other
+    shapes (taper.nim:69-74)."""
+    return _DEFAULT_PARAM.get(shape, math.nan)
 
 
 @dataclass(frozen=True)
 class SweepTaper:
-    """taper.nim:60-77 (the shapes without a special function)."""
+    """The ramps at the two ends of a sweep (taper.nim:60-67): lengths in ms
+    (0 or NaN: none), one shape for both, and the shape's parameter (NaN:
+    its default wherever the taper is used)."""
     startMs: float = 0.0
     endMs: float = 0.0
     shape: int = tpCos2
+    param: float = math.nan
+
+    def validate(self):
+        """taper.nim:79-97: the lengths ≥ 0 and finite (or NaN), β in 0 .. 50,
+        σ and p > 0 and finite. Raises ``ValueError``."""
+        if self.shape not in range(9):
+            raise ValueError(f"taper shape {self.shape} is not one of 0 .. 8")
+        for name, v in (("startMs", self.startMs), ("endMs", self.endMs)):
+            if not math.isnan(v) and not (v >= 0 and v < math.inf):
+                raise ValueError(f"a taper {name} must be ≥ 0 and finite (or NaN for none), got {v}")
+        p = defaultTaperParam(self.shape) if math.isnan(self.param) else self.param
+        if self.shape == tpKaiser and not (0 <= p <= 50):
+            raise ValueError(f"a Kaiser taper needs 0 ≤ β ≤ 50, got {p}")
+        if self.shape == tpGaussian and not (0 < p < math.inf):
+            raise ValueError(f"a Gaussian taper needs σ > 0, got {p}")
+        if self.shape == tpPower and not (0 < p < math.inf):
+            raise ValueError(f"a power taper needs an exponent > 0, got {p}")
+
+    def segyTaperType(self) -> int:
+        return segyTaperType(self.shape)
 
 
-def initSweepTaper(startMs: float, endMs: float, shape: int = tpCos2) -> SweepTaper:
-    for name, v in (("startMs", startMs), ("endMs", endMs)):
-        if not math.isnan(v) and not (v >= 0 and v < math.inf):
-            raise ValueError(f"a taper {name} must be ≥ 0 and finite (or NaN for none), got {v}")
-    return SweepTaper(startMs, endMs, shape)
+def initSweepTaper(startMs: float, endMs: float, shape: int = tpCos2, param: float = math.nan) -> SweepTaper:
+    """taper.nim:99-111: a NaN ``param`` takes the shape's default."""
+    t = SweepTaper(float(startMs), float(endMs), shape,
+                   defaultTaperParam(shape) if math.isnan(param) else float(param))
+    t.validate()
+    return t
 
 
 def noTaper() -> SweepTaper:
-    return SweepTaper(0.0, 0.0, tpLinear)
+    """taper.nim:113-115."""
+    return SweepTaper(0.0, 0.0, tpLinear, math.nan)
+
+
+def segyTaperType(shape: int) -> int:
+    """The SEG-Y taper type code: 1 linear, 2 cos², 3 other (taper.nim:117-123)."""
+    return 1 if shape == tpLinear else 2 if shape == tpCos2 else 3
+
+
+def taperWeight(shape: int, x: float, param: float = math.nan) -> float:
+    """taper.nim:125-145 through ``psg_taper_weight``."""
+    out = C.c_double()
+    A.check(A.lib().psg_taper_weight(int(shape), float(x), float(param), C.byref(out)))
+    return out.value
+
+
+def applyTaper(x: np.ndarray, dtMs: float, t: SweepTaper) -> None:
+    """taper.nim:160-179 through ``psg_apply_taper``: in place on a
+    contiguous float32 or float64 array; ``ValueError`` with nothing written
+    for a bad ``dtMs`` or taper, or ramps that overlap."""
+    if not isinstance(x, np.ndarray) or x.dtype not in (np.float32, np.float64) or not x.flags.c_contiguous:
+        raise TypeError("applyTaper takes a contiguous float32 or float64 numpy array")
+    dt = A.F32 if x.dtype == np.float32 else A.F64
+    A.check(A.lib().psg_apply_taper(dt, x.ctypes.data_as(C.c_void_p), x.size, float(dtMs), float(t.startMs),
+                                    float(t.endMs), int(t.shape), float(t.param)))
 
 
 @dataclass(frozen=True)
@@ -45,7 +100,7 @@ class SweepSpec:
     f2Hz: float
     lengthMs: float
     dtMs: float
-    taper: SweepTaper = SweepTaper(0.0, 0.0, tpLinear)
+    taper: SweepTaper = SweepTaper(0.0, 0.0, tpLinear, math.nan)
     startPhaseDeg: float = 0.0
     amplitude: float = 1.0
     maxNyquistFraction: float = 0.8
@@ -55,8 +110,8 @@ class SweepSpec:
         n = C.c_int64()
         dt = A.F32 if dtype == np.float32 else A.F64
         args = (self.f1Hz, self.f2Hz, self.lengthMs, self.dtMs, self.taper.startMs,
-                self.taper.endMs, self.taper.shape, self.startPhaseDeg, self.amplitude,
-                self.maxNyquistFraction, dt)
+                self.taper.endMs, self.taper.shape, self.taper.param, self.startPhaseDeg,
+                self.amplitude, self.maxNyquistFraction, dt)
         A.check(A.lib().psg_linear_sweep(*args, None, C.byref(n)))
         x = np.zeros(n.value, dtype)
         A.check(A.lib().psg_linear_sweep(*args, x.ctypes.data_as(C.c_void_p), C.byref(n)))
