@@ -462,11 +462,62 @@ int psg_taper_weight(int32_t shape, double x, double param, double* out);
  * longer than n·dt_ms together. */
 int psg_apply_taper(int32_t dtype, void* x, int64_t n, double dt_ms, double start_ms,
                     double end_ms, int32_t shape, double param);
-/* linearSweep + sweepInto + generatePilot, src/processSEG/vibroseis/
- * sweep.nim:126-342, taper.nim:125-179, pilot.nim:115-119: phase in float64,
- * each sample rounded to dtype, then the ramps of taper_shape / taper_param
- * (as psg_apply_taper). `out` is host memory of *n_out values of dtype
- * (NULL: just report the length). */
+/* Sweep laws (SweepLaw, src/processSEG/vibroseis/sweep.nim:68-74): the
+ * instantaneous frequency from f1 at 0 to f2 at length_ms, linear in time,
+ * with the amplitude spectrum boosted by boost_db per octave or per Hz,
+ * exponential in time, or piecewise linear through a table. */
+enum psg_sweep_law {
+  PSG_SL_LINEAR = 0, PSG_SL_DB_PER_OCTAVE = 1, PSG_SL_DB_PER_HZ = 2,
+  PSG_SL_EXPONENTIAL = 3, PSG_SL_TABLE = 4
+};
+/* SweepPoint, sweep.nim:76-79. */
+typedef struct psg_sweep_point {
+  double t_ms;
+  double f_hz;
+} psg_sweep_point;
+/* SweepSpec, sweep.nim:81-94 (the taper's fields inline). A table sweep's
+ * f1_hz / f2_hz / length_ms are its first and last points' (tableSweep,
+ * sweep.nim:221-232); the table is borrowed for the call. */
+typedef struct psg_sweep {
+  int32_t law;                  /* psg_sweep_law */
+  int32_t taper_shape;          /* psg_taper_shape */
+  double f1_hz, f2_hz, length_ms, dt_ms;
+  double boost_db;              /* dB per octave or per Hz */
+  const psg_sweep_point* table; /* PSG_SL_TABLE only */
+  int64_t n_table;
+  double start_phase_deg, amplitude;
+  double taper_start_ms, taper_end_ms, taper_param;
+  double max_nyquist_fraction;  /* 0.8 in the reference's builders */
+} psg_sweep;
+/* SweepHarmonic, sweep.nim:96-103: amp · sin(order·φ + phase_deg in rad). */
+typedef struct psg_sweep_harmonic {
+  double order, amp, phase_deg;
+} psg_sweep_harmonic;
+
+/* validate, sweep.nim:132-183 (with the taper's checkFits): PSG_EINVAL and
+ * the reference's message for an invalid spec. */
+int psg_sweep_validate(const psg_sweep* spec);
+/* sweepLen, sweep.nim:112-119: lengthMs / dtMs in whole samples; 0 for a
+ * length or interval that validate refuses. */
+int psg_sweep_len(const psg_sweep* spec, int64_t* n);
+/* frequencyAt, sweep.nim:248-284 (t_ms clamped to 0 .. length_ms); phaseAt,
+ * sweep.nim:436-463 (NaN for the two boosted laws, which have no closed
+ * form). The spec is validated first. */
+int psg_sweep_frequency_at(const psg_sweep* spec, double t_ms, double* out);
+int psg_sweep_phase_at(const psg_sweep* spec, double t_ms, double* out);
+/* sweepInto / sweepHarmonicsInto, sweep.nim:292-434: n host samples of dtype
+ * (n_harmonics 0 and n = sweepLen: the sweep alone; a longer buffer is the
+ * sweep followed by zeros, a shorter one its first n samples). The phase is
+ * in float64: closed form for the linear and table laws, 4-point
+ * Gauss–Legendre per sample interval for the others; each sample rounds to
+ * dtype before the ramps. SEG-Y sweep type (segySweepType, :465-473) in
+ * *segy_type when it is not NULL. */
+int psg_sweep_samples(const psg_sweep* spec, const psg_sweep_harmonic* harmonics,
+                      int32_t n_harmonics, int32_t dtype, void* out, int64_t n,
+                      int32_t* segy_type);
+/* linearSweep + sweepSamples (a psg_sweep of PSG_SL_LINEAR through
+ * psg_sweep_samples). `out` is host memory of *n_out values of dtype (NULL:
+ * just report the length). */
 int psg_linear_sweep(double f1_hz, double f2_hz, double length_ms, double dt_ms,
                      double taper_start_ms, double taper_end_ms, int32_t taper_shape,
                      double taper_param, double start_phase_deg, double amplitude,

@@ -72,6 +72,10 @@ def lib():
             "orc_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, C.c_int, DBL, DBL, DBL,
                                            C.c_int, P, C.POINTER(I64)]),
             "orc_taper_weight": (C.c_int, [C.c_int, DBL, DBL, C.POINTER(DBL)]),
+            "orc_sweep_samples": (C.c_int, [C.c_int, DBL, DBL, DBL, DBL, DBL, P, C.c_int, P, C.c_int, DBL,
+                                            DBL, DBL, DBL, C.c_int, DBL, C.c_int, P, I64]),
+            "orc_sweep_frequency_at": (C.c_int, [C.c_int, DBL, DBL, DBL, DBL, DBL, P, C.c_int, DBL,
+                                                 C.POINTER(DBL)]),
             "orc_correlate": (C.c_int, [P, I64, DBL, DBL, C.c_int, DBL, I64, I64, C.c_int, DBL,
                                         C.c_int, P, P, I64, I64, P, C.POINTER(I64),
                                         C.POINTER(DBL)]),
@@ -380,6 +384,34 @@ def linear_sweep(f1, f2, lengthMs, dtMs, taperStart=0.0, taperEnd=0.0, shape=2, 
     _check(lib().orc_linear_sweep(f1, f2, lengthMs, dtMs, taperStart, taperEnd, shape, param, phaseDeg,
                                   amplitude, dt, _ptr(x), C.byref(n)))
     return x
+
+
+def _sweep_args(spec):
+    tab = np.array([[p.tMs, p.fHz] for p in spec.table] or [[0.0, 0.0]], np.float64)
+    return (spec.law, spec.f1Hz, spec.f2Hz, spec.lengthMs, spec.dtMs, spec.boostDb, _ptr(tab),
+            len(spec.table)), tab
+
+
+def sweep_samples(spec, dtype=np.float64, harmonics=(), n=0):
+    """The oracle's sweep of a ``processseg_b200.SweepSpec`` (its fields
+    only; the spec is assumed valid)."""
+    args, tab = _sweep_args(spec)
+    if n == 0:
+        steps = spec.lengthMs / spec.dtMs
+        n = int(round(steps)) if abs(steps - round(steps)) <= 1e-6 else int(math.floor(steps))
+    h = np.array([[x.order, x.amp, x.phaseDeg] for x in harmonics] or [[0.0, 0.0, 0.0]], np.float64)
+    x = np.zeros(n, dtype)
+    t = spec.taper
+    _check(lib().orc_sweep_samples(*args, _ptr(h), len(harmonics), spec.startPhaseDeg, spec.amplitude,
+                                   t.startMs, t.endMs, t.shape, t.param, _dt(x), _ptr(x), n))
+    return x
+
+
+def sweep_frequency_at(spec, tMs):
+    args, tab = _sweep_args(spec)
+    out = C.c_double()
+    _check(lib().orc_sweep_frequency_at(*args, tMs, C.byref(out)))
+    return out.value
 
 
 def taper_weight(shape, x, param=math.nan):

@@ -1686,6 +1686,125 @@ std::vector<T> linearSweep(double f1, double f2, double lengthMs, double dtMs, d
   return x;
 }
 
+// vibroseis/sweep.nim:234-329 and :375-420: the non-linear laws' frequency,
+// the phase integral (closed form for linear and table, Gauss–Legendre with
+// 4 points per interval otherwise) and the harmonics, without validation
+// (the tests feed valid specs). Law codes: 0 linear, 1 dB/octave, 2 dB/Hz,
+// 3 exponential, 4 table.
+struct OSweep {
+  int law;
+  double f1, f2, lengthMs, dtMs, boostDb;
+  std::vector<double> tt, tf;  // table times (ms) and frequencies
+};
+double oExpm1(double x) {  // sweep.nim:236-241
+  double u = std::exp(x);
+  if (u == 1) return x;
+  if (u - 1 == -1) return -1.0;
+  return (u - 1) * x / std::log(u);
+}
+double oLn1p(double x) {  // sweep.nim:243-246
+  double u = 1 + x;
+  if (u == 1) return x;
+  return std::log(u) * x / (u - 1);
+}
+double oFrequencyAt(const OSweep& s, double tMs) {  // sweep.nim:248-284
+  double T = s.lengthMs;
+  double x = std::clamp(tMs, 0.0, T) / T;
+  double f1 = s.f1, f2 = s.f2;
+  if (x <= 0) return f1;
+  if (x >= 1) return f2;
+  auto within = [&](double f) { return std::clamp(f, std::min(f1, f2), std::max(f1, f2)); };
+  if (s.law == 0) return within(f1 + (f2 - f1) * x);
+  if (s.law == 3) return within(f1 * std::pow(f2 / f1, x));
+  if (s.law == 1) {
+    double octaveDb = 20 * std::log10(2.0) / 2;
+    double m = s.boostDb / octaveDb + 1;
+    if (std::fabs(m) < 1e-12) return within(f1 * std::pow(f2 / f1, x));
+    return within(f1 * std::pow(1 + x * oExpm1(m * std::log(f2 / f1)), 1 / m));
+  }
+  if (s.law == 2) {
+    double k = s.boostDb * std::log(10.0) / 10;
+    double e = oExpm1(k * (f2 - f1));
+    if (std::fabs(k * (f2 - f1)) < 1e-12) return within(f1 + (f2 - f1) * x);
+    return within(f1 + oLn1p(x * e) / k);
+  }
+  double t = std::clamp(tMs, 0.0, T);
+  size_t i = 1;
+  while (i < s.tt.size() - 1 && s.tt[i] < t) i++;
+  return s.tf[i - 1] + (s.tf[i] - s.tf[i - 1]) * (t - s.tt[i - 1]) / (s.tt[i] - s.tt[i - 1]);
+}
+std::vector<double> oPhases(const OSweep& s, int64_t n) {  // sweep.nim:292-329
+  std::vector<double> ph(n);
+  double dt = s.dtMs / 1000, T = s.lengthMs / 1000;
+  if (s.law == 0) {
+    double rate = (s.f2 - s.f1) / T;
+    for (int64_t j = 0; j < n; j++) {
+      double t = (double)j * dt;
+      ph[j] = 2 * PI * (s.f1 * t + 0.5 * rate * t * t);
+    }
+  } else if (s.law == 4) {
+    double acc = 0;
+    size_t i = 1;
+    for (int64_t j = 0; j < n; j++) {
+      double tMs = (double)j * s.dtMs;
+      while (i < s.tt.size() - 1 && s.tt[i] <= tMs) {
+        acc += 0.5 * (s.tf[i - 1] + s.tf[i]) * (s.tt[i] - s.tt[i - 1]) / 1000;
+        i++;
+      }
+      double sec = (std::min(tMs, s.tt[i]) - s.tt[i - 1]) / 1000;
+      double slope = (s.tf[i] - s.tf[i - 1]) / ((s.tt[i] - s.tt[i - 1]) / 1000);
+      ph[j] = 2 * PI * (acc + s.tf[i - 1] * sec + 0.5 * slope * sec * sec);
+    }
+  } else {
+    static const double nodes[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526};
+    static const double weights[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538};
+    double acc = 0;
+    if (n > 0) ph[0] = 0;
+    for (int64_t j = 1; j < n; j++) {
+      double a = (double)(j - 1) * s.dtMs, h = 0.5 * s.dtMs, sum = 0;
+      for (int q = 0; q < 4; q++) sum += weights[q] * oFrequencyAt(s, a + h + h * nodes[q]);
+      acc += sum * h / 1000;
+      ph[j] = 2 * PI * acc;
+    }
+  }
+  return ph;
+}
+// sweepHarmonicsInto (sweep.nim:375-420) into n samples of T; harmonics as
+// (order, amp, phaseDeg) triples; nh 0: the plain sweep.
+template <class T>
+std::vector<T> oSweepSamples(const OSweep& s, const double* harm, int nh, double phaseDeg, double amplitude,
+                             double ts, double te, int shape, double param, int64_t n) {
+  double steps = s.lengthMs / s.dtMs, r = std::round(steps);
+  int64_t nSweep = std::fabs(steps - r) <= 1e-6 ? (int64_t)r : (int64_t)std::floor(steps);
+  int64_t m = std::min(n, nSweep);
+  std::vector<double> ph = oPhases(s, m);
+  double p0 = phaseDeg * (PI / 180.0), nyq = 500.0 / s.dtMs;
+  std::vector<T> x(n, T(0));
+  for (int64_t j = 0; j < m; j++) {
+    double p = p0 + ph[j], v = 0;
+    if (nh == 0) {
+      v = std::sin(p);
+    } else {
+      double f = oFrequencyAt(s, (double)j * s.dtMs);
+      for (int k = 0; k < nh; k++) {
+        double order = harm[3 * k], amp = harm[3 * k + 1], pd = harm[3 * k + 2];
+        if (order == 1 || order * f < nyq) v += amp * std::sin(order * p + pd * (PI / 180.0));
+      }
+    }
+    x[j] = (T)(amplitude * v);
+  }
+  double sa = std::isnan(ts) ? 0.0 : ts, ea = std::isnan(te) ? 0.0 : te;
+  int64_t len = std::min(n, nSweep);
+  double sweepMs = n >= nSweep ? (double)nSweep * s.dtMs : s.lengthMs;
+  if (sa > 0)
+    for (int64_t j = 0; j < len && (double)j * s.dtMs < sa; j++)
+      x[j] = (T)((double)x[j] * taperWeight(shape, (double)j * s.dtMs / sa, param));
+  if (ea > 0)
+    for (int64_t j = len - 1; j >= 0 && sweepMs - (double)j * s.dtMs < ea; j--)
+      x[j] = (T)((double)x[j] * taperWeight(shape, (sweepMs - (double)j * s.dtMs) / ea, param));
+  return x;
+}
+
 template <class T> struct CorrPlan {
   FftPlan<T> fft;
   std::vector<T> mulRe, mulIm;
@@ -2069,6 +2188,36 @@ int orc_panel_stats(int dtype, const void* b, int64_t rows, int64_t cols, const 
 int orc_percentile_abs(int dtype, const void* x, int64_t n, double p, double* out) {
   return guard([&] {
     *out = dtype == PSG_F32 ? percentileAbs((const float*)x, n, p) : percentileAbs((const double*)x, n, p);
+  });
+}
+// table: n_table (t_ms, f_hz) pairs; harm: nh (order, amp, phaseDeg) triples
+int orc_sweep_samples(int law, double f1, double f2, double lengthMs, double dtMs, double boostDb,
+                      const double* table, int n_table, const double* harm, int nh, double phaseDeg, double amp,
+                      double ts, double te, int shape, double param, int dtype, void* out, int64_t n) {
+  return guard([&] {
+    OSweep s{law, f1, f2, lengthMs, dtMs, boostDb, {}, {}};
+    for (int i = 0; i < n_table; i++) {
+      s.tt.push_back(table[2 * i]);
+      s.tf.push_back(table[2 * i + 1]);
+    }
+    if (dtype == PSG_F32) {
+      auto v = oSweepSamples<float>(s, harm, nh, phaseDeg, amp, ts, te, shape, param, n);
+      std::memcpy(out, v.data(), v.size() * 4);
+    } else {
+      auto v = oSweepSamples<double>(s, harm, nh, phaseDeg, amp, ts, te, shape, param, n);
+      std::memcpy(out, v.data(), v.size() * 8);
+    }
+  });
+}
+int orc_sweep_frequency_at(int law, double f1, double f2, double lengthMs, double dtMs, double boostDb,
+                           const double* table, int n_table, double tMs, double* out) {
+  return guard([&] {
+    OSweep s{law, f1, f2, lengthMs, dtMs, boostDb, {}, {}};
+    for (int i = 0; i < n_table; i++) {
+      s.tt.push_back(table[2 * i]);
+      s.tf.push_back(table[2 * i + 1]);
+    }
+    *out = oFrequencyAt(s, tMs);
   });
 }
 int orc_taper_weight(int shape, double x, double param, double* out) {

@@ -36,9 +36,10 @@ mkTime, mkTable, mkLmo = _abi.MK_TIME, _abi.MK_TABLE, _abi.MK_LMO
 ipZero, ipMinimum = _abi.IP_ZERO, _abi.IP_MINIMUM
 from .meta import ChunkMeta, initChunkMeta, liveMeta
 from .plan import PipelinePlan, Workspace, compile, initWorkspace
-from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepSpec, SweepTaper, applyTaper,
-                        defaultTaperParam, generatePilot, initCorrelationPlan, initPilot, initRecordStack,
-                        initSweepTaper, linearSweep, noTaper, segyTaperType, taperWeight, tpBlackman,
-                        tpBlackmanHarris, tpCos2, tpCosine, tpGaussian, tpHamming, tpKaiser, tpLinear,
-                        tpPower)
+from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepHarmonic, SweepPoint, SweepSpec, SweepTaper,
+                        applyTaper, dbPerHzSweep, dbPerOctaveSweep, defaultTaperParam, exponentialSweep,
+                        generatePilot, initCorrelationPlan, initPilot, initRecordStack, initSweepTaper,
+                        linearSweep, noTaper, segyTaperType, slDbPerHz, slDbPerOctave, slExponential, slLinear,
+                        slTable, sweepHarmonics, tableSweep, taperWeight, tpBlackman, tpBlackmanHarris, tpCos2,
+                        tpCosine, tpGaussian, tpHamming, tpKaiser, tpLinear, tpPower)
 from .server import Server

@@ -76,6 +76,9 @@ class GainCurveC(C.Structure):
                 ("db_per_s", C.c_double), ("knots", GainKnotC * MAX_KNOTS)]
 
 
+SL_LINEAR, SL_DB_PER_OCTAVE, SL_DB_PER_HZ, SL_EXPONENTIAL, SL_TABLE = range(5)
+
+
 class MuteCurveC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("n_knots", C.c_int32), ("t_ms", C.c_double),
                 ("velocity", C.c_double), ("t0_ms", C.c_double), ("pad_ms", C.c_double),
@@ -85,6 +88,23 @@ class MuteCurveC(C.Structure):
 class KeysC(C.Structure):
     _fields_ = [("offset", C.c_void_p), ("t0_ms", C.c_void_p), ("first_sample", C.c_int32),
                 ("_pad", C.c_int32)]
+
+
+class SweepPointC(C.Structure):
+    _fields_ = [("t_ms", C.c_double), ("f_hz", C.c_double)]
+
+
+class SweepC(C.Structure):
+    _fields_ = [("law", C.c_int32), ("taper_shape", C.c_int32), ("f1_hz", C.c_double),
+                ("f2_hz", C.c_double), ("length_ms", C.c_double), ("dt_ms", C.c_double),
+                ("boost_db", C.c_double), ("table", C.c_void_p), ("n_table", C.c_int64),
+                ("start_phase_deg", C.c_double), ("amplitude", C.c_double),
+                ("taper_start_ms", C.c_double), ("taper_end_ms", C.c_double),
+                ("taper_param", C.c_double), ("max_nyquist_fraction", C.c_double)]
+
+
+class SweepHarmonicC(C.Structure):
+    _fields_ = [("order", C.c_double), ("amp", C.c_double), ("phase_deg", C.c_double)]
 
 
 class OpC(C.Structure):
@@ -173,6 +193,12 @@ def _declare(lib):
         "psg_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, I32, DBL, DBL, DBL, DBL, I32, P,
                                        C.POINTER(I64)]),
         "psg_taper_weight": (C.c_int, [I32, DBL, DBL, C.POINTER(DBL)]),
+        "psg_sweep_validate": (C.c_int, [C.POINTER(SweepC)]),
+        "psg_sweep_len": (C.c_int, [C.POINTER(SweepC), C.POINTER(I64)]),
+        "psg_sweep_frequency_at": (C.c_int, [C.POINTER(SweepC), DBL, C.POINTER(DBL)]),
+        "psg_sweep_phase_at": (C.c_int, [C.POINTER(SweepC), DBL, C.POINTER(DBL)]),
+        "psg_sweep_samples": (C.c_int, [C.POINTER(SweepC), C.POINTER(SweepHarmonicC), I32, I32, P, I64,
+                                        C.POINTER(I32)]),
         "psg_apply_taper": (C.c_int, [I32, P, I64, DBL, DBL, DBL, I32, DBL]),
         "psg_corr_plan_create": (C.c_int, [P, I32, I64, DBL, DBL, I32, DBL, I32, I32, I32, DBL, I32,
                                            C.POINTER(P)]),

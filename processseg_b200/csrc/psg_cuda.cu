@@ -1997,21 +1997,102 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
 }
 
 // ------------------------------------------------------------- vibroseis
+namespace {
+SweepHost sweep_host(const psg_sweep* p) {
+  if (!p) throw InvalidArg("null argument");
+  SweepHost s;
+  s.law = p->law;
+  s.f1 = p->f1_hz;
+  s.f2 = p->f2_hz;
+  s.length_ms = p->length_ms;
+  s.dt_ms = p->dt_ms;
+  s.boost_db = p->boost_db;
+  if (p->law == PSG_SL_TABLE) {
+    if (p->n_table < 0 || p->n_table > (1 << 24) || (p->n_table > 0 && !p->table))
+      throw InvalidArg("a sweep table needs 0 .. 2²⁴ points and a pointer to them");
+    s.table.assign(p->table, p->table + p->n_table);
+  }
+  s.phase_deg = p->start_phase_deg;
+  s.amplitude = p->amplitude;
+  s.taper_start = p->taper_start_ms;
+  s.taper_end = p->taper_end_ms;
+  s.taper_shape = p->taper_shape;
+  s.taper_param = p->taper_param;
+  s.max_nyq = p->max_nyquist_fraction;
+  return s;
+}
+void put_samples(const std::vector<double>& x, int32_t dtype, void* out) {
+  if (dtype == PSG_F32)
+    for (size_t i = 0; i < x.size(); i++) ((float*)out)[i] = (float)x[i];
+  else
+    std::memcpy(out, x.data(), x.size() * 8);
+}
+}  // namespace
+
+int psg_sweep_validate(const psg_sweep* spec) {
+  return guarded([&] { sweep_validate(sweep_host(spec)); });
+}
+
+int psg_sweep_len(const psg_sweep* spec, int64_t* n) {
+  return guarded([&] {
+    if (!n) throw InvalidArg("null argument");
+    *n = sweep_len(sweep_host(spec));
+  });
+}
+
+int psg_sweep_frequency_at(const psg_sweep* spec, double t_ms, double* out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    SweepHost s = sweep_host(spec);
+    sweep_validate(s);
+    *out = sweep_frequency_at(s, t_ms);
+  });
+}
+
+int psg_sweep_phase_at(const psg_sweep* spec, double t_ms, double* out) {
+  return guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    SweepHost s = sweep_host(spec);
+    sweep_validate(s);
+    *out = sweep_phase_at(s, t_ms);
+  });
+}
+
+int psg_sweep_samples(const psg_sweep* spec, const psg_sweep_harmonic* harmonics, int32_t n_harmonics, int32_t dtype,
+                      void* out, int64_t n, int32_t* segy_type) {
+  return guarded([&] {
+    if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
+    if (!out || n_harmonics < 0 || (n_harmonics > 0 && !harmonics)) throw InvalidArg("null argument");
+    SweepHost s = sweep_host(spec);
+    std::vector<psg_sweep_harmonic> hs(harmonics, harmonics + n_harmonics);
+    std::vector<double> x = sweep_samples(s, hs, n, dtype);
+    put_samples(x, dtype, out);
+    if (segy_type) *segy_type = sweep_segy_type(s);
+  });
+}
+
 int psg_linear_sweep(double f1, double f2, double length_ms, double dt_ms, double ts, double te, int32_t shape,
                      double taper_param, double phase_deg, double amplitude, double max_nyq, int32_t dtype,
                      void* out, int64_t* n_out) {
   return guarded([&] {
     if (!n_out) throw InvalidArg("null argument");
     if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be float32 or float64");
-    std::vector<double> x =
-        linear_sweep(f1, f2, length_ms, dt_ms, ts, te, shape, taper_param, phase_deg, amplitude, max_nyq, dtype);
-    *n_out = (int64_t)x.size();
-    if (out) {
-      if (dtype == PSG_F32)
-        for (size_t i = 0; i < x.size(); i++) ((float*)out)[i] = (float)x[i];
-      else
-        std::memcpy(out, x.data(), x.size() * 8);
-    }
+    SweepHost s;
+    s.law = PSG_SL_LINEAR;
+    s.f1 = f1;
+    s.f2 = f2;
+    s.length_ms = length_ms;
+    s.dt_ms = dt_ms;
+    s.phase_deg = phase_deg;
+    s.amplitude = amplitude;
+    s.taper_start = ts;
+    s.taper_end = te;
+    s.taper_shape = shape;
+    s.taper_param = taper_param;
+    s.max_nyq = max_nyq;
+    sweep_validate(s);
+    *n_out = sweep_len(s);
+    if (out) put_samples(sweep_samples(s, {}, *n_out, dtype), dtype, out);
   });
 }
 

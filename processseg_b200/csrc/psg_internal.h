@@ -152,9 +152,23 @@ struct CorrHost {
 };
 CorrHost corr_plan(const double* pilot, int64_t plen, double pilot_dt, double pilot_t0, double dt_ms,
                    int64_t record, int64_t out, int mode, double eps_percent, bool normalize, int max_radix = 16);
-std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
-                                 double t_end, int shape, double param, double phase_deg, double amplitude,
-                                 double max_nyq_fraction, int dtype);
+// vibroseis/sweep.nim: a SweepSpec with its taper inline.
+struct SweepHost {
+  int law = PSG_SL_LINEAR;
+  double f1 = 0, f2 = 0, length_ms = 0, dt_ms = 0, boost_db = 0;
+  std::vector<psg_sweep_point> table;
+  double phase_deg = 0, amplitude = 1;
+  double taper_start = 0, taper_end = 0, taper_param = 0;
+  int taper_shape = 0;
+  double max_nyq = 0.8;
+};
+int64_t sweep_len(const SweepHost& s);
+void sweep_validate(const SweepHost& s);
+double sweep_frequency_at(const SweepHost& s, double t_ms);
+double sweep_phase_at(const SweepHost& s, double t_ms);
+int sweep_segy_type(const SweepHost& s);
+std::vector<double> sweep_samples(const SweepHost& s, const std::vector<psg_sweep_harmonic>& harmonics, int64_t n,
+                                  int dtype);
 double taper_default_param(int shape);
 void check_taper(double start_ms, double end_ms, int shape, double param);
 double taper_weight(int shape, double x, double param);

@@ -890,36 +890,255 @@ void apply_taper(int dtype, double* x, int64_t n, double dt_ms, double start_ms,
       x[j] = as_dtype(dtype, x[j] * taper_weight(shape, (sweep_ms - (double)j * dt_ms) / e, param));
 }
 
-// vibroseis/sweep.nim:126-192 (validate, linearSweep), :292-301 (linear
-// phase, float64), :331-342 (sweepInto: each sample rounded to dtype),
-// taper.nim:160-179 (applyTaper).
-std::vector<double> linear_sweep(double f1, double f2, double length_ms, double dt_ms, double t_start,
-                                 double t_end, int shape, double param, double phase_deg, double amplitude,
-                                 double max_nyq_fraction, int dtype) {
-  need(dt_ms > 0 && dt_ms < kInf, "dtMs must be finite and positive, got " + num(dt_ms));
-  need(length_ms >= dt_ms && length_ms < kInf, "lengthMs must be at least one sample interval, got " + num(length_ms));
-  double steps = length_ms / dt_ms;
-  need(steps <= 2147483647.0, "a sweep is over 2³¹ samples");
-  need(std::fabs(steps - std::round(steps)) <= 1e-6, "lengthMs = " + num(length_ms) + " must be a whole number of samples of " + num(dt_ms) + " ms");
-  need(max_nyq_fraction > 0 && max_nyq_fraction <= 1, "maxNyquistFraction must be in (0, 1]");
-  need(fin(amplitude), "the amplitude must be finite");
-  need(fin(phase_deg), "startPhaseDeg must be finite");
-  double nyq = 500 / dt_ms, limit = max_nyq_fraction * nyq;
-  for (double f : {f1, f2}) {
-    need(f > 0 && f < kInf, "a sweep frequency must be > 0 Hz, got " + num(f));
-    need(!(f > nyq), "a sweep frequency of " + num(f) + " Hz is above Nyquist (" + num(nyq) + " Hz)");
-    need(!(f > limit * (1 + 1e-12)), "a sweep frequency of " + num(f) + " Hz is above the anti-alias limit " + num(limit) + " Hz");
+// ------------------------------------------------------------------ sweeps
+namespace {
+// 20·log10(2)/2: dB per octave of dt/df ∝ f (sweep.nim:234).
+const double kOctaveDb = 20 * std::log10(2.0) / 2;
+const double kMaxDbPerOctaveTotal = 300, kMaxDbPerHzTotal = 150;
+
+// exp(x) − 1 and ln(1 + x) by Kahan's correction, as sweep.nim:236-246
+// writes them (not libm's expm1 / log1p: the phases must match its bits).
+double kahan_expm1(double x) {
+  double u = std::exp(x);
+  if (u == 1) return x;
+  if (u - 1 == -1) return -1.0;
+  return (u - 1) * x / std::log(u);
+}
+double kahan_ln1p(double x) {
+  double u = 1 + x;
+  return u == 1 ? x : std::log(u) * x / (u - 1);
+}
+
+void check_freq(double f, double limit, double nyq, const std::string& what) {
+  need(f > 0 && f < kInf, what + " must be > 0 Hz, got " + num(f));
+  need(!(f > nyq), what + " = " + num(f) + " Hz is above Nyquist (" + num(nyq) + " Hz): it would alias");
+  need(!(f > limit * (1 + 1e-12)), what + " = " + num(f) + " Hz is above the anti-alias limit " + num(limit) +
+                                       " Hz (maxNyquistFraction · Nyquist); raise maxNyquistFraction to allow it");
+}
+
+// The 4-point Gauss–Legendre rule on [−1, 1]: nodes ±√(3/7 ∓ (2/7)√(6/5)),
+// weights (18 ± √30)/36, as the decimal values sweep.nim:286-290 holds.
+const double kGlNodes[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526};
+const double kGlWeights[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538};
+
+// sweep.nim:292-329 (phasesInto): 2π·∫₀ᵗ f in radians, without φ₀.
+void sweep_phases(const SweepHost& s, double* phase, int64_t n) {
+  const double dt = s.dt_ms / 1000, T = s.length_ms / 1000;
+  if (s.law == PSG_SL_LINEAR) {
+    const double rate = (s.f2 - s.f1) / T;
+    for (int64_t j = 0; j < n; j++) {
+      double t = (double)j * dt;
+      phase[j] = 2 * kPi * (s.f1 * t + 0.5 * rate * t * t);
+    }
+  } else if (s.law == PSG_SL_TABLE) {
+    // piecewise linear f: the phase is piecewise quadratic, exact per piece
+    const auto& tab = s.table;
+    double acc = 0;
+    size_t i = 1;
+    for (int64_t j = 0; j < n; j++) {
+      const double tms = (double)j * s.dt_ms;
+      while (i < tab.size() - 1 && tab[i].t_ms <= tms) {
+        acc += 0.5 * (tab[i - 1].f_hz + tab[i].f_hz) * (tab[i].t_ms - tab[i - 1].t_ms) / 1000;
+        i++;
+      }
+      const psg_sweep_point a = tab[i - 1], b = tab[i];
+      const double sec = (std::min(tms, b.t_ms) - a.t_ms) / 1000;
+      const double slope = (b.f_hz - a.f_hz) / ((b.t_ms - a.t_ms) / 1000);
+      phase[j] = 2 * kPi * (acc + a.f_hz * sec + 0.5 * slope * sec * sec);
+    }
+  } else {
+    double acc = 0;
+    if (n > 0) phase[0] = 0;
+    for (int64_t j = 1; j < n; j++) {
+      const double a = (double)(j - 1) * s.dt_ms, h = 0.5 * s.dt_ms;
+      double sum = 0;
+      for (int q = 0; q < 4; q++) sum += kGlWeights[q] * sweep_frequency_at(s, a + h + h * kGlNodes[q]);
+      acc += sum * h / 1000;
+      phase[j] = 2 * kPi * acc;
+    }
   }
-  check_taper(t_start, t_end, shape, param);
-  int64_t n = (int64_t)std::round(steps);
-  std::vector<double> x(n);
-  double dt = dt_ms / 1000, T = length_ms / 1000, rate = (f2 - f1) / T;
-  double p0 = phase_deg * (kPi / 180);
-  for (int64_t j = 0; j < n; j++) {
-    double t = (double)j * dt;
-    x[j] = as_dtype(dtype, amplitude * std::sin(p0 + 2 * kPi * (f1 * t + 0.5 * rate * t * t)));
+}
+}  // namespace
+
+// sweep.nim:112-119 (sweepLen) with core/types.nim:147-160 (samplesInLength:
+// a quotient within 1e-6 of a whole number is that number, else floor).
+int64_t sweep_len(const SweepHost& s) {
+  if (!(s.dt_ms > 0 && s.dt_ms < kInf)) return 0;
+  if (!(s.length_ms > 0 && s.length_ms < kInf)) return 0;
+  const double steps = s.length_ms / s.dt_ms;
+  if (!(steps >= 1 && steps <= 2147483647.0)) return 0;
+  const double r = std::round(steps);
+  return std::fabs(steps - r) <= 1e-6 ? (int64_t)r : (int64_t)std::floor(steps);
+}
+
+// sweep.nim:132-183 (validate, with checkFreq :123-130 and the taper's
+// checkFits, taper.nim:147-158).
+void sweep_validate(const SweepHost& s) {
+  need(s.dt_ms > 0 && s.dt_ms < kInf, "dtMs must be finite and positive, got " + num(s.dt_ms));
+  need(s.length_ms >= s.dt_ms && s.length_ms < kInf, "lengthMs must be at least one sample interval, got " + num(s.length_ms));
+  const double steps = s.length_ms / s.dt_ms;
+  need(!(steps > 2147483647.0), "a sweep of " + num(s.length_ms) + " ms at " + num(s.dt_ms) + " ms is over 2³¹ samples");
+  need(!(std::fabs(steps - std::round(steps)) > 1e-6),
+       "lengthMs = " + num(s.length_ms) + " must be a whole number of samples of " + num(s.dt_ms) + " ms");
+  need(s.max_nyq > 0 && s.max_nyq <= 1, "maxNyquistFraction must be in (0, 1], got " + num(s.max_nyq));
+  need(fin(s.amplitude), "the amplitude must be finite, got " + num(s.amplitude));
+  need(fin(s.phase_deg), "startPhaseDeg must be finite, got " + num(s.phase_deg));
+  const double nyq = 500 / s.dt_ms, limit = s.max_nyq * nyq;
+  check_freq(s.f1, limit, nyq, "f1Hz");
+  check_freq(s.f2, limit, nyq, "f2Hz");
+  switch (s.law) {
+    case PSG_SL_DB_PER_OCTAVE:
+    case PSG_SL_DB_PER_HZ: {
+      need(fin(s.boost_db), "boostDb must be finite, got " + num(s.boost_db));
+      const bool hz = s.law == PSG_SL_DB_PER_HZ;
+      const double total = hz ? std::fabs(s.boost_db * (s.f2 - s.f1)) : std::fabs(s.boost_db * std::log2(s.f2 / s.f1));
+      const double lim = hz ? kMaxDbPerHzTotal : kMaxDbPerOctaveTotal;
+      need(!(total > lim), "a boost of " + num(s.boost_db) + (hz ? " dB/Hz" : " dB/octave") + " from " + num(s.f1) +
+                               " to " + num(s.f2) + " Hz adds up to " + num(std::round(10 * total) / 10) +
+                               " dB, over the limit of " + num(lim));
+      break;
+    }
+    case PSG_SL_TABLE: {
+      const auto& t = s.table;
+      need(t.size() >= 2, "a table sweep needs at least two points");
+      need(t[0].t_ms == 0, "a sweep table must start at 0 ms, got " + num(t[0].t_ms));
+      need(!(std::fabs(t.back().t_ms - s.length_ms) > 1e-9 * s.length_ms),
+           "a sweep table must end at lengthMs = " + num(s.length_ms) + ", got " + num(t.back().t_ms));
+      for (size_t i = 0; i < t.size(); i++) {
+        check_freq(t[i].f_hz, limit, nyq, "the table frequency at " + num(t[i].t_ms) + " ms");
+        need(i == 0 || t[i].t_ms > t[i - 1].t_ms,
+             "sweep table times must increase: " + num(i ? t[i - 1].t_ms : 0) + " then " + num(t[i].t_ms));
+      }
+      need(s.f1 == t[0].f_hz && s.f2 == t.back().f_hz, "a table sweep's f1Hz and f2Hz must be its first and last frequencies");
+      break;
+    }
+    case PSG_SL_LINEAR:
+    case PSG_SL_EXPONENTIAL: break;
+    default: throw InvalidArg("sweep law " + std::to_string(s.law) + " is not one of 0 .. 4");
   }
-  apply_taper(dtype, x.data(), n, dt_ms, t_start, t_end, shape, param);
+  check_taper(s.taper_start, s.taper_end, s.taper_shape, s.taper_param);
+  const double ts = std::isnan(s.taper_start) ? 0.0 : s.taper_start, te = std::isnan(s.taper_end) ? 0.0 : s.taper_end;
+  need(!(ts + te > s.length_ms * (1 + 1e-9)), "the sweep tapers overlap: " + num(ts) + " + " + num(te) +
+                                                  " ms is longer than the " + num(s.length_ms) + " ms sweep");
+}
+
+// sweep.nim:248-284 (frequencyAt): f1 at 0 and f2 at lengthMs exactly, the
+// laws clamped between the two; the spec is assumed valid.
+double sweep_frequency_at(const SweepHost& s, double t_ms) {
+  const double T = s.length_ms, f1 = s.f1, f2 = s.f2;
+  const double x = std::min(std::max(t_ms, 0.0), T) / T;
+  if (x <= 0) return f1;
+  if (x >= 1) return f2;
+  const double lo = std::min(f1, f2), hi = std::max(f1, f2);
+  auto within = [&](double f) { return std::min(std::max(f, lo), hi); };
+  switch (s.law) {
+    case PSG_SL_LINEAR: return within(f1 + (f2 - f1) * x);
+    case PSG_SL_EXPONENTIAL: return within(f1 * std::pow(f2 / f1, x));
+    case PSG_SL_DB_PER_OCTAVE: {
+      // f^m linear in time, written in f2/f1 so that no power of a frequency overflows
+      const double m = s.boost_db / kOctaveDb + 1;
+      if (std::fabs(m) < 1e-12) return within(f1 * std::pow(f2 / f1, x));
+      return within(f1 * std::pow(1 + x * kahan_expm1(m * std::log(f2 / f1)), 1 / m));
+    }
+    case PSG_SL_DB_PER_HZ: {
+      const double k = s.boost_db * std::log(10.0) / 10;  // dt/df ∝ exp(k·f)
+      const double e = kahan_expm1(k * (f2 - f1));
+      if (std::fabs(k * (f2 - f1)) < 1e-12) return within(f1 + (f2 - f1) * x);
+      return within(f1 + kahan_ln1p(x * e) / k);
+    }
+    default: {
+      const double t = std::min(std::max(t_ms, 0.0), T);
+      const auto& tab = s.table;
+      size_t i = 1;
+      while (i < tab.size() - 1 && tab[i].t_ms < t) i++;
+      const psg_sweep_point a = tab[i - 1], b = tab[i];
+      return a.f_hz + (b.f_hz - a.f_hz) * (t - a.t_ms) / (b.t_ms - a.t_ms);
+    }
+  }
+}
+
+// sweep.nim:436-463 (phaseAt): φ₀ + 2π·∫₀ᵗ f for the laws with a closed
+// form; NaN for the boosted ones.
+double sweep_phase_at(const SweepHost& s, double t_ms) {
+  const double t = std::min(std::max(t_ms, 0.0), s.length_ms) / 1000, T = s.length_ms / 1000;
+  const double p0 = s.phase_deg * (kPi / 180);
+  switch (s.law) {
+    case PSG_SL_LINEAR: return p0 + 2 * kPi * (s.f1 * t + 0.5 * (s.f2 - s.f1) / T * t * t);
+    case PSG_SL_EXPONENTIAL: {
+      const double r = std::log(s.f2 / s.f1);
+      if (std::fabs(r) < 1e-12) return p0 + 2 * kPi * s.f1 * t;
+      return p0 + 2 * kPi * s.f1 * T / r * kahan_expm1(r * t / T);
+    }
+    case PSG_SL_TABLE: {
+      double acc = 0;
+      const double tm = t * 1000;
+      const auto& tab = s.table;
+      for (size_t i = 1; i < tab.size(); i++) {
+        const psg_sweep_point a = tab[i - 1], b = tab[i];
+        if (tm <= b.t_ms) {
+          const double sec = (tm - a.t_ms) / 1000;
+          const double slope = (b.f_hz - a.f_hz) / ((b.t_ms - a.t_ms) / 1000);
+          return p0 + 2 * kPi * (acc + a.f_hz * sec + 0.5 * slope * sec * sec);
+        }
+        acc += 0.5 * (a.f_hz + b.f_hz) * (b.t_ms - a.t_ms) / 1000;
+      }
+      return p0 + 2 * kPi * acc;
+    }
+    default: return kNaN;
+  }
+}
+
+// sweep.nim:465-473 (segySweepType): 1 linear, 3 exponential (or a dB/octave
+// law of −3.0103 dB), 4 other.
+int sweep_segy_type(const SweepHost& s) {
+  switch (s.law) {
+    case PSG_SL_LINEAR: return 1;
+    case PSG_SL_EXPONENTIAL: return 3;
+    case PSG_SL_DB_PER_OCTAVE: return std::fabs(s.boost_db + kOctaveDb) < 1e-9 ? 3 : 4;
+    default: return 4;
+  }
+}
+
+// sweep.nim:331-342 (sweepInto) and :351-420 (checkHarmonic, taperPrefix,
+// sweepHarmonicsInto): n samples of dtype held as doubles, each rounded to
+// dtype before the ramps; samples past the sweep are 0.
+std::vector<double> sweep_samples(const SweepHost& s, const std::vector<psg_sweep_harmonic>& harmonics, int64_t n,
+                                  int dtype) {
+  sweep_validate(s);
+  need(n >= 1, "a sweep buffer needs at least one sample, got " + std::to_string(n));
+  for (const auto& h : harmonics) {
+    need(h.order > 0 && h.order < kInf, "a harmonic order must be finite and > 0, got " + num(h.order));
+    need(fin(h.amp), "a harmonic amplitude must be finite, got " + num(h.amp));
+    need(fin(h.phase_deg), "a harmonic phase must be finite, got " + num(h.phase_deg));
+  }
+  const int64_t n_sweep = sweep_len(s), m = std::min(n, n_sweep);
+  std::vector<double> phase((size_t)m), x((size_t)n, 0.0);
+  sweep_phases(s, phase.data(), m);
+  const double p0 = s.phase_deg * (kPi / 180), nyq = 500.0 / s.dt_ms;
+  for (int64_t j = 0; j < m; j++) {
+    const double p = p0 + phase[j];
+    double v = 0;
+    if (harmonics.empty()) {
+      v = std::sin(p);
+    } else {
+      const double f = sweep_frequency_at(s, (double)j * s.dt_ms);
+      for (const auto& h : harmonics)
+        if (h.order == 1 || h.order * f < nyq) v += h.amp * std::sin(h.order * p + h.phase_deg * (kPi / 180));
+    }
+    x[j] = as_dtype(dtype, s.amplitude * v);
+  }
+  if (n >= n_sweep) {
+    apply_taper(dtype, x.data(), n_sweep, s.dt_ms, s.taper_start, s.taper_end, s.taper_shape, s.taper_param);
+  } else {
+    // the ramps of the whole sweep on its first n samples (taperPrefix)
+    const double ts = std::isnan(s.taper_start) ? 0.0 : s.taper_start, te = std::isnan(s.taper_end) ? 0.0 : s.taper_end;
+    if (ts > 0)
+      for (int64_t j = 0; j < n && (double)j * s.dt_ms < ts; j++)
+        x[j] = as_dtype(dtype, x[j] * taper_weight(s.taper_shape, (double)j * s.dt_ms / ts, s.taper_param));
+    if (te > 0)
+      for (int64_t j = n - 1; j >= 0 && s.length_ms - (double)j * s.dt_ms < te; j--)
+        x[j] = as_dtype(dtype, x[j] * taper_weight(s.taper_shape, (s.length_ms - (double)j * s.dt_ms) / te, s.taper_param));
+  }
   return x;
 }
 

@@ -93,9 +93,33 @@ def applyTaper(x: np.ndarray, dtMs: float, t: SweepTaper) -> None:
                                     float(t.endMs), int(t.shape), float(t.param)))
 
 
+slLinear, slDbPerOctave, slDbPerHz, slExponential, slTable = (A.SL_LINEAR, A.SL_DB_PER_OCTAVE, A.SL_DB_PER_HZ,
+                                                               A.SL_EXPONENTIAL, A.SL_TABLE)
+
+
+@dataclass(frozen=True)
+class SweepPoint:
+    """A point of a table sweep: the frequency ``fHz`` at ``tMs`` (sweep.nim:76-79)."""
+    tMs: float
+    fHz: float
+
+
+@dataclass(frozen=True)
+class SweepHarmonic:
+    """One term ``amp · sin(order·φ + rad(phaseDeg))`` of a distorted sweep,
+    φ the fundamental's phase (sweep.nim:96-103)."""
+    order: float = 1.0
+    amp: float = 1.0
+    phaseDeg: float = 0.0
+
+
 @dataclass(frozen=True)
 class SweepSpec:
-    """A linear sweep (sweep.nim:81-95, law slLinear)."""
+    """A vibroseis sweep (sweep.nim:81-94). Make one with ``linearSweep``,
+    ``dbPerOctaveSweep``, ``dbPerHzSweep``, ``exponentialSweep`` or
+    ``tableSweep``, which validate it; the host library computes the
+    samples (float64 phase: closed form for the linear and table laws,
+    4-point Gauss–Legendre per interval for the others)."""
     f1Hz: float
     f2Hz: float
     lengthMs: float
@@ -104,26 +128,124 @@ class SweepSpec:
     startPhaseDeg: float = 0.0
     amplitude: float = 1.0
     maxNyquistFraction: float = 0.8
+    law: int = slLinear
+    boostDb: float = 0.0
+    table: tuple = ()
 
-    def samples(self, dtype=np.float64) -> np.ndarray:
-        """sweepSamples (sweep.nim:331-348): phase in float64."""
+    def _c(self):
+        pts = (A.SweepPointC * max(1, len(self.table)))(*[A.SweepPointC(p.tMs, p.fHz) for p in self.table])
+        c = A.SweepC(self.law, self.taper.shape, self.f1Hz, self.f2Hz, self.lengthMs, self.dtMs, self.boostDb,
+                     C.cast(pts, C.c_void_p), len(self.table), self.startPhaseDeg, self.amplitude,
+                     self.taper.startMs, self.taper.endMs, self.taper.param, self.maxNyquistFraction)
+        c._keep = pts
+        return c
+
+    def validate(self):
+        """sweep.nim:132-183. Raises ``ValueError``."""
+        A.check(A.lib().psg_sweep_validate(C.byref(self._c())))
+
+    def sweepLen(self) -> int:
+        """sweep.nim:112-119: 0 for a length or interval ``validate`` refuses."""
         n = C.c_int64()
-        dt = A.F32 if dtype == np.float32 else A.F64
-        args = (self.f1Hz, self.f2Hz, self.lengthMs, self.dtMs, self.taper.startMs,
-                self.taper.endMs, self.taper.shape, self.taper.param, self.startPhaseDeg,
-                self.amplitude, self.maxNyquistFraction, dt)
-        A.check(A.lib().psg_linear_sweep(*args, None, C.byref(n)))
-        x = np.zeros(n.value, dtype)
-        A.check(A.lib().psg_linear_sweep(*args, x.ctypes.data_as(C.c_void_p), C.byref(n)))
+        A.check(A.lib().psg_sweep_len(C.byref(self._c()), C.byref(n)))
+        return n.value
+
+    def frequencyAt(self, tMs: float) -> float:
+        """sweep.nim:248-284."""
+        out = C.c_double()
+        A.check(A.lib().psg_sweep_frequency_at(C.byref(self._c()), float(tMs), C.byref(out)))
+        return out.value
+
+    def phaseAt(self, tMs: float) -> float:
+        """sweep.nim:436-463 (NaN for the boosted laws)."""
+        out = C.c_double()
+        A.check(A.lib().psg_sweep_phase_at(C.byref(self._c()), float(tMs), C.byref(out)))
+        return out.value
+
+    def segySweepType(self) -> int:
+        """sweep.nim:465-473: 1 linear, 3 exponential, 4 other."""
+        t = C.c_int32()
+        x = np.zeros(1)
+        A.check(A.lib().psg_sweep_samples(C.byref(self._c()), None, 0, A.F64, x.ctypes.data_as(C.c_void_p), 1,
+                                          C.byref(t)))
+        return t.value
+
+    def samples(self, dtype=np.float64, harmonics=(), samples: int = 0) -> np.ndarray:
+        """sweepSamples / sweepHarmonics (sweep.nim:344-349, 422-434):
+        ``samples`` 0 is ``sweepLen``; a longer buffer is the sweep followed
+        by zeros, a shorter one its first samples."""
+        self.validate()
+        n = self.sweepLen() if samples == 0 else int(samples)
+        if n < 1:
+            raise ValueError(f"samples must be ≥ 1, got {n}")
+        dt = A.F32 if np.dtype(dtype) == np.float32 else A.F64
+        hs = (A.SweepHarmonicC * max(1, len(harmonics)))(
+            *[A.SweepHarmonicC(h.order, h.amp, h.phaseDeg) for h in harmonics])
+        x = np.zeros(n, np.float32 if dt == A.F32 else np.float64)
+        A.check(A.lib().psg_sweep_samples(C.byref(self._c()), hs, len(harmonics), dt,
+                                          x.ctypes.data_as(C.c_void_p), n, None))
         return x
+
+    def sweepInto(self, x: np.ndarray, harmonics=()) -> None:
+        """sweepInto / sweepHarmonicsInto (sweep.nim:331-342, 375-420) on a
+        float32 or float64 array; without harmonics its length must be
+        ``sweepLen``."""
+        if not harmonics and x.size != self.sweepLen():
+            self.validate()
+            raise ValueError(f"the sweep has {self.sweepLen()} samples, the buffer {x.size}")
+        x[...] = self.samples(x.dtype, harmonics, x.size)
+
+
+def sweepHarmonics(spec: SweepSpec, dtype=np.float64, harmonics=(), samples: int = 0) -> np.ndarray:
+    return spec.samples(dtype, harmonics, samples)
+
+
+def _built(**kw) -> SweepSpec:
+    s = SweepSpec(**kw)
+    s.validate()
+    return s
 
 
 def linearSweep(f1Hz, f2Hz, lengthMs, dtMs, taper: SweepTaper = None, startPhaseDeg=0.0,
                 amplitude=1.0, maxNyquistFraction=0.8) -> SweepSpec:
-    s = SweepSpec(f1Hz, f2Hz, lengthMs, dtMs, taper or noTaper(), startPhaseDeg, amplitude,
-                  maxNyquistFraction)
-    s.samples()  # validates (sweep.nim:126-178)
-    return s
+    """sweep.nim:185-192."""
+    return _built(f1Hz=f1Hz, f2Hz=f2Hz, lengthMs=lengthMs, dtMs=dtMs, taper=taper or noTaper(),
+                  startPhaseDeg=startPhaseDeg, amplitude=amplitude, maxNyquistFraction=maxNyquistFraction)
+
+
+def dbPerOctaveSweep(f1Hz, f2Hz, lengthMs, dtMs, boostDb, taper: SweepTaper = None, startPhaseDeg=0.0,
+                     amplitude=1.0, maxNyquistFraction=0.8) -> SweepSpec:
+    """sweep.nim:194-201."""
+    return _built(f1Hz=f1Hz, f2Hz=f2Hz, lengthMs=lengthMs, dtMs=dtMs, taper=taper or noTaper(),
+                  startPhaseDeg=startPhaseDeg, amplitude=amplitude, maxNyquistFraction=maxNyquistFraction,
+                  law=slDbPerOctave, boostDb=boostDb)
+
+
+def dbPerHzSweep(f1Hz, f2Hz, lengthMs, dtMs, boostDb, taper: SweepTaper = None, startPhaseDeg=0.0,
+                 amplitude=1.0, maxNyquistFraction=0.8) -> SweepSpec:
+    """sweep.nim:203-210."""
+    return _built(f1Hz=f1Hz, f2Hz=f2Hz, lengthMs=lengthMs, dtMs=dtMs, taper=taper or noTaper(),
+                  startPhaseDeg=startPhaseDeg, amplitude=amplitude, maxNyquistFraction=maxNyquistFraction,
+                  law=slDbPerHz, boostDb=boostDb)
+
+
+def exponentialSweep(f1Hz, f2Hz, lengthMs, dtMs, taper: SweepTaper = None, startPhaseDeg=0.0,
+                     amplitude=1.0, maxNyquistFraction=0.8) -> SweepSpec:
+    """sweep.nim:212-219."""
+    return _built(f1Hz=f1Hz, f2Hz=f2Hz, lengthMs=lengthMs, dtMs=dtMs, taper=taper or noTaper(),
+                  startPhaseDeg=startPhaseDeg, amplitude=amplitude, maxNyquistFraction=maxNyquistFraction,
+                  law=slExponential)
+
+
+def tableSweep(points, dtMs, taper: SweepTaper = None, startPhaseDeg=0.0, amplitude=1.0,
+               maxNyquistFraction=0.8) -> SweepSpec:
+    """sweep.nim:221-232: f1/f2/length from the first and last points."""
+    pts = tuple(points)
+    if len(pts) < 2:
+        raise ValueError("a table sweep needs at least two points")
+    return _built(f1Hz=pts[0].fHz, f2Hz=pts[-1].fHz, lengthMs=pts[-1].tMs, dtMs=dtMs, taper=taper or noTaper(),
+                  startPhaseDeg=startPhaseDeg, amplitude=amplitude, maxNyquistFraction=maxNyquistFraction,
+                  law=slTable, table=pts)
 
 
 @dataclass
