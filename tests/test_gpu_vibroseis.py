@@ -118,3 +118,34 @@ def test_sweeps_in_one_block_stack_as_sweep_by_sweep():
     assert torch.equal(fa, fb) and int(fa.max()) == sweeps
     ref = float(oa.abs().max())
     assert float((oa - ob).abs().max()) <= 1e-6 * ref
+
+
+@pytest.mark.parametrize("law", ["dbPerOctave", "dbPerHz", "exponential", "table"])
+def test_correlation_with_nonlinear_pilots_matches_oracle(law):
+    """The non-linear laws' pilots (with Kaiser, Gaussian or power ramps and
+    a harmonic-free float32 pilot) correlated on the device against the
+    oracle's correlation of the same samples, at the float32 bar."""
+    taper = {"dbPerOctave": P.initSweepTaper(300, 300, P.tpKaiser),
+             "dbPerHz": P.initSweepTaper(250, 400, P.tpGaussian),
+             "exponential": P.initSweepTaper(300, 300, P.tpPower, 3.0),
+             "table": P.initSweepTaper(200, 200, P.tpBlackmanHarris)}[law]
+    spec = {"dbPerOctave": lambda: P.dbPerOctaveSweep(8, 80, 8000, 2, 3, taper),
+            "dbPerHz": lambda: P.dbPerHzSweep(8, 80, 8000, 2, 0.05, taper),
+            "exponential": lambda: P.exponentialSweep(6, 90, 8000, 2, taper),
+            "table": lambda: P.tableSweep([P.SweepPoint(0, 8), P.SweepPoint(3000, 30),
+                                           P.SweepPoint(8000, 80)], 2, taper)}[law]()
+    pilot = P.generatePilot(spec, np.float32)
+    assert pilot.samples.dtype == np.float32 and len(pilot) == 4000
+    recs = synth.vibroseis_records(pilot.samples.astype(np.float64), channels=24, sweeps=1, samples=8001)
+    src = recs[0].astype(np.float32)
+    rows = src.shape[0]
+    meta = P.initChunkMeta(np.full(rows, P.tsLive, np.int32), np.full(rows, 8001, np.int32), 2.0)
+    plan = P.initCorrelationPlan(P.float32, pilot, 2.0, 8001, outSamples=2000)
+    s = torch.from_numpy(src).cuda()
+    d = torch.zeros(rows, 2000, dtype=s.dtype, device="cuda")
+    plan.correlateInto(s, d, meta)
+    torch.cuda.synchronize()
+    live, _ = meta.flat(8001, 1)
+    want, _, _ = O.correlate(pilot.samples.astype(np.float64), 2.0, 0.0, src, live, 2.0, 8001, outSamples=2000)
+    peak = np.max(np.abs(want))
+    assert np.max(np.abs(d.cpu().numpy() - want)) <= 2e-5 * peak
