@@ -241,6 +241,13 @@ int psg_rows_flatten(const int32_t* status, const int32_t* num_samples,
                      int32_t cols, int32_t mode, int32_t* live_out,
                      double* start_ms_out);
 
+/* checkApply, src/processSEG/pipeline.nim:619-641: the checks psg_apply
+ * makes before touching a sample, without any device work: a compiled plan,
+ * src (NULL: in place) and dst of rows × cols not overlapping unless they
+ * are the same block, dt_ms the plan's interval (relative 1e-9), cols at
+ * most the plan's samples. PSG_EINVAL with the reference's message. */
+int psg_check_apply(const psg_plan* plan, const void* src, const void* dst, int64_t rows,
+                    int32_t cols, double dt_ms);
 /* --------------------------------------------------------------- apply
  * apply(plan, src, dst, meta, ws), src/processSEG/pipeline.nim:736-772.
  * Device pointers; `src` NULL (or equal to `dst`) runs in place. `live` and

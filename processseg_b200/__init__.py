@@ -38,7 +38,8 @@ from .meta import ChunkMeta, initChunkMeta, liveMeta
 from .plan import PipelinePlan, Workspace, compile, initWorkspace
 from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepHarmonic, SweepPoint, SweepSpec, SweepTaper,
                         applyTaper, dbPerHzSweep, dbPerOctaveSweep, defaultTaperParam, exponentialSweep,
-                        generatePilot, initCorrelationPlan, initPilot, initRecordStack, initSweepTaper,
+                        generatePilot, initCorrelationPlan, initPilot, initRecordStack, initSweepTaper, pilotFromRow,
+                        sweepFromHeaders, sweepOverrides,
                         linearSweep, noTaper, segyTaperType, slDbPerHz, slDbPerOctave, slExponential, slLinear,
                         slTable, sweepHarmonics, tableSweep, taperWeight, tpBlackman, tpBlackmanHarris, tpCos2,
                         tpCosine, tpGaussian, tpHamming, tpKaiser, tpLinear, tpPower)

@@ -193,6 +193,7 @@ def _declare(lib):
         "psg_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, I32, DBL, DBL, DBL, DBL, I32, P,
                                        C.POINTER(I64)]),
         "psg_taper_weight": (C.c_int, [I32, DBL, DBL, C.POINTER(DBL)]),
+        "psg_check_apply": (C.c_int, [P, P, P, I64, I32, DBL]),
         "psg_sweep_validate": (C.c_int, [C.POINTER(SweepC)]),
         "psg_sweep_len": (C.c_int, [C.POINTER(SweepC), C.POINTER(I64)]),
         "psg_sweep_frequency_at": (C.c_int, [C.POINTER(SweepC), DBL, C.POINTER(DBL)]),

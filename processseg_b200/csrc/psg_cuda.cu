@@ -1496,6 +1496,17 @@ static void check_apply(const psg_plan* plan, psg_workspace* ws, const void* src
   }
 }
 
+int psg_check_apply(const psg_plan* plan, const void* src, const void* dst, int64_t rows, int32_t cols, double dt_ms) {
+  return guarded([&] {
+    // the checks apply makes before any sample changes; the rows' liveness
+    // and keys are the caller's, so stand-ins pass their presence checks
+    const int32_t live = 0;
+    const psg_keys keys{};
+    check_apply(plan, nullptr, src, const_cast<void*>(dst), rows, cols, &live, dt_ms, false,
+                plan && plan->needs_keys ? &keys : nullptr);
+  });
+}
+
 int psg_apply(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
               const int32_t* live, const double* start_ms, double dt_ms, void* stream) {
   return psg_apply_keyed(plan, ws, src, dst, rows, cols, live, start_ms, nullptr, dt_ms, stream);

@@ -155,6 +155,26 @@ class PipelinePlan:
             if not x.flags.c_contiguous:
                 raise ValueError(f"{name} must be C-contiguous (row-major)")
 
+    def checkApply(self, src, dst, meta: ChunkMeta):
+        """pipeline.nim:619-641: the checks ``apply`` makes before touching a
+        sample (src None: in place), raising ``ValueError``: the shapes and
+        sample types, the meta's rows, src and dst overlapping without being
+        the same block, the interval and the width."""
+        if self.h is None:
+            raise ValueError("a PipelinePlan must come from compile")
+        self._check_block(dst, "dst")
+        rows, cols = int(dst.shape[0]), int(dst.shape[1])
+        if src is not None:
+            self._check_block(src, "src")
+            if tuple(src.shape) != tuple(dst.shape):
+                raise ValueError(f"src is {src.shape[0]} × {src.shape[1]}, dst {rows} × {cols}")
+            if _is_torch(src) != _is_torch(dst):
+                raise ValueError("src and dst must both be CUDA tensors or both numpy arrays")
+        meta.checkShape(rows)
+        ptr = (lambda a: a.data_ptr()) if _is_torch(dst) else (lambda a: a.ctypes.data)
+        A.check(A.lib().psg_check_apply(self.h, None if src is None else ptr(src), ptr(dst), rows, cols,
+                                        meta.dtMs))
+
     def apply(self, *args, stream=None, wait=True):
         """``apply(b, meta, ws)`` in place, or ``apply(src, dst, meta, ws)``
         from src into dst (pipeline.nim:736-772). With host arrays and

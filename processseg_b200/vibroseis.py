@@ -14,7 +14,7 @@ from typing import Optional
 import numpy as np
 
 from . import _abi as A
-from .meta import ChunkMeta
+from .meta import ChunkMeta, same_interval
 
 tpLinear, tpCosine, tpCos2, tpHamming, tpBlackman, tpBlackmanHarris, tpKaiser, tpGaussian, tpPower = range(9)
 
@@ -250,7 +250,8 @@ def tableSweep(points, dtMs, taper: SweepTaper = None, startPhaseDeg=0.0, amplit
 
 @dataclass
 class Pilot:
-    """pilot.nim:55-62."""
+    """A pilot sweep: its samples at ``dtMs``, sample 0 at ``t0Ms`` from the
+    time break, and the sweep it is when known (pilot.nim:55-62)."""
     samples: np.ndarray
     dtMs: float
     t0Ms: float = 0.0
@@ -259,13 +260,115 @@ class Pilot:
     def __len__(self):
         return int(self.samples.size)
 
+    @property
+    def lengthMs(self) -> float:
+        """``len·dtMs`` (pilot.nim:84-87)."""
+        return float(self.samples.size) * self.dtMs if self.samples.size > 0 else 0.0
+
+    def validate(self):
+        """pilot.nim:89-106: at least two samples, all finite, not all zero; a
+        finite positive ``dtMs``; a finite ``t0Ms``; the sweep's ``dtMs`` equal
+        to the pilot's. Raises ``ValueError``."""
+        x = np.asarray(self.samples, dtype=np.float64).reshape(-1)
+        if x.size < 2:
+            raise ValueError(f"a pilot needs at least two samples, got {x.size}")
+        if not (self.dtMs > 0 and self.dtMs < math.inf):
+            raise ValueError(f"a pilot's dtMs must be finite and positive, got {self.dtMs}")
+        if not math.isfinite(self.t0Ms):
+            raise ValueError(f"a pilot's t0Ms must be finite, got {self.t0Ms}")
+        bad = np.flatnonzero(~np.isfinite(x))
+        if bad.size:
+            raise ValueError(f"pilot sample {int(bad[0])} is not finite")
+        if not np.any(x != 0):
+            raise ValueError("the pilot is all zeros")
+        if self.sweep is not None and not same_interval(self.sweep.dtMs, self.dtMs):
+            raise ValueError(f"the pilot's sweep is sampled at {self.sweep.dtMs} ms, the pilot at {self.dtMs} ms")
+
 
 def generatePilot(spec: SweepSpec, dtype=np.float64) -> Pilot:
+    """The pilot of ``spec`` from ``t0Ms = 0``, with ``sweep`` set
+    (pilot.nim:115-119). Raises ``ValueError`` for an invalid spec."""
     return Pilot(spec.samples(dtype), spec.dtMs, 0.0, spec)
 
 
-def initPilot(samples, dtMs, t0Ms=0.0) -> Pilot:
-    return Pilot(np.asarray(samples), float(dtMs), float(t0Ms))
+def initPilot(samples, dtMs, t0Ms=0.0, sweep: Optional[SweepSpec] = None) -> Pilot:
+    """A pilot from samples the caller has (pilot.nim:108-113). Raises
+    ``ValueError`` as ``Pilot.validate``."""
+    p = Pilot(np.asarray(samples), float(dtMs), float(t0Ms), sweep)
+    p.validate()
+    return p
+
+
+def pilotFromRow(meta: ChunkMeta, data, row: int, t0Ms: float = math.nan,
+                 sweep: Optional[SweepSpec] = None) -> Pilot:
+    """The pilot recorded in row ``row`` of a block (pilot.nim:121-141): its
+    live samples, the meta's ``dtMs`` and its start time (that of column 0,
+    ``firstSample`` included) unless ``t0Ms`` is given. The row need not be
+    live but must not be a failed one. ``data`` is a numpy array or a tensor
+    ``[rows, cols]``."""
+    rows = int(data.shape[0])
+    meta.checkShape(rows)
+    if not 0 <= row < len(meta):
+        raise ValueError(f"row {row} is outside 0 ..< {len(meta)}")
+    if meta.isFailed(row):
+        raise ValueError(f"row {row} could not be decoded")
+    n = meta.liveSamples(row, int(data.shape[1]))
+    r = data[row, :n]
+    s = r.detach().cpu().numpy().copy() if hasattr(r, "detach") else np.array(r, copy=True)
+    t0 = meta.sampleTimeMs(row, 0) if math.isnan(t0Ms) else float(t0Ms)
+    if math.isnan(t0):
+        raise ValueError(f"row {row} has no start time in its keys: pass t0Ms")
+    return initPilot(s, meta.dtMs, t0, sweep)
+
+
+def _int16_field(v: float, what: str, unit: str) -> int:
+    r = math.floor(abs(v) + 0.5) * (1 if v >= 0 else -1) if math.isfinite(v) else v
+    if not (-32768 <= r <= 32767):
+        raise ValueError(f"{what} = {v} does not fit a SEG-Y int16 field")
+    if abs(v - r) > 1e-9 * max(1.0, abs(r)):
+        raise ValueError(f"{what} = {v} {unit} is not a whole number: the SEG-Y sweep fields hold whole {unit}, "
+                         "and a rounded value would be read back as the sweep (write the trace without them)")
+    return int(r)
+
+
+def sweepOverrides(spec: SweepSpec, binary: bool = False):
+    """The SEG-Y sweep fields of ``spec`` as (name, value) pairs, trace bytes
+    127-140 or with ``binary`` the binary header's 3233-3248 (pilot.nim:
+    164-184): whole Hz and ms, ``ValueError`` for a value that is not a whole
+    number or does not fit an int16."""
+    pre = "binary." if binary else "trace."
+    t = spec.taper
+    ts = 0.0 if math.isnan(t.startMs) else t.startMs
+    te = 0.0 if math.isnan(t.endMs) else t.endMs
+    return [(pre + "sweepFreqStart", _int16_field(spec.f1Hz, "f1Hz", "Hz")),
+            (pre + "sweepFreqEnd", _int16_field(spec.f2Hz, "f2Hz", "Hz")),
+            (pre + "sweepLength", _int16_field(spec.lengthMs, "lengthMs", "ms")),
+            (pre + "sweepType", spec.segySweepType()),
+            (pre + "sweepTaperStart", _int16_field(ts, "taper startMs", "ms")),
+            (pre + "sweepTaperEnd", _int16_field(te, "taper endMs", "ms")),
+            (pre + "taperType", t.segyTaperType())]
+
+
+def sweepFromHeaders(f1Hz, f2Hz, lengthMs, sweepType, taperStartMs, taperEndMs, taperType, dtMs,
+                     samples: int = 0) -> Optional[SweepSpec]:
+    """The sweep SEG-Y sweep fields describe when a trace at ``dtMs`` can hold
+    it (pilot.nim:186-212): type 1 (linear) or 3 (exponential), valid at
+    ``dtMs`` with frequencies up to Nyquist, and with ``samples`` no longer
+    than the trace; else None. The ramps are linear for taper type 1, cos²
+    otherwise."""
+    if sweepType not in (1.0, 3.0) or not (dtMs > 0 and dtMs < math.inf):
+        return None
+    if samples > 0 and not (lengthMs <= float(samples) * dtMs):
+        return None
+    spec = SweepSpec(f1Hz, f2Hz, lengthMs, dtMs,
+                     SweepTaper(max(taperStartMs, 0.0), max(taperEndMs, 0.0),
+                                tpLinear if taperType == 1 else tpCos2, math.nan),
+                     0.0, 1.0, 1.0, slLinear if sweepType == 1 else slExponential)
+    try:
+        spec.validate()
+    except ValueError:
+        return None
+    return spec
 
 
 class CorrelationPlan:

@@ -505,3 +505,38 @@ def test_async_host_applies_across_layouts(monkeypatch):
     ws.synchronize()
     for i, (_, _, dst, _, want) in enumerate(cases):
         assert np.array_equal(dst.numpy(), want), i
+
+
+def test_check_apply_refuses_what_apply_refuses():
+    """checkApply (pipeline.nim:619-641) raises the ValueError apply would,
+    for device tensors and host arrays alike, and touches no sample."""
+    plan = P.initPipeline(C1_FLOW).compile(P.float32, 2.0, 2001)
+    meta = P.liveMeta(8, 2001, 2.0)
+    x = torch.randn(16, 2001, device="cuda")
+    src, dst = x[:8], torch.empty(8, 2001, device="cuda")
+    before = x.clone()
+    plan.checkApply(src, dst, meta)
+    plan.checkApply(None, dst, meta)
+    plan.checkApply(dst, dst, meta)  # the same block: in place
+    bad = [
+        (lambda: plan.checkApply(x[:8], x[4:12], meta), "overlap"),
+        (lambda: plan.checkApply(src, dst, P.liveMeta(8, 2001, 4.0)), "dtMs"),
+        (lambda: plan.checkApply(None, torch.empty(8, 2002, device="cuda"), meta), "columns"),
+        (lambda: plan.checkApply(None, dst, P.liveMeta(9, 2001, 2.0)), "rows"),
+        (lambda: plan.checkApply(None, dst.double(), meta), "float"),
+        (lambda: plan.checkApply(torch.empty(8, 100, device="cuda"), dst, meta), "×"),
+    ]
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=8, cols=2001)
+    for f, what in bad:
+        with pytest.raises(ValueError, match=what):
+            f()
+    # apply refuses the same overlap before any sample changes
+    with pytest.raises(ValueError, match="overlap"):
+        plan.apply(x[:8], x[4:12], meta, ws)
+    torch.cuda.synchronize()
+    assert torch.equal(x, before)
+    h = np.zeros((8, 2001), np.float32)
+    plan.checkApply(h.copy(), h, meta)
+    with pytest.raises(ValueError, match="dtMs"):
+        plan.checkApply(None, h, P.liveMeta(8, 2001, 1.0))
