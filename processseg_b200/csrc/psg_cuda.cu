@@ -305,8 +305,8 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
       __syncthreads();
       constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
       const int zo = cfft_forward<T, MAXR>(mem, 0, m, a.fft, tw);
-      split_bridge<T>(mem, zo, m, reinterpret_cast<const Quad<T>*>(a.bridge));
-      y = buf + cfft_forward<T, MAXR>(mem, zo, zo == 0 ? m : 0, a.fft, tw);
+      const BridgeLoad<T, M> bridge{mem, zo, m, reinterpret_cast<const Quad<T>*>(a.bridge)};
+      y = buf + cfft_forward_loaded<T, MAXR, 0>(mem, zo == 0 ? m : 0, zo, a.fft, tw, bridge);
     }
     // lagSpans / scatter: the output at column c reads lag c + shift
     // (wrapped by nfft for negative lags).
@@ -726,7 +726,7 @@ static std::vector<typename C2<T>::type> as_c(const std::vector<double>& re, con
   for (size_t i = 0; i < re.size(); i++) o[i] = {(T)re[i], (T)im[i]};
   return o;
 }
-// The split · multiplier · unsplit map of each pair of bins (split_bridge):
+// The split · multiplier · unsplit map of each pair of bins (BridgeLoad):
 // for k ≥ 1, with ω = exp(−2πik/n), c1 = 1 + i·conj ω, c2 = 1 − i·conj ω,
 // a1 = (1 − iω)/2, a2 = (1 + iω)/2 and j = m − k:
 //   A = c1·a1·M[k] + c2·conj(c2)/2·conj M[j],  B = c1·a2·M[k] + c2·conj(c1)/2·conj M[j],

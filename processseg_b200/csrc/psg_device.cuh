@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "psg_dft_consts.h"
 
 namespace psgd {
@@ -249,49 +251,39 @@ struct FftDesc {
   unsigned magic[24];  // ⌈2^32 / s⌉ of each pass, 0 for s = 1
 };
 
-// Forward complex FFT of the m points at offset `ao`, `bo` the second
-// buffer. Returns the offset holding the result; ends with a
-// __syncthreads(). MAXR bounds the radices compiled in (and with them the
-// registers a pass needs); the plan's factorization never uses a larger one.
-// NT: the CTA's thread count when known at compile time (0: blockDim.x).
-template <class T, int MAXR, int NT = 0, class M>
-__device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const FftDesc& d,
-                                         const typename C2<T>::type* tw) {
-  int x = ao, y = bo;
-  int cur = d.m, s = 1;
-  for (int i = 0; i < d.npass; i++) {
+// Runs f(std::integral_constant<int, R>) for the plan's radix r at run time;
+// radices above MAXR are not compiled in (the plan never uses them).
+template <int MAXR, class F> __device__ __forceinline__ void with_radix(int r, F&& f) {
+  switch (r) {
+    case 16: if constexpr (MAXR >= 16) f(std::integral_constant<int, 16>{}); break;
+    case 15: if constexpr (MAXR >= 15) f(std::integral_constant<int, 15>{}); break;
+    case 12: if constexpr (MAXR >= 12) f(std::integral_constant<int, 12>{}); break;
+    case 10: if constexpr (MAXR >= 10) f(std::integral_constant<int, 10>{}); break;
+    case 9: if constexpr (MAXR >= 9) f(std::integral_constant<int, 9>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    default: f(std::integral_constant<int, 2>{}); break;
+  }
+}
+
+// The passes i0 .. npass − 1 of a transform, from the buffer at x (the
+// other at y), `cur` points per sub-transform and stride s at pass i0.
+// Returns the offset holding the result; each pass ends with a
+// __syncthreads().
+template <class T, int MAXR, int NT, class M>
+__device__ __forceinline__ int cfft_passes(const M& mem, int x, int y, const FftDesc& d,
+                                        const typename C2<T>::type* tw, int i0, int cur, int s) {
+  for (int i = i0; i < d.npass; i++) {
     const int r = d.radix[i];
     const int sub = cur / r;
     const unsigned mg = d.magic[i];
-    if (sub == 1) {
-      switch (r) {
-        case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 8: fft_pass<8, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 6: fft_pass<6, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 5: fft_pass<5, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 4: fft_pass<4, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        case 3: fft_pass<3, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-        default: fft_pass<2, T, NT, true>(mem, x, y, s, sub, mg, tw); break;
-      }
-    } else {
-      switch (r) {
-        case 16: if (MAXR >= 16) fft_pass<(MAXR >= 16 ? 16 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 15: if (MAXR >= 15) fft_pass<(MAXR >= 15 ? 15 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 12: if (MAXR >= 12) fft_pass<(MAXR >= 12 ? 12 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 10: if (MAXR >= 10) fft_pass<(MAXR >= 10 ? 10 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 9: if (MAXR >= 9) fft_pass<(MAXR >= 9 ? 9 : 2), T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 8: fft_pass<8, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 6: fft_pass<6, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 5: fft_pass<5, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 4: fft_pass<4, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        case 3: fft_pass<3, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-        default: fft_pass<2, T, NT, false>(mem, x, y, s, sub, mg, tw); break;
-      }
-    }
+    with_radix<MAXR>(r, [&](auto R) {
+      if (sub == 1) fft_pass<decltype(R)::value, T, NT, true>(mem, x, y, s, sub, mg, tw);
+      else fft_pass<decltype(R)::value, T, NT, false>(mem, x, y, s, sub, mg, tw);
+    });
     __syncthreads();
     cur = sub;
     s *= r;
@@ -300,6 +292,58 @@ __device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const 
     y = tmp;
   }
   return x;
+}
+
+// Forward complex FFT of the m points at offset `ao`, `bo` the second
+// buffer. Returns the offset holding the result; ends with a
+// __syncthreads(). MAXR bounds the radices compiled in (and with them the
+// registers a pass needs); the plan's factorization never uses a larger one.
+// NT: the CTA's thread count when known at compile time (0: blockDim.x).
+template <class T, int MAXR, int NT = 0, class M>
+__device__ __forceinline__ int cfft_forward(const M& mem, int ao, int bo, const FftDesc& d,
+                                         const typename C2<T>::type* tw) {
+  return cfft_passes<T, MAXR, NT>(mem, ao, bo, d, tw, 0, d.m, 1);
+}
+
+// The first pass (stride 1) with its inputs from ld(c, j == 0), the c-th
+// complex input of the transform (c = p + j·sub, so c = 0 only for j = 0),
+// instead of a buffer: the pass that fuses its inputs' producer into its
+// loads. The outputs go to the buffer at yo.
+template <int R, class T, int NT, bool LAST, class M, class LD>
+__device__ __forceinline__ void fft_pass_loaded(const M& mem, int yo, int sub, const typename C2<T>::type* __restrict__ tw,
+                                                const LD& ld) {
+  const int nt = NT ? NT : (int)blockDim.x;
+  typedef typename C2<T>::type V;
+  V* buf = reinterpret_cast<V*>(mem.base());
+  for (int p = threadIdx.x; p < sub; p += nt) {
+    V v[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) v[j] = ld(p + j * sub, j == 0);
+    Dft<V, T, R>::run(v);
+    if (!LAST) {
+#pragma unroll
+      for (int k = 1; k < R; k++) v[k] = cmul(v[k], __ldg(&tw[p * k]));
+    }
+    V* y = buf + (yo + R * p);
+#pragma unroll
+    for (int k = 0; k < R; k++) y[k] = v[k];
+  }
+}
+
+// Forward complex FFT whose m inputs come from ld (as fft_pass_loaded) rather
+// than a buffer; `bo` and `ao` are the two work buffers (the first pass
+// writes bo, so ld may read ao). Returns the offset holding the result.
+template <class T, int MAXR, int NT, class M, class LD>
+__device__ __forceinline__ int cfft_forward_loaded(const M& mem, int bo, int ao, const FftDesc& d,
+                                                const typename C2<T>::type* tw, const LD& ld) {
+  const int r = d.radix[0];
+  const int sub = d.m / r;
+  with_radix<MAXR>(r, [&](auto R) {
+    if (sub == 1) fft_pass_loaded<decltype(R)::value, T, NT, true>(mem, bo, sub, tw, ld);
+    else fft_pass_loaded<decltype(R)::value, T, NT, false>(mem, bo, sub, tw, ld);
+  });
+  __syncthreads();
+  return cfft_passes<T, MAXR, NT>(mem, bo, ao, d, tw, 1, sub, r);
 }
 
 // Four values of T: a bin's pair of complex coefficients.
@@ -316,29 +360,28 @@ template <class T> struct alignas(4 * sizeof(T)) Quad { T x, y, z, w; };
 // M[k], M[m − k] and 1/n (bridge_table). Bin 0 keeps the reference's real
 // forms of the DC and Nyquist bins (the imaginary parts of M·X there are
 // dropped): ab[0] = (Re M[0]/n, Re M[m]/n).
-template <class T, int NT = 0, class M>
-__device__ __forceinline__ void split_bridge(const M& mem, int zo, int m, const Quad<T>* __restrict__ ab) {
+// z'[c] is computed where it is read: the first pass of the inverse transform
+// loads its inputs through BridgeLoad instead of a buffer (a pass, a barrier
+// and a store per bin fewer than bridging in place). Reads z at zo.
+template <class T, class M> struct BridgeLoad {
   typedef typename C2<T>::type V;
-  V* z = reinterpret_cast<V*>(mem.base()) + zo;
-  const int nt = NT ? NT : (int)blockDim.x;
-  for (int k = threadIdx.x; k <= m / 2; k += nt) {
-    if (k == 0) {
+  const M& mem;
+  int zo, m;
+  const Quad<T>* __restrict__ ab;
+  __device__ __forceinline__ V operator()(int c, bool maybe_zero) const {
+    const V* z = reinterpret_cast<const V*>(mem.base()) + zo;
+    if (maybe_zero && c == 0) {
       const V z0 = z[0];
-      const Quad<T> c = ab[0];
-      const T x0 = (z0.x + z0.y) * c.x, xm = (z0.x - z0.y) * c.y;
-      z[0] = {x0 - xm, x0 + xm};
-      continue;
+      const Quad<T> q = ab[0];
+      const T x0 = (z0.x + z0.y) * q.x, xm = (z0.x - z0.y) * q.y;
+      return V{x0 - xm, x0 + xm};
     }
-    const int j = m - k;
-    const V a = z[k], b = z[j];
-    const Quad<T> ck = ab[k], cj = ab[j];
+    const V a = z[c], b = z[m - c];
+    const Quad<T> q = ab[c];
     // A·conj(a) + B·b
-    z[k] = {ck.x * a.x + ck.y * a.y + ck.z * b.x - ck.w * b.y, ck.y * a.x - ck.x * a.y + ck.z * b.y + ck.w * b.x};
-    if (j != k)
-      z[j] = {cj.x * b.x + cj.y * b.y + cj.z * a.x - cj.w * a.y, cj.y * b.x - cj.x * b.y + cj.z * a.y + cj.w * a.x};
+    return V{q.x * a.x + q.y * a.y + q.z * b.x - q.w * b.y, q.y * a.x - q.x * a.y + q.z * b.y + q.w * b.x};
   }
-  __syncthreads();
-}
+};
 
 // ------------------------------------------------- bulk copies (TMA, 1-D)
 // A row moves from global into shared memory with one cp.async.bulk issued

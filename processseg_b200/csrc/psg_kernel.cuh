@@ -370,8 +370,9 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
   __syncthreads();
   const V* tw = reinterpret_cast<const V*>(st.tw);
   const int zo = cfft_forward<T, MAXR, kNT>(mem, ao, bo, st.fft, tw);
-  split_bridge<T, kNT>(mem, zo, m, reinterpret_cast<const Quad<T>*>(st.bridge));
-  const int yo = cfft_forward<T, MAXR, kNT>(mem, zo, zo == ao ? bo : ao, st.fft, tw);
+  // the real-FFT bridge fused into the inverse transform's first pass
+  const BridgeLoad<T, M> bridge{mem, zo, m, reinterpret_cast<const Quad<T>*>(st.bridge)};
+  const int yo = cfft_forward_loaded<T, MAXR, kNT>(mem, zo == ao ? bo : ao, zo, st.fft, tw, bridge);
   // unpackFrom: the output is swap(y): sample 2k is y[k].im and 2k + 1 is
   // y[k].re, so sample j of the real view is Yr[j ^ 1].
   const T* Yr = reinterpret_cast<const T*>(reinterpret_cast<const V*>(mem.base()) + yo);
