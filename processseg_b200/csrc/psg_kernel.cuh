@@ -331,6 +331,23 @@ __device__ __forceinline__ void trend_from(int trend, const Stats& st, int n, do
 // NEED_K: the next step's statistics when known at compile time. The two
 // transform buffers are at byte `work_off` of `mem` (shared memory, or a
 // CTA's slice of global memory for traces too long for it).
+// packInto's value of complex input c of the forward transform (real
+// samples 2c and 2c + 1 of the padded trace) for zero pads: the detrended
+// sample x[k − p] − (a + b·(k − p)) in float64 rounded to T inside the trace,
+// 0 in the pads.
+template <class T> struct PackLoad {
+  typedef typename C2<T>::type V;
+  const T* X;
+  int n, p;
+  T pre;
+  double a, b;
+  __device__ __forceinline__ T at(int k) const {
+    const int i = k - p;
+    return (unsigned)i < (unsigned)n ? (T)((double)(X[i] - pre) - (a + b * (double)i)) : (T)0;
+  }
+  __device__ __forceinline__ V operator()(int c, bool) const { return V{at(2 * c), at(2 * c + 1)}; }
+};
+
 template <class T, int MAXR, int NEED_K = -1, class M = InShared>
 __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in, T* X, int n, int work_off, Shared& S,
                                              T pre = (T)0, const M& mem = M()) {
@@ -340,14 +357,21 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
   V* A = reinterpret_cast<V*>(mem.base()) + ao;
   double a, b;
   trend_from(st.trend, in, n, a, b);
-  const T* fall = reinterpret_cast<const T*>(st.fall);
-  T* Ar = reinterpret_cast<T*>(A);
-  // packInto: the detrended samples at p .. p+n (a loop of its own, so that
-  // the pads' arithmetic is not evaluated for them), then the pads — odd
-  // reflections tapered by `fall`, or zeros — and zeros to nfft.
-  for (int i = threadIdx.x; i < n; i += kNT) Ar[p + i] = (T)((double)(X[i] - pre) - (a + b * (double)i));
-  const int rest = nfft - n;  // [0, p) and [p + n, nfft)
-  if (st.reflect) {
+  const V* tw = reinterpret_cast<const V*>(st.tw);
+  int zo;
+  if (!st.reflect) {
+    // packInto with zero pads: each value is computed where the forward
+    // transform's first pass reads it (PackLoad) rather than stored first
+    const PackLoad<T> pack{X, n, p, pre, a, b};
+    zo = cfft_forward_loaded<T, MAXR, kNT>(mem, bo, ao, st.fft, tw, pack);
+  } else {
+    // packInto with reflected pads: the detrended samples at p .. p+n (a loop
+    // of its own, so that the pads' arithmetic is not evaluated for them),
+    // then the odd reflections tapered by `fall`, and zeros to nfft
+    const T* fall = reinterpret_cast<const T*>(st.fall);
+    T* Ar = reinterpret_cast<T*>(A);
+    for (int i = threadIdx.x; i < n; i += kNT) Ar[p + i] = (T)((double)(X[i] - pre) - (a + b * (double)i));
+    const int rest = nfft - n;  // [0, p) and [p + n, nfft)
     const T d0 = (T)((double)(X[0] - pre) - a);
     const T dn = (T)((double)(X[n - 1] - pre) - (a + b * (double)(n - 1)));
     for (int t = threadIdx.x; t < rest; t += kNT) {
@@ -364,12 +388,9 @@ __device__ __forceinline__ Stats step_filter(const DevStep& st, const Stats& in,
       }
       Ar[j] = v;
     }
-  } else {
-    for (int t = threadIdx.x; t < rest; t += kNT) Ar[t < p ? t : t + n] = (T)0;
+    __syncthreads();
+    zo = cfft_forward<T, MAXR, kNT>(mem, ao, bo, st.fft, tw);
   }
-  __syncthreads();
-  const V* tw = reinterpret_cast<const V*>(st.tw);
-  const int zo = cfft_forward<T, MAXR, kNT>(mem, ao, bo, st.fft, tw);
   // the real-FFT bridge fused into the inverse transform's first pass
   const BridgeLoad<T, M> bridge{mem, zo, m, reinterpret_cast<const Quad<T>*>(st.bridge)};
   const int yo = cfft_forward_loaded<T, MAXR, kNT>(mem, zo == ao ? bo : ao, zo, st.fft, tw, bridge);
