@@ -268,6 +268,18 @@ struct CorrArgs {
   int stack_on;
 };
 
+// Complex input c of a record's forward transform: samples 2c and 2c + 1
+// of the record (read-only global memory), 0 past its n samples.
+template <class T> struct RecordLoad {
+  typedef typename C2<T>::type V;
+  const T* x;
+  int n;
+  __device__ __forceinline__ V operator()(int c, bool) const {
+    const int k = 2 * c;
+    return V{k < n ? __ldg(x + k) : (T)0, k + 1 < n ? __ldg(x + k + 1) : (T)0};
+  }
+};
+
 // correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
 // pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
 template <class T, class M>
@@ -286,25 +298,11 @@ __device__ __forceinline__ void corr_rows(const CorrArgs& a, const M& mem, Share
     const V* y = nullptr;
     if (n > 0) {
       const T* x = src + r * (long long)a.cols;
-      T* Ar = reinterpret_cast<T*>(buf);
-      // the record: 16-byte loads over its aligned body, element loads at the
-      // ends, zeros to nfft
-      constexpr int per = 16 / (int)sizeof(T);
-      const int head = min((int)(((16 - ((uintptr_t)x & 15)) & 15) / sizeof(T)), n);
-      const int nv = (n - head) / per, tail0 = head + nv * per;
-      typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type Q;
-      const Q* xv = reinterpret_cast<const Q*>(x + head);
-      for (int v = threadIdx.x; v < nv; v += blockDim.x) {
-        const Q q = __ldg(xv + v);
-        const T* e = reinterpret_cast<const T*>(&q);
-#pragma unroll
-        for (int u = 0; u < per; u++) Ar[head + per * v + u] = e[u];
-      }
-      for (int j = threadIdx.x; j < head; j += blockDim.x) Ar[j] = x[j];
-      for (int j = tail0 + threadIdx.x; j < a.nfft; j += blockDim.x) Ar[j] = j < n ? x[j] : (T)0;
-      __syncthreads();
+      // the record, zero-padded to nfft, read by the forward transform's
+      // first pass straight from global memory (RecordLoad)
       constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
-      const int zo = cfft_forward<T, MAXR>(mem, 0, m, a.fft, tw);
+      const RecordLoad<T> rec{x, n};
+      const int zo = cfft_forward_loaded<T, MAXR, 0>(mem, m, 0, a.fft, tw, rec);
       const BridgeLoad<T, M> bridge{mem, zo, m, reinterpret_cast<const Quad<T>*>(a.bridge)};
       y = buf + cfft_forward_loaded<T, MAXR, 0>(mem, zo == 0 ? m : 0, zo, a.fft, tw, bridge);
     }
