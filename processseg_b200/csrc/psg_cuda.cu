@@ -427,6 +427,27 @@ struct SpecArgs {
 // transform in the CTA's buffers, and per bin either the scaled power added
 // to this CTA's accumulator (AVG; rows in order, so the sums are the same on
 // every run) or the scaled amplitude and the phase of the row.
+// Complex input c of a window's forward transform: (x[j] − mean)·w[j] for
+// j < n (w the window's taper, min(w[j], w[n − 1 − j]) for a short window),
+// 0 up to nfft; samples 2c and 2c + 1 for an even nfft, sample c (real) for
+// an odd one.
+template <class T> struct WindowLoad {
+  typedef typename C2<T>::type V;
+  const T* x;
+  const T* taper;
+  int n, W;
+  T mean;
+  bool odd;
+  __device__ __forceinline__ T at(int j) const {
+    if (j >= n) return (T)0;
+    const T w = n == W ? __ldg(taper + j) : min(__ldg(taper + j), __ldg(taper + n - 1 - j));
+    return (__ldg(x + j) - mean) * w;
+  }
+  __device__ __forceinline__ V operator()(int c, bool) const {
+    return odd ? V{at(c), (T)0} : V{at(2 * c), at(2 * c + 1)};
+  }
+};
+
 template <class T, bool AVG, class M>
 __device__ __forceinline__ void spectrum_rows(const SpecArgs& a, const M& mem, SharedMem& S) {
   typedef typename C2<T>::type V;
@@ -448,24 +469,20 @@ __device__ __forceinline__ void spectrum_rows(const SpecArgs& a, const M& mem, S
     sum = block_sum(sum, S.red[0][0]);
     const bool finite = sum - sum == 0;
     const T mean = a.demean && n > 0 && finite ? (T)(sum / (double)n) : (T)0;
-    double sw = 0;
-    T* Ar = reinterpret_cast<T*>(buf);
-    for (int j = threadIdx.x; j < n2; j += blockDim.x) {
-      T v = (T)0;
-      if (j < n) {
-        const T w = n == W ? taper[j] : min(taper[j], taper[n - 1 - j]);
-        v = (x[j] - mean) * w;
-        if (n != W) sw += (double)w;
-      }
-      if (a.odd) buf[j] = V{v, (T)0};
-      else Ar[j] = v;
+    double sw = a.taper_sum;
+    if (n != W) {
+      // a short window: its own taper, min(w[j], w[n − 1 − j]), and its sum
+      sw = 0;
+      for (int j = threadIdx.x; j < n; j += blockDim.x) sw += (double)min(taper[j], taper[n - 1 - j]);
+      sw = block_sum(sw, S.red[1][0]);
     }
-    sw = n == W ? a.taper_sum : block_sum(sw, S.red[1][0]);
     if (!finite) sw = NAN;
     if (AVG && !(sw > 0)) continue;  // a NaN or infinite sample: the row is left out
-    __syncthreads();
+    // the demeaned, tapered window, zero-padded to nfft, read by the forward
+    // transform's first pass straight from global memory (WindowLoad)
     constexpr int MAXR = sizeof(T) == 4 ? 16 : 8;
-    const V* z = buf + cfft_forward<T, MAXR>(mem, 0, mc, a.fft, tw);
+    const WindowLoad<T> win{x, taper, n, W, mean, (bool)a.odd};
+    const V* z = buf + cfft_forward_loaded<T, MAXR, 0>(mem, mc, 0, a.fft, tw, win);
     const double sc = AVG ? 1 / (sw * sw) : 0.0;
     for (int k = threadIdx.x; k < a.bins; k += blockDim.x) {
       T re, im;
