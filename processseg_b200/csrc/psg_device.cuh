@@ -336,6 +336,14 @@ __device__ __forceinline__ void fft_pass_loaded(const M& mem, int yo, int sub, c
 template <class T, int MAXR, int NT, class M, class LD>
 __device__ __forceinline__ int cfft_forward_loaded(const M& mem, int bo, int ao, const FftDesc& d,
                                                 const typename C2<T>::type* tw, const LD& ld) {
+  if (d.npass == 0) {
+    // a transform of one point (no passes): the input itself, in bo
+    typedef typename C2<T>::type V;
+    V* buf = reinterpret_cast<V*>(mem.base());
+    for (int c = threadIdx.x; c < d.m; c += (NT ? NT : (int)blockDim.x)) buf[bo + c] = ld(c, true);
+    __syncthreads();
+    return bo;
+  }
   const int r = d.radix[0];
   const int sub = d.m / r;
   with_radix<MAXR>(r, [&](auto R) {
