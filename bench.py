@@ -100,22 +100,123 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(steps=3, warmup=1):
+def config(world):
+    """The workload's config, the same dict in both arms."""
+    return {"workload": WORKLOAD, "rows": ROWS, "cols": COLS, "parallelism": f"traces x{world}",
+            "l2": "inputs larger than L2: 8 rotating src/dst panel pairs (384 MB)"}
+
+
+def cpu_baseline(warmup=3, samples=15, min_sample_ms=20.0):
     """The oracle (the C++ restatement of the reference's path) through its
-    ProcessPool clone on all host cores, on the same panel."""
+    ProcessPool clone on the same panel, timed by the reference harness's
+    method (bench/benchutil.nim:96-126: 3 warm-up applies, then 15 samples of
+    doubling batches of at least 20 ms each; median and minimum), on all host
+    cores and on one thread. Only the oracle's library is loaded: the rows are
+    flattened by the oracle and the ops are plain descriptors."""
+    from processseg_b200 import synth
+    import processseg_b200 as P
+    from oracle import oracle as O
+    g = synth.c2()
+    live, start = O.rows_flatten(g.status, g.numSamples, g.t0Ms, 0, DT, g.failed, COLS, 0)
+    plan = O.OraclePlan(flow(), P.F32, DT, COLS)
+    cores = os.cpu_count() or 1
+    med, mn, n = plan.bench(g.data, live, start, threads=cores, warm=warmup, samples=samples,
+                            min_sample_ms=min_sample_ms)
+    med1, mn1, n1 = plan.bench(g.data, live, start, threads=1, warm=warmup, samples=samples,
+                               min_sample_ms=min_sample_ms)
+    return {"value": ROWS * COLS / med / 1e6, "unit": "Msamples/s", "cores": cores, "kind": "port",
+            "sample": f"the full 2000x3001 panel: {warmup} warm-up applies, then {samples} samples of >= "
+                      f"{min_sample_ms:g} ms ({n} applies), median {med * 1e3:.2f} ms (min {mn * 1e3:.2f} ms) "
+                      f"on {cores} threads of the ProcessPool clone",
+            "method": "bench/benchutil.nim:96-126 (3 warm-ups, 15 samples >= 20 ms, median)",
+            "samples": samples,
+            "one_thread": {"value": ROWS * COLS / med1 / 1e6, "unit": "Msamples/s", "cores": 1,
+                           "median_ms": med1 * 1e3, "min_ms": mn1 * 1e3, "applies": n1},
+            "all_cores": {"median_ms": med * 1e3, "min_ms": mn * 1e3, "applies": n}}
+
+
+def trace_errors(got, want, live):
+    """Per trace with live samples: max |got - want| over its live samples
+    divided by the RMS of ``want`` there (the reference's error measure)."""
     import numpy as np
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    cols = want.shape[1]
+    mask = np.arange(cols)[None, :] < np.asarray(live)[:, None]
+    n = mask.sum(axis=1)
+    keep = n > 0
+    rms = np.sqrt(np.where(mask, want * want, 0).sum(axis=1)[keep] / n[keep])
+    err = np.where(mask, np.abs(got - want), 0).max(axis=1)[keep]
+    ok = rms > 0
+    return err[ok] / rms[ok]
+
+
+def error_summary(e, what):
+    import numpy as np
+    return {"max": float(np.max(e)), "p99": float(np.percentile(e, 99)), "mean": float(np.mean(e)),
+            "traces": int(e.size), "above_1e-5": int(np.sum(e > 1e-5)), "of": what}
+
+
+def error_report(dst_c2):
+    """Each output's max error relative to its trace's RMS, against the FP64
+    oracle (and, for parity, against the float32 oracle), computed after the
+    timed region: C2 on the bench's own panel (all 2000 traces, the device
+    output of the timed steps), C3 on a 32-channel gather and C5 on a
+    2000-trace panel of its configuration (same generator, plan and interval)."""
+    import numpy as np
+    import torch
     import processseg_b200 as P
     from processseg_b200 import synth
     from oracle import oracle as O
-    g = synth.c2()
-    meta = g.meta()
-    live, start = meta.flat(COLS)
-    plan = O.OraclePlan(flow(), P.F32, DT, COLS)
     cores = os.cpu_count() or 1
-    med, mn = plan.bench(g.data, live, start, threads=cores, warm=warmup, iters=steps)
-    return {"value": ROWS * COLS / med / 1e6, "unit": "Msamples/s", "cores": cores, "kind": "port",
-            "sample": f"{steps} applies of the full 2000x3001 panel (median {med * 1e3:.1f} ms, "
-                      f"min {mn * 1e3:.1f} ms), ProcessPool clone, {cores} threads"}
+    out = {}
+    g = synth.c2()
+    live, start = O.rows_flatten(g.status, g.numSamples, g.t0Ms, 0, DT, g.failed, COLS, 0)
+    got = dst_c2.cpu().numpy()
+    w64 = O.OraclePlan(flow(), P.F64, DT, COLS).apply(g.data.astype(np.float64), live, start, threads=cores)
+    w32 = O.OraclePlan(flow(), P.F32, DT, COLS).apply(g.data, live, start, threads=cores)
+    out["c2"] = {"vs_fp64": error_summary(trace_errors(got, w64, live), "device float32 vs FP64 oracle"),
+                 "vs_f32_oracle": error_summary(trace_errors(got, w32, live), "device vs float32 oracle"),
+                 "f32_oracle_vs_fp64": error_summary(trace_errors(w32, w64, live), "float32 oracle vs FP64 oracle")}
+    # C5: a 2000-trace panel of the 50000x6001 configuration
+    g5 = synth.c5(rows=2000)
+    flow5 = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(2, 5, 120, 150))), P.agcOp(250),
+             P.normalizeOp(P.normPercentile, P.perTrace, percentile=99.0)]
+    live5, start5 = O.rows_flatten(g5.status, g5.numSamples, g5.t0Ms, 0, 1.0, g5.failed, 6001, 0)
+    plan5 = P.initPipeline(flow5).compile(P.float32, 1.0, 6001)
+    ws = P.initWorkspace()
+    ws.reserve(plan5, rows=2000, cols=6001)
+    s5 = torch.from_numpy(g5.data).cuda()
+    d5 = torch.empty_like(s5)
+    plan5.apply(s5, d5, g5.meta(), ws)
+    got5 = d5.cpu().numpy()
+    w64 = O.OraclePlan(flow5, P.F64, 1.0, 6001).apply(g5.data.astype(np.float64), live5, start5, threads=cores)
+    w32 = O.OraclePlan(flow5, P.F32, 1.0, 6001).apply(g5.data, live5, start5, threads=cores)
+    out["c5"] = {"vs_fp64": error_summary(trace_errors(got5, w64, live5), "device float32 vs FP64 oracle"),
+                 "vs_f32_oracle": error_summary(trace_errors(got5, w32, live5), "device vs float32 oracle"),
+                 "f32_oracle_vs_fp64": error_summary(trace_errors(w32, w64, live5), "float32 oracle vs FP64 oracle"),
+                 "sample": "a 2000x6001 panel of the C5 configuration (synth.c5(rows=2000))"}
+    # C3: one sweep of a 32-channel gather, correlated to 6 s
+    spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
+    pilot = P.generatePilot(spec, np.float64)
+    recs = synth.vibroseis_records(pilot.samples, channels=32, sweeps=1)[0]
+    rows3 = recs.shape[0]
+    meta3 = P.initChunkMeta(np.full(rows3, P.tsLive, np.int32), np.full(rows3, 10001, np.int32), 2.0)
+    cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, 10001, outSamples=3000)
+    x3 = torch.from_numpy(np.ascontiguousarray(recs.astype(np.float32))).cuda()
+    d3 = torch.zeros(rows3, 3000, device="cuda")
+    cplan.correlateInto(x3, d3, meta3)
+    got3 = d3.cpu().numpy()
+    live3 = np.full(rows3, 10001, np.int32)
+    w64, _, _ = O.correlate(pilot.samples, 2.0, 0.0, recs.astype(np.float64), live3, 2.0, 10001, outSamples=3000)
+    w32, _, _ = O.correlate(pilot.samples, 2.0, 0.0, recs.astype(np.float32), live3, 2.0, 10001, outSamples=3000)
+    l3 = np.full(rows3, 3000)
+    out["c3"] = {"vs_fp64": error_summary(trace_errors(got3, w64, l3), "device float32 vs FP64 oracle"),
+                 "vs_f32_oracle": error_summary(trace_errors(got3, w32, l3), "device vs float32 oracle"),
+                 "vs_fp64_of_peak": float(np.max(np.abs(got3 - w64)) / np.max(np.abs(w64))),
+                 "sample": "one sweep of a 32-channel gather (10001 samples, 6 s out)"}
+    out["oracle"] = "the C++ restatement of the reference (oracle/psg_oracle.cpp); parity is against it, not the Nim reference, which cannot run here"
+    return out
 
 
 def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
@@ -327,14 +428,19 @@ def workloads_leg(peak):
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU implementation of the path,
+    here the oracle port (the reference is Nim, which cannot build here),
+    through its ProcessPool clone on all host cores, rank 0 only. It loads
+    no part of the CUDA library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    b = cpu_baseline(steps=max(1, args.steps), warmup=max(1, min(args.warmup, 3)))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    b = cpu_baseline()
     line = {"impl": "reference", "metric": METRIC, "value": b["value"], "unit": "Msamples/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "rows": ROWS, "cols": COLS},
+            "data": "synthetic", "config": config(world),
             "cpu_baseline": b,
             "e2e": {"value": b["value"], "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -452,8 +558,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rows": ROWS, "cols": COLS, "parallelism": f"traces x{world}",
-                       "l2": "inputs larger than L2: 8 rotating src/dst panel pairs (384 MB)"},
+            "config": config(world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "pipeline_kernel<float>", "algorithmic_bytes": alg_bytes},
@@ -482,8 +587,10 @@ def run_ours(args):
             line["serving"] = serving_leg()
         if world == 1 and not args.no_workloads:
             line["workloads"] = workloads_leg(peak)
+        if world == 1 and not args.no_errors:
+            line["error_vs_fp64"] = error_report(dsts[0])
         if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(steps=3, warmup=1)
+            line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -499,6 +606,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-load leg")
     ap.add_argument("--no-workloads", action="store_true", help="skip the C1/C3/C5 legs")
+    ap.add_argument("--no-errors", action="store_true", help="skip the error report against the oracle")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -221,6 +221,9 @@ int64_t psg_plan_workspace_bytes(const psg_plan* plan, int64_t rows, int32_t col
  * entry points. One per thread (or stream) of callers. */
 int psg_workspace_create(psg_workspace** out);
 void psg_workspace_destroy(psg_workspace* ws);
+/* Grows ws for `plan` applied to up to `rows` rows (and the staging of a
+ * host-memory apply `cols` wide); with plan NULL, for the statistics of up to
+ * `rows` rows (psg_panel_stats; panelStatsWorkspace, gain/stats.nim:57-58). */
 int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows,
                           int32_t cols);
 int64_t psg_workspace_bytes(const psg_workspace* ws);
@@ -233,8 +236,11 @@ int64_t psg_workspace_bytes(const psg_workspace* ws);
  * processing rule (live or unknown status, not failed); mode 1 the
  * correlation rule (not dead, not failed: auxiliary rows are correlated,
  * src/processSEG/vibroseis/correlate.nim:442-443); mode 2 every row that is
- * not failed (scaleRows, core/calibrate.nim:575-581). `t0_ms` may be NULL
- * (NaN). */
+ * not failed (scaleRows, core/calibrate.nim:575-581); mode 3 the processing
+ * rule of mode 0 with the rows it does not take marked −1, so that a live row
+ * with no live samples (0) stays apart from a row that is not live
+ * (traceStatsInto, src/processSEG/gain/stats.nim:186-199). `t0_ms` may be
+ * NULL (NaN). */
 int psg_rows_flatten(const int32_t* status, const int32_t* num_samples,
                      const double* t0_ms, int64_t rows, int32_t first_sample,
                      double dt_ms, const int64_t* failed, int64_t n_failed,
@@ -347,13 +353,20 @@ int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double
 
 /* ----------------------------------------------------------- statistics */
 /* traceStatsInto, src/processSEG/gain/stats.nim:186-199: rms and maxAbs per
- * row (NaN for rows with live[r] == 0), device arrays of `rows` doubles. */
+ * row into device arrays of `rows` doubles. `live` is psg_rows_flatten's
+ * mode 3 (on the device): a row with live[r] < 0 is not live and reads NaN
+ * for both; a live row reads the statistics of its first min(live[r], cols)
+ * samples, (0, 0) when it has none (statsOf, stats.nim:124-127). PSG_EINVAL
+ * for a dtype other than PSG_F32 or PSG_F64. */
 int psg_trace_stats(const void* block, int32_t dtype, int64_t rows, int32_t cols,
                     const int32_t* live, double* rms_out, double* max_abs_out,
                     void* stream);
 /* panelStats, src/processSEG/gain/stats.nim:253-304. out (device) receives
  * {rms, maxAbs, clip, rows, samples} as doubles. clip_percentile NaN skips
- * the histogram. */
+ * the histogram. `live` is psg_rows_flatten's mode 3 (on the device): rows
+ * with live[r] < 0 are not live and left out; a live row with no live
+ * samples (0) counts among `rows` and adds no samples, as in the reference.
+ * PSG_EINVAL for a dtype other than PSG_F32 or PSG_F64. */
 int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t rows,
                     int32_t cols, const int32_t* live, double clip_percentile,
                     double* out, void* stream);
@@ -371,7 +384,8 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
  * that first call before any stream capture. Every call shares the one
  * array and it keeps the last call's contents, so calls that overlap on the
  * GPU (on different streams, or from different host threads) race: order
- * them on one stream. */
+ * them on one stream. The cached address does not survive a device reset
+ * (cudaDeviceReset): do not call this again on a device after resetting it. */
 #define PSG_STATIC_MAX_ROWS 65536
 int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32_t cols,
                            const int32_t* live, double clip_percentile, double* out,
@@ -594,8 +608,11 @@ void psg_server_destroy(psg_server* server);
 int psg_submit(psg_server* server, const psg_plan* plan, const void* src_host, void* dst_host,
                int64_t rows, int32_t cols, const int32_t* live_host,
                const double* start_ms_host, double dt_ms, uint64_t* ticket);
-/* Waits for a request (PSG_ETIMEOUT after timeout_ms) and releases its ticket;
- * PSG_ECANCELED for a request cancelled before it started. */
+/* Waits for a request (PSG_ETIMEOUT after timeout_ms; a timeout that is not
+ * finite or above 1e12 ms waits until the request finishes) and releases its
+ * ticket; PSG_ECANCELED for a request cancelled before it started. A ticket
+ * has one waiter: a second thread that waits on it while the first does
+ * gets PSG_EINVAL. */
 int psg_wait(psg_server* server, uint64_t ticket, double timeout_ms);
 /* *done = 1 when the request has finished (or was cancelled), without
  * waiting or releasing its ticket. */

@@ -64,10 +64,11 @@ def lib():
             "orc_iir_apply": (C.c_int, [C.POINTER(A.FilterSpecC), C.c_double, I64, C.c_int, C.c_int, P, I64]),
             "orc_spectrum": (C.c_int, [C.c_int, C.c_double, I64, C.c_double, I64, C.c_int, P, I64, I64, P, I64,
                                        I64, I64, P, P, P, P, P, P]),
-            "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int,
-                                          C.POINTER(DBL), C.POINTER(DBL)]),
+            "orc_bench_apply": (C.c_int, [P, P, P, I64, I64, P, P, C.c_int, C.c_int, C.c_int, DBL,
+                                          C.POINTER(DBL), C.POINTER(DBL), C.POINTER(I64)]),
             "orc_agc_row": (C.c_int, [C.c_int, DBL, DBL, C.c_int, DBL, DBL, P, I64]),
-            "orc_panel_stats": (C.c_int, [C.c_int, P, I64, I64, P, DBL, P]),
+            "orc_panel_stats": (C.c_int, [C.c_int, P, I64, I64, P, DBL, C.c_int, P]),
+            "orc_trace_stats": (C.c_int, [C.c_int, P, I64, I64, P, P, P]),
             "orc_percentile_abs": (C.c_int, [C.c_int, P, I64, DBL, C.POINTER(DBL)]),
             "orc_linear_sweep": (C.c_int, [DBL, DBL, DBL, DBL, DBL, DBL, C.c_int, DBL, DBL, DBL,
                                            C.c_int, P, C.POINTER(I64)]),
@@ -217,18 +218,21 @@ class OraclePlan:
                                         _ptr(st), threads))
         return dst
 
-    def bench(self, src, live, startMs=None, threads=1, warm=3, iters=15):
+    def bench(self, src, live, startMs=None, threads=1, warm=3, samples=15, min_sample_ms=20.0):
         """Median and minimum seconds of one src → dst apply through the pool
-        clone (bench/benchutil.nim:96-126 method)."""
+        clone, and the applies run, by the reference harness's method
+        (bench/benchutil.nim:96-126): ``warm`` applies, then ``samples``
+        samples of doubling batches of at least ``min_sample_ms`` each."""
         src = np.ascontiguousarray(src)
         rows, cols = src.shape
         dst = np.zeros_like(src)
         live = np.ascontiguousarray(live, dtype=np.int32)
         st = None if startMs is None else np.ascontiguousarray(startMs, dtype=np.float64)
-        med, mn = C.c_double(), C.c_double()
+        med, mn, n = C.c_double(), C.c_double(), C.c_int64()
         _check(lib().orc_bench_apply(self.h, _ptr(src), _ptr(dst), rows, cols, _ptr(live), _ptr(st),
-                                     threads, warm, iters, C.byref(med), C.byref(mn)))
-        return med.value, mn.value
+                                     threads, warm, samples, min_sample_ms, C.byref(med), C.byref(mn),
+                                     C.byref(n)))
+        return med.value, mn.value, n.value
 
 
 def iir_info(spec, dtMs, samples, phase=A.IP_ZERO, trend=A.TR_LINEAR, freqs=()):
@@ -358,13 +362,27 @@ def agc_row(x, windowMs, dtMs, mode=A.AGC_RMS, target=1.0, eps=1e-9):
     return y
 
 
-def panel_stats(b, live, clipP):
+def panel_stats(b, live, clipP, signed=False):
+    """panelStats (stats.nim:253-304) of the rows ``live`` selects: with
+    ``signed`` a row with live < 0 is not live and live == 0 is a live row
+    without samples (flattening mode 3); otherwise live == 0 is not live."""
     b = np.ascontiguousarray(b)
     live = np.ascontiguousarray(live, dtype=np.int32)
     out = np.zeros(5)
     _check(lib().orc_panel_stats(_dt(b), _ptr(b), b.shape[0], b.shape[1], _ptr(live), clipP,
-                                 _ptr(out)))
+                                 1 if signed else 0, _ptr(out)))
     return dict(rms=out[0], maxAbs=out[1], clip=out[2], rows=int(out[3]), samples=int(out[4]))
+
+
+def trace_stats(b, live):
+    """traceStatsInto (stats.nim:186-199): (rms, maxAbs) per row, NaN for a
+    row with live < 0, (0, 0) for a live row without samples."""
+    b = np.ascontiguousarray(b)
+    live = np.ascontiguousarray(live, dtype=np.int32)
+    rms = np.zeros(b.shape[0])
+    mx = np.zeros(b.shape[0])
+    _check(lib().orc_trace_stats(_dt(b), _ptr(b), b.shape[0], b.shape[1], _ptr(live), _ptr(rms), _ptr(mx)))
+    return rms, mx
 
 
 def percentile_abs(x, p):

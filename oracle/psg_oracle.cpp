@@ -754,14 +754,19 @@ static double orderStat(const std::vector<uint32_t>& h, int64_t j, double mx) {
 }
 struct PanelStats { double rms = 0, maxAbs = 0, clip = NaN; int64_t rows = 0, samples = 0; };
 // gain/stats.nim:253-304 (the four interleaved ways fold to one histogram)
+// signedLive: live[i] < 0 marks a row that is not live and live[i] == 0 a
+// live row with no samples (isLive true, liveSamples 0), which the reference
+// counts: sumSqMaxAbs of nothing is (0, 0) and usable (:267-276). Otherwise
+// (the pipeline's flattening) live[i] == 0 is a row that is not processed.
 template <class T>
-PanelStats panelStats(const T* b, int64_t rows, int64_t cols, const int32_t* live, double clipP) {
+PanelStats panelStats(const T* b, int64_t rows, int64_t cols, const int32_t* live, double clipP,
+                      bool signedLive = false) {
   PanelStats r;
   double sum = 0, mx = 0;
   std::vector<char> use(rows, 0);
   for (int64_t i = 0; i < rows; i++) {
-    if (live[i] <= 0) continue;
-    int64_t n = live[i];
+    if (signedLive ? live[i] < 0 : live[i] <= 0) continue;
+    int64_t n = std::min<int64_t>(live[i], cols);
     double s = sumSq64(b + i * cols, n), m = maxAbs(b + i * cols, n);
     if (std::isnan(m) || std::isinf(m) || s == INF) continue;  // usable, :232-235
     use[i] = 1;
@@ -780,7 +785,7 @@ PanelStats panelStats(const T* b, int64_t rows, int64_t cols, const int32_t* liv
   for (int64_t i = 0; i < rows; i++) {
     if (!use[i]) continue;
     const T* x = b + i * cols;
-    for (int64_t j = 0; j < live[i]; j++) h[keyOf((float)std::fabs((double)x[j]))]++;
+    for (int64_t j = 0; j < std::min<int64_t>(live[i], cols); j++) h[keyOf((float)std::fabs((double)x[j]))]++;
   }
   double rank = (double)(r.samples - 1) * clipP / 100;
   int64_t k = std::min((int64_t)std::floor(rank), r.samples - 1);
@@ -788,6 +793,29 @@ PanelStats panelStats(const T* b, int64_t rows, int64_t cols, const int32_t* liv
   double f = rank - (double)k;
   r.clip = (f == 0 || k + 1 >= r.samples) ? lower : lower + f * (orderStat(h, k + 1, mx) - lower);
   return r;
+}
+
+// traceStatsInto (gain/stats.nim:186-199) with statsOf (:124-127) and
+// traceStats (:129-133): per row, NaN for a row that is not live
+// (live[r] < 0), (0, 0) for a live row without samples, else the RMS and
+// max |x| of its first live[r] samples (sumSq64's eight accumulators).
+template <class T>
+void traceStatsInto(const T* b, int64_t rows, int64_t cols, const int32_t* live, double* rms, double* mxo) {
+  for (int64_t r = 0; r < rows; r++) {
+    if (live[r] < 0) {
+      rms[r] = NaN;
+      mxo[r] = NaN;
+      continue;
+    }
+    int64_t n = std::min<int64_t>(live[r], cols);
+    if (n == 0) {
+      rms[r] = 0;
+      mxo[r] = 0;
+      continue;
+    }
+    rms[r] = std::sqrt(sumSq64(b + r * cols, n) / (double)n);
+    mxo[r] = maxAbs(b + r * cols, n);
+  }
 }
 
 // ------------------------------------------------------------------- AGC --
@@ -2106,10 +2134,11 @@ int orc_rows_flatten(const int32_t* status, const int32_t* numSamples, const dou
     for (int64_t i = 0; i < nfailed; i++)
       if (failed[i] >= 0 && failed[i] < rows) isFailed[failed[i]] = 1;
     for (int64_t r = 0; r < rows; r++) {
-      bool use = mode == 0 ? ((status[r] == PSG_TS_LIVE || status[r] == PSG_TS_UNKNOWN) && !isFailed[r])
-                           : (status[r] != PSG_TS_DEAD && !isFailed[r]);
+      // mode 3: the rule of mode 0, with the rows it leaves out marked -1
+      bool use = mode == 0 || mode == 3 ? ((status[r] == PSG_TS_LIVE || status[r] == PSG_TS_UNKNOWN) && !isFailed[r])
+                                        : (status[r] != PSG_TS_DEAD && !isFailed[r]);
       int64_t n = std::clamp<int64_t>((int64_t)numSamples[r] - first, 0, cols);
-      live[r] = use ? (int32_t)n : 0;
+      live[r] = use ? (int32_t)n : (mode == 3 ? -1 : 0);
       if (startMs) startMs[r] = (t0 ? t0[r] : NaN) + (double)(first) * dtMs;
     }
   });
@@ -2150,24 +2179,43 @@ int orc_plan_apply_keyed(void* h, const void* src, void* dst, int64_t rows, int6
 // `threads` workers (created once, as a viewer's pool is), each sample timed;
 // returns the median and minimum seconds (bench/benchutil.nim:96-126 method,
 // warm-up included in `warm`).
+// The reference harness's timing (bench/benchutil.nim:96-126): `warm` runs,
+// then `samples` samples, each running batches of 1, 2, 4 … applies until at
+// least min_sample_ms have passed, timed as elapsed / applies; the median and
+// the minimum of the samples, and the applies run in all.
 int orc_bench_apply(void* h, const void* src, void* dst, int64_t rows, int64_t cols, const int32_t* live,
-                    const double* startMs, int threads, int warm, int iters, double* median_s, double* min_s) {
+                    const double* startMs, int threads, int warm, int samples, double min_sample_ms,
+                    double* median_s, double* min_s, int64_t* applies) {
   return guard([&] {
     OrcPlan* op = (OrcPlan*)h;
     Pool pool(threads);
-    std::vector<double> t;
-    for (int i = 0; i < warm + iters; i++) {
-      auto t0 = std::chrono::steady_clock::now();
+    auto once = [&] {
       if (op->dtype == PSG_F32)
         applyPool(&pool, *(Plan<float>*)op->p, (const float*)src, (float*)dst, rows, cols, live, startMs);
       else
         applyPool(&pool, *(Plan<double>*)op->p, (const double*)src, (double*)dst, rows, cols, live, startMs);
-      auto t1 = std::chrono::steady_clock::now();
-      if (i >= warm) t.push_back(std::chrono::duration<double>(t1 - t0).count());
+    };
+    for (int i = 0; i < warm; i++) once();
+    std::vector<double> t;
+    int64_t total = 0;
+    for (int k = 0; k < samples; k++) {
+      int64_t n = 0, batch = 1;
+      auto t0 = std::chrono::steady_clock::now();
+      double el = 0;
+      while (true) {
+        for (int64_t b = 0; b < batch; b++) once();
+        n += batch;
+        batch *= 2;
+        el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el * 1e3 >= min_sample_ms) break;
+      }
+      t.push_back(el / (double)n);
+      total += n;
     }
     std::sort(t.begin(), t.end());
     *median_s = t.empty() ? 0 : t[t.size() / 2];
     *min_s = t.empty() ? 0 : t[0];
+    if (applies) *applies = total;
   });
 }
 // Single-op kernels on one row, for unit checks.
@@ -2178,11 +2226,18 @@ int orc_agc_row(int dtype, double windowMs, double dtMs, int mode, double target
   });
 }
 int orc_panel_stats(int dtype, const void* b, int64_t rows, int64_t cols, const int32_t* live, double clipP,
-                    double* out5) {
+                    int signedLive, double* out5) {
   return guard([&] {
-    PanelStats s = dtype == PSG_F32 ? panelStats((const float*)b, rows, cols, live, clipP)
-                                    : panelStats((const double*)b, rows, cols, live, clipP);
+    PanelStats s = dtype == PSG_F32 ? panelStats((const float*)b, rows, cols, live, clipP, signedLive != 0)
+                                    : panelStats((const double*)b, rows, cols, live, clipP, signedLive != 0);
     out5[0] = s.rms; out5[1] = s.maxAbs; out5[2] = s.clip; out5[3] = (double)s.rows; out5[4] = (double)s.samples;
+  });
+}
+int orc_trace_stats(int dtype, const void* b, int64_t rows, int64_t cols, const int32_t* live, double* rms,
+                    double* mx) {
+  return guard([&] {
+    if (dtype == PSG_F32) traceStatsInto((const float*)b, rows, cols, live, rms, mx);
+    else traceStatsInto((const double*)b, rows, cols, live, rms, mx);
   });
 }
 int orc_percentile_abs(int dtype, const void* x, int64_t n, double p, double* out) {

@@ -44,3 +44,4 @@ from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepHarmonic, Swee
                         slTable, sweepHarmonics, tableSweep, taperWeight, tpBlackman, tpBlackmanHarris, tpCos2,
                         tpCosine, tpGaussian, tpHamming, tpKaiser, tpLinear, tpPower)
 from .server import Server
+from .stats import PanelStats, TraceStats, panelStats, traceStatsInto

@@ -88,14 +88,22 @@ __device__ __forceinline__ bool usable_d(double ssr, double mxr, int n) {
 }
 
 // One CTA: fold the rows; for `stat` < 0 no factor is computed.
+// signed_live: live[r] < 0 marks a row that is not live and live[r] == 0 a
+// live row with no live samples, which panelStats counts among its rows
+// (gain/stats.nim:267-276: sumSqMaxAbs of no samples is (0, 0), usable);
+// otherwise (the pipeline's flattening) live[r] == 0 is a row not processed.
 __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int cols, const int* __restrict__ live,
                                                           const double* __restrict__ ss, const double* __restrict__ mx,
-                                                          PanelOut* out) {
+                                                          PanelOut* out, int signed_live = 0) {
   __shared__ SharedMem S;
   double sum = 0, cnt = 0, nr = 0;
   unsigned long long mb = 0;
   for (long long r = threadIdx.x; r < rows; r += blockDim.x) {
     int n = min(max(live[r], 0), cols);
+    if (signed_live && live[r] == 0) {
+      nr += 1;
+      continue;
+    }
     if (!usable_d(ss[r], mx[r], n)) continue;
     sum += ss[r];
     cnt += (double)n;
@@ -1452,8 +1460,14 @@ static void ws_grow_for(psg_workspace* ws, const psg_plan* p, int64_t rows, int3
 }
 int psg_workspace_reserve(psg_workspace* ws, const psg_plan* plan, int64_t rows, int32_t cols) {
   return guarded([&] {
-    if (!ws || !plan) throw InvalidArg("null argument");
+    if (!ws) throw InvalidArg("null argument");
     if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if (!plan) {
+      // no plan: the statistics' scratch for `rows` rows (panelStatsWorkspace)
+      ensure_device();
+      ws_grow(ws, ws_device_bytes(rows));
+      return;
+    }
     ws_grow_for(ws, plan, rows, cols);
   });
 }
@@ -1477,11 +1491,11 @@ int psg_rows_flatten(const int32_t* status, const int32_t* num_samples, const do
       while (fi < n_failed && failed[fi] < r) fi++;
       if (fi < n_failed && failed[fi] == r) is_failed = true;
       int32_t st = status[r];
-      bool use = mode == 0   ? ((st == PSG_TS_LIVE || st == PSG_TS_UNKNOWN) && !is_failed)
+      bool use = mode == 0 || mode == 3 ? ((st == PSG_TS_LIVE || st == PSG_TS_UNKNOWN) && !is_failed)
                  : mode == 1 ? (st != PSG_TS_DEAD && !is_failed)
                              : !is_failed;
       int64_t n = std::min<int64_t>(std::max<int64_t>((int64_t)num_samples[r] - first_sample, 0), cols);
-      live_out[r] = use ? (int32_t)n : 0;
+      live_out[r] = use ? (int32_t)n : (mode == 3 ? -1 : 0);
       if (start_ms_out) start_ms_out[r] = (t0_ms ? t0_ms[r] : NAN) + (double)first_sample * dt_ms;
     }
   });
@@ -1908,11 +1922,20 @@ int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double
   });
 }
 
+// The sample types the statistics kernels are built for; anything else is
+// refused before a launch (a float32 block read as float64 would be read
+// past its end).
+static void check_dtype(int32_t dtype) {
+  if (dtype != PSG_F32 && dtype != PSG_F64) throw InvalidArg("dtype must be PSG_F32 or PSG_F64, got " + std::to_string(dtype));
+}
+
 int psg_trace_stats(const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live, double* rms_out,
                     double* max_abs_out, void* stream) {
   return guarded([&] {
+    check_dtype(dtype);
     if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
     if (rows == 0) return;
+    if (!block || !live || !rms_out || !max_abs_out) throw InvalidArg("null argument");
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
     int g = (int)std::min<int64_t>(rows, (int64_t)g_sm_count * 8);
@@ -1927,8 +1950,11 @@ int psg_trace_stats(const void* block, int32_t dtype, int64_t rows, int32_t cols
 int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live,
                     double clip_percentile, double* out, void* stream) {
   return guarded([&] {
+    check_dtype(dtype);
     if (!std::isnan(clip_percentile) && !(clip_percentile >= 0 && clip_percentile <= 100))
       throw InvalidArg("a percentile must be in 0 .. 100, got " + std::to_string(clip_percentile));
+    if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
+    if ((rows > 0 && (!block || !live)) || !out) throw InvalidArg("null argument");
     if (!ws || ws->bytes < ws_device_bytes(rows)) throw WorkspaceError("reserve the workspace first (psg_workspace_reserve)");
     ensure_device();
     cudaStream_t s = (cudaStream_t)stream;
@@ -1942,7 +1968,7 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
       if (dtype == PSG_F32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
       else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
     }
-    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po);
+    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po, 1);
     if (!std::isnan(clip_percentile)) {
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
       if (rows > 0) {
@@ -1968,12 +1994,17 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
 static const int64_t kStaticBytes = 512 + (int64_t)PSG_STATIC_MAX_ROWS * 16 + kHist;
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 static std::mutex g_static_mu;
+// The array's device address per device, looked up on the first call on that
+// device. A device reset (cudaDeviceReset) unloads the module and with it the
+// array: after one, the cached address is stale, so a process that resets a
+// device must not call psg_panel_stats_static on it again.
 static void* g_static_addr[128];
 extern "C" {
 
 int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32_t cols, const int32_t* live,
                            double clip_percentile, double* out, void* stream) {
   return guarded([&] {
+    check_dtype(dtype);
     if (!std::isnan(clip_percentile) && !(clip_percentile >= 0 && clip_percentile <= 100))
       throw InvalidArg("a percentile must be in 0 .. 100, got " + std::to_string(clip_percentile));
     if (rows < 0 || cols < 0) throw InvalidArg("rows and cols must be ≥ 0");
@@ -2007,7 +2038,7 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
       if (dtype == PSG_F32) row_stats_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx);
       else row_stats_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx);
     }
-    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po);
+    panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po, 1);
     if (!std::isnan(clip_percentile)) {
       // The array keeps the previous call's counts: the histogram starts at zero.
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
@@ -2518,13 +2549,21 @@ int psg_stack_fold(const psg_stack* st, int32_t* dst, void* stream) {
 }  // extern "C"
 
 // traceStatsInto's finish: rms = sqrt(Σx²/n) for live rows, NaN for others.
+// statsOf (gain/stats.nim:124-127) per row: a row that is not live
+// (live[r] < 0) reads NaN for both; a live row with no live samples reads
+// (0, 0); otherwise rms = sqrt(Σx²/n).
 __global__ void trace_stats_finish(double* rms, double* mx, const int* live, long long rows, int cols) {
   long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  int n = min(max(live[r], 0), cols);
-  if (n == 0) {
+  if (live[r] < 0) {
     rms[r] = NAN;
     mx[r] = NAN;
+    return;
+  }
+  int n = min(live[r], cols);
+  if (n == 0) {
+    rms[r] = 0;
+    mx[r] = 0;
   } else {
     rms[r] = sqrt(rms[r] / (double)n);
   }
@@ -2603,6 +2642,7 @@ struct Req {
   double t_submit = 0, t_done = 0;
   int status = PSG_OK;
   bool done = false;
+  bool claimed = false;      // a thread is in psg_wait on it (one waiter per ticket)
   cudaEvent_t in = nullptr;  // its copy in finished
 };
 
@@ -2934,6 +2974,12 @@ int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* 
   });
 }
 
+// A ticket has one waiter: the thread that waits claims the request under
+// the lock, a second thread that waits on the same ticket meanwhile gets
+// PSG_EINVAL, and only the claiming thread erases and frees it (after a
+// timeout the claim is dropped and the ticket can be waited on again). A
+// timeout that is not finite, or longer than about 30 years, waits until the
+// request finishes; a negative one polls once.
 int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
   if (!S) {
     t_err = "null argument";
@@ -2946,15 +2992,25 @@ int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
     return PSG_EINVAL;
   }
   Req* r = it->second;
-  auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000));
+  if (r->claimed) {
+    t_err = "another thread is waiting on ticket " + std::to_string(ticket);
+    return PSG_EINVAL;
+  }
+  r->claimed = true;
+  const bool forever = !(timeout_ms <= 1e12);  // NaN, +Inf and huge values
+  const double ms = forever ? 0.0 : std::max(timeout_ms, 0.0);
+  auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((int64_t)(ms * 1000));
   while (!r->done) {
-    if (S->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !r->done) {
+    if (forever) {
+      S->cv_done.wait(lk);
+    } else if (S->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !r->done) {
+      r->claimed = false;
       t_err = "the request did not finish within " + std::to_string(timeout_ms) + " ms";
       return PSG_ETIMEOUT;
     }
   }
   int st = r->status;
-  S->by_ticket.erase(it);
+  S->by_ticket.erase(ticket);
   delete r;
   if (st == PSG_ECANCELED) t_err = "the request was cancelled";
   else if (st != PSG_OK) t_err = S->error.empty() ? "a CUDA call of the request loop failed" : S->error;

@@ -130,16 +130,20 @@ def test_rows_flatten_matches_oracle():
     ns = rng.integers(0, 700, rows).astype(np.int32)
     t0 = rng.uniform(-100, 100, rows)
     failed = np.array([3, 10, 11, 50], np.int64)
+    status[0], ns[0] = P.tsLive, 0  # a live row with no samples
     for first in (0, 37):
-        for mode in (0, 1):
+        for mode in (0, 1, 3):
             meta = P.initChunkMeta(status, ns, 2.0, t0, first, failed)
             live, start = meta.flat(cols, mode)
             ol, os_ = O.rows_flatten(status, ns, t0, first, 2.0, failed, cols, mode)
             assert np.array_equal(live, ol) and np.array_equal(start, os_)
             for r in range(rows):
-                want = meta.liveSamples(r, cols) if (meta.isLive(r) if mode == 0 else (
-                    status[r] != P.tsDead and not meta.isFailed(r))) else 0
+                use = meta.isLive(r) if mode in (0, 3) else (status[r] != P.tsDead and not meta.isFailed(r))
+                want = meta.liveSamples(r, cols) if use else (-1 if mode == 3 else 0)
                 assert live[r] == want
+            if mode == 3:
+                # a live row with an empty live window stays apart from a row not live
+                assert np.any(live == 0) and np.any(live == -1)
     with pytest.raises(ValueError):
         P.initChunkMeta(status, ns, 2.0, t0, 0, [5, 5]).flat(cols)
 
@@ -190,3 +194,30 @@ def test_no_cpu_fallback_without_a_device():
     with pytest.raises(Exception) as e:
         P.initPipeline([P.demeanOp()]).compile(P.float32, 2.0, 100)
     assert not isinstance(e.value, ValueError) or "device" in str(e.value).lower()
+
+
+def test_statistics_refuse_a_bad_dtype_before_any_launch():
+    # checked before the device is touched: no GPU needed, nothing launched
+    lib = A.lib()
+    out = (C.c_double * 5)()
+    for dtype in (2, -1, 7):
+        assert lib.psg_trace_stats(None, dtype, 4, 4, None, out, out, None) == A.EINVAL
+        assert "dtype" in lib.psg_last_error().decode()
+        assert lib.psg_panel_stats(None, None, dtype, 4, 4, None, 99.0, out, None) == A.EINVAL
+        assert "dtype" in lib.psg_last_error().decode()
+        assert lib.psg_panel_stats_static(None, dtype, 4, 4, None, 99.0, out, None) == A.EINVAL
+        assert "dtype" in lib.psg_last_error().decode()
+
+
+def test_trace_stats_oracle_follows_stats_of():
+    # the checker itself: NaN for rows not live, (0, 0) for an empty live row,
+    # float64 sums of squares over the live samples
+    b = np.arange(12, dtype=np.float32).reshape(3, 4) - 5
+    rms, mx = O.trace_stats(b, np.array([-1, 0, 3], np.int32))
+    assert math.isnan(rms[0]) and math.isnan(mx[0])
+    assert rms[1] == 0 and mx[1] == 0
+    assert rms[2] == math.sqrt((3 * 3 + 4 * 4 + 5 * 5) / 3) and mx[2] == 5
+    st = O.panel_stats(b, np.array([-1, 0, 3], np.int32), math.nan, signed=True)
+    assert st["rows"] == 2 and st["samples"] == 3
+    st = O.panel_stats(b, np.array([0, 0, 3], np.int32), math.nan)
+    assert st["rows"] == 1 and st["samples"] == 3
