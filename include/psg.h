@@ -351,6 +351,22 @@ int psg_applied_response(const psg_op* ops, int32_t n_ops, int32_t dtype, double
                          int32_t samples, const double* hz, int32_t n_hz, double* gain,
                          psg_workspace* ws);
 
+/* ------------------------------------------------------------ graph replay
+ * One psg_apply_keyed call (device pointers) captured into a CUDA graph for
+ * replay (the "CUDA-graph replay" of the batched path; no counterpart in the
+ * reference, whose apply is a CPU call): psg_graph_launch then runs the same
+ * apply on `stream` with one host call instead of the checks and per-part
+ * launches. The checks run once, at capture (PSG_EINVAL / PSG_EWORKSPACE as
+ * psg_apply). The graph keeps the call's pointers: the plan, the workspace
+ * (not grown while the graph lives), src, dst and the row arrays must stay
+ * valid, and their contents are read at each launch. */
+typedef struct psg_graph psg_graph;
+int psg_graph_capture(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst,
+                      int64_t rows, int32_t cols, const int32_t* live, const double* start_ms,
+                      const psg_keys* keys, double dt_ms, psg_graph** out);
+int psg_graph_launch(psg_graph* graph, void* stream);
+void psg_graph_destroy(psg_graph* graph);
+
 /* ----------------------------------------------------------- statistics */
 /* traceStatsInto, src/processSEG/gain/stats.nim:186-199: rms and maxAbs per
  * row into device arrays of `rows` doubles. `live` is psg_rows_flatten's

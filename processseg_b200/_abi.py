@@ -170,6 +170,9 @@ def _declare(lib):
         "psg_apply_host_keyed": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P]),
         "psg_apply_host_async": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P]),
         "psg_workspace_sync": (C.c_int, [P]),
+        "psg_graph_capture": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, C.POINTER(P)]),
+        "psg_graph_launch": (C.c_int, [P, P]),
+        "psg_graph_destroy": (None, [P]),
         "psg_plan_needs_keys": (I32, [P]),
         "psg_applied_response": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, P, I32, P, P]),
         "psg_spectrum_plan_create": (C.c_int, [I32, DBL, I32, DBL, I32, I32, C.POINTER(P)]),

@@ -11,10 +11,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 OUT = os.path.join(PKG, "libpsgcuda.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["psg_pipe_f32.cu", "psg_recipe_f32.cu", "psg_pipe_f64.cu", "psg_recipe_f64.cu", "psg_cuda.cu",
-           "psg_plan.cpp"]
-DEPS = SOURCES + ["psg_kernel.cuh", "psg_device.cuh", "psg_internal.h", "psg_dft_consts.h",
-                  os.path.join("..", "..", "include", "psg.h")]
+SOURCES = ["psg_pipe_f32.cu", "psg_recipe_f32.cu", "psg_pipe_f64.cu", "psg_recipe_f64.cu", "psg_trace_f32.cu",
+           "psg_cuda.cu", "psg_plan.cpp"]
+PUBLIC = os.path.join("..", "..", "include", "psg.h")
+# the headers each unit includes (a unit recompiles when it or one of them changes)
+KERNEL_HEADERS = ["psg_kernel.cuh", "psg_device.cuh", "psg_internal.h", "psg_dft_consts.h", "psg_trace.h", PUBLIC]
+HEADERS = {src: KERNEL_HEADERS for src in SOURCES}
+HEADERS["psg_trace_f32.cu"] = KERNEL_HEADERS + ["psg_trace.cuh"]
+HEADERS["psg_plan.cpp"] = ["psg_internal.h", PUBLIC]
+DEPS = SOURCES + sorted({h for hs in HEADERS.values() for h in hs})
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -28,8 +33,27 @@ def stale() -> bool:
     return any(os.path.getmtime(os.path.join(HERE, d)) > t for d in DEPS)
 
 
-def _compile(src):
-    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+def _obj(src):
+    return os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+
+
+def _unit_stale(src, force):
+    obj = _obj(src)
+    if force or not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(os.path.join(HERE, d)) > t for d in [src] + HEADERS[src])
+
+
+class _Done:
+    returncode, stdout, stderr = 0, "", "(up to date)\n"
+
+
+def _compile(args):
+    src, force = args
+    obj = _obj(src)
+    if not _unit_stale(src, force):
+        return src, obj, _Done()
     r = subprocess.run([NVCC, *FLAGS, "-c", "-o", obj, os.path.join(HERE, src)], cwd=HERE,
                        capture_output=True, text=True)
     return src, obj, r
@@ -40,7 +64,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return OUT
     os.makedirs(OBJ, exist_ok=True)
     with ThreadPoolExecutor(len(SOURCES)) as ex:
-        results = list(ex.map(_compile, SOURCES))
+        results = list(ex.map(_compile, [(src, force) for src in SOURCES]))
     log = []
     for src, _, r in results:
         log.append(f"== {src}\n{r.stdout}{r.stderr}")

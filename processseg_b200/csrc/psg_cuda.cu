@@ -43,6 +43,7 @@ void set_error(const std::string& m) { t_err = m; }
 }  // namespace psg
 
 #include "psg_kernel.cuh"
+#include "psg_trace.h"
 
 namespace psg {
 
@@ -256,37 +257,7 @@ __global__ void partial_to_out_kernel(const double* __restrict__ partial, PanelO
 }
 
 // ============================================================ correlation
-struct CorrArgs {
-  const void* src;
-  void* dst;
-  long long rows;
-  int cols, out, nfft, shift, pilot_len, record;
-  const int* live;
-  const void* bridge;  // Quad<T>[m]: the split · multiplier · unsplit map of each bin pair
-  const void* tw;
-  FftDesc fft;
-  void* gwork;        // per-CTA global scratch when shared memory is too small (else NULL)
-  // stack epilogue
-  double* num;
-  int* cnt;
-  int stack_samples;
-  long long stack_rows;
-  const int* row_map;
-  const int* stack_live;
-  int stack_on;
-};
-
-// Complex input c of a record's forward transform: samples 2c and 2c + 1
-// of the record (read-only global memory), 0 past its n samples.
-template <class T> struct RecordLoad {
-  typedef typename C2<T>::type V;
-  const T* x;
-  int n;
-  __device__ __forceinline__ V operator()(int c, bool) const {
-    const int k = 2 * c;
-    return V{k < n ? __ldg(x + k) : (T)0, k + 1 < n ? __ldg(x + k + 1) : (T)0};
-  }
-};
+// CorrArgs and RecordLoad: psg_kernel.cuh.
 
 // correlateInto (vibroseis/correlate.nim:205-300, 421-464) one record per CTA
 // pass, with the vertical-stack add (vstack.nim:186-202) fused after it.
@@ -818,6 +789,14 @@ struct psg_plan {
   bool wide = false;
   int64_t gwork_stride = 0, gwork_bytes = 0;
   bool needs_keys = false;  // a mute reads each row's offset and t0Ms
+  // Per part: the float32 trace kernel that runs it (psg_trace.cuh), or
+  // nullptr for pipeline_kernel; its recipe slot (0: demean, filter, AGC;
+  // 1: then a per-trace normalization), prefetch, shared memory and grid.
+  std::vector<const TracePlanInfo*> trace;
+  std::vector<int> trace_recipe;
+  bool trace_pf = false;
+  size_t trace_smem = 0;
+  int trace_work_off = 0, trace_grid = 1;
 };
 
 struct psg_workspace {
@@ -857,6 +836,11 @@ struct psg_corr_plan {
   size_t smem = 0;
   int grid = 1;
   FftDesc fft{};
+  // the compile-time correlation kernel (float32, a transform length it is
+  // built for), its twiddles pass by pass and its grid; else corr_kernel
+  const TracePlanInfo* trace = nullptr;
+  void* tw_pass = nullptr;
+  int trace_grid = 1;
 };
 
 struct psg_spectrum_plan {
@@ -1033,6 +1017,116 @@ static void iir_scan_table(const Biquad& q, int lmax, std::vector<double>& out) 
   }
 }
 
+// The trace kernel's twiddles, pass by pass: pass i (all but the last) of
+// radix R after radices of product S holds, for each of its m/(S·R)
+// butterflies p, the R − 1 twiddles ω_m^{p·k·S} (k = 1 .. R − 1, padded to
+// an even count): the values of the transform's one table ω_m^e, e = p·k·S,
+// laid out in the order a butterfly reads them.
+static std::vector<float2> trace_twiddles(const TracePlanInfo& t) {
+  std::vector<float2> out;
+  int64_t S = 1;
+  for (int i = 0; i + 1 < t.np; i++) {
+    const int R = t.radix[i], tws = (R - 1 + 1) & ~1;
+    const int64_t sub = t.m / (S * R);
+    for (int64_t pp = 0; pp < sub; pp++)
+      for (int k = 1; k <= tws; k++) {
+        float2 v{0.f, 0.f};
+        if (k < R) {
+          const int64_t e = pp * k * S;
+          const double a = -2 * 3.141592653589793 * (double)e / (double)t.m;
+          v = float2{(float)std::cos(a), (float)std::sin(a)};
+        }
+        out.push_back(v);
+      }
+    S *= R;
+  }
+  return out;
+}
+
+// The reference's stages of an m-point transform (fft/plan.nim:120-132): 4s
+// first, then a 2, then 3s and 5s.
+static std::vector<int> reference_stages(int64_t m) {
+  std::vector<int> r;
+  while (m % 4 == 0) {
+    r.push_back(4);
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    r.push_back(2);
+    m /= 2;
+  }
+  for (int q : {3, 5})
+    while (m % q == 0) {
+      r.push_back(q);
+      m /= q;
+    }
+  return r;
+}
+static bool runs_reference_stages(const TracePlanInfo& t) {
+  std::vector<int> st;
+  for (int i = 0; i < t.np; i++) {
+    st.push_back(t.g1[i]);
+    if (t.g2[i]) st.push_back(t.g2[i]);
+  }
+  return st == reference_stages(t.m);
+}
+// A twiddle as the reference tabulates it (fft/plan.nim:146-155): angle
+// −2π·e/cur in float64, its cosine and sine rounded to float32.
+static float2 ref_twiddle(int64_t e, int64_t cur) {
+  const double a = -2 * 3.14159265358979323846 * (double)e / (double)cur;
+  return float2{(float)std::cos(a), (float)std::sin(a)};
+}
+// The trace kernel's twiddles, pass by pass (psg_trace.cuh ref_pass): for
+// each butterfly p of pass i (stride S, radix R, m/(S·R) butterflies), the
+// first stage's R2·(R1 − 1) twiddles ω_cur^{((p + jB·m/(S·R))·kA) mod cur}
+// (cur = m/S), then the second stage's R2 − 1 twiddles
+// ω_{cur/R1}^{(p·kB) mod (cur/R1)}, padded to an even count.
+static std::vector<float2> ref_twiddles(const TracePlanInfo& t) {
+  std::vector<float2> out;
+  int64_t S = 1;
+  for (int i = 0; i < t.np; i++) {
+    const int R = t.radix[i], r1 = t.g1[i], r2 = t.g2[i], tws = (R - 1 + 1) & ~1;
+    const int64_t curA = t.m / S, sub = t.m / (S * R);
+    for (int64_t pp = 0; pp < sub; pp++) {
+      size_t n0 = out.size();
+      if (r2) {
+        for (int jB = 0; jB < r2; jB++) {
+          const int64_t pA = pp + jB * sub;
+          for (int kA = 1; kA < r1; kA++) out.push_back(ref_twiddle((pA * kA) % curA, curA));
+        }
+        const int64_t curB = curA / r1;
+        for (int kB = 1; kB < r2; kB++) out.push_back(ref_twiddle((pp * kB) % curB, curB));
+      } else {
+        for (int k = 1; k < r1; k++) out.push_back(ref_twiddle((pp * k) % curA, curA));
+      }
+      while (out.size() - n0 < (size_t)tws) out.push_back(float2{0.f, 0.f});
+    }
+    S *= R;
+  }
+  return out;
+}
+
+// The trace kernel for part `part` of a float32 plan, or nullptr: a part of
+// exactly demean, filter (zero pads), AGC (and a per-trace normalization)
+// whose transform length and AGC window one of its builds serves, with the
+// row fitting the transform's buffers. PSG_TRACE=0 in the environment (read
+// at compile time) keeps every plan on pipeline_kernel.
+static const TracePlanInfo* trace_plan_of(const psg_plan* p, int part) {
+  if (const char* e = getenv("PSG_TRACE"))
+    if (atoi(e) == 0) return nullptr;
+  if (p->host.dtype != PSG_F32) return nullptr;
+  const int rc = p->recipe[part];
+  if (rc != RC_DFA && rc != RC_DFAN) return nullptr;
+  const int first = p->host.parts[part].first;
+  const StepHost& f = p->host.steps[first + 1];
+  const StepHost& ag = p->host.steps[first + 2];
+  if (f.kind != ST_FILTER || ag.kind != ST_AGC || f.filter.reflect) return nullptr;
+  const int64_t m = f.filter.fft.m;
+  if (4 * m < p->host.samples + 8) return nullptr;  // the output row lives in the transform buffers
+  const TracePlanInfo* const* c = trace_plans_for((int)m, (int)(2 * ag.half + 1));
+  return c[0] && runs_reference_stages(*c[0]) ? c[0] : nullptr;
+}
+
 template <class T> static void build_device_steps(psg_plan* p) {
   typedef typename C2<T>::type V;
   std::vector<DevStep> ds;
@@ -1057,6 +1151,26 @@ template <class T> static void build_device_steps(psg_plan* p) {
       d.bridge = upload(p->keep, bridge_table<T>(f.fft, f.gain, std::vector<double>(f.gain.size(), 0.0)));
       d.fall = upload(p->keep, as_t<T>(f.fall));
       d.tw = upload(p->keep, as_c<T>(f.fft.tw_re, f.fft.tw_im));
+      for (size_t part = 0; part < p->trace.size(); part++)
+        if (p->trace[part] && &p->host.steps[p->host.parts[part].first + 1] == &s) {
+          // the trace kernel's tables: twiddles pass by pass, and the split
+          // twiddles and gains of each bin pair (c, m − c) as the reference
+          // rounds them to float32 (fft/plan.nim:156-159, filter/apply.nim:141)
+          d.tw_pass = upload(p->keep, ref_twiddles(*p->trace[part]));
+          const int64_t m = f.fft.m, nf = f.fft.n;
+          std::vector<float4> sp((size_t)m);
+          std::vector<float2> gg((size_t)m);
+          auto split = [&](int64_t k) { return ref_twiddle(k, nf); };
+          for (int64_t c = 0; c < m; c++) {
+            const float2 a = split(c), b = split(m - c);
+            sp[(size_t)c] = float4{a.x, a.y, b.x, b.y};
+            gg[(size_t)c] = c == 0 ? float2{(float)f.gain[0], (float)f.gain[m]}
+                                   : float2{(float)f.gain[c], (float)f.gain[m - c]};
+          }
+          d.ref_split = upload(p->keep, sp);
+          d.ref_gain = upload(p->keep, gg);
+          d.ref_scale = 1.0f / (float)nf;
+        }
       work = std::max<int64_t>(work, 2 * f.fft.m * (int64_t)sizeof(V));
     } else if (s.kind == ST_AGC) {
       d.half = (int)s.half;
@@ -1184,6 +1298,34 @@ template <class T> static void build_device_steps(psg_plan* p) {
   CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p->threads, p->smem));
   p->grid = std::max(1, per_sm) * g_sm_count;
   if (p->wide) p->gwork_bytes = p->gwork_stride * p->grid;
+  // The trace kernel: the row buffer (two with the next row's copy in flight,
+  // when that keeps as many CTAs on an SM) and the two transform buffers.
+  const TracePlanInfo* tp = nullptr;
+  for (auto* t : p->trace) tp = t ? t : tp;
+  if (tp && !p->wide) {
+    const int64_t fw = 2 * (int64_t)tp->m * 8;
+    auto occ = [&](bool pf) {
+      const size_t sm = (size_t)((pf ? 2 : 1) * p->x_bytes + fw);
+      int best = 0;
+      for (int r = 0; r < 2; r++) {
+        const void* k = tp->kernel[r][pf ? 1 : 0];
+        allow_smem(k);
+        int per = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, tp->nt, sm));
+        best = r == 0 ? per : std::min(best, per);
+      }
+      return best;
+    };
+    const int one = occ(false), two = occ(true);
+    p->trace_pf = two > 0 && two >= one;
+    if (const char* e = getenv("PSG_PREFETCH")) p->trace_pf = atoi(e) != 0 && two > 0;
+    p->trace_work_off = (p->trace_pf ? 2 : 1) * p->x_bytes;
+    p->trace_smem = (size_t)(p->trace_work_off + fw);
+    p->trace_grid = std::max(1, p->trace_pf ? two : one) * g_sm_count;
+    if ((p->trace_pf ? two : one) <= 0) std::fill(p->trace.begin(), p->trace.end(), nullptr);
+  } else {
+    std::fill(p->trace.begin(), p->trace.end(), nullptr);
+  }
 }
 
 // The per-panel factor of part `part` (which starts with a per-panel
@@ -1251,6 +1393,15 @@ static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void*
     a.gwork = (unsigned char*)ws->g;
     a.gwork_stride = p->gwork_stride;
   }
+  if (const TracePlanInfo* tp = part < (int)p->trace.size() ? p->trace[part] : nullptr) {
+    if (!factor) {
+      const void* kern = tp->kernel[p->trace_recipe[part]][p->trace_pf ? 1 : 0];
+      a.work_off = p->trace_work_off;
+      allow_smem(kern);
+      launch_pipe(kern, (int)std::min<int64_t>(rows, p->trace_grid), tp->nt, p->trace_smem, stream, a);
+      return;
+    }
+  }
   const void* kern = p->wide ? wide_kernel_for<T>() : pipe_kernel_for<T>(p->recipe[part], p->prefetch);
   allow_smem(kern);
   launch_pipe(kern, grid, p->threads, p->smem, stream, a);
@@ -1273,6 +1424,20 @@ template <class T> static void corr_upload(psg_corr_plan* p) {
   p->fft = fft_desc(p->host.fft);
   size_t need = (size_t)(2 * p->host.fft.m * sizeof(V));
   int limit = g_max_smem - (int)sizeof(SharedMem) - 1024;
+  // PSG_TRACE=0 in the environment (read at plan creation) keeps corr_kernel
+  const char* te = getenv("PSG_TRACE");
+  if (sizeof(T) == 4 && !(te && atoi(te) == 0) && (int64_t)need <= limit) {
+    if (const TracePlanInfo* tp = corr_plans_for((int)p->host.fft.m)[0]) {
+      allow_smem(tp->kernel[0][0]);
+      int per = 0;
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tp->kernel[0][0], tp->nt, need));
+      if (per > 0) {
+        p->trace = tp;
+        p->tw_pass = upload(p->keep, trace_twiddles(*tp));
+        p->trace_grid = per * g_sm_count;
+      }
+    }
+  }
   allow_smem((const void*)corr_kernel<T>);
   if ((int64_t)need <= limit) {
     p->smem = need;
@@ -1362,6 +1527,10 @@ static std::unique_ptr<psg_plan> make_plan(const psg_op* ops, int32_t n_ops, int
   }
   ensure_device();
   CUDA_OK(cudaGetDevice(&p->device));
+  for (size_t part = 0; part < p->host.parts.size(); part++) {
+    p->trace.push_back(trace_plan_of(p.get(), (int)part));
+    p->trace_recipe.push_back(p->recipe[part] == RC_DFAN ? 1 : 0);
+  }
   if (dtype == PSG_F32) build_device_steps<float>(p.get());
   else build_device_steps<double>(p.get());
   if (p->wide) std::fill(p->recipe.begin(), p->recipe.end(), (int)RC_GENERIC);
@@ -1554,6 +1723,77 @@ int psg_apply_keyed(const psg_plan* plan, psg_workspace* ws, const void* src, vo
     }
     CUDA_OK(cudaGetLastError());
   });
+}
+
+// ------------------------------------------------------------ graph replay
+// One psg_apply_keyed captured into a CUDA graph on a stream of its own, for
+// replay: a launch then costs the host one call (no checks, no per-part
+// launches). The graph holds the call's pointers: the plan's tables, the
+// workspace's slots, the blocks and the row arrays.
+}  // extern "C"
+struct psg_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+extern "C" {
+
+int psg_graph_capture(const psg_plan* plan, psg_workspace* ws, const void* src, void* dst, int64_t rows, int32_t cols,
+                      const int32_t* live, const double* start_ms, const psg_keys* keys, double dt_ms,
+                      psg_graph** out) {
+  cudaStream_t s = nullptr;
+  std::unique_ptr<psg_graph> g(new psg_graph());
+  int st = guarded([&] {
+    if (!out) throw InvalidArg("null argument");
+    *out = nullptr;
+    check_apply(plan, ws, src, dst, rows, cols, live, dt_ms, true, keys);
+    ensure_device();
+    CUDA_OK(cudaGetDevice(&g->device));
+    // the kernels' shared-memory attributes are set before the capture
+    for (int part = 0; part < (int)plan->host.parts.size(); part++) {
+      if (part < (int)plan->trace.size() && plan->trace[part])
+        allow_smem(plan->trace[part]->kernel[plan->trace_recipe[part]][plan->trace_pf ? 1 : 0]);
+      allow_smem(plan->wide ? (plan->host.dtype == PSG_F32 ? wide_kernel_for<float>() : wide_kernel_for<double>())
+                            : (plan->host.dtype == PSG_F32 ? pipe_kernel_for<float>(plan->recipe[part], plan->prefetch)
+                                                           : pipe_kernel_for<double>(plan->recipe[part], plan->prefetch)));
+    }
+    CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_OK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      for (int part = 0; part < (int)plan->host.parts.size(); part++) {
+        const void* from = part == 0 ? src : nullptr;
+        if (plan->host.dtype == PSG_F32)
+          launch_part<float>(plan, ws, part, from, dst, rows, cols, live, start_ms, s, keys, dt_ms);
+        else
+          launch_part<double>(plan, ws, part, from, dst, rows, cols, live, start_ms, s, keys, dt_ms);
+      }
+    } catch (...) {
+      cudaGraph_t dead = nullptr;
+      cudaStreamEndCapture(s, &dead);
+      if (dead) cudaGraphDestroy(dead);
+      throw;
+    }
+    CUDA_OK(cudaStreamEndCapture(s, &g->graph));
+    CUDA_OK(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  });
+  if (s) cudaStreamDestroy(s);
+  if (st == PSG_OK) *out = g.release();
+  else if (g->graph) cudaGraphDestroy(g->graph);
+  return st;
+}
+
+int psg_graph_launch(psg_graph* g, void* stream) {
+  return guarded([&] {
+    if (!g || !g->exec) throw InvalidArg("null argument");
+    CUDA_OK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  });
+}
+
+void psg_graph_destroy(psg_graph* g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
 }
 
 int psg_apply_host(const psg_plan* plan, psg_workspace* ws, const void* src_host, void* dst_host, int64_t rows,
@@ -2239,8 +2479,16 @@ static int corr_launch(const psg_corr_plan* plan, psg_stack* st, const void* src
     }
     int grid = (int)std::min<int64_t>(rows, plan->grid);
     cudaStream_t s = (cudaStream_t)stream;
-    if (plan->dtype == PSG_F32) corr_kernel<float><<<grid, kCorrThreads, plan->smem, s>>>(a);
-    else corr_kernel<double><<<grid, kCorrThreads, plan->smem, s>>>(a);
+    if (plan->trace) {
+      a.tw_pass = plan->tw_pass;
+      void* args[] = {&a};
+      CUDA_OK(cudaLaunchKernel(plan->trace->kernel[0][0], dim3((int)std::min<int64_t>(rows, plan->trace_grid)),
+                               dim3(plan->trace->nt), args, plan->smem, s));
+    } else if (plan->dtype == PSG_F32) {
+      corr_kernel<float><<<grid, kCorrThreads, plan->smem, s>>>(a);
+    } else {
+      corr_kernel<double><<<grid, kCorrThreads, plan->smem, s>>>(a);
+    }
     CUDA_OK(cudaGetLastError());
   });
 }

@@ -38,6 +38,12 @@ struct DevStep {
   const void* bridge;  // Quad<T>[m]: the split · gain · unsplit map of each bin pair
   const void* fall;
   const void* tw;
+  const void* tw_pass;  // the trace kernel's twiddles, pass by pass (psg_trace.cuh)
+  // the trace kernel's split twiddles (float4 per bin pair: bins c and m − c)
+  // and bin gains (float2 per bin pair), and 1/nfft in float32
+  const void* ref_split;
+  const void* ref_gain;
+  float ref_scale, _pad3;
   const void* table;
   psg_gain_curve curve;
   // mutes: the curve (knots: |offset| knots then their times) and the taper
@@ -1245,6 +1251,42 @@ __global__ void __launch_bounds__(kNT, (GW || sizeof(T) == 8 ? 2 : 4)) pipeline_
     __syncthreads();
   }
 }
+
+// ============================================================ correlation
+// One launch of correlateInto (psg_cuda.cu corr_kernel, psg_trace.cuh
+// corr_trace_kernel).
+struct CorrArgs {
+  const void* src;
+  void* dst;
+  long long rows;
+  int cols, out, nfft, shift, pilot_len, record;
+  const int* live;
+  const void* bridge;  // Quad<T>[m]: the split · multiplier · unsplit map of each bin pair
+  const void* tw;
+  const void* tw_pass;  // the compile-time transform's twiddles, pass by pass (corr_trace_kernel)
+  FftDesc fft;
+  void* gwork;        // per-CTA global scratch when shared memory is too small (else NULL)
+  // stack epilogue
+  double* num;
+  int* cnt;
+  int stack_samples;
+  long long stack_rows;
+  const int* row_map;
+  const int* stack_live;
+  int stack_on;
+};
+
+// Complex input c of a record's forward transform: samples 2c and 2c + 1
+// of the record (read-only global memory), 0 past its n samples.
+template <class T> struct RecordLoad {
+  typedef typename C2<T>::type V;
+  const T* x;
+  int n;
+  __device__ __forceinline__ V operator()(int c, bool) const {
+    const int k = 2 * c;
+    return V{k < n ? __ldg(x + k) : (T)0, k + 1 < n ? __ldg(x + k + 1) : (T)0};
+  }
+};
 
 // The kernel instantiations: a pointer for cudaLaunchKernel, the occupancy
 // query and the shared-memory attribute. BATCH is float32 only.

@@ -214,6 +214,30 @@ class PipelinePlan:
             A.check(fn(self.h, ws.h, None if src is None else p(src), p(dst), rows, cols, p(live), p(start), keys,
                        meta.dtMs, stream if stream is not None else None))
 
+    def capture(self, src, dst, meta: ChunkMeta, ws: Workspace) -> "ApplyGraph":
+        """``apply(src, dst, meta, ws)`` on CUDA tensors (src None: in place)
+        captured into a CUDA graph: ``replay()`` reruns it with one host
+        call. The checks run here, once; the tensors, the meta's device
+        arrays and the workspace must outlive the graph, and the workspace
+        must not be grown while it lives."""
+        import torch
+        self._check_block(dst, "dst")
+        if not _is_torch(dst):
+            raise ValueError("capture takes CUDA tensors")
+        rows, cols = int(dst.shape[0]), int(dst.shape[1])
+        if src is not None:
+            self._check_block(src, "src")
+            if tuple(src.shape) != tuple(dst.shape):
+                raise ValueError(f"src is {src.shape[0]} × {src.shape[1]}, dst {rows} × {cols}")
+        meta.checkShape(rows)
+        live, start = meta.device(cols, 0, dst.device.index)
+        keys = self._keys(meta, dst.device.index)
+        h = C.c_void_p()
+        A.check(A.lib().psg_graph_capture(self.h, ws.h, None if src is None else src.data_ptr(), dst.data_ptr(),
+                                          rows, cols, live.data_ptr(), start.data_ptr(), keys, meta.dtMs,
+                                          C.byref(h)))
+        return ApplyGraph(h, (self, ws, src, dst, live, start, keys))
+
     @property
     def needsKeys(self) -> bool:
         """The plan mutes: it reads each row's offset and t0Ms."""
@@ -301,6 +325,26 @@ class PipelinePlan:
         A.check(A.lib().psg_panel_factor(self.h, ws.h, part, b.data_ptr(), rows, cols,
                                          live.data_ptr(), out.data_ptr(), st))
         return float(out.item())
+
+
+class ApplyGraph:
+    """A captured apply (``PipelinePlan.capture``): ``replay(stream)`` runs it
+    on ``stream`` (the current stream when None)."""
+
+    def __init__(self, h, keep):
+        self.h = h
+        self._keep = keep  # what the graph points at stays alive with it
+
+    def replay(self, stream=None):
+        import torch
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        A.check(A.lib().psg_graph_launch(self.h, st))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and A._lib is not None:
+            A._lib.psg_graph_destroy(h)
+            self.h = None
 
 
 def compile(pipeline, T, dtMs: float, samples: int, recordSamples: int = 0) -> PipelinePlan:

@@ -43,6 +43,8 @@ def test_trace_stats_match_oracle(dt):
     assert len(got) == data.shape[0]
     for r, s in enumerate(got):
         for g, w in ((s.rms, want_rms[r]), (s.maxAbs, want_mx[r])):
+            if g == w:
+                continue
             if math.isnan(w):
                 assert math.isnan(g), (r, g, w)
             else:
@@ -67,6 +69,8 @@ def test_panel_stats_match_oracle(dt, clip):
     got = P.panelStats(torch.from_numpy(data).cuda(), meta, clipPercentile=clip)
     assert got.rows == want["rows"] and got.samples == want["samples"]
     for g, w in ((got.rms, want["rms"]), (got.maxAbs, want["maxAbs"]), (got.clip, want["clip"])):
+        if g == w:
+            continue
         if math.isnan(w):
             assert math.isnan(g)
         else:
