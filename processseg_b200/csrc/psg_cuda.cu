@@ -1303,18 +1303,20 @@ template <class T> static void build_device_steps(psg_plan* p) {
   const TracePlanInfo* tp = nullptr;
   for (auto* t : p->trace) tp = t ? t : tp;
   if (tp && !p->wide) {
-    const int64_t fw = 2 * (int64_t)tp->m * 8;
+    const int64_t fw = 2 * (int64_t)tp->buf * 8;
+    // the CTAs per SM of the recipes the plan's parts use (the smallest)
     auto occ = [&](bool pf) {
       const size_t sm = (size_t)((pf ? 2 : 1) * p->x_bytes + fw);
-      int best = 0;
-      for (int r = 0; r < 2; r++) {
-        const void* k = tp->kernel[r][pf ? 1 : 0];
+      int best = -1;
+      for (size_t part = 0; part < p->trace.size(); part++) {
+        if (!p->trace[part]) continue;
+        const void* k = p->trace[part]->kernel[p->trace_recipe[part]][pf ? 1 : 0];
         allow_smem(k);
         int per = 0;
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, tp->nt, sm));
-        best = r == 0 ? per : std::min(best, per);
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, p->trace[part]->nt, sm));
+        best = best < 0 ? per : std::min(best, per);
       }
-      return best;
+      return std::max(best, 0);
     };
     const int one = occ(false), two = occ(true);
     p->trace_pf = two > 0 && two >= one;

@@ -57,6 +57,15 @@ template <int M_, int NT_, int MINB_, int... Rs> struct FPlan {
 
 __device__ __forceinline__ float2* smem_c() { return reinterpret_cast<float2*>(psg_dyn_smem); }
 
+// A row of floats in the block's dynamic shared memory, held as an offset
+// from the shared symbol (in floats): accesses through it compile to 32-bit
+// shared loads and stores, where a pointer chosen at run time between the
+// row buffers would be a generic 64-bit one.
+struct SRow {
+  int o;
+  __device__ __forceinline__ float& operator[](int i) const { return reinterpret_cast<float*>(psg_dyn_smem)[o + i]; }
+};
+
 // A pass's inputs from the buffer at complex offset o.
 struct BufLd {
   int o;
@@ -244,6 +253,15 @@ template <int M_, int NT_, int MINB_, class... Gs> struct RPlan {
     return o;
   }
   static_assert(stride(NP) == M, "the stages multiply to M");
+  // The first pass writes outputs R·b + k (stride 1): for an even R, lanes
+  // of a warp store 8-byte values R·8 bytes apart, into a quarter or less of
+  // the banks. Its buffer is then laid out with one spare element after
+  // every R (output c at c + c/R), which spreads those stores over all banks;
+  // the second pass reads it so (input c = b + j·B at b + b/R + j·(B + B/R),
+  // B a multiple of R).
+  static constexpr int PAD = (NP > 1 && radix(0) % 2 == 0) ? radix(0) : 0;
+  // complex elements of one transform buffer
+  static constexpr int BUF = M + (PAD ? M / (PAD ? PAD : 1) : 0);
 };
 
 // Pass I of RPlan P. The first stage's butterflies are p + jB·(M/(S·R))
@@ -254,20 +272,31 @@ template <int M_, int NT_, int MINB_, class... Gs> struct RPlan {
 // The last stage of a transform has p = 0 and unit twiddles (the reference
 // multiplies by (1, −0), which leaves every value as it is): they are
 // skipped.
-template <class P, int I, class LD, class ST>
+// OUTPAD (the first pass, stride 1): its outputs go to the padded layout
+// (output c = R·p + k at c + p); INPAD (the second pass): ld is a BufLd of a
+// buffer in that layout.
+template <class P, int I, int OUTPAD = 0, int INPAD = 0, class LD, class ST>
 __device__ __forceinline__ void ref_pass(const float2* __restrict__ tw, const LD& ld, const ST& st) {
   constexpr int R = P::radix(I), R1 = P::G1[I], R2 = P::G2[I], S = P::stride(I), M = P::M, NT = P::NT;
   constexpr int B = M / R;
   constexpr bool LAST = I == P::NP - 1;
   constexpr int U = (B + NT - 1) / NT;
   constexpr int TW = P::tws(R);
+  static_assert(OUTPAD == 0 || (S == 1 && OUTPAD == R), "the padded layout is the first pass's");
+  static_assert(INPAD == 0 || B % INPAD == 0, "the second pass's inputs stay B + B/R apart");
 #pragma unroll
   for (int u = 0; u < U; u++) {
     const int b = (int)threadIdx.x + u * NT;
     if (B % NT != 0 && b >= B) continue;
     float2 v[R];
+    if constexpr (INPAD != 0) {
+      const float2* x = smem_c() + ld.o + b + b / INPAD;
 #pragma unroll
-    for (int j = 0; j < R; j++) v[j] = ld(b + j * B, j);
+      for (int j = 0; j < R; j++) v[j] = x[j * (B + B / INPAD)];
+    } else {
+#pragma unroll
+      for (int j = 0; j < R; j++) v[j] = ld(b + j * B, j);
+    }
     const int p = LAST ? 0 : b / S;
     const float2* t = tw + P::tw_off(I) + p * TW;
     float2 out[R];
@@ -297,7 +326,7 @@ __device__ __forceinline__ void ref_pass(const float2* __restrict__ tw, const LD
           out[R1 * kB + kA] = (kB == 0 || LAST) ? c[kB] : mul_tw(c[kB], __ldg(t + R2 * (R1 - 1) + kB - 1));
       }
     }
-    const int base = b + (S * (R - 1)) * p;
+    const int base = b + (S * (R - 1)) * p + (OUTPAD ? p : 0);
 #pragma unroll
     for (int k = 0; k < R; k++) st(base + S * k, out[k]);
   }
@@ -305,10 +334,11 @@ __device__ __forceinline__ void ref_pass(const float2* __restrict__ tw, const LD
 
 template <class P, int I> struct RefPasses {
   template <class ST> static __device__ __forceinline__ void run(int x, int y, const float2* tw, const ST& last) {
+    constexpr int IN = I == 1 ? P::PAD : 0;
     if constexpr (I == P::NP - 1) {
-      ref_pass<P, I>(tw, BufLd{x}, last);
+      ref_pass<P, I, 0, IN>(tw, BufLd{x}, last);
     } else {
-      ref_pass<P, I>(tw, BufLd{x}, BufSt{y});
+      ref_pass<P, I, 0, IN>(tw, BufLd{x}, BufSt{y});
       __syncthreads();
       RefPasses<P, I + 1>::run(y, x, tw, last);
     }
@@ -320,7 +350,7 @@ __device__ __forceinline__ void ref_fft(int a, int b, const float2* tw, const LD
   if constexpr (P::NP == 1) {
     ref_pass<P, 0>(tw, ld, last);
   } else {
-    ref_pass<P, 0>(tw, ld, BufSt{b});
+    ref_pass<P, 0, P::PAD>(tw, ld, BufSt{b});
     __syncthreads();
     RefPasses<P, 1>::run(b, a, tw, last);
   }
@@ -370,13 +400,72 @@ struct RefBridgeLd {
   }
 };
 
+// The same steps for a pair of inputs at once, in place: bins c and m − c
+// come from z[c] and z[m − c] and give the inverse transform's inputs c and
+// m − c, so one thread splits, scales and unsplits both (every rounding as
+// RefBridgeLd's: the pair's even and odd parts are shared, up to exact sign
+// changes and commuted sums). The thread taking c = 0 also takes c = m/2
+// when m is even (both their own partners).
+template <int M, int NT>
+__device__ __forceinline__ void ref_bridge_pairs(int zo, const float4* __restrict__ sp, const float2* __restrict__ g,
+                                                 float scale) {
+  float2* z = smem_c() + zo;
+  constexpr int PAIRS = (M - 1) / 2;  // c = 1 .. PAIRS with m − c > c
+  for (int t = threadIdx.x; t <= PAIRS; t += NT) {
+    if (t == 0) {
+      const float2 z0 = z[0];
+      const float2 gg = __ldg(g);
+      const float x0 = fm(fa(z0.x, z0.y), gg.x), xm = fm(fs(z0.x, z0.y), gg.y);
+      z[0] = make_float2(fm(fs(x0, xm), scale), fm(fa(x0, xm), scale));
+      if constexpr (M % 2 == 0) {
+        // c = m/2 pairs with itself: bin m/2 from A = B = z[m/2]
+        constexpr int c = M / 2;
+        const float2 A = z[c];
+        const float4 w = __ldg(sp + c);
+        const float gc = __ldg(g + c).x;
+        const float er = fm(0.5f, fa(A.x, A.x)), ei = fm(0.5f, fs(A.y, A.y));
+        const float orr = fm(0.5f, fa(A.y, A.y)), oi = fm(0.5f, fs(A.x, A.x));
+        const float Xr = fm(fs(fa(er, fm(w.x, orr)), fm(w.y, oi)), gc);
+        const float Xi = fm(fa(fa(ei, fm(w.x, oi)), fm(w.y, orr)), gc);
+        const float e_r = fa(Xr, Xr), e_i = fs(Xi, Xi), dr = fs(Xr, Xr), di = fa(Xi, Xi);
+        const float wr = w.x, wi = -w.y;
+        const float o_r = fs(fm(dr, wr), fm(di, wi)), o_i = fa(fm(dr, wi), fm(di, wr));
+        z[c] = make_float2(fm(fa(e_i, o_r), scale), fm(fs(e_r, o_i), scale));
+      }
+      continue;
+    }
+    const int c = t, d = M - t;
+    const float2 A = z[c], Bv = z[d];
+    const float4 w = __ldg(sp + c);  // split twiddles of bins c (x, y) and m − c (z, w)
+    const float2 gg = __ldg(g + c);  // gains of bins c and m − c
+    const float er = fm(0.5f, fa(A.x, Bv.x)), ei = fm(0.5f, fs(A.y, Bv.y));
+    const float orr = fm(0.5f, fa(A.y, Bv.y)), oi = fm(0.5f, fs(Bv.x, A.x));
+    const float Xr = fm(fs(fa(er, fm(w.x, orr)), fm(w.y, oi)), gg.x);
+    const float Xi = fm(fa(fa(ei, fm(w.x, oi)), fm(w.y, orr)), gg.x);
+    const float Yr = fm(fs(fa(er, fm(w.z, orr)), fm(w.w, -oi)), gg.y);
+    const float Yi = fm(fa(fa(-ei, fm(w.z, -oi)), fm(w.w, orr)), gg.y);
+    // splitInverse of bin c (a = X, b = Y) and of bin m − c (a = Y, b = X)
+    const float e_r = fa(Xr, Yr), e_i = fs(Xi, Yi), dr = fs(Xr, Yr), di = fa(Xi, Yi);
+    {
+      const float wr = w.x, wi = -w.y;
+      const float o_r = fs(fm(dr, wr), fm(di, wi)), o_i = fa(fm(dr, wi), fm(di, wr));
+      z[c] = make_float2(fm(fa(e_i, o_r), scale), fm(fs(e_r, o_i), scale));
+    }
+    {
+      const float wr = w.z, wi = -w.w;
+      const float o_r = fs(fm(-dr, wr), fm(di, wi)), o_i = fa(fm(-dr, wi), fm(di, wr));
+      z[d] = make_float2(fm(fa(-e_i, o_r), scale), fm(fs(e_r, o_i), scale));
+    }
+  }
+}
+
 // ----------------------------------------------------------- pack, unpack
 // packInto with zero pads (filter/apply.nim:194-216) as the first pass reads
 // it: complex input c holds real samples 2c and 2c + 1 of the padded trace,
 // sample j = i + p being x[i] − pre − (a + b·i) in float64 rounded once to
 // float32 for 0 ≤ i < n, 0 in the pads.
 struct PackLd {
-  const float* X;
+  SRow X;
   int n, p;
   float pre;
   double a, b;
@@ -421,7 +510,7 @@ struct BridgeLd {
 // goes to x[i] for 0 ≤ i < n, plus the trend ga + gb·i in float64 when the
 // filter passes it. The thread's Σx² of what it writes accumulates in s2.
 template <bool ADD> struct UnpackSt {
-  float* X;
+  SRow X;
   int n, p;
   double ga, gb;
   mutable float s2;
@@ -489,7 +578,7 @@ template <int NT> __device__ __forceinline__ void fold2(const TkShared<NT>& S, i
 // The sums, divisors (w; i + h + 1 at the head; n at the whole-trace head;
 // n − (i − h) at the tail) and gain are pipeline_kernel's.
 template <int NT, int E, bool NEED_MX>
-__device__ __forceinline__ unsigned long long agc_groups(const float* __restrict__ X, float* __restrict__ Y, int n,
+__device__ __forceinline__ unsigned long long agc_groups(const SRow X, const SRow Y, int n,
                                                          int h, bool rms_mode, float r, float k, float eps) {
   constexpr int W = NT / 32;
   const int w = 2 * h + 1;
@@ -587,13 +676,20 @@ __device__ __forceinline__ unsigned long long agc_groups(const float* __restrict
 // Stores a row from shared memory: 16-byte vectors where the destination
 // allows, Y's elements [0, len) (Y placed so that Y + head is 16-byte
 // aligned when `to` + head is).
-template <int NT> __device__ __forceinline__ void store_row(const float* Y, float* __restrict__ to, int len) {
+template <int NT> __device__ __forceinline__ void store_row(const SRow Y, float* __restrict__ to, int len) {
   const int head = min((int)((4 - (((uintptr_t)to >> 2) & 3)) & 3), len);
   const int nv = (len - head) >> 2;
   for (int i = threadIdx.x; i < head; i += NT) to[i] = Y[i];
-  const float4* yv = reinterpret_cast<const float4*>(Y + head);
   float4* gv = reinterpret_cast<float4*>(to + head);
-  for (int v = threadIdx.x; v < nv; v += NT) __stcs(gv + v, yv[v]);
+  if (((Y.o + head) & 3) == 0) {
+    const float4* yv = reinterpret_cast<const float4*>(psg_dyn_smem) + ((Y.o + head) >> 2);
+    for (int v = threadIdx.x; v < nv; v += NT) __stcs(gv + v, yv[v]);
+  } else {
+    for (int v = threadIdx.x; v < nv; v += NT) {
+      const int i = head + 4 * v;
+      __stcs(gv + v, make_float4(Y[i], Y[i + 1], Y[i + 2], Y[i + 3]));
+    }
+  }
   for (int i = head + 4 * nv + threadIdx.x; i < len; i += NT) to[i] = Y[i];
 }
 
@@ -645,7 +741,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   __syncthreads();
   // the two transform buffers (complex offsets) and, after the transforms,
   // the output row Y in their place
-  const int ao = a.work_off / 8, bo = ao + P::M;
+  const int ao = a.work_off / 8, bo = ao + P::BUF;
   uint32_t phase[2] = {0, 0};
   int cur = 0;
   for (long long t = blockIdx.x; t < total; t += gridDim.x, cur = PF ? cur ^ 1 : 0) {
@@ -675,14 +771,14 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
     phase[cur] ^= 1;
     const RowCtx<float> c = row_ctx<float, false>(a, t);
     const RowSlot sl = slot[cur];
-    float* X = reinterpret_cast<float*>(psg_dyn_smem + cur * a.x_bytes + sl.off);
+    const SRow X{(cur * a.x_bytes + sl.off) >> 2};
     for (int i = threadIdx.x; i < sl.head; i += NT) X[i] = c.from[i];
     for (int i = sl.tail + threadIdx.x; i < sl.len; i += NT) X[i] = c.from[i];
     if (sl.head > 0 || sl.tail < sl.len) __syncthreads();
     const int n = c.n;
     const int len = c.copy ? c.cols : n;
     // Y: the output row, aligned like the destination row
-    float* Y = reinterpret_cast<float*>(smem_c() + ao) + (((uintptr_t)c.to >> 2) & 3);
+    const SRow Y{2 * ao + (int)(((uintptr_t)c.to >> 2) & 3)};
     bool from_y = false;
     if (n > 0) {
       const DevStep* d = c.steps + c.first;
@@ -736,8 +832,10 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       const double gb = tb * fd.dc_gain;
       const double ga = fd.zero_dc ? -gb * (double)(n - 1) / 2 : ta * fd.dc_gain;
       const int za = zo == ao ? bo : ao;  // the inverse's first pass writes the other buffer
-      const RefBridgeLd br{zo, P::M, reinterpret_cast<const float4*>(fd.ref_split),
-                           reinterpret_cast<const float2*>(fd.ref_gain), fd.ref_scale};
+      ref_bridge_pairs<P::M, NT>(zo, reinterpret_cast<const float4*>(fd.ref_split),
+                                 reinterpret_cast<const float2*>(fd.ref_gain), fd.ref_scale);
+      __syncthreads();
+      const BufLd br{zo};
       if (ga == 0 && gb == 0) {
         const UnpackSt<false> un{X, n, pad, 0, 0, 0.f};
         ref_fft<P>(zo, za, tw, br, un);
@@ -796,7 +894,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       if constexpr (RECIPE == RC_DFAN) {
         // (6) per-trace normalization of the AGC's output (its max |x| for
         // the NaN rule of the percentile, gain/gain.nim:198-219)
-        float* Z = from_y ? Y : X;
+        float* Z = reinterpret_cast<float*>(psg_dyn_smem) + (from_y ? Y.o : X.o);
         Stats st{0, 0, 0, 0};
         st.mx = bits_value(block_max_u64(mx, SN.m->redu[SN.flip]), 0.f);
         SN.flip ^= 1;
@@ -823,7 +921,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
         store_row<NT>(Y, c.to, len);
       } else {
         __syncthreads();
-        store_out(X, c.to, len);
+        store_row<NT>(X, c.to, len);
       }
     }
     __syncthreads();

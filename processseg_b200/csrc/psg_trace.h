@@ -18,6 +18,7 @@ struct TracePlanInfo {
   int g1[8], g2[8];
   int agc_e;
   int min_blocks;            // the CTAs per SM its launch bounds ask for
+  int buf;                   // complex elements of each of its two transform buffers
   const void* kernel[2][2];  // [recipe][prefetch]
 };
 

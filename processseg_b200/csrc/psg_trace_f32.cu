@@ -26,6 +26,7 @@ template <class P, int E> TracePlanInfo info() {
   }
   t.agc_e = E;
   t.min_blocks = P::MINB;
+  t.buf = P::BUF;
   t.kernel[0][0] = (const void*)tk::trace_kernel<P, RC_DFA, false, E>;
   t.kernel[0][1] = (const void*)tk::trace_kernel<P, RC_DFA, true, E>;
   t.kernel[1][0] = (const void*)tk::trace_kernel<P, RC_DFAN, false, E>;
@@ -43,6 +44,7 @@ template <class P> TracePlanInfo corr_info() {
     t.g1[i] = P::radix(i);
   }
   t.min_blocks = P::MINB;
+  t.buf = P::M;
   t.kernel[0][0] = (const void*)tk::corr_trace_kernel<P>;
   return t;
 }
