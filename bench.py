@@ -549,8 +549,8 @@ def run_ours(args):
         try:
             with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
                 tj = json.load(f)
-            traffic = tj.get("pipeline_kernel_c2_bytes")
-            insts = tj.get("pipeline_kernel_c2_warp_instructions")
+            traffic = tj.get("trace_kernel_c2_bytes")
+            insts = tj.get("trace_kernel_c2_warp_instructions")
         except Exception:
             pass
         line = {
@@ -561,7 +561,7 @@ def run_ours(args):
             "config": config(world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "pipeline_kernel<float>", "algorithmic_bytes": alg_bytes},
+                         "kernel": "trace_kernel<RPlan<1944>> (float32 demean/filter/AGC)", "algorithmic_bytes": alg_bytes},
             # the bound that sets the time: warp-instruction issue, with the
             # launch's instruction count from its ncu capture over the measured
             # kernel time, against 4 schedulers x SMs x the clock seen
