@@ -318,6 +318,18 @@ def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
                           "requests_per_launch": sat_launch}}
 
 
+def launch_of(plan, rows):
+    """The trace-kernel launch shape the tuner chose for a call of ``rows``
+    rows (the first one untuned), with its per-shape times (µs per launch)."""
+    tun = plan.tuning()
+    if not tun["parts"]:
+        return None
+    part = tun["parts"][0]
+    rec = next((t for t in tun["tuned"] if t["part"] == part["part"] and t["class"] == int(rows).bit_length()), None)
+    return {"chosen": part["shapes"][rec["choice"] if rec else 0], "tuner_us_per_shape": rec["us"] if rec else None,
+            "shapes": part["shapes"]}
+
+
 def workloads_leg(peak):
     """The other configurations, device-resident, each timed with CUDA events
     after a warm-up: C1 (48×2001, demean → band-pass 4-8-60-80 → AGC 500 ms),
@@ -351,8 +363,13 @@ def workloads_leg(peak):
     src = torch.from_numpy(g.data).cuda()
     dst = torch.empty_like(src)
     t = timed(lambda: plan.apply(src, dst, meta, ws), 200)
+    # the same apply captured once and replayed: one host call per panel
+    gr = plan.capture(src, dst, meta, ws)
+    tg = timed(gr.replay, 200)
+    del gr
     out["c1"] = {"workload": "48x2001 f32 @2ms: demean -> bandpass 4-8-60-80 -> AGC 500 ms", "us_per_panel": t * 1e6,
-                 "msamples_per_s": 48 * 2001 / t / 1e6, "hbm_frac": 2 * 48 * 2001 * 4 / t / 1e9 / peak}
+                 "msamples_per_s": 48 * 2001 / t / 1e6, "hbm_frac": 2 * 48 * 2001 * 4 / t / 1e9 / peak,
+                 "us_per_panel_graph_replay": tg * 1e6, "launch": launch_of(plan, 48)}
 
     spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
     pilot = P.generatePilot(spec, np.float64)
@@ -390,7 +407,7 @@ def workloads_leg(peak):
     t = timed(lambda: plan.apply(src, dst, meta, ws), 3)
     out["c5"] = {"workload": "50000x6001 f32 @1ms (1.2 GB), live U{4000..6001}: demean -> bandpass 2/5/120/150 -> AGC 250 ms -> per-trace p99",
                  "ms_per_panel": t * 1e3, "msamples_per_s": 50000 * 6001 / t / 1e6,
-                 "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak}
+                 "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak, "launch": launch_of(plan, 50000)}
     del src, dst
     torch.cuda.empty_cache()
 
@@ -577,6 +594,7 @@ def run_ours(args):
                     "one_at_a_time": e2e_sync},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
+            "launch": launch_of(plan, ROWS),
         }
         if line["issue"]:
             line["issue"]["frac"] = line["issue"]["achieved"] / line["issue"]["peak"]

@@ -205,6 +205,33 @@ int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part);
 /* 1 when the plan mutes: it is applied with its rows' keys (the _keyed
  * entry points; the others refuse it with PSG_EINVAL). */
 int32_t psg_plan_needs_keys(const psg_plan* plan);
+/* ------------------------------------------------------------ launch tuning
+ * A float32 part of exactly demean, filter (zero pads), AGC (and a per-trace
+ * normalization) whose transform length has compile-time builds runs on the
+ * trace kernel. Its launch shapes: each build (the reference's FFT stages
+ * grouped into passes one way, a register budget, a CTA width), with or
+ * without the next row's copy in flight, on a persistent grid or one CTA
+ * per row. Every shape gives the same bits. The first apply of such a part
+ * at a row count of a new class (the count's bit length) times every shape
+ * on the call's own input into a scratch block (waiting for the stream once)
+ * and keeps the fastest for that class; PSG_TUNE=0 in the environment at
+ * compile keeps the first shape, and so does an apply under stream capture
+ * before the class is tuned. No counterpart in the reference, whose FFT plan
+ * has one factorization per length (fft/plan.nim:120-160). */
+/* The number of launch shapes of part `part` (0 when the part runs on
+ * pipeline_kernel or does not exist). */
+int32_t psg_plan_trace_shapes(const psg_plan* plan, int32_t part);
+/* Pins part `part` to launch shape `shape` for every row count (-1 unpins:
+ * the tuner's choices apply again). PSG_EINVAL for a part without shapes or
+ * a shape out of range. */
+int psg_plan_pin_trace(psg_plan* plan, int32_t part, int32_t shape);
+/* The launch shapes and the tuner's record as JSON, written into buf (cap
+ * bytes with the terminating NUL, truncated to fit); *needed (when not
+ * NULL) gets the full length + 1. {"parts": [{"part", "pinned", "shapes":
+ * [{"m", "threads", "min_blocks", "passes", "prefetch", "grid",
+ * "ctas_per_sm", "smem"}]}], "tuned": [{"part", "class", "rows", "us",
+ * "choice"}]}. */
+int psg_plan_tuning(const psg_plan* plan, char* buf, int64_t cap, int64_t* needed);
 int32_t psg_plan_len(const psg_plan* plan);
 /* For step i of the plan: its FFT length (0 for steps without one) and the
  * pad laid out each side (FilterPlan.nfft / pad, filter/apply.nim:161-164). */

@@ -174,6 +174,9 @@ def _declare(lib):
         "psg_graph_launch": (C.c_int, [P, P]),
         "psg_graph_destroy": (None, [P]),
         "psg_plan_needs_keys": (I32, [P]),
+        "psg_plan_trace_shapes": (I32, [P, I32]),
+        "psg_plan_pin_trace": (C.c_int, [P, I32, I32]),
+        "psg_plan_tuning": (C.c_int, [P, P, I64, C.POINTER(I64)]),
         "psg_applied_response": (C.c_int, [C.POINTER(OpC), I32, I32, DBL, I32, P, I32, P, P]),
         "psg_spectrum_plan_create": (C.c_int, [I32, DBL, I32, DBL, I32, I32, C.POINTER(P)]),
         "psg_spectrum_plan_destroy": (None, [P]),

@@ -11,13 +11,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 OUT = os.path.join(PKG, "libpsgcuda.so")
 OBJ = os.path.join(HERE, "_build")
-SOURCES = ["psg_pipe_f32.cu", "psg_recipe_f32.cu", "psg_pipe_f64.cu", "psg_recipe_f64.cu", "psg_trace_f32.cu",
+TRACE_UNITS = ["psg_trace_f32.cu", "psg_trace_m1944.cu", "psg_trace_m1125.cu", "psg_trace_m3375.cu"]
+SOURCES = ["psg_pipe_f32.cu", "psg_recipe_f32.cu", "psg_pipe_f64.cu", "psg_recipe_f64.cu", *TRACE_UNITS,
            "psg_cuda.cu", "psg_plan.cpp"]
 PUBLIC = os.path.join("..", "..", "include", "psg.h")
 # the headers each unit includes (a unit recompiles when it or one of them changes)
 KERNEL_HEADERS = ["psg_kernel.cuh", "psg_device.cuh", "psg_internal.h", "psg_dft_consts.h", "psg_trace.h", PUBLIC]
 HEADERS = {src: KERNEL_HEADERS for src in SOURCES}
-HEADERS["psg_trace_f32.cu"] = KERNEL_HEADERS + ["psg_trace.cuh"]
+for _u in TRACE_UNITS:
+    HEADERS[_u] = KERNEL_HEADERS + ["psg_trace.cuh"]
 HEADERS["psg_plan.cpp"] = ["psg_internal.h", PUBLIC]
 DEPS = SOURCES + sorted({h for hs in HEADERS.values() for h in hs})
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -770,6 +771,26 @@ using namespace psg;
 __global__ void trace_stats_finish(double* rms, double* mx, const int* live, long long rows, int cols);
 
 // =================================================================== plans
+// A launch shape of a trace-kernel build: the build, the next row's bulk
+// copy in flight (pf), one CTA per row (the block scheduler balancing
+// ragged rows) or a persistent grid of per_sm CTAs per SM, the row
+// buffers' size before the transform buffers (work_off), the dynamic
+// shared memory, and the build's twiddles pass by pass.
+struct TraceCand {
+  const TracePlanInfo* tp = nullptr;
+  bool pf = false, per_row = false;
+  int per_sm = 0, work_off = 0;
+  size_t smem = 0;
+  const void* tw = nullptr;
+};
+// What the tuner measured for one (part, row-count class): each launch
+// shape's time per launch (µs) and the one it chose.
+struct TraceTuning {
+  int choice = 0;
+  int64_t rows = 0;
+  std::vector<float> us;
+};
+
 struct psg_plan {
   PlanHost host;
   std::vector<std::unique_ptr<DeviceBuf>> keep;
@@ -789,14 +810,19 @@ struct psg_plan {
   bool wide = false;
   int64_t gwork_stride = 0, gwork_bytes = 0;
   bool needs_keys = false;  // a mute reads each row's offset and t0Ms
-  // Per part: the float32 trace kernel that runs it (psg_trace.cuh), or
+  // Per part: the float32 trace kernel's first build (psg_trace.cuh), or
   // nullptr for pipeline_kernel; its recipe slot (0: demean, filter, AGC;
-  // 1: then a per-trace normalization), prefetch, shared memory and grid.
+  // 1: then a per-trace normalization); the launch shapes of its builds
+  // (the first one the untuned choice).
   std::vector<const TracePlanInfo*> trace;
   std::vector<int> trace_recipe;
-  bool trace_pf = false;
-  size_t trace_smem = 0;
-  int trace_work_off = 0, trace_grid = 1;
+  std::vector<std::vector<TraceCand>> trace_cands;
+  // The tuner's choices by (part, bit length of the row count), with the
+  // times it measured; a part's pinned choice (−1: none) overrides them.
+  bool tune = true;
+  mutable std::mutex tune_mu;
+  mutable std::map<std::pair<int, int>, TraceTuning> tuned;
+  mutable std::vector<int> pinned;
 };
 
 struct psg_workspace {
@@ -1156,7 +1182,6 @@ template <class T> static void build_device_steps(psg_plan* p) {
           // the trace kernel's tables: twiddles pass by pass, and the split
           // twiddles and gains of each bin pair (c, m − c) as the reference
           // rounds them to float32 (fft/plan.nim:156-159, filter/apply.nim:141)
-          d.tw_pass = upload(p->keep, ref_twiddles(*p->trace[part]));
           const int64_t m = f.fft.m, nf = f.fft.n;
           std::vector<float4> sp((size_t)m);
           std::vector<float2> gg((size_t)m);
@@ -1298,36 +1323,58 @@ template <class T> static void build_device_steps(psg_plan* p) {
   CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p->threads, p->smem));
   p->grid = std::max(1, per_sm) * g_sm_count;
   if (p->wide) p->gwork_bytes = p->gwork_stride * p->grid;
-  // The trace kernel: the row buffer (two with the next row's copy in flight,
-  // when that keeps as many CTAs on an SM) and the two transform buffers.
-  const TracePlanInfo* tp = nullptr;
-  for (auto* t : p->trace) tp = t ? t : tp;
-  if (tp && !p->wide) {
-    const int64_t fw = 2 * (int64_t)tp->buf * 8;
-    // the CTAs per SM of the recipes the plan's parts use (the smallest)
-    auto occ = [&](bool pf) {
-      const size_t sm = (size_t)((pf ? 2 : 1) * p->x_bytes + fw);
-      int best = -1;
-      for (size_t part = 0; part < p->trace.size(); part++) {
-        if (!p->trace[part]) continue;
-        const void* k = p->trace[part]->kernel[p->trace_recipe[part]][pf ? 1 : 0];
+  // The trace kernel's launch shapes, part by part: each build of the part's
+  // transform length, with the row buffer (two with the next row's copy in
+  // flight) and its two transform buffers, on a persistent grid or one CTA
+  // per row. The first shape is the untuned choice: the first build, the
+  // prefetch when it keeps as many CTAs on an SM, the persistent grid.
+  p->trace_cands.assign(p->trace.size(), {});
+  p->pinned.assign(p->trace.size(), -1);
+  const char* pf_env = getenv("PSG_PREFETCH");
+  for (size_t part = 0; part < p->trace.size(); part++) {
+    if (!p->trace[part] || p->wide) {
+      p->trace[part] = nullptr;
+      continue;
+    }
+    const int rc = p->trace_recipe[part];
+    const StepHost& ag = p->host.steps[p->host.parts[part].first + 2];
+    const TracePlanInfo* const* builds = trace_plans_for(p->trace[part]->m, (int)(2 * ag.half + 1));
+    std::vector<TraceCand>& cs = p->trace_cands[part];
+    for (int bi = 0; builds[bi]; bi++) {
+      const TracePlanInfo* tb = builds[bi];
+      if (!tb->kernel[rc][0] || !runs_reference_stages(*tb)) continue;
+      const void* tw = upload(p->keep, ref_twiddles(*tb));
+      const int64_t fw = 2 * (int64_t)tb->buf * 8;
+      int per[2] = {0, 0};
+      for (int pf = 0; pf < 2; pf++) {
+        const void* k = tb->kernel[rc][pf];
         allow_smem(k);
-        int per = 0;
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, p->trace[part]->nt, sm));
-        best = best < 0 ? per : std::min(best, per);
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[pf], k, tb->nt,
+                                                              (size_t)((pf + 1) * p->x_bytes + fw)));
       }
-      return std::max(best, 0);
-    };
-    const int one = occ(false), two = occ(true);
-    p->trace_pf = two > 0 && two >= one;
-    if (const char* e = getenv("PSG_PREFETCH")) p->trace_pf = atoi(e) != 0 && two > 0;
-    p->trace_work_off = (p->trace_pf ? 2 : 1) * p->x_bytes;
-    p->trace_smem = (size_t)(p->trace_work_off + fw);
-    p->trace_grid = std::max(1, p->trace_pf ? two : one) * g_sm_count;
-    if ((p->trace_pf ? two : one) <= 0) std::fill(p->trace.begin(), p->trace.end(), nullptr);
-  } else {
-    std::fill(p->trace.begin(), p->trace.end(), nullptr);
+      bool pf_first = per[1] > 0 && per[1] >= per[0];
+      if (pf_env) pf_first = atoi(pf_env) != 0 && per[1] > 0;
+      for (int o = 0; o < 2; o++) {
+        const int pf = o == 0 ? (int)pf_first : (int)!pf_first;
+        if (per[pf] <= 0 || (pf_env && pf != (int)pf_first)) continue;
+        for (int per_row = 0; per_row < 2; per_row++) {
+          if (pf && per_row) continue;  // one row per CTA: nothing to prefetch
+          TraceCand c;
+          c.tp = tb;
+          c.pf = pf != 0;
+          c.per_row = per_row != 0;
+          c.per_sm = per[pf];
+          c.work_off = (pf + 1) * p->x_bytes;
+          c.smem = (size_t)(c.work_off + fw);
+          c.tw = tw;
+          cs.push_back(c);
+        }
+      }
+    }
+    if (cs.empty()) p->trace[part] = nullptr;
+    else p->trace[part] = cs[0].tp;
   }
+  if (const char* e = getenv("PSG_TUNE")) p->tune = atoi(e) != 0;
 }
 
 // The per-panel factor of part `part` (which starts with a per-panel
@@ -1357,6 +1404,83 @@ static const double* panel_factor_dev(const psg_plan* p, psg_workspace* ws, int 
 static bool part_needs_panel(const psg_plan* p, int part) {
   auto range = p->host.parts[part];
   return range.first < range.second && p->host.steps[range.first].kind == ST_NORM_PANEL;
+}
+
+// Launches launch shape c of part `part`'s trace kernel.
+static void launch_trace(const psg_plan* p, int part, const TraceCand& c, PipeArgs a, int64_t rows,
+                         cudaStream_t stream) {
+  const void* k = c.tp->kernel[p->trace_recipe[part]][c.pf ? 1 : 0];
+  a.work_off = c.work_off;
+  a.tw_pass = c.tw;
+  allow_smem(k);
+  const int64_t grid = c.per_row ? rows : std::min<int64_t>(rows, (int64_t)c.per_sm * g_sm_count);
+  launch_pipe(k, (int)std::min<int64_t>(grid, 1 << 30), c.tp->nt, c.smem, stream, a);
+}
+
+// The launch shape of part `part`'s trace kernel for a call of `rows` rows:
+// its pinned choice, else the tuner's for the row count's class (its bit
+// length), else, tuning now: every shape runs on the call's own input into
+// a scratch block on `stream` (one launch to warm up, then three timed with
+// events, over two rounds; the least time per launch wins) and the choice
+// is kept for the class. The shapes give the same bits, so the choice never
+// changes a result. No tuning under stream capture, with tuning off
+// (PSG_TUNE=0), or when the scratch block cannot be had: the first shape.
+static int trace_choice(const psg_plan* p, int part, const PipeArgs& a, int64_t rows, int32_t cols, size_t esz,
+                        cudaStream_t stream) {
+  const std::vector<TraceCand>& cs = p->trace_cands[part];
+  std::lock_guard<std::mutex> lk(p->tune_mu);
+  if (p->pinned[part] >= 0 && p->pinned[part] < (int)cs.size()) return p->pinned[part];
+  if (cs.size() < 2 || !p->tune || rows <= 0) return 0;
+  int cls = 0;
+  for (int64_t r = rows; r; r >>= 1) cls++;
+  auto it = p->tuned.find({part, cls});
+  if (it != p->tuned.end()) return it->second.choice;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_OK(cudaStreamIsCapturing(stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return 0;
+  // at most 1 GiB of scratch: the first rows of a larger call
+  const int64_t row_bytes = (int64_t)cols * (int64_t)esz;
+  const int64_t trows = std::max<int64_t>(1, std::min<int64_t>(rows, (int64_t(1) << 30) / std::max<int64_t>(row_bytes, 1)));
+  void* scratch = nullptr;
+  if (cudaMalloc(&scratch, (size_t)(trows * row_bytes)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  PipeArgs t = a;
+  t.job.src = a.job.src ? a.job.src : a.job.dst;
+  t.job.dst = scratch;
+  t.job.rows = trows;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  TraceTuning res;
+  res.rows = trows;
+  res.us.assign(cs.size(), INFINITY);
+  auto done = [&] {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(scratch);
+  };
+  try {
+    CUDA_OK(cudaEventCreate(&e0));
+    CUDA_OK(cudaEventCreate(&e1));
+    for (int round = 0; round < 2; round++)
+      for (size_t i = 0; i < cs.size(); i++) {
+        launch_trace(p, part, cs[i], t, trows, stream);
+        CUDA_OK(cudaEventRecord(e0, stream));
+        for (int k = 0; k < 3; k++) launch_trace(p, part, cs[i], t, trows, stream);
+        CUDA_OK(cudaEventRecord(e1, stream));
+        CUDA_OK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        res.us[i] = std::min(res.us[i], ms * 1000.f / 3);
+      }
+  } catch (...) {
+    done();
+    throw;
+  }
+  done();
+  res.choice = (int)(std::min_element(res.us.begin(), res.us.end()) - res.us.begin());
+  p->tuned[{part, cls}] = res;
+  return res.choice;
 }
 
 // runPart (pipeline.nim:690-723): the steps of part `part` after its
@@ -1395,14 +1519,10 @@ static void run_part(const psg_plan* p, psg_workspace* ws, int part, const void*
     a.gwork = (unsigned char*)ws->g;
     a.gwork_stride = p->gwork_stride;
   }
-  if (const TracePlanInfo* tp = part < (int)p->trace.size() ? p->trace[part] : nullptr) {
-    if (!factor) {
-      const void* kern = tp->kernel[p->trace_recipe[part]][p->trace_pf ? 1 : 0];
-      a.work_off = p->trace_work_off;
-      allow_smem(kern);
-      launch_pipe(kern, (int)std::min<int64_t>(rows, p->trace_grid), tp->nt, p->trace_smem, stream, a);
-      return;
-    }
+  if (part < (int)p->trace.size() && p->trace[part] && !factor) {
+    const int k = trace_choice(p, part, a, rows, cols, sizeof(T), stream);
+    launch_trace(p, part, p->trace_cands[part][k], a, rows, stream);
+    return;
   }
   const void* kern = p->wide ? wide_kernel_for<T>() : pipe_kernel_for<T>(p->recipe[part], p->prefetch);
   allow_smem(kern);
@@ -1562,6 +1682,71 @@ int32_t psg_plan_step_nfft(const psg_plan* p, int32_t i) {
 }
 
 int32_t psg_plan_needs_keys(const psg_plan* plan) { return plan && plan->needs_keys ? 1 : 0; }
+int32_t psg_plan_trace_shapes(const psg_plan* plan, int32_t part) {
+  if (!plan || part < 0 || part >= (int)plan->trace_cands.size() || !plan->trace[part]) return 0;
+  return (int32_t)plan->trace_cands[part].size();
+}
+int psg_plan_pin_trace(psg_plan* plan, int32_t part, int32_t shape) {
+  return guarded([&] {
+    const int n = psg_plan_trace_shapes(plan, part);
+    if (n == 0) throw InvalidArg("the part has no trace-kernel launch shapes");
+    if (shape < -1 || shape >= n) throw InvalidArg("launch shape out of range");
+    std::lock_guard<std::mutex> lk(plan->tune_mu);
+    plan->pinned[part] = shape;
+  });
+}
+int psg_plan_tuning(const psg_plan* plan, char* buf, int64_t cap, int64_t* needed) {
+  return guarded([&] {
+    if (!plan || (!buf && cap > 0)) throw InvalidArg("null argument");
+    std::string j = "{\"parts\": [";
+    char tmp[256];
+    std::lock_guard<std::mutex> lk(plan->tune_mu);
+    bool first = true;
+    for (size_t part = 0; part < plan->trace_cands.size(); part++) {
+      if (!plan->trace[part]) continue;
+      snprintf(tmp, sizeof tmp, "%s{\"part\": %d, \"pinned\": %d, \"shapes\": [", first ? "" : ", ", (int)part,
+               plan->pinned[part]);
+      j += tmp;
+      first = false;
+      const auto& cs = plan->trace_cands[part];
+      for (size_t i = 0; i < cs.size(); i++) {
+        const TracePlanInfo& t = *cs[i].tp;
+        std::string passes;
+        for (int k = 0; k < t.np; k++) {
+          passes += (k ? " " : "") + std::to_string(t.g1[k]);
+          if (t.g2[k]) passes += "x" + std::to_string(t.g2[k]);
+        }
+        snprintf(tmp, sizeof tmp,
+                 "%s{\"m\": %d, \"threads\": %d, \"min_blocks\": %d, \"passes\": \"%s\", \"prefetch\": %s, "
+                 "\"grid\": \"%s\", \"ctas_per_sm\": %d, \"smem\": %lld}",
+                 i ? ", " : "", t.m, t.nt, t.min_blocks, passes.c_str(), cs[i].pf ? "true" : "false",
+                 cs[i].per_row ? "per_row" : "persistent", cs[i].per_sm, (long long)cs[i].smem);
+        j += tmp;
+      }
+      j += "]}";
+    }
+    j += "], \"tuned\": [";
+    first = true;
+    for (const auto& kv : plan->tuned) {
+      snprintf(tmp, sizeof tmp, "%s{\"part\": %d, \"class\": %d, \"rows\": %lld, \"choice\": %d, \"us\": [",
+               first ? "" : ", ", kv.first.first, kv.first.second, (long long)kv.second.rows, kv.second.choice);
+      j += tmp;
+      first = false;
+      for (size_t i = 0; i < kv.second.us.size(); i++) {
+        snprintf(tmp, sizeof tmp, "%s%.3f", i ? ", " : "", kv.second.us[i]);
+        j += tmp;
+      }
+      j += "]}";
+    }
+    j += "]}";
+    if (needed) *needed = (int64_t)j.size() + 1;
+    if (cap > 0) {
+      const size_t n = std::min<size_t>(j.size(), (size_t)cap - 1);
+      memcpy(buf, j.data(), n);
+      buf[n] = 0;
+    }
+  });
+}
 int32_t psg_plan_part_needs_panel(const psg_plan* plan, int32_t part) {
   if (!plan || part < 0 || part >= (int)plan->host.parts.size()) return 0;
   return part_needs_panel(plan, part) ? 1 : 0;
@@ -1754,7 +1939,8 @@ int psg_graph_capture(const psg_plan* plan, psg_workspace* ws, const void* src, 
     // the kernels' shared-memory attributes are set before the capture
     for (int part = 0; part < (int)plan->host.parts.size(); part++) {
       if (part < (int)plan->trace.size() && plan->trace[part])
-        allow_smem(plan->trace[part]->kernel[plan->trace_recipe[part]][plan->trace_pf ? 1 : 0]);
+        for (const TraceCand& c : plan->trace_cands[part])
+          allow_smem(c.tp->kernel[plan->trace_recipe[part]][c.pf ? 1 : 0]);
       allow_smem(plan->wide ? (plan->host.dtype == PSG_F32 ? wide_kernel_for<float>() : wide_kernel_for<double>())
                             : (plan->host.dtype == PSG_F32 ? pipe_kernel_for<float>(plan->recipe[part], plan->prefetch)
                                                            : pipe_kernel_for<double>(plan->recipe[part], plan->prefetch)));

@@ -38,7 +38,6 @@ struct DevStep {
   const void* bridge;  // Quad<T>[m]: the split · gain · unsplit map of each bin pair
   const void* fall;
   const void* tw;
-  const void* tw_pass;  // the trace kernel's twiddles, pass by pass (psg_trace.cuh)
   // the trace kernel's split twiddles (float4 per bin pair: bins c and m − c)
   // and bin gains (float2 per bin pair), and 1/nfft in float32
   const void* ref_split;
@@ -92,6 +91,9 @@ struct PipeArgs {
   // L2-resident), gwork + blockIdx.x · gwork_stride.
   unsigned char* gwork;
   long long gwork_stride;
+  // the trace kernel's twiddles, pass by pass, for the build launched
+  // (psg_trace.cuh; its passes group the stages their own way)
+  const void* tw_pass;
 };
 
 // ----------------------------------------------------------- device helpers

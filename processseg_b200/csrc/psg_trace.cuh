@@ -508,17 +508,15 @@ struct BridgeLd {
 // writes: output c is the swapped pair of real samples 2c (its imaginary
 // part) and 2c + 1 (its real part); sample j = i + p of the padded trace
 // goes to x[i] for 0 ≤ i < n, plus the trend ga + gb·i in float64 when the
-// filter passes it. The thread's Σx² of what it writes accumulates in s2.
+// filter passes it.
 template <bool ADD> struct UnpackSt {
   SRow X;
   int n, p;
   double ga, gb;
-  mutable float s2;
   __device__ __forceinline__ void put(int i, float v) const {
     if ((unsigned)i < (unsigned)n) {
       if (ADD) v = __double2float_rn(__dadd_rn((double)v, __dadd_rn(ga, __dmul_rn(gb, (double)i))));
       X[i] = v;
-      s2 = fmaf(v, v, s2);
     }
   }
   __device__ __forceinline__ void operator()(int c, float2 v) const {
@@ -702,7 +700,7 @@ template <int NT> __device__ __forceinline__ void store_row(const SRow Y, float*
 template <class P, int RECIPE, bool PF, int E>
 __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   constexpr int NT = P::NT;
-  static_assert(NT == kNT, "the normalization step and the row loops share the pipeline kernels' CTA width");
+  static_assert(RECIPE != RC_DFAN || NT == kNT, "the normalization step runs at the pipeline kernels' CTA width");
   __shared__ TkShared<NT> S;
   __shared__ SharedMem smem;  // the radix selection of the normalization
   Shared SN{&smem, 0};
@@ -784,10 +782,15 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       const DevStep* d = c.steps + c.first;
       const DevStep& fd = d[1];
       // (1) the demean (core/basic.nim:52-58): the mean of the live samples
-      // from a float64 sum, rounded to float32; x' = x − mean in float32
+      // from a float64 sum, rounded to float32; x' = x − mean in float32.
+      // Every float64 sum of the kernel runs in the same order whatever the
+      // build: kNT lanes each summing samples kNT apart, then the warps'
+      // trees in warp order (a wider CTA's other warps add zeros), so the
+      // builds of one transform length give the same bits.
       {
         double s1 = 0;
-        for (int i = threadIdx.x; i < n; i += NT) s1 += (double)X[i];
+        if (threadIdx.x < kNT)
+          for (int i = threadIdx.x; i < n; i += kNT) s1 += (double)X[i];
         warp_sums2<NT>(s1, 0.0, S, 0);
       }
       __syncthreads();
@@ -802,11 +805,12 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       // Σi·x' in float64
       {
         double s1 = 0, si = 0, ti = (double)threadIdx.x;
-        for (int i = threadIdx.x; i < n; i += NT, ti += (double)NT) {
-          const double v = (double)fs(X[i], mean);
-          s1 += v;
-          si += ti * v;
-        }
+        if (threadIdx.x < kNT)
+          for (int i = threadIdx.x; i < n; i += kNT, ti += (double)kNT) {
+            const double v = (double)fs(X[i], mean);
+            s1 += v;
+            si += ti * v;
+          }
         warp_sums2<NT>(s1, si, S, 1);
       }
       __syncthreads();
@@ -820,7 +824,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       }
       __syncthreads();
       const double ta = S.dsc[0], tb = S.dsc[1];
-      const float2* tw = reinterpret_cast<const float2*>(fd.tw_pass);  // the per-pass twiddles
+      const float2* tw = reinterpret_cast<const float2*>(a.tw_pass);  // the build's per-pass twiddles
       const int pad = fd.pad;
       // (3) the forward transform of the packed trace
       ref_fft<P>(ao, bo, tw, PackLd{X, n, pad, mean, ta, tb}, BufSt{last_out<P>(ao, bo)});
@@ -828,7 +832,6 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       const int zo = last_out<P>(ao, bo);
       // (4) split, gains, unsplit and the inverse transform, its last pass
       // unpacking into X
-      float s2 = 0.f;
       const double gb = tb * fd.dc_gain;
       const double ga = fd.zero_dc ? -gb * (double)(n - 1) / 2 : ta * fd.dc_gain;
       const int za = zo == ao ? bo : ao;  // the inverse's first pass writes the other buffer
@@ -837,40 +840,27 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       __syncthreads();
       const BufLd br{zo};
       if (ga == 0 && gb == 0) {
-        const UnpackSt<false> un{X, n, pad, 0, 0, 0.f};
-        ref_fft<P>(zo, za, tw, br, un);
-        s2 = un.s2;
+        ref_fft<P>(zo, za, tw, br, UnpackSt<false>{X, n, pad, 0, 0});
       } else {
-        const UnpackSt<true> un{X, n, pad, ga, gb, 0.f};
-        ref_fft<P>(zo, za, tw, br, un);
-        s2 = un.s2;
+        ref_fft<P>(zo, za, tw, br, UnpackSt<true>{X, n, pad, ga, gb});
       }
-      warp_sums2<NT>((double)s2, 0.0, S, 1);
       __syncthreads();
-      // (5) the AGC's level from Σx² (a float64 pass when the float32 sums
-      // may have left the float32 range)
+      // (5) the AGC's level from Σx² of the filtered trace in float64 (each
+      // square exact there)
+      {
+        double acc = 0;
+        if (threadIdx.x < kNT)
+          for (int i = threadIdx.x; i < n; i += kNT) {
+            const double v = (double)X[i];
+            acc = fma(v, v, acc);
+          }
+        warp_sums2<NT>(acc, 0.0, S, 0);
+      }
+      __syncthreads();
       const DevStep& ag = d[2];
       if (threadIdx.x == 0) {
         double s2d, unused;
-        fold2<NT>(S, 1, s2d, unused);
-        S.dsc[2] = s2d;
-        S.isc[0] = (isfinite(s2d) && s2d >= 1e-30) ? 1 : 0;
-      }
-      __syncthreads();
-      double s2d = S.dsc[2];
-      if (!S.isc[0]) {
-        double acc = 0;
-        for (int i = threadIdx.x; i < n; i += NT) acc += (double)X[i] * (double)X[i];
-        warp_sums2<NT>(acc, 0.0, S, 0);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          double u;
-          fold2<NT>(S, 0, S.dsc[2], u);
-        }
-        __syncthreads();
-        s2d = S.dsc[2];
-      }
-      if (threadIdx.x == 0) {
+        fold2<NT>(S, 0, s2d, unused);
         const double rms = sqrt(s2d / (double)n);
         const bool run = !(rms == 0 || !fits_d<float>(ag.target / rms / ag.epsilon));
         S.isc[1] = run ? 1 : 0;
@@ -1003,6 +993,47 @@ __global__ void __launch_bounds__(P::NT, P::MINB) corr_trace_kernel(CorrArgs a) 
     }
     __syncthreads();
   }
+}
+
+// The host's description of a trace-kernel build (psg_trace.h): plan P with
+// AGC lane width E, its kernels by recipe and prefetch (the normalization
+// recipe only at the pipeline kernels' CTA width).
+template <class P, int E> TracePlanInfo info() {
+  TracePlanInfo t{};
+  t.m = P::M;
+  t.nt = P::NT;
+  t.np = P::NP;
+  for (int i = 0; i < P::NP; i++) {
+    t.radix[i] = P::radix(i);
+    t.g1[i] = P::G1[i];
+    t.g2[i] = P::G2[i];
+  }
+  t.agc_e = E;
+  t.min_blocks = P::MINB;
+  t.buf = P::BUF;
+  t.kernel[0][0] = (const void*)trace_kernel<P, RC_DFA, false, E>;
+  t.kernel[0][1] = (const void*)trace_kernel<P, RC_DFA, true, E>;
+  if constexpr (P::NT == kNT) {
+    t.kernel[1][0] = (const void*)trace_kernel<P, RC_DFAN, false, E>;
+    t.kernel[1][1] = (const void*)trace_kernel<P, RC_DFAN, true, E>;
+  }
+  return t;
+}
+
+// The same for a correlation build (kernel[0][0]).
+template <class P> TracePlanInfo corr_info() {
+  TracePlanInfo t{};
+  t.m = P::M;
+  t.nt = P::NT;
+  t.np = P::NP;
+  for (int i = 0; i < P::NP; i++) {
+    t.radix[i] = P::radix(i);
+    t.g1[i] = P::radix(i);
+  }
+  t.min_blocks = P::MINB;
+  t.buf = P::M;
+  t.kernel[0][0] = (const void*)corr_trace_kernel<P>;
+  return t;
 }
 
 }  // namespace tk

@@ -1,0 +1,28 @@
+// psg_trace_m1944.cu — trace-kernel builds for m = 1944 (nfft 3888): traces
+// of 2001..3888 samples, e.g. 2000 × 3001 at 2 ms with a band-pass + notch and
+// a 300 ms AGC (w = 151, E = 5). The reference's stages 4, 2, 3, 3, 3, 3, 3
+// (fft/plan.nim:120-132) grouped into passes three ways; every build rounds
+// as those stages do, so they give the same bits and the tuner picks by time.
+#include "psg_trace.cuh"
+
+namespace psg {
+namespace {
+
+using tk::Grp;
+// 4·2 | 3·3 | 3·3 | 3, four CTAs per SM (64 registers)
+using A = tk::RPlan<1944, 256, 4, Grp<4, 2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
+// the same passes with 85 registers (three CTAs per SM, no spills)
+using B = tk::RPlan<1944, 256, 3, Grp<4, 2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
+// 4 | 2·3 | 3·3 | 3·3: more butterflies in the first pass
+using C = tk::RPlan<1944, 256, 4, Grp<4>, Grp<2, 3>, Grp<3, 3>, Grp<3, 3>>;
+
+const TracePlanInfo a = tk::info<A, 5>();
+const TracePlanInfo b = tk::info<B, 5>();
+const TracePlanInfo c = tk::info<C, 5>();
+const TracePlanInfo* const builds[] = {&a, &b, &c, nullptr};
+
+}  // namespace
+
+const TracePlanInfo* const* trace_builds_m1944_e5() { return builds; }
+
+}  // namespace psg

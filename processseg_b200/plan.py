@@ -238,6 +238,29 @@ class PipelinePlan:
                                           C.byref(h)))
         return ApplyGraph(h, (self, ws, src, dst, live, start, keys))
 
+    def traceShapes(self, part: int = 0) -> int:
+        """How many launch shapes of the trace kernel part ``part`` can run
+        on (0: the part runs on the general kernel). Every shape gives the
+        same bits; the first apply at a new row-count class times them all
+        and keeps the fastest (``PSG_TUNE=0`` keeps the first)."""
+        return int(A.lib().psg_plan_trace_shapes(self.h, part))
+
+    def pinTrace(self, part: int, shape: int):
+        """Runs part ``part`` with launch shape ``shape`` whatever the row
+        count (-1: back to the tuner's choices)."""
+        A.check(A.lib().psg_plan_pin_trace(self.h, part, shape))
+
+    def tuning(self) -> dict:
+        """The launch shapes of each trace-kernel part and what the tuner
+        measured: ``{"parts": [{"part", "pinned", "shapes": [...]}],
+        "tuned": [{"part", "class", "rows", "us", "choice"}]}``."""
+        import json
+        need = C.c_int64(0)
+        A.check(A.lib().psg_plan_tuning(self.h, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(int(need.value) + 64)
+        A.check(A.lib().psg_plan_tuning(self.h, buf, len(buf), C.byref(need)))
+        return json.loads(buf.value.decode())
+
     @property
     def needsKeys(self) -> bool:
         """The plan mutes: it reads each row's offset and t0Ms."""
