@@ -213,8 +213,9 @@ int32_t psg_plan_needs_keys(const psg_plan* plan);
  * without the next row's copy in flight, on a persistent grid or one CTA
  * per row. Every shape gives the same bits. The first apply of such a part
  * at a row count of a new class (the count's bit length) times every shape
- * on the call's own input into a scratch block (waiting for the stream once)
- * and keeps the fastest for that class; PSG_TUNE=0 in the environment at
+ * on the call's own input into a scratch block, each timed launch after a
+ * write of twice the L2's size has flushed that input from it (waiting for
+ * the stream once), and keeps the fastest for that class; PSG_TUNE=0 in the environment at
  * compile keeps the first shape, and so does an apply under stream capture
  * before the class is tuned. No counterpart in the reference, whose FFT plan
  * has one factorization per length (fft/plan.nim:120-160). */

@@ -693,10 +693,14 @@ template <int NT> __device__ __forceinline__ void store_row(const SRow Y, float*
 
 // The trace kernel: P the filter's transform, RECIPE the step chain
 // (RC_DFA: demean, filter, AGC; RC_DFAN: then a per-trace normalization),
-// PF the next row's bulk copy in flight while a row is processed, E the
-// AGC's samples per lane (its window w ≤ 32·E). Row handling (bulk copy,
-// ragged ends, src → dst copy of dead rows and of samples past the live
-// length) is pipeline_kernel's.
+// PF the next row's bulk copy issued as soon as the row buffer is free (after
+// the forward transform, or after a row that is only copied) so that it
+// lands under the rest of the row's work, E the AGC's samples per lane (its
+// window w ≤ 32·E). Row handling (bulk copy, ragged ends, src → dst copy of
+// dead rows and of samples past the live length) is pipeline_kernel's.
+// Shared memory: the row buffer X, then the two transform buffers; the
+// filtered trace F and the AGC's output Y take the transform buffers' place
+// once the inverse transform no longer needs them.
 template <class P, int RECIPE, bool PF, int E>
 __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   constexpr int NT = P::NT;
@@ -704,12 +708,13 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   __shared__ TkShared<NT> S;
   __shared__ SharedMem smem;  // the radix selection of the normalization
   Shared SN{&smem, 0};
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ RowSlot slot[2];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ RowSlot slot;
   __shared__ int s_ok;
   const long long total = a.job.rows;
   constexpr int esz = 4;
-  auto issue = [&](long long t, int b) {
+  // thread 0: the bulk copy of row t into the row buffer
+  auto issue = [&](long long t) {
     const RowCtx<float> c = row_ctx<float, false>(a, t);
     const int len = c.copy ? c.cols : c.n;
     const uintptr_t ga = (uintptr_t)c.from, ge = ga + (uintptr_t)len * esz;
@@ -717,67 +722,56 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
     uintptr_t lo = ga & ~(uintptr_t)15, hi = (ge + 15) & ~(uintptr_t)15;
     if (lo < (uintptr_t)c.blk_lo) lo += 16;
     if (hi > (uintptr_t)c.blk_hi) hi -= 16;
-    unsigned char* xb = psg_dyn_smem + b * a.x_bytes;
     if (len > 0 && hi > lo) {
       const int head = lo > ga ? (int)((lo - ga) / esz) : 0;
       const int tail = hi < ge ? (int)((hi - ga) / esz) : len;
       const uint32_t body = (uint32_t)(hi - lo);
-      slot[b] = RowSlot{head, tail, (int)body, len, off};
-      mbar_arrive_expect_tx(&bars[b], body);
-      bulk_load(xb + off + ((long long)lo - (long long)ga), reinterpret_cast<const void*>(lo), body, &bars[b]);
+      slot = RowSlot{head, tail, (int)body, len, off};
+      mbar_arrive_expect_tx(&bar, body);
+      bulk_load(psg_dyn_smem + off + ((long long)lo - (long long)ga), reinterpret_cast<const void*>(lo), body, &bar);
     } else {
-      slot[b] = RowSlot{len, len, 0, len, off};
-      mbar_arrive(&bars[b]);
+      slot = RowSlot{len, len, 0, len, off};
+      mbar_arrive(&bar);
     }
   };
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    mbar_init(&bar, 1);
     mbar_init_fence();
-    if (PF && blockIdx.x < total) issue(blockIdx.x, 0);
+    if (PF && blockIdx.x < total) issue(blockIdx.x);
   }
   __syncthreads();
-  // the two transform buffers (complex offsets) and, after the transforms,
-  // the output row Y in their place
+  // the two transform buffers (complex offsets), after the row buffer
   const int ao = a.work_off / 8, bo = ao + P::BUF;
-  uint32_t phase[2] = {0, 0};
-  int cur = 0;
-  for (long long t = blockIdx.x; t < total; t += gridDim.x, cur = PF ? cur ^ 1 : 0) {
+  uint32_t phase = 0;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
     const long long tn = t + gridDim.x;
-    if (threadIdx.x == 0) {
-      if (PF && tn < total) {
-        fence_proxy_async();
-        issue(tn, cur ^ 1);
-      } else if (!PF) {
-        fence_proxy_async();
-        issue(t, 0);
-      }
+    if (!PF && threadIdx.x == 0) {
+      fence_proxy_async();
+      issue(t);
     }
     if (threadIdx.x < 32) {
-      const bool ok = mbar_wait(&bars[cur], phase[cur], 1ll << 26);
+      const bool ok = mbar_wait(&bar, phase, 1ll << 26);
       if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
     }
     __syncthreads();
     if (!s_ok) {
       if (threadIdx.x == 0) {
         atomicExch(a.status, 1);
-        mbar_wait(&bars[cur], phase[cur], 1ll << 26);
+        mbar_wait(&bar, phase, 1ll << 26);
       }
       return;
     }
-    mbar_try_wait(&bars[cur], phase[cur]);
-    phase[cur] ^= 1;
+    mbar_try_wait(&bar, phase);
+    phase ^= 1;
     const RowCtx<float> c = row_ctx<float, false>(a, t);
-    const RowSlot sl = slot[cur];
-    const SRow X{(cur * a.x_bytes + sl.off) >> 2};
+    const RowSlot sl = slot;
+    const SRow X{sl.off >> 2};
     for (int i = threadIdx.x; i < sl.head; i += NT) X[i] = c.from[i];
     for (int i = sl.tail + threadIdx.x; i < sl.len; i += NT) X[i] = c.from[i];
     if (sl.head > 0 || sl.tail < sl.len) __syncthreads();
     const int n = c.n;
     const int len = c.copy ? c.cols : n;
-    // Y: the output row, aligned like the destination row
-    const SRow Y{2 * ao + (int)(((uintptr_t)c.to >> 2) & 3)};
-    bool from_y = false;
+    bool issued = false;  // the same in every thread
     if (n > 0) {
       const DevStep* d = c.steps + c.first;
       const DevStep& fd = d[1];
@@ -826,23 +820,39 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       const double ta = S.dsc[0], tb = S.dsc[1];
       const float2* tw = reinterpret_cast<const float2*>(a.tw_pass);  // the build's per-pass twiddles
       const int pad = fd.pad;
+      // the samples past the live length go out now, from the row buffer
+      // that the next row's copy takes over after the forward transform
+      for (int i = n + threadIdx.x; i < len; i += NT) c.to[i] = X[i];
       // (3) the forward transform of the packed trace
       ref_fft<P>(ao, bo, tw, PackLd{X, n, pad, mean, ta, tb}, BufSt{last_out<P>(ao, bo)});
       __syncthreads();
+      if (PF && tn < total) {
+        if (threadIdx.x == 0) {
+          fence_proxy_async();
+          issue(tn);
+        }
+        issued = true;
+      }
       const int zo = last_out<P>(ao, bo);
       // (4) split, gains, unsplit and the inverse transform, its last pass
-      // unpacking into X
+      // unpacking the filtered trace F into the buffer that pass does not
+      // read; the AGC's output Y (aligned like the destination row) then
+      // takes the buffer it read
       const double gb = tb * fd.dc_gain;
       const double ga = fd.zero_dc ? -gb * (double)(n - 1) / 2 : ta * fd.dc_gain;
       const int za = zo == ao ? bo : ao;  // the inverse's first pass writes the other buffer
+      constexpr bool EVEN = P::NP % 2 == 0;
+      const SRow F{2 * (EVEN ? zo : za)};
+      const int yal = (int)(((uintptr_t)c.to >> 2) & 3);
+      const SRow Y{2 * (EVEN ? za : zo) + (n + yal <= 2 * P::BUF ? yal : 0)};
       ref_bridge_pairs<P::M, NT>(zo, reinterpret_cast<const float4*>(fd.ref_split),
                                  reinterpret_cast<const float2*>(fd.ref_gain), fd.ref_scale);
       __syncthreads();
       const BufLd br{zo};
       if (ga == 0 && gb == 0) {
-        ref_fft<P>(zo, za, tw, br, UnpackSt<false>{X, n, pad, 0, 0});
+        ref_fft<P>(zo, za, tw, br, UnpackSt<false>{F, n, pad, 0, 0});
       } else {
-        ref_fft<P>(zo, za, tw, br, UnpackSt<true>{X, n, pad, ga, gb});
+        ref_fft<P>(zo, za, tw, br, UnpackSt<true>{F, n, pad, ga, gb});
       }
       __syncthreads();
       // (5) the AGC's level from Σx² of the filtered trace in float64 (each
@@ -851,7 +861,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
         double acc = 0;
         if (threadIdx.x < kNT)
           for (int i = threadIdx.x; i < n; i += kNT) {
-            const double v = (double)X[i];
+            const double v = (double)F[i];
             acc = fma(v, v, acc);
           }
         warp_sums2<NT>(acc, 0.0, S, 0);
@@ -872,19 +882,19 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
       const bool agc_run = S.isc[1] != 0;
       unsigned long long mx = 0;
       if (agc_run) {
-        from_y = true;
-        mx = agc_groups<NT, E, RECIPE == RC_DFAN>(X, Y, n, ag.half, ag.agc_mode == PSG_AGC_RMS, S.sc[1], S.sc[2],
+        mx = agc_groups<NT, E, RECIPE == RC_DFAN>(F, Y, n, ag.half, ag.agc_mode == PSG_AGC_RMS, S.sc[1], S.sc[2],
                                                   S.sc[3]);
       } else if (RECIPE == RC_DFAN) {
         for (int i = threadIdx.x; i < n; i += NT) {
-          const unsigned long long bb = abs_bits(X[i]);
+          const unsigned long long bb = abs_bits(F[i]);
           mx = bb > mx ? bb : mx;
         }
       }
+      const SRow Z = agc_run ? Y : F;  // the row's processed samples
       if constexpr (RECIPE == RC_DFAN) {
         // (6) per-trace normalization of the AGC's output (its max |x| for
         // the NaN rule of the percentile, gain/gain.nim:198-219)
-        float* Z = reinterpret_cast<float*>(psg_dyn_smem) + (from_y ? Y.o : X.o);
+        float* z = reinterpret_cast<float*>(psg_dyn_smem) + Z.o;
         Stats st{0, 0, 0, 0};
         st.mx = bits_value(block_max_u64(mx, SN.m->redu[SN.flip]), 0.f);
         SN.flip ^= 1;
@@ -893,28 +903,27 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
           // Σx² of the normalization's input: a float64 pass (not fused; the
           // benchmarked chains normalize by a percentile)
           double acc = 0;
-          for (int i = threadIdx.x; i < n; i += NT) acc += (double)Z[i] * (double)Z[i];
+          for (int i = threadIdx.x; i < n; i += NT) acc += (double)z[i] * (double)z[i];
           st.s2 = block_sum(acc, SN.m->red[SN.flip][0]);
           SN.flip ^= 1;
           __syncthreads();
         }
         __syncthreads();
-        step_norm_trace<float, 0>(nd, st, Z, n, SN);
+        step_norm_trace<float, 0>(nd, st, z, n, SN);
       }
-    }
-    // (7) the row out: Y for the processed samples, X past them (and for
-    // dead rows), 16-byte stores where the destination allows
-    if (c.copy || n > 0) {
-      if (from_y) {
-        for (int i = n + threadIdx.x; i < len; i += NT) Y[i] = X[i];
-        __syncthreads();
-        store_row<NT>(Y, c.to, len);
-      } else {
-        __syncthreads();
-        store_row<NT>(X, c.to, len);
-      }
+      // (7) the processed samples out, 16-byte stores where the
+      // destination allows
+      __syncthreads();
+      store_row<NT>(Z, c.to, n);
+    } else if (c.copy) {
+      // a dead row (or one with no live samples): copied as it is
+      store_row<NT>(X, c.to, len);
     }
     __syncthreads();
+    if (PF && !issued && tn < total && threadIdx.x == 0) {
+      fence_proxy_async();
+      issue(tn);
+    }
   }
 }
 
