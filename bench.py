@@ -219,12 +219,17 @@ def error_report(dst_c2):
     return out
 
 
-def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
-    """The served viewer load (Poisson arrivals at ``rate_hz``; trace counts
-    log-uniform in 48..5000; shown windows log-uniform in 200..4000 samples
-    of a 6001-sample record, decoded with each plan's margin; three plans):
-    the request loop against the plain per-call apply on the same request
-    sequence. Latency is arrival to completion."""
+def serving_leg(n_req=150, rates=(2000.0, 5000.0, 10000.0, 20000.0, 40000.0), slots=16):
+    """The served viewer load (Poisson arrivals; trace counts log-uniform in
+    48..5000; shown windows log-uniform in 200..4000 samples of a 6001-sample
+    record, decoded with each plan's margin; three plans) at a sweep of
+    offered rates, the request loop against the plain per-call apply (one
+    caller, in arrival order, each call waiting for its result) on the same
+    request sequence. Two forms: host buffers (copies in and out in every
+    request's latency) and device-resident requests (the blocks already in
+    HBM). Latency is arrival to completion. ``equal_p99``: at each p99 the
+    plain path reached in the sweep, the best throughput each path sustains
+    with its p99 within it, and their ratio."""
     import threading
     import numpy as np
     import torch
@@ -232,7 +237,8 @@ def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
     from processseg_b200 import synth
     flows = synth.viewer_flows()
     margins = [P.initPipeline(f).requiredMargin(DT) for f in flows]
-    reqs = synth.viewer_requests(n_req, rate_hz=rate_hz, margins=margins)
+    base = rates[0]
+    reqs = synth.viewer_requests(n_req, rate_hz=base, margins=margins)
     plans = {}
     for r in reqs:
         key = (r.flow, r.cols)
@@ -240,82 +246,100 @@ def serving_leg(n_req=150, rate_hz=2000.0, slots=16):
             plans[key] = P.initPipeline(flows[r.flow]).compile(P.float32, DT, r.cols, recordSamples=6001)
     maxn = max(r.rows * r.cols for r in reqs)
     g = synth.shot_gather(5000, 6001, DT, seed=9, workload="c4", live_range=(3000, 6001))
-    pool = torch.from_numpy(g.data.reshape(-1)[:maxn].copy()).pin_memory().numpy()
-    outs = [torch.empty(maxn, dtype=torch.float32).pin_memory().numpy() for _ in range(slots)]
+    pool_h = torch.from_numpy(g.data.reshape(-1)[:maxn].copy()).pin_memory()
+    outs_h = [torch.empty(maxn, dtype=torch.float32).pin_memory() for _ in range(slots)]
+    pool_d = pool_h.cuda()
+    outs_d = [torch.empty(maxn, dtype=torch.float32, device="cuda") for _ in range(slots)]
     metas = {}
-    jobs = []
+    jobs = {"host": [], "device": []}
     for i, r in enumerate(reqs):
         key = (r.rows, r.first, r.cols)
         if key not in metas:
             metas[key] = P.initChunkMeta(g.status[:r.rows], g.numSamples[:r.rows], DT, g.t0Ms[:r.rows], r.first)
             metas[key].flat(r.cols)
-        src = pool[:r.rows * r.cols].reshape(r.rows, r.cols)
-        dst = outs[i % slots][:r.rows * r.cols].reshape(r.rows, r.cols)
-        jobs.append((r.arrival_s, plans[(r.flow, r.cols)], src, dst, metas[key]))
+            metas[key].device(r.cols)
+        n = r.rows * r.cols
+        plan = plans[(r.flow, r.cols)]
+        jobs["host"].append((r.arrival_s, plan, pool_h.numpy()[:n].reshape(r.rows, r.cols),
+                             outs_h[i % slots].numpy()[:n].reshape(r.rows, r.cols), metas[key]))
+        jobs["device"].append((r.arrival_s, plan, pool_d[:n].view(r.rows, r.cols),
+                               outs_d[i % slots][:n].view(r.rows, r.cols), metas[key]))
     total = sum(r.rows * r.cols for r in reqs)
-    # plain per-call: one caller, in arrival order
     ws = P.initWorkspace()
-    for _, plan, src, dst, meta in jobs[:3]:
+    for _, plan, src, dst, meta in jobs["host"]:
         ws.reserve(plan, rows=5000, cols=src.shape[1])
-        plan.apply(src, dst, meta, ws)
-    for _, plan, src, dst, meta in jobs:
-        ws.reserve(plan, rows=5000, cols=src.shape[1])
-    lat = []
-    t0 = time.perf_counter()
-    for arr, plan, src, dst, meta in jobs:
-        while time.perf_counter() - t0 < arr:
+
+    def spin_until(t0, t):
+        while time.perf_counter() - t0 < t:
             pass
-        plan.apply(src, dst, meta, ws)
-        lat.append(time.perf_counter() - t0 - arr)
-    plain_span = time.perf_counter() - t0
-    plain = {"p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
-             "msamples_per_s": total / plain_span / 1e6}
-    # the request loop: submits at the arrival times, a second thread waits
-    with P.Server(arena_bytes=3 << 30) as srv:
-        for _, plan, src, dst, meta in jobs[:3]:
-            srv.wait(srv.submit(plan, src, dst, meta))
+
+    def plain_run(form, scale):
+        lat = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for arr, plan, src, dst, meta in jobs[form]:
+            spin_until(t0, arr * scale)
+            plan.apply(src, dst, meta, ws)
+            if form == "device":
+                torch.cuda.current_stream().synchronize()
+            lat.append(time.perf_counter() - t0 - arr * scale)
+        span = time.perf_counter() - t0
+        return {"p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
+                "msamples_per_s": total / span / 1e6}
+
+    def served_run(srv, form, scale):
         srv.stats(reset=True)
+        c0 = srv.counters()
         tickets = []
-        done = threading.Event()
 
         def waiter():
             k = 0
-            while k < len(jobs):
+            while k < len(jobs[form]):
                 if k < len(tickets):
                     srv.wait(tickets[k], 60000)
                     k += 1
                 else:
                     time.sleep(0.0001)
-            done.set()
 
         th = threading.Thread(target=waiter)
+        torch.cuda.synchronize()
         th.start()
         t0 = time.perf_counter()
-        for arr, plan, src, dst, meta in jobs:
-            while time.perf_counter() - t0 < arr:
-                pass
+        for arr, plan, src, dst, meta in jobs[form]:
+            spin_until(t0, arr * scale)
             tickets.append(srv.submit(plan, src, dst, meta))
         th.join()
-        st = srv.stats()
-        # saturation: the same requests all at once (makespan throughput)
-        srv.stats(reset=True)
-        t0 = time.perf_counter()
-        burst = [srv.submit(plan, src, dst, meta) for _, plan, src, dst, meta in jobs]
-        for tk in burst:
-            srv.wait(tk, 60000)
-        served_sat = total / (time.perf_counter() - t0) / 1e6
-        sat_launch = srv.stats()["requests_per_launch"]
-    t0 = time.perf_counter()
-    for _, plan, src, dst, meta in jobs:
-        plan.apply(src, dst, meta, ws)
-    plain_sat = total / (time.perf_counter() - t0) / 1e6
-    return {"workload": "served viewer load: Poisson 2000 req/s, traces log-U[48,5000], windows log-U[200,4000] of 6001 + plan margins, 3 plans",
-            "requests": n_req, "offered_rps": rate_hz, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
-            "msamples_per_s": st["msamples_per_s"], "requests_per_launch": st["requests_per_launch"],
-            "plain_per_call": plain,
-            "saturated": {"what": "all requests submitted at once, host buffers in and out; Msamples/s over the makespan",
-                          "served_msamples_per_s": served_sat, "plain_msamples_per_s": plain_sat,
-                          "requests_per_launch": sat_launch}}
+        span = time.perf_counter() - t0
+        st, c1 = srv.stats(), srv.counters()
+        return {"p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3, "msamples_per_s": total / span / 1e6,
+                "requests_per_batch": st["requests_per_launch"],
+                "batches_beside_running": c1["overlapped"] - c0["overlapped"]}
+
+    out = {"workload": "served viewer load: Poisson arrivals, traces log-U[48,5000], windows log-U[200,4000] of 6001 "
+                       "+ plan margins, 3 plans",
+           "requests": n_req, "forms": {}}
+    with P.Server(arena_bytes=3 << 30) as srv:
+        for form in ("host", "device"):
+            for _, plan, src, dst, meta in jobs[form][:3]:  # warm-up (and the tuner, where a plan has one)
+                plan.apply(src, dst, meta, ws)
+                srv.wait(srv.submit(plan, src, dst, meta), 60000)
+            torch.cuda.synchronize()
+            sweep = []
+            for rate in rates:
+                scale = base / rate
+                sweep.append({"offered_rps": rate, "plain": plain_run(form, scale),
+                              "served": served_run(srv, form, scale)})
+            # at each p99 the plain path reached: the best throughput each
+            # path sustains with its p99 within it
+            eq = []
+            for bound in sorted({s["plain"]["p99_ms"] for s in sweep}):
+                best = lambda path: max([s[path]["msamples_per_s"] for s in sweep if s[path]["p99_ms"] <= bound]
+                                        or [0.0])
+                sp, ss = best("plain"), best("served")
+                eq.append({"p99_bound_ms": bound, "plain_msamples_per_s": sp, "served_msamples_per_s": ss,
+                           "ratio": ss / sp if sp > 0 else None})
+            out["forms"][form] = {"sweep": sweep, "equal_p99": eq}
+    return out
 
 
 def launch_of(plan, rows):

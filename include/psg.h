@@ -639,10 +639,18 @@ int psg_stack_fold(const psg_stack* st, int32_t* dst, void* stream);
  * tests/utils/viewersim.nim:155-200, calls pool.apply per stale entry; here
  * requests from any thread are batched on the GPU as they arrive). Requests
  * are admitted by device footprint into a fixed arena of `arena_bytes`,
- * copied in, run together in one launch of the batched pipeline kernel
- * (each trace with its own request's plan and width), and copied out, so the
- * copies of one request overlap the kernels of others. Float32 plans without
- * a per-panel normalization. Results equal psg_apply_host's bit for bit. */
+ * copied in, run in batches, and copied out, so the copies of one request
+ * overlap the kernels of others. In a batch, the float32 single-part
+ * requests run together: one launch of the batched pipeline kernel for the
+ * plans without a trace kernel (each trace with its own request's plan and
+ * width), one launch of each transform length's batched trace kernel for
+ * the others; requests of any other plan (a per-panel normalization, whose
+ * factor comes from the request's own rows; float64; IIR filters; mutes;
+ * traces too long for shared memory) run after them with the plain apply's
+ * launches. A batch starts when none is running, or beside running ones
+ * when the requests ready for it hold at least four rows per SM (up to four
+ * batches at once, each on its own streams). Results equal psg_apply_host's
+ * (psg_apply's for device buffers) bit for bit. */
 typedef struct psg_server psg_server;
 int psg_server_create(int device, int64_t arena_bytes, psg_server** out);
 void psg_server_destroy(psg_server* server);
@@ -652,6 +660,21 @@ void psg_server_destroy(psg_server* server);
 int psg_submit(psg_server* server, const psg_plan* plan, const void* src_host, void* dst_host,
                int64_t rows, int32_t cols, const int32_t* live_host,
                const double* start_ms_host, double dt_ms, uint64_t* ticket);
+/* psg_submit for a plan that mutes: its rows' keys (host arrays, copied in
+ * with the block; psg_submit refuses such a plan with PSG_EINVAL). */
+int psg_submit_keyed(psg_server* server, const psg_plan* plan, const void* src_host,
+                     void* dst_host, int64_t rows, int32_t cols, const int32_t* live_host,
+                     const double* start_ms_host, const psg_keys* keys_host, double dt_ms,
+                     uint64_t* ticket);
+/* A request whose buffers are already on the server's device (src, dst,
+ * live, start_ms and the keys' arrays: device memory): no copies, the
+ * kernels read src and write dst directly; no arena bytes. The request runs
+ * after the work queued on `stream` (the caller's, or NULL when the buffers
+ * are final already) at the time of the call. `keys` only for a plan that
+ * mutes (else NULL). */
+int psg_submit_device(psg_server* server, const psg_plan* plan, const void* src, void* dst,
+                      int64_t rows, int32_t cols, const int32_t* live, const double* start_ms,
+                      const psg_keys* keys, double dt_ms, void* stream, uint64_t* ticket);
 /* Waits for a request (PSG_ETIMEOUT after timeout_ms; a timeout that is not
  * finite or above 1e12 ms waits until the request finishes) and releases its
  * ticket; PSG_ECANCELED for a request cancelled before it started. A ticket
@@ -669,6 +692,10 @@ int psg_cancel(psg_server* server, uint64_t ticket);
 /* out[8]: completed, samples, launches, requests per launch, p50 and p99
  * latency (s, submit to completion), Msamples/s, refused; reset != 0 clears. */
 int psg_server_stats(psg_server* server, double* out, int reset);
+/* The loop's counters since it was created: {batches, kernel launches
+ * (batched launches and the part launches of requests run alone), batches
+ * started beside running ones, requests completed}. */
+int psg_server_counters(psg_server* server, int64_t* out4);
 
 #ifdef __cplusplus
 }

@@ -3079,16 +3079,39 @@ struct Arena {
   }
 };
 
+// How the loop runs a request: rows of the batched generic kernel (float32
+// single-part plans without a per-trace kernel of their own), rows of the
+// batched trace kernel of its transform length (plans the plain apply runs
+// on the trace kernel), or alone, part by part through the plain apply's
+// launches (per-panel normalizations, float64, IIR filters, mutes, long
+// traces). Each gives what the plain apply gives, bit for bit.
+enum { K_GENERIC = 0, K_TRACE = 1, K_SOLO = 2 };
+
 struct Req {
   uint64_t ticket = 0;
   const psg_plan* plan = nullptr;
-  const void* src = nullptr;
+  const void* src = nullptr;  // host memory (staged through the arena) or device memory
   void* dst = nullptr;
   const int32_t* live = nullptr;
   const double* start = nullptr;
+  const double* key_off = nullptr;  // a muting plan's rows' offsets and t0Ms
+  const double* key_t0 = nullptr;
+  int32_t first_sample = 0;
+  double dt_ms = 0;
   int64_t rows = 0;
   int32_t cols = 0;
+  int esz = 4;
+  bool device = false;  // the buffers are device memory: no copies in or out
+  int kind = K_GENERIC;
+  const TracePlanInfo* trace = nullptr;  // K_TRACE: the build whose batched kernel runs it
   int64_t off = -1, bytes = 0;
+  // the device addresses the kernels read and write (the arena's or the caller's)
+  char* d_data = nullptr;
+  const char* d_src = nullptr;
+  const int* d_live = nullptr;
+  const double* d_start = nullptr;
+  const double* d_off = nullptr;
+  const double* d_t0 = nullptr;
   double t_submit = 0, t_done = 0;
   int status = PSG_OK;
   bool done = false;
@@ -3098,8 +3121,9 @@ struct Req {
 
 struct Batch {
   std::vector<Req*> reqs;
-  cudaEvent_t kern = nullptr;  // its kernel finished
+  cudaEvent_t kern = nullptr;  // its kernels finished
   cudaEvent_t done = nullptr;  // its copies out finished
+  bool kern_done = false;
   int slot = 0;
 };
 }  // namespace
@@ -3109,8 +3133,11 @@ struct psg_server {
   int device = 0;
   char* arena_d = nullptr;
   Arena arena;
-  cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
   static const int kSlots = 4, kMaxJobs = 64;
+  // copies in on one stream; each batch slot its own kernel and copy-out
+  // streams, so a batch can start while another one's kernels run
+  cudaStream_t s_in = nullptr, s_comp[kSlots] = {}, s_out[kSlots] = {};
+  psg_workspace* ws[kSlots] = {};  // the plain apply's scratch for requests run alone
   Job* jobs_h = nullptr;  // pinned, kSlots × kMaxJobs
   long long* begin_h = nullptr;
   Job* jobs_d = nullptr;
@@ -3125,11 +3152,10 @@ struct psg_server {
   std::vector<Req*> staged;
   std::vector<Batch*> inflight;
   std::vector<cudaEvent_t> events;  // a pool of reusable events
-  cudaEvent_t last_kernel = nullptr;
   std::unordered_map<uint64_t, Req*> by_ticket;
   uint64_t next_ticket = 1;
   // statistics
-  int64_t completed = 0, samples = 0, launches = 0, batched_reqs = 0, refused = 0;
+  int64_t completed = 0, samples = 0, launches = 0, batched_reqs = 0, refused = 0, kernels = 0, overlapped = 0;
   std::vector<double> lat;
   double t_first = 0, t_last = 0;
   std::string error;
@@ -3137,8 +3163,12 @@ struct psg_server {
 
 namespace psg {
 namespace {
+// Arena bytes of a host request: its block, live lengths, window starts
+// and (a muting plan) its rows' offsets and t0Ms; none for device buffers.
 int64_t req_bytes(const Req& r) {
-  return align256(r.rows * (int64_t)r.cols * 4) + align256(r.rows * 4) + align256(r.rows * 8);
+  if (r.device) return 0;
+  return align256(r.rows * (int64_t)r.cols * r.esz) + align256(r.rows * 4) + align256(r.rows * 8) +
+         (r.key_off ? 2 * align256(r.rows * 8) : 0);
 }
 
 cudaEvent_t get_event(psg_server* S) {
@@ -3155,30 +3185,87 @@ void put_event(psg_server* S, cudaEvent_t e) {
   if (e) S->events.push_back(e);
 }
 
-// Moves pending requests that fit the arena to staged, starting their copies in.
+// Moves pending requests to staged: device requests at once; host requests
+// when their bytes fit the arena (first come, first served), starting their
+// copies in.
 void admit(psg_server* S) {
   while (!S->pending.empty()) {
     Req* r = S->pending.front();
+    if (r->device) {
+      S->pending.pop_front();
+      r->d_src = (const char*)r->src;
+      r->d_data = (char*)r->dst;
+      r->d_live = r->live;
+      r->d_start = r->start;
+      r->d_off = r->key_off;
+      r->d_t0 = r->key_t0;
+      S->staged.push_back(r);
+      continue;
+    }
     int64_t off = S->arena.alloc(r->bytes);
     if (off < 0) break;  // waits for memory to free up (FIFO)
     S->pending.pop_front();
     r->off = off;
     char* base = S->arena_d + off;
-    size_t db = (size_t)(r->rows * (int64_t)r->cols * 4);
-    CUDA_OK(cudaMemcpyAsync(base, r->src, db, cudaMemcpyHostToDevice, S->s_in));
-    CUDA_OK(cudaMemcpyAsync(base + align256((int64_t)db), r->live, r->rows * 4, cudaMemcpyHostToDevice, S->s_in));
-    if (r->start)
-      CUDA_OK(cudaMemcpyAsync(base + align256((int64_t)db) + align256(r->rows * 4), r->start, r->rows * 8,
-                              cudaMemcpyHostToDevice, S->s_in));
+    const int64_t db = align256(r->rows * (int64_t)r->cols * r->esz), lb = align256(r->rows * 4),
+                  sb = align256(r->rows * 8);
+    r->d_src = nullptr;  // applied in place in the arena
+    r->d_data = base;
+    r->d_live = (const int*)(base + db);
+    r->d_start = r->start ? (const double*)(base + db + lb) : nullptr;
+    CUDA_OK(cudaMemcpyAsync(base, r->src, (size_t)(r->rows * (int64_t)r->cols * r->esz), cudaMemcpyHostToDevice,
+                            S->s_in));
+    CUDA_OK(cudaMemcpyAsync(base + db, r->live, r->rows * 4, cudaMemcpyHostToDevice, S->s_in));
+    if (r->start) CUDA_OK(cudaMemcpyAsync(base + db + lb, r->start, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+    if (r->key_off) {
+      r->d_off = (const double*)(base + db + lb + sb);
+      r->d_t0 = (const double*)(base + db + lb + 2 * sb);
+      CUDA_OK(cudaMemcpyAsync(base + db + lb + sb, r->key_off, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+      CUDA_OK(cudaMemcpyAsync(base + db + lb + 2 * sb, r->key_t0, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+    }
     r->in = get_event(S);
     CUDA_OK(cudaEventRecord(r->in, S->s_in));
     S->staged.push_back(r);
   }
 }
 
-// One launch over every staged request whose copy in has finished (up to
-// kMaxJobs), then their copies out. Called when no kernel is running, so
-// that requests arriving meanwhile join the next launch.
+// A staged request whose input is on the device.
+bool ready(psg_server* S, Req* r) {
+  if (!r->in) return true;
+  if (cudaEventQuery(r->in) != cudaSuccess) return false;
+  put_event(S, r->in);
+  r->in = nullptr;
+  return true;
+}
+
+Job job_of(const Req* r) {
+  const psg_plan* p = r->plan;
+  Job j{};
+  j.src = r->d_src;
+  j.dst = r->d_data;
+  j.live = r->d_live;
+  j.start_ms = r->d_start;
+  j.steps = p->d_steps;
+  j.rows = r->rows;
+  j.cols = r->cols;
+  j.first = p->host.parts[0].first;
+  j.last = p->host.parts[0].second;
+  j.dt_ms = r->dt_ms > 0 ? r->dt_ms : p->host.dt_ms;
+  return j;
+}
+
+// A status from one of this library's entry points as an exception.
+void throw_unless_ok(int st) {
+  if (st == PSG_EINVAL) throw InvalidArg(t_err);
+  if (st != PSG_OK) throw std::runtime_error(t_err);
+}
+
+void launch_batch_reqs(psg_server* S, Batch* b);
+
+// One batch on a free slot: every staged request whose input is on the
+// device (up to kMaxJobs, in arrival order). The generic rows go in one
+// launch, each trace build's rows in one launch, the requests run alone
+// after them part by part; then the host requests' copies out.
 void launch_batch(psg_server* S) {
   int slot = -1;
   for (int i = 0; i < psg_server::kSlots; i++)
@@ -3187,90 +3274,178 @@ void launch_batch(psg_server* S) {
       break;
     }
   if (slot < 0 || S->staged.empty()) return;
-  Batch* b = new Batch();
+  std::unique_ptr<Batch> b(new Batch());
   b->slot = slot;
   for (size_t i = 0; i < S->staged.size() && b->reqs.size() < (size_t)psg_server::kMaxJobs;) {
     Req* r = S->staged[i];
-    if (cudaEventQuery(r->in) == cudaSuccess) {
-      put_event(S, r->in);
-      r->in = nullptr;
+    if (ready(S, r)) {
       b->reqs.push_back(r);
       S->staged.erase(S->staged.begin() + i);
     } else {
       i++;
     }
   }
-  if (b->reqs.empty()) {
-    delete b;
+  if (b->reqs.empty()) return;
+  try {
+    launch_batch_reqs(S, b.get());
+  } catch (const std::exception& e) {
+    // the batch's requests fail; what was queued for them finishes first,
+    // so that their arena memory is free to reuse
+    S->error = e.what();
+    cudaStreamSynchronize(S->s_comp[slot]);
+    cudaStreamSynchronize(S->s_out[slot]);
+    cudaGetLastError();
+    const int code = dynamic_cast<const InvalidArg*>(&e) ? PSG_EINVAL : PSG_ECUDA;
+    for (Req* r : b->reqs) {
+      r->status = code;
+      r->done = true;
+      if (r->off >= 0) S->arena.release(r->off, r->bytes);
+      r->off = -1;
+    }
+    put_event(S, b->kern);
+    put_event(S, b->done);
+    S->cv_done.notify_all();
     return;
   }
-  size_t take = b->reqs.size();
+  S->slot_busy[slot] = true;
+  S->launches++;
+  S->batched_reqs += (int64_t)b->reqs.size();
+  S->inflight.push_back(b.release());
+}
+
+void launch_batch_reqs(psg_server* S, Batch* b) {
+  const int slot = b->slot;
+  cudaStream_t sc = S->s_comp[slot], so = S->s_out[slot];
+  // the launches over many requests' rows: the generic group first, then
+  // one group per (trace build, recipe)
+  struct Group {
+    const TracePlanInfo* tp = nullptr;
+    int rc = 0;
+    std::vector<Req*> reqs;
+  };
+  std::vector<Group> groups(1);
+  std::vector<Req*> solo;
+  for (Req* r : b->reqs) {
+    if (r->kind == K_SOLO) {
+      solo.push_back(r);
+      continue;
+    }
+    if (r->kind == K_GENERIC) {
+      groups[0].reqs.push_back(r);
+      continue;
+    }
+    const int rc = r->plan->trace_recipe[0];
+    size_t g = 1;
+    while (g < groups.size() && !(groups[g].tp == r->trace && groups[g].rc == rc)) g++;
+    if (g == groups.size()) {
+      groups.push_back(Group{});
+      groups[g].tp = r->trace;
+      groups[g].rc = rc;
+    }
+    groups[g].reqs.push_back(r);
+  }
   Job* jh = S->jobs_h + slot * psg_server::kMaxJobs;
   long long* bh = S->begin_h + slot * psg_server::kMaxJobs;
-  long long total = 0;
-  int xb = 0;
-  size_t work = 0;
-  for (size_t i = 0; i < take; i++) {
-    Req* r = b->reqs[i];
-    const psg_plan* p = r->plan;
-    char* base = S->arena_d + r->off;
-    size_t db = (size_t)(r->rows * (int64_t)r->cols * 4);
-    Job j{};
-    j.src = nullptr;
-    j.dst = base;
-    j.live = (const int*)(base + align256((int64_t)db));
-    j.start_ms = r->start ? (const double*)(base + align256((int64_t)db) + align256(r->rows * 4)) : nullptr;
-    j.steps = p->d_steps;
-    j.rows = r->rows;
-    j.cols = r->cols;
-    j.first = p->host.parts[0].first;
-    j.last = p->host.parts[0].second;
-    jh[i] = j;
-    bh[i] = total;
-    total += r->rows;
-    xb = std::max(xb, p->x_bytes);
-    work = std::max(work, p->smem - (size_t)p->work_off);
+  size_t nj = 0;
+  std::vector<size_t> first(groups.size());
+  for (size_t g = 0; g < groups.size(); g++) {
+    first[g] = nj;
+    long long total = 0;
+    for (Req* r : groups[g].reqs) {
+      jh[nj] = job_of(r);
+      bh[nj] = total;
+      total += r->rows;
+      nj++;
+    }
   }
-  CUDA_OK(cudaMemcpyAsync(S->jobs_d + slot * psg_server::kMaxJobs, jh, take * sizeof(Job), cudaMemcpyHostToDevice, S->s_comp));
-  CUDA_OK(cudaMemcpyAsync(S->begin_d + slot * psg_server::kMaxJobs, bh, take * sizeof(long long), cudaMemcpyHostToDevice, S->s_comp));
-  PipeArgs a{};
-  a.jobs = S->jobs_d + slot * psg_server::kMaxJobs;
-  a.row_begin = S->begin_d + slot * psg_server::kMaxJobs;
-  a.njobs = (int)take;
-  a.total_rows = total;
-  a.x_bytes = xb;
-  a.status = S->status_d;
-  // one row buffer, or two when the prefetch costs no occupancy
-  auto occ = [&](bool pf, size_t& sm) {
-    sm = (size_t)((pf ? 2 : 1) * xb) + work;
-    auto k = batch_kernel_for(pf);
-    allow_smem(k);
-    int per = 0;
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kNT, sm));
-    return per;
-  };
-  size_t sm1, sm2;
-  int o1 = occ(false, sm1), o2 = occ(true, sm2);
-  bool pf = o2 > 0 && o2 >= o1;
-  a.work_off = (pf ? 2 : 1) * xb;
-  int per = pf ? o2 : o1;
-  if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
-  int grid = (int)std::min<long long>(total, (long long)per * g_sm_count);
-  if (total > 0) launch_pipe(batch_kernel_for(pf), grid, kNT, pf ? sm2 : sm1, S->s_comp, a);
+  if (nj) {
+    CUDA_OK(cudaMemcpyAsync(S->jobs_d + slot * psg_server::kMaxJobs, jh, nj * sizeof(Job), cudaMemcpyHostToDevice, sc));
+    CUDA_OK(cudaMemcpyAsync(S->begin_d + slot * psg_server::kMaxJobs, bh, nj * sizeof(long long),
+                            cudaMemcpyHostToDevice, sc));
+  }
+  for (size_t g = 0; g < groups.size(); g++) {
+    const Group& G = groups[g];
+    if (G.reqs.empty()) continue;
+    PipeArgs a{};
+    a.jobs = S->jobs_d + slot * psg_server::kMaxJobs + first[g];
+    a.row_begin = S->begin_d + slot * psg_server::kMaxJobs + first[g];
+    a.njobs = (int)G.reqs.size();
+    a.status = S->status_d;
+    long long total = 0;
+    int xb = 0;
+    size_t work = 0;
+    for (Req* r : G.reqs) {
+      total += r->rows;
+      xb = std::max(xb, r->plan->x_bytes);
+      work = std::max(work, r->plan->smem - (size_t)r->plan->work_off);
+    }
+    a.total_rows = total;
+    if (total == 0) continue;
+    if (G.tp) {
+      // the trace build's batched kernel: one row buffer, its transform buffers
+      const void* k = G.tp->batch[G.rc];
+      const size_t sm = (size_t)xb + 2 * (size_t)G.tp->buf * 8;
+      allow_smem(k);
+      int per = 0;
+      CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, G.tp->nt, sm));
+      if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
+      a.x_bytes = xb;
+      a.work_off = xb;
+      a.tw_pass = G.reqs[0]->plan->trace_cands[0][0].tw;  // the build's table (every plan's holds the same)
+      launch_pipe(k, (int)std::min<long long>(total, (long long)per * g_sm_count), G.tp->nt, sm, sc, a);
+    } else {
+      // one row buffer, or two when the prefetch costs no occupancy
+      auto occ = [&](bool pf, size_t& sm) {
+        sm = (size_t)((pf ? 2 : 1) * xb) + work;
+        auto k = batch_kernel_for(pf);
+        allow_smem(k);
+        int per = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kNT, sm));
+        return per;
+      };
+      size_t sm1, sm2;
+      int o1 = occ(false, sm1), o2 = occ(true, sm2);
+      bool pf = o2 > 0 && o2 >= o1;
+      a.x_bytes = xb;
+      a.work_off = (pf ? 2 : 1) * xb;
+      int per = pf ? o2 : o1;
+      if (per <= 0) throw InvalidArg("a batch's traces do not fit the device's shared memory");
+      launch_pipe(batch_kernel_for(pf), (int)std::min<long long>(total, (long long)per * g_sm_count), kNT,
+                  pf ? sm2 : sm1, sc, a);
+    }
+    S->kernels++;
+  }
+  // requests run alone: the plain apply's part-by-part launches, with this
+  // slot's workspace for per-panel statistics and long-trace work areas
+  for (Req* r : solo) {
+    const psg_plan* p = r->plan;
+    throw_unless_ok(psg_workspace_reserve(S->ws[slot], p, r->rows, r->cols));
+    psg_keys k{};
+    k.offset = r->d_off;
+    k.t0_ms = r->d_t0;
+    k.first_sample = r->first_sample;
+    const psg_keys* kp = p->needs_keys ? &k : nullptr;
+    for (int part = 0; part < (int)p->host.parts.size(); part++) {
+      const void* from = part == 0 ? r->d_src : nullptr;
+      if (p->host.dtype == PSG_F32)
+        launch_part<float>(p, S->ws[slot], part, from, r->d_data, r->rows, r->cols, r->d_live, r->d_start, sc, kp,
+                           r->dt_ms);
+      else
+        launch_part<double>(p, S->ws[slot], part, from, r->d_data, r->rows, r->cols, r->d_live, r->d_start, sc, kp,
+                            r->dt_ms);
+      S->kernels++;
+    }
+  }
   CUDA_OK(cudaGetLastError());
   b->kern = get_event(S);
-  CUDA_OK(cudaEventRecord(b->kern, S->s_comp));
-  S->last_kernel = b->kern;
-  CUDA_OK(cudaStreamWaitEvent(S->s_out, b->kern, 0));
+  CUDA_OK(cudaEventRecord(b->kern, sc));
+  CUDA_OK(cudaStreamWaitEvent(so, b->kern, 0));
   for (Req* r : b->reqs)
-    CUDA_OK(cudaMemcpyAsync(r->dst, S->arena_d + r->off, (size_t)(r->rows * (int64_t)r->cols * 4),
-                            cudaMemcpyDeviceToHost, S->s_out));
+    if (!r->device)
+      CUDA_OK(cudaMemcpyAsync(r->dst, r->d_data, (size_t)(r->rows * (int64_t)r->cols * r->esz),
+                              cudaMemcpyDeviceToHost, so));
   b->done = get_event(S);
-  CUDA_OK(cudaEventRecord(b->done, S->s_out));
-  S->slot_busy[slot] = true;
-  S->inflight.push_back(b);
-  S->launches++;
-  S->batched_reqs += (int64_t)take;
+  CUDA_OK(cudaEventRecord(b->done, so));
 }
 
 // Retires finished batches: their requests are done and their memory free.
@@ -3288,13 +3463,12 @@ bool retire(psg_server* S) {
       r->status = e == cudaSuccess ? PSG_OK : PSG_ECUDA;
       r->t_done = t;
       r->done = true;
-      S->arena.release(r->off, r->bytes);
+      if (r->off >= 0) S->arena.release(r->off, r->bytes);
       S->completed++;
       S->samples += r->rows * (int64_t)r->cols;
       S->lat.push_back(t - r->t_submit);
       S->t_last = t;
     }
-    if (S->last_kernel == b->kern) S->last_kernel = nullptr;
     put_event(S, b->kern);
     put_event(S, b->done);
     S->slot_busy[b->slot] = false;
@@ -3305,16 +3479,31 @@ bool retire(psg_server* S) {
   return any;
 }
 
+// The loop: admits what fits, launches a batch when no batch's kernels are
+// running, or, while some are, when the requests ready to run hold enough
+// rows to fill the device on their own (a CTA per row on every SM, four
+// deep): that batch then runs beside the others on its slot's streams.
+// Requests arriving during a batch otherwise join the next one.
 void sched_loop(psg_server* S) {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lk(S->mu);
+  const int64_t fill_rows = 4 * (int64_t)g_sm_count;
   while (true) {
     if (S->stop && S->pending.empty() && S->staged.empty() && S->inflight.empty()) break;
     try {
       admit(S);
-      // launch when no kernel is running: arrivals during a kernel join the next launch
-      bool gpu_idle = S->last_kernel == nullptr || cudaEventQuery(S->last_kernel) == cudaSuccess;
-      if (!S->staged.empty() && gpu_idle) launch_batch(S);
+      int running = 0;
+      for (Batch* b : S->inflight) {
+        if (!b->kern_done) b->kern_done = cudaEventQuery(b->kern) == cudaSuccess;
+        if (!b->kern_done) running++;
+      }
+      int64_t ready_rows = 0;
+      for (Req* r : S->staged)
+        if (ready(S, r)) ready_rows += std::max<int64_t>(r->rows, 1);
+      if (ready_rows > 0 && (running == 0 || ready_rows >= fill_rows)) {
+        if (running > 0) S->overlapped++;
+        launch_batch(S);
+      }
       if (retire(S)) S->cv_done.notify_all();
     } catch (const std::exception& e) {
       S->error = e.what();
@@ -3350,8 +3539,11 @@ int psg_server_create(int device, int64_t arena_bytes, psg_server** out) {
     CUDA_OK(cudaMalloc(&S->arena_d, (size_t)arena_bytes));
     S->arena.init(arena_bytes);
     CUDA_OK(cudaStreamCreateWithFlags(&S->s_in, cudaStreamNonBlocking));
-    CUDA_OK(cudaStreamCreateWithFlags(&S->s_comp, cudaStreamNonBlocking));
-    CUDA_OK(cudaStreamCreateWithFlags(&S->s_out, cudaStreamNonBlocking));
+    for (int i = 0; i < psg_server::kSlots; i++) {
+      CUDA_OK(cudaStreamCreateWithFlags(&S->s_comp[i], cudaStreamNonBlocking));
+      CUDA_OK(cudaStreamCreateWithFlags(&S->s_out[i], cudaStreamNonBlocking));
+      throw_unless_ok(psg_workspace_create(&S->ws[i]));
+    }
     const int nj = psg_server::kSlots * psg_server::kMaxJobs;
     CUDA_OK(cudaMallocHost(&S->jobs_h, nj * sizeof(Job)));
     CUDA_OK(cudaMallocHost(&S->begin_h, nj * sizeof(long long)));
@@ -3382,38 +3574,72 @@ void psg_server_destroy(psg_server* S) {
   cudaFreeHost(S->jobs_h);
   cudaFreeHost(S->begin_h);
   cudaStreamDestroy(S->s_in);
-  cudaStreamDestroy(S->s_comp);
-  cudaStreamDestroy(S->s_out);
+  for (int i = 0; i < psg_server::kSlots; i++) {
+    if (S->s_comp[i]) cudaStreamDestroy(S->s_comp[i]);
+    if (S->s_out[i]) cudaStreamDestroy(S->s_out[i]);
+    psg_workspace_destroy(S->ws[i]);
+  }
   delete S;
 }
 
-int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* dst_host, int64_t rows, int32_t cols,
-               const int32_t* live_host, const double* start_ms_host, double dt_ms, uint64_t* ticket) {
+}  // extern "C"
+
+namespace psg {
+namespace {
+// Queues a request: host buffers (staged through the arena) or device
+// buffers (the kernels read and write them in place), keys for a muting
+// plan. Where the plain apply would take a request, so does the loop.
+int submit(psg_server* S, const psg_plan* plan, const void* src, void* dst, int64_t rows, int32_t cols,
+           const int32_t* live, const double* start_ms, const psg_keys* keys, double dt_ms, bool device,
+           void* stream, uint64_t* ticket) {
   return guarded([&] {
     if (!S || !ticket) throw InvalidArg("null argument");
-    check_apply(plan, nullptr, src_host, dst_host, rows, cols, live_host, dt_ms, false);
-    if (plan->host.dtype != PSG_F32) throw InvalidArg("the request loop serves float32 plans");
-    if (plan->host.parts.size() != 1) throw InvalidArg("the request loop serves plans without a per-panel normalization");
-    if (plan->wide) throw InvalidArg("the request loop serves plans whose traces and FFTs fit the device's shared memory");
-    if (plan->needs_keys) throw InvalidArg("the request loop serves plans without mutes");
-    for (const StepHost& st : plan->host.steps)
-      if (st.kind == ST_IIR) throw InvalidArg("the request loop serves plans without IIR filters");
-    if (!src_host) throw InvalidArg("src is required");
+    check_apply(plan, nullptr, src, dst, rows, cols, live, dt_ms, false, keys);
+    if (!src) throw InvalidArg("src is required");
+    if (plan->needs_keys && (!keys->offset || !keys->t0_ms)) throw InvalidArg("the keys' offset and t0_ms are required");
     std::unique_ptr<Req> r(new Req());
     r->plan = plan;
-    r->src = src_host;
-    r->dst = dst_host;
+    r->src = src;
+    r->dst = dst;
     r->rows = rows;
     r->cols = cols;
-    r->live = live_host;
-    r->start = start_ms_host;
+    r->live = live;
+    r->start = start_ms;
+    r->dt_ms = dt_ms;
+    r->esz = plan->host.dtype == PSG_F32 ? 4 : 8;
+    r->device = device;
+    if (plan->needs_keys) {
+      r->key_off = keys->offset;
+      r->key_t0 = keys->t0_ms;
+      r->first_sample = keys->first_sample;
+    }
+    // how it runs: as the plain apply would, in a batch where it can
+    bool single = plan->host.dtype == PSG_F32 && plan->host.parts.size() == 1 && !part_needs_panel(plan, 0) &&
+                  !plan->wide && !plan->needs_keys;
+    for (const StepHost& st : plan->host.steps)
+      if (st.kind == ST_IIR) single = false;
+    r->kind = K_SOLO;
+    if (single) {
+      const TracePlanInfo* tp = plan->trace.empty() ? nullptr : plan->trace[0];
+      if (!tp) {
+        r->kind = K_GENERIC;
+      } else if (tp->batch[plan->trace_recipe[0]]) {
+        r->kind = K_TRACE;
+        r->trace = tp;
+      }
+    }
     r->bytes = req_bytes(*r);
     r->t_submit = now_s();
     std::lock_guard<std::mutex> g(S->mu);
     if (r->bytes > S->arena.size) {
       S->refused++;
       throw NoMemory("admission refused: the request needs " + std::to_string(r->bytes) +
-                               " bytes of device memory, the loop holds " + std::to_string(S->arena.size));
+                     " bytes of device memory, the loop holds " + std::to_string(S->arena.size));
+    }
+    if (device && stream) {
+      // the caller's work on the buffers, queued on `stream`, comes first
+      r->in = get_event(S);
+      CUDA_OK(cudaEventRecord(r->in, (cudaStream_t)stream));
     }
     if (S->completed == 0 && S->by_ticket.empty()) S->t_first = r->t_submit;
     r->ticket = S->next_ticket++;
@@ -3422,6 +3648,29 @@ int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* 
     S->pending.push_back(r.release());
     S->cv.notify_all();
   });
+}
+}  // namespace
+}  // namespace psg
+
+extern "C" {
+
+int psg_submit(psg_server* S, const psg_plan* plan, const void* src_host, void* dst_host, int64_t rows, int32_t cols,
+               const int32_t* live_host, const double* start_ms_host, double dt_ms, uint64_t* ticket) {
+  return submit(S, plan, src_host, dst_host, rows, cols, live_host, start_ms_host, nullptr, dt_ms, false, nullptr,
+                ticket);
+}
+
+int psg_submit_keyed(psg_server* S, const psg_plan* plan, const void* src_host, void* dst_host, int64_t rows,
+                     int32_t cols, const int32_t* live_host, const double* start_ms_host, const psg_keys* keys_host,
+                     double dt_ms, uint64_t* ticket) {
+  return submit(S, plan, src_host, dst_host, rows, cols, live_host, start_ms_host, keys_host, dt_ms, false, nullptr,
+                ticket);
+}
+
+int psg_submit_device(psg_server* S, const psg_plan* plan, const void* src, void* dst, int64_t rows, int32_t cols,
+                      const int32_t* live, const double* start_ms, const psg_keys* keys, double dt_ms, void* stream,
+                      uint64_t* ticket) {
+  return submit(S, plan, src, dst, rows, cols, live, start_ms, keys, dt_ms, true, stream, ticket);
 }
 
 // A ticket has one waiter: the thread that waits claims the request under
@@ -3500,9 +3749,24 @@ int psg_cancel(psg_server* S, uint64_t ticket) {
     return PSG_EINVAL;
   }
   S->pending.erase(q);
+  put_event(S, r->in);  // a device request's wait on its caller's stream
+  r->in = nullptr;
   r->done = true;
   r->status = PSG_ECANCELED;
   S->cv_done.notify_all();
+  return PSG_OK;
+}
+
+int psg_server_counters(psg_server* S, int64_t* out4) {
+  if (!S || !out4) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::lock_guard<std::mutex> g(S->mu);
+  out4[0] = S->launches;
+  out4[1] = S->kernels;
+  out4[2] = S->overlapped;
+  out4[3] = S->completed;
   return PSG_OK;
 }
 

@@ -696,12 +696,14 @@ template <int NT> __device__ __forceinline__ void store_row(const SRow Y, float*
 // PF the next row's bulk copy issued as soon as the row buffer is free (after
 // the forward transform, or after a row that is only copied) so that it
 // lands under the rest of the row's work, E the AGC's samples per lane (its
-// window w ≤ 32·E). Row handling (bulk copy, ragged ends, src → dst copy of
-// dead rows and of samples past the live length) is pipeline_kernel's.
+// window w ≤ 32·E), BATCH the rows of many requests' jobs in one launch
+// (the request loop: a.jobs, a.row_begin, a.total_rows). Row handling (bulk
+// copy, ragged ends, src → dst copy of dead rows and of samples past the
+// live length) is pipeline_kernel's.
 // Shared memory: the row buffer X, then the two transform buffers; the
 // filtered trace F and the AGC's output Y take the transform buffers' place
 // once the inverse transform no longer needs them.
-template <class P, int RECIPE, bool PF, int E>
+template <class P, int RECIPE, bool PF, int E, bool BATCH = false>
 __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   constexpr int NT = P::NT;
   static_assert(RECIPE != RC_DFAN || NT == kNT, "the normalization step runs at the pipeline kernels' CTA width");
@@ -711,11 +713,11 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
   __shared__ __align__(8) uint64_t bar;
   __shared__ RowSlot slot;
   __shared__ int s_ok;
-  const long long total = a.job.rows;
+  const long long total = BATCH ? a.total_rows : a.job.rows;
   constexpr int esz = 4;
   // thread 0: the bulk copy of row t into the row buffer
   auto issue = [&](long long t) {
-    const RowCtx<float> c = row_ctx<float, false>(a, t);
+    const RowCtx<float> c = row_ctx<float, BATCH>(a, t);
     const int len = c.copy ? c.cols : c.n;
     const uintptr_t ga = (uintptr_t)c.from, ge = ga + (uintptr_t)len * esz;
     const int off = (int)(ga & 15);
@@ -763,7 +765,7 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
     }
     mbar_try_wait(&bar, phase);
     phase ^= 1;
-    const RowCtx<float> c = row_ctx<float, false>(a, t);
+    const RowCtx<float> c = row_ctx<float, BATCH>(a, t);
     const RowSlot sl = slot;
     const SRow X{sl.off >> 2};
     for (int i = threadIdx.x; i < sl.head; i += NT) X[i] = c.from[i];
@@ -1026,6 +1028,14 @@ template <class P, int E> TracePlanInfo info() {
     t.kernel[1][0] = (const void*)trace_kernel<P, RC_DFAN, false, E>;
     t.kernel[1][1] = (const void*)trace_kernel<P, RC_DFAN, true, E>;
   }
+  return t;
+}
+
+// The same with the request loop's batched kernels (the prefetch form).
+template <class P, int E> TracePlanInfo info_served() {
+  TracePlanInfo t = info<P, E>();
+  t.batch[0] = (const void*)trace_kernel<P, RC_DFA, true, E, true>;
+  if constexpr (P::NT == kNT) t.batch[1] = (const void*)trace_kernel<P, RC_DFAN, true, E, true>;
   return t;
 }
 

@@ -19,7 +19,10 @@ struct TracePlanInfo {
   int agc_e;
   int min_blocks;            // the CTAs per SM its launch bounds ask for
   int buf;                   // complex elements of each of its two transform buffers
-  const void* kernel[2][2];  // [recipe][prefetch]
+  const void* kernel[2][2];  // [recipe][prefetch]; nullptr where not built
+  // [recipe]: the request loop's kernel over many requests' rows (the
+  // prefetch form; nullptr where not built)
+  const void* batch[2];
 };
 
 // The builds for transform length m whose E serves AGC window w, in the

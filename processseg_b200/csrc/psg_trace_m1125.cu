@@ -17,7 +17,7 @@ using B = tk::RPlan<1125, 512, 1, Grp<3>, Grp<3>, Grp<5>, Grp<5>, Grp<5>>;
 // 3·3 | 5 | 5 | 5 over 256 threads
 using C = tk::RPlan<1125, 256, 3, Grp<3, 3>, Grp<5>, Grp<5>, Grp<5>>;
 
-const TracePlanInfo a = tk::info<A, 9>();
+const TracePlanInfo a = tk::info_served<A, 9>();
 const TracePlanInfo b = tk::info<B, 9>();
 const TracePlanInfo c = tk::info<C, 9>();
 const TracePlanInfo* const builds[] = {&a, &b, &c, nullptr};

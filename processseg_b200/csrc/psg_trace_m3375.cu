@@ -15,7 +15,7 @@ using A = tk::RPlan<3375, 256, 2, Grp<3, 3>, Grp<3, 5>, Grp<5, 5>>;
 // 3·3 | 3 | 5·5 | 5
 using B = tk::RPlan<3375, 256, 2, Grp<3, 3>, Grp<3>, Grp<5, 5>, Grp<5>>;
 
-const TracePlanInfo a = tk::info<A, 9>();
+const TracePlanInfo a = tk::info_served<A, 9>();
 const TracePlanInfo b = tk::info<B, 9>();
 const TracePlanInfo* const builds[] = {&a, &b, nullptr};
 

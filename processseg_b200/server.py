@@ -5,8 +5,13 @@ The reference's viewer loop (tests/utils/viewersim.nim:155-200) applies a
 plan per stale buffer through its ``ProcessPool``, one call at a time. Here
 requests from any thread are queued, admitted by their device footprint,
 and run together: requests that arrive while others are on the GPU join the
-next launch, and the copies of one overlap the kernels of others. Each
-result is the plain ``apply``'s, bit for bit.
+next batch (or start one beside it when they can fill the device), and the
+copies of one overlap the kernels of others. Requests whose buffers are
+already on the device (CUDA tensors) skip the copies. Any plan the plain
+apply takes is served: single-part float32 plans in batched launches, the
+rest (per-panel normalizations, float64, IIR filters, mutes, long traces)
+with the plain apply's own launches inside a batch. Each result is the
+plain ``apply``'s, bit for bit.
 """
 from __future__ import annotations
 
@@ -45,17 +50,41 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
-    def submit(self, plan: PipelinePlan, src: np.ndarray, dst: np.ndarray, meta: ChunkMeta) -> int:
-        """Queues ``plan`` on ``src`` into ``dst`` (host arrays of the same
-        shape); returns a ticket for ``wait``."""
-        rows, cols = src.shape
+    def submit(self, plan: PipelinePlan, src, dst, meta: ChunkMeta) -> int:
+        """Queues ``plan`` on ``src`` into ``dst`` (host arrays, or CUDA
+        tensors on the server's device, of the same shape and the plan's
+        dtype); returns a ticket for ``wait``. A plan that mutes reads the
+        meta's offsets and t0Ms."""
+        rows, cols = int(src.shape[0]), int(src.shape[1])
         meta.checkShape(rows)
-        live, start = meta.flat(cols, 0)
         t = C.c_uint64()
+        try:
+            import torch
+            on_device = isinstance(src, torch.Tensor)
+        except ImportError:
+            on_device = False
+        if on_device:
+            if not (src.is_cuda and dst.is_cuda and src.is_contiguous() and dst.is_contiguous()):
+                raise ValueError("device requests take contiguous CUDA tensors")
+            dev = src.device.index
+            live, start = meta.device(cols, 0, dev)
+            keys = plan._keys(meta, dev)
+            st = torch.cuda.current_stream(dev).cuda_stream  # the caller's writes come first
+            A.check(A.lib().psg_submit_device(self.h, plan.h, src.data_ptr(), dst.data_ptr(), rows, cols,
+                                              live.data_ptr(), start.data_ptr(), keys, meta.dtMs, st,
+                                              C.byref(t)))
+            self._keep[t.value] = (plan, src, dst, live, start, keys)
+            return t.value
+        live, start = meta.flat(cols, 0)
         p = lambda a: a.ctypes.data_as(C.c_void_p)
-        A.check(A.lib().psg_submit(self.h, plan.h, p(src), p(dst), rows, cols, p(live), p(start),
-                                   meta.dtMs, C.byref(t)))
-        self._keep[t.value] = (plan, src, dst, live, start)
+        keys = plan._keys(meta, None)
+        if keys is None:
+            A.check(A.lib().psg_submit(self.h, plan.h, p(src), p(dst), rows, cols, p(live), p(start),
+                                       meta.dtMs, C.byref(t)))
+        else:
+            A.check(A.lib().psg_submit_keyed(self.h, plan.h, p(src), p(dst), rows, cols, p(live), p(start), keys,
+                                             meta.dtMs, C.byref(t)))
+        self._keep[t.value] = (plan, src, dst, live, start, keys, meta)
         return t.value
 
     def wait(self, ticket: int, timeout_ms: float = 10000.0):
@@ -85,6 +114,13 @@ class Server:
         if "unknown ticket" in msg:
             raise ValueError(msg)
         return False
+
+    def counters(self) -> dict:
+        """Counters since the loop was created: batches, kernel launches,
+        batches started beside running ones, requests completed."""
+        out = (C.c_int64 * 4)()
+        A.check(A.lib().psg_server_counters(self.h, out))
+        return dict(zip(["batches", "kernels", "overlapped", "completed"], list(out)))
 
     def stats(self, reset: bool = False) -> dict:
         out = (C.c_double * 8)()
