@@ -342,6 +342,76 @@ def serving_leg(n_req=150, rates=(2000.0, 5000.0, 10000.0, 20000.0, 40000.0), sl
     return out
 
 
+def multi_gpu_legs(args, world, rank, dist):
+    """The two splits beside the weak-scaled panels, run on every rank (their
+    collectives are the path's exchanges), timed with events on each rank
+    after W warm-up steps, the max over ranks: ``sharded_panel``, a per-panel
+    p99 normalization over a panel split by rows (the C2 chain with the
+    normalization before the AGC; ``applySharded``: two all-reduces of the
+    partial statistics per step; each rank 2000 × 3001 rows, weak scaling),
+    and ``c3_by_channel``, the 4-sweep 240-channel gather split by channel
+    (each rank correlates and stacks every sweep of its channels, one
+    all-gather assembles the 240 × 3000 stack; strong scaling)."""
+    import numpy as np
+    import torch
+    import processseg_b200 as P
+    from processseg_b200 import shard, synth
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    out = {}
+    flow = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(3, 6, 70, 90)).withNotch(50, 2)),
+            P.normalizeOp(P.normPercentile, P.perPanel, percentile=99.0), P.agcOp(300)]
+    plan = P.initPipeline(flow).compile(P.float32, DT, COLS)
+    g = synth.c2(seed=40 + rank)
+    meta = g.meta()
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=ROWS, cols=COLS)
+    src = torch.from_numpy(g.data).cuda()
+    dst = torch.empty_like(src)
+    ms = timed(lambda: shard.applySharded(plan, src, dst, meta, ws))
+    out["sharded_panel"] = {
+        "workload": f"{world} x 2000 x 3001 f32 panel split by rows: demean -> band-pass + notch -> per-panel p99 "
+                    "-> AGC 300 ms (applySharded, two all-reduces per step)",
+        "ms_per_step": ms, "msamples_per_s": world * ROWS * COLS / (ms * 1e-3) / 1e6, "scaling": "weak"}
+    del src, dst
+
+    spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
+    pilot = P.generatePilot(spec, np.float64)
+    recs = synth.vibroseis_records(pilot.samples, channels=240, sweeps=4)
+    sweeps, ch, ns = recs.shape
+    block = recs.reshape(sweeps * ch, ns)
+    rmap = (np.arange(sweeps * ch) % ch).astype(np.int32)
+    cmeta = P.initChunkMeta(np.full(sweeps * ch, P.tsLive, np.int32), np.full(sweeps * ch, ns, np.int32), 2.0)
+    cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=3000)
+    idx, _, _ = shard.channelShard(rmap, ch, world, rank)
+    x = torch.from_numpy(block).cuda()  # every record in HBM; each rank reads its channels' records
+    split = shard.ChannelSplit(cplan, cmeta, rmap, ch)
+    ms = timed(lambda: split.run(x))
+    out["c3_by_channel"] = {
+        "workload": "4 sweeps x 240 channels x 10001 f32, nfft 16200, 6 s out, split by channel, stack all-gathered",
+        "ms_per_gather": ms, "records_this_rank": int(idx.size),
+        "msamples_per_s": sweeps * ch * ns / (ms * 1e-3) / 1e6, "scaling": "strong"}
+    return out
+
+
 def launch_of(plan, rows):
     """The trace-kernel launch shape the tuner chose for a call of ``rows``
     rows (the first one untuned), with its per-shape times (µs per launch)."""
@@ -580,6 +650,7 @@ def run_ours(args):
     e2e_run(False)  # the first streamed run sizes the pinned staging
     e2e = e2e_run(False)
     e2e_sync = e2e_run(True)
+    multi = None if args.no_multi else multi_gpu_legs(args, world, rank, dist)
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -620,6 +691,8 @@ def run_ours(args):
             "clocks": clk.summary(),
             "launch": launch_of(plan, ROWS),
         }
+        if multi:
+            line["multi_gpu"] = multi
         if line["issue"]:
             line["issue"]["frac"] = line["issue"]["achieved"] / line["issue"]["peak"]
         # the one-GPU legs: the served load, the other configurations and the
@@ -647,6 +720,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-load leg")
+    ap.add_argument("--no-multi", action="store_true", help="skip the split-panel and by-channel legs")
     ap.add_argument("--no-workloads", action="store_true", help="skip the C1/C3/C5 legs")
     ap.add_argument("--no-errors", action="store_true", help="skip the error report against the oracle")
     args = ap.parse_args()

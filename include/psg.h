@@ -696,6 +696,10 @@ int psg_server_stats(psg_server* server, double* out, int reset);
  * (batched launches and the part launches of requests run alone), batches
  * started beside running ones, requests completed}. */
 int psg_server_counters(psg_server* server, int64_t* out4);
+/* The loop's outstanding work now: {requests, samples} queued, staged or in
+ * a running batch (what a front end placing requests over several devices'
+ * loops reads to pick the least loaded). */
+int psg_server_load(psg_server* server, int64_t* out2);
 
 #ifdef __cplusplus
 }

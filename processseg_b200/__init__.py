@@ -43,5 +43,5 @@ from .vibroseis import (CorrelationPlan, Pilot, RecordStack, SweepHarmonic, Swee
                         linearSweep, noTaper, segyTaperType, slDbPerHz, slDbPerOctave, slExponential, slLinear,
                         slTable, sweepHarmonics, tableSweep, taperWeight, tpBlackman, tpBlackmanHarris, tpCos2,
                         tpCosine, tpGaussian, tpHamming, tpKaiser, tpLinear, tpPower)
-from .server import Server
+from .server import Server, ServerPool, leastLoaded
 from .stats import PanelStats, TraceStats, panelStats, traceStatsInto

@@ -3757,6 +3757,26 @@ int psg_cancel(psg_server* S, uint64_t ticket) {
   return PSG_OK;
 }
 
+int psg_server_load(psg_server* S, int64_t* out2) {
+  if (!S || !out2) {
+    t_err = "null argument";
+    return PSG_EINVAL;
+  }
+  std::lock_guard<std::mutex> g(S->mu);
+  int64_t n = 0, samples = 0;
+  auto add = [&](const Req* r) {
+    n++;
+    samples += r->rows * (int64_t)r->cols;
+  };
+  for (const Req* r : S->pending) add(r);
+  for (const Req* r : S->staged) add(r);
+  for (const Batch* b : S->inflight)
+    for (const Req* r : b->reqs) add(r);
+  out2[0] = n;
+  out2[1] = samples;
+  return PSG_OK;
+}
+
 int psg_server_counters(psg_server* S, int64_t* out4) {
   if (!S || !out4) {
     t_err = "null argument";

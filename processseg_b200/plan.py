@@ -83,10 +83,13 @@ class PipelinePlan:
     """A compiled pipeline (pipeline.nim:200-211): immutable, shared by any
     number of callers, each with its own ``Workspace``."""
 
-    def __init__(self, h, dtype: int, dtMs: float):
+    def __init__(self, h, dtype: int, dtMs: float, args=None, device: Optional[int] = None):
         self.h = h
         self.dtype = dtype
         self._dtMs = dtMs
+        self._args = args      # what compile took, to compile a twin on another device
+        self.device = device   # the device its tables live on
+        self._twins = {}
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -238,6 +241,19 @@ class PipelinePlan:
                                           C.byref(h)))
         return ApplyGraph(h, (self, ws, src, dst, live, start, keys))
 
+    def forDevice(self, device: int) -> "PipelinePlan":
+        """This plan compiled for ``device`` (itself when its tables are
+        there; else a twin, compiled once and kept)."""
+        if device == self.device:
+            return self
+        if device not in self._twins:
+            if self._args is None:
+                raise ValueError("the plan was not made by compile")
+            import torch
+            with torch.cuda.device(device):
+                self._twins[device] = compile(*self._args)
+        return self._twins[device]
+
     def traceShapes(self, part: int = 0) -> int:
         """How many launch shapes of the trace kernel part ``part`` can run
         on (0: the part runs on the general kernel). Every shape gives the
@@ -381,4 +397,11 @@ def compile(pipeline, T, dtMs: float, samples: int, recordSamples: int = 0) -> P
     h = C.c_void_p()
     A.check(A.lib().psg_plan_compile(arr, len(ops), dt, float(dtMs), int(samples),
                                      int(recordSamples), C.byref(h)))
-    return PipelinePlan(h, dt, float(dtMs))
+    dev = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            dev = torch.cuda.current_device()
+    except ImportError:
+        pass
+    return PipelinePlan(h, dt, float(dtMs), (ops, T, dtMs, samples, recordSamples), dev)

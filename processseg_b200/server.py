@@ -34,6 +34,7 @@ class Server:
         h = C.c_void_p()
         A.check(A.lib().psg_server_create(device, arena_bytes, C.byref(h)))
         self.h = h
+        self.device = device
         self._keep = {}
 
     def close(self):
@@ -128,3 +129,79 @@ class Server:
         keys = ["completed", "samples", "launches", "requests_per_launch", "p50_s", "p99_s",
                 "msamples_per_s", "refused"]
         return dict(zip(keys, list(out)))
+
+    def load(self) -> tuple:
+        """(requests, samples) outstanding: queued, staged or running."""
+        out = (C.c_int64 * 2)()
+        A.check(A.lib().psg_server_load(self.h, out))
+        return int(out[0]), int(out[1])
+
+
+def leastLoaded(loads) -> int:
+    """The index of the least loaded of ``loads`` ((requests, samples) per
+    loop): the fewest outstanding samples, then the fewest requests, then
+    the lowest index."""
+    loads = list(loads)
+    if not loads:
+        raise ValueError("no loops to choose from")
+    return min(range(len(loads)), key=lambda i: (loads[i][1], loads[i][0], i))
+
+
+class ServerPool:
+    """One request loop per device, requests placed on the least loaded one
+    (its outstanding samples). A request whose buffers are CUDA tensors runs
+    on their device; host requests go where the load is least, with the plan
+    compiled for that device once (``PipelinePlan.forDevice``). ``submit``
+    returns a (loop index, ticket) pair for ``wait``, ``poll`` and
+    ``cancel``."""
+
+    def __init__(self, devices=None, arena_bytes: int = 2 << 30, loops=None):
+        if loops is not None:
+            self.loops = list(loops)       # loops made elsewhere (their device attribute set)
+        else:
+            import torch
+            devs = list(range(torch.cuda.device_count())) if devices is None else list(devices)
+            self.loops = []
+            for d in devs:
+                s = Server(d, arena_bytes)
+                s.device = d
+                self.loops.append(s)
+        if not self.loops:
+            raise ValueError("a pool needs at least one loop")
+
+    def close(self):
+        for s in self.loops:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def place(self, src) -> int:
+        """The loop a request on ``src`` goes to."""
+        dev = getattr(src, "device", None)
+        if dev is not None and getattr(dev, "type", None) == "cuda":
+            for i, s in enumerate(self.loops):
+                if s.device == dev.index:
+                    return i
+            raise ValueError(f"no loop on cuda:{dev.index}")
+        return leastLoaded(s.load() for s in self.loops)
+
+    def submit(self, plan: PipelinePlan, src, dst, meta: ChunkMeta):
+        i = self.place(src)
+        s = self.loops[i]
+        return i, s.submit(plan.forDevice(s.device), src, dst, meta)
+
+    def wait(self, ticket, timeout_ms: float = 10000.0):
+        i, t = ticket
+        self.loops[i].wait(t, timeout_ms)
+
+    def poll(self, ticket) -> bool:
+        i, t = ticket
+        return self.loops[i].poll(t)
+
+    def cancel(self, ticket) -> bool:
+        i, t = ticket
+        return self.loops[i].cancel(t)

@@ -102,3 +102,57 @@ def test_parts_api_errors():
         plan.runPart(None, b, m, 5, None, ws)
     with pytest.raises(ValueError):
         plan.runPart(None, torch.zeros(10, 101, device="cuda"), P.liveMeta(10, 101, 2.0), 0, None, ws)
+
+
+def test_correlate_stack_by_channel_in_one_process_equals_the_whole_gather():
+    """correlateStackSharded without a process group (one rank: every
+    channel) gives correlateInto + stack over all records; and each channel
+    block of two shards, stacked on its own, matches the whole stack's rows
+    bit for bit (the rows a two-rank all-gather puts together)."""
+    spec = P.linearSweep(8, 80, 4000, 2, P.initSweepTaper(200, 200, P.tpCos2))
+    pilot = P.generatePilot(spec, np.float64)
+    recs = synth.vibroseis_records(pilot.samples, channels=12, samples=4001, sweeps=3)
+    sweeps, ch, ns = recs.shape
+    block = recs.reshape(sweeps * ch, ns)
+    rmap = (np.arange(sweeps * ch) % ch).astype(np.int32)
+    meta = P.initChunkMeta(np.full(sweeps * ch, P.tsLive, np.int32), np.full(sweeps * ch, ns, np.int32), 2.0)
+    cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=1500)
+    st = P.initRecordStack(ch, 1500, 2.0)
+    cplan.correlateInto(torch.from_numpy(block).cuda(), None, meta, stack=st,
+                        rowMap=torch.from_numpy(rmap).cuda())
+    want = torch.empty(ch, 1500, device="cuda")
+    st.stackInto(want)
+    got = shard.correlateStackSharded(cplan, torch.from_numpy(block).cuda(), meta, rmap, ch)
+    assert torch.equal(got, want)
+    parts = []
+    for r in range(2):
+        idx, lmap, (c0, c1) = shard.channelShard(rmap, ch, 2, r)
+        s2 = P.initRecordStack(c1 - c0, 1500, 2.0)
+        sub = P.initChunkMeta(meta.status[idx], meta.numSamples[idx], 2.0)
+        cplan.correlateInto(torch.from_numpy(np.ascontiguousarray(block[idx])).cuda(), None, sub, stack=s2,
+                            rowMap=torch.from_numpy(lmap).cuda())
+        o = torch.empty(c1 - c0, 1500, device="cuda")
+        s2.stackInto(o)
+        parts.append(o)
+    assert torch.equal(torch.cat(parts), want)
+
+
+def test_server_pool_places_requests_over_two_loops():
+    """Two request loops (here both on device 0): host requests go to the
+    less loaded one, each result the plain apply's."""
+    plan = P.initPipeline(FLOWS["pct"]).compile(P.float32, 2.0, 3001)
+    g = synth.c2(seed=22, rows=400)
+    meta = g.meta()
+    ws = P.initWorkspace()
+    ws.reserve(plan, rows=400, cols=3001)
+    want = np.zeros_like(g.data)
+    plan.apply(g.data, want, meta, ws)
+    loops = [P.Server(0, 256 << 20), P.Server(0, 256 << 20)]
+    with P.ServerPool(loops=loops) as pool:
+        outs = [np.zeros_like(g.data) for _ in range(8)]
+        tickets = [pool.submit(plan, g.data, o, meta) for o in outs]
+        for t in tickets:
+            pool.wait(t, 30000)
+    assert {i for i, _ in tickets} == {0, 1}
+    for o in outs:
+        assert np.array_equal(o, want)

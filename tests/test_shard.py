@@ -129,6 +129,32 @@ class NumpyPlan:
                 dst[r, :n] *= np.float32(0.5)
 
 
+def gather_case(channels=6, sweeps=4, samples=700, seed=21):
+    """A small vibroseis gather: ``sweeps`` records per channel, in sweep
+    order (record r on channel r % channels), with one dead record."""
+    g = np.random.default_rng(seed)
+    n = channels * sweeps
+    recs = g.standard_normal((n, samples)).astype(np.float32)
+    live = np.full(n, samples, np.int32)
+    live[5] = 0
+    return recs, live, (np.arange(n) % channels).astype(np.int32), channels
+
+
+PILOT = np.random.default_rng(5).standard_normal(150)
+
+
+def oracle_stack(recs, live, rmap, channels, out=400):
+    """The oracle's correlateInto of ``recs`` with the vertical stack of each
+    on its channel (vibroseis/vstack.nim:186-202, 439-471), float32."""
+    from oracle import oracle as O
+    num = np.zeros((channels, out))
+    cnt = np.zeros((channels, out), np.int32)
+    if len(recs):
+        corr, _, _ = O.correlate(PILOT, 2.0, 0.0, recs, live, 2.0, recs.shape[1], out)
+        O.stack_add(num, cnt, corr, np.where(live > 0, out, 0).astype(np.int32), rmap)
+    return O.stack_result(num, cnt, np.float32)
+
+
 def free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -143,7 +169,13 @@ def _worker(rank, world, port, job, q):
         b, live = panel()
         a0, a1 = shard.shardRows(b.shape[0], world, rank)
         mine, my_live = b[a0:a1].copy(), live[a0:a1].copy()
-        if job["kind"] == "merge":
+        if job["kind"] == "channels":
+            recs, live, rmap, nch = gather_case()
+            idx, lmap, (c0, c1) = shard.channelShard(rmap, nch, world, rank)
+            local = oracle_stack(recs[idx], live[idx], lmap, c1 - c0)
+            whole = shard.gatherChannels(torch.from_numpy(local), nch)
+            q.put((rank, "ok", (idx, whole.numpy())))
+        elif job["kind"] == "merge":
             part = torch.from_numpy(np_partials(mine, my_live))
             shard.mergePartials(part)
             q.put((rank, "ok", part.numpy()))
@@ -253,3 +285,35 @@ def test_a_failed_rank_ends_the_others_collective():
     status, val = out.get(0, ("missing", None))
     assert status == "error", (status, val)
     assert val[1] < 60
+
+
+def test_channel_shards_cover_every_record_once():
+    recs, live, rmap, nch = gather_case()
+    for world in (1, 2, 3, 4):
+        seen = []
+        for r in range(world):
+            idx, lmap, (c0, c1) = shard.channelShard(rmap, nch, world, r)
+            assert np.all((rmap[idx] >= c0) & (rmap[idx] < c1))
+            assert np.array_equal(lmap, rmap[idx] - c0)
+            seen.extend(idx.tolist())
+        assert sorted(seen) == list(range(len(rmap)))
+    # a record mapped to no channel goes to no rank
+    bad = rmap.copy()
+    bad[0] = -1
+    assert 0 not in shard.channelShard(bad, nch, 1, 0)[0]
+
+
+def test_stack_by_channel_over_two_gloo_ranks():
+    """Each rank correlates and stacks the records of its channels (every
+    sweep of them); the all-gather of the stacked rows equals one stack of
+    the whole gather, bit for bit."""
+    out = run_ranks({"kind": "channels"})
+    assert set(out) == {0, 1}, out
+    recs, live, rmap, nch = gather_case()
+    want = oracle_stack(recs, live, rmap, nch)
+    for r in (0, 1):
+        status, val = out[r]
+        assert status == "ok", val
+        idx, whole = val
+        assert np.array_equal(whole, want)
+    assert sorted(out[0][1][0].tolist() + out[1][1][0].tolist()) == list(range(len(rmap)))
