@@ -17,11 +17,19 @@ using A = tk::RPlan<1944, 256, 4, Grp<4>, Grp<2, 3>, Grp<3, 3>, Grp<3, 3>>;
 using B = tk::RPlan<1944, 256, 4, Grp<4, 2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
 // the same passes with 85 registers (three CTAs per SM, no spills)
 using C = tk::RPlan<1944, 256, 3, Grp<4, 2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
+// over 512 threads, two CTAs per SM (64 registers): half the latency of a
+// trace for the last rows of a panel and for small panels (demean, filter,
+// AGC only); 4 | 2·3 | 3·3 | 3·3, and 4 | 2 | 3·3 | 3·3 | 3 with more
+// butterflies in the later passes
+using D = tk::RPlan<1944, 512, 2, Grp<4>, Grp<2, 3>, Grp<3, 3>, Grp<3, 3>>;
+using F = tk::RPlan<1944, 512, 2, Grp<4>, Grp<2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
 
 const TracePlanInfo a = tk::info_served<A, 5>();
 const TracePlanInfo b = tk::info<B, 5>();
 const TracePlanInfo c = tk::info<C, 5>();
-const TracePlanInfo* const builds[] = {&a, &b, &c, nullptr};
+const TracePlanInfo d = tk::info<D, 5>();
+const TracePlanInfo f = tk::info<F, 5>();
+const TracePlanInfo* const builds[] = {&a, &b, &c, &d, &f, nullptr};
 
 }  // namespace
 
