@@ -140,10 +140,14 @@ def test_iir_plan_api_and_serving():
     torch.cuda.synchronize()
     want = oracle([P.iirOp(P.butterBandPass(4, 60, 24))], ref.cpu().numpy(), P.liveMeta(6, 500, 2.0), P.F32, 2.0)
     assert max_rel(x.cpu().numpy(), want, [500] * 6) <= 1e-5
+    # the request loop serves an IIR plan with the plain apply's launches: the same bits
     compiled = P.initPipeline([P.iirOp(P.butterBandPass(4, 60, 24))]).compile(P.float32, 2.0, 500)
-    srv = P.Server()
-    try:
-        with pytest.raises(ValueError):
-            srv.submit(compiled, np.ones((4, 500), np.float32), np.zeros((4, 500), np.float32), P.liveMeta(4, 500, 2.0))
-    finally:
-        srv.close()
+    src = np.random.default_rng(4).standard_normal((4, 500)).astype(np.float32)
+    plain = np.zeros_like(src)
+    ws2 = P.initWorkspace()
+    ws2.reserve(compiled, rows=4, cols=500)
+    compiled.apply(src, plain, P.liveMeta(4, 500, 2.0), ws2)
+    served = np.zeros_like(src)
+    with P.Server(arena_bytes=16 << 20) as srv:
+        srv.wait(srv.submit(compiled, src, served, P.liveMeta(4, 500, 2.0)), 30000)
+    assert np.array_equal(served, plain)

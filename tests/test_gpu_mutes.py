@@ -142,7 +142,7 @@ def test_mute_flows_match_oracle(name, dtype):
     assert np.array_equal(host, got)
 
 
-def test_mute_plan_needs_keys_and_is_not_served():
+def test_mute_plan_needs_keys_and_is_served_with_them():
     plan = P.initPipeline([P.muteTopOp(P.timeMute(100))]).compile(P.float32, 2.0, 500)
     assert plan.needsKeys
     assert not P.initPipeline([P.demeanOp()]).compile(P.float32, 2.0, 500).needsKeys
@@ -159,12 +159,12 @@ def test_mute_plan_needs_keys_and_is_not_served():
     plan.apply(src, meta, ws)
     torch.cuda.synchronize()
     assert float(src[:, :50].abs().max()) == 0 and float(src[:, 50:].min()) == 1
-    srv = P.Server()
-    try:
-        with pytest.raises(ValueError):
-            srv.submit(plan, np.ones((4, 500), np.float32), np.zeros((4, 500), np.float32), meta)
-    finally:
-        srv.close()
+    # served: the loop copies the rows' keys in with the block (psg_submit_keyed)
+    x = np.ones((4, 500), np.float32)
+    y = np.zeros_like(x)
+    with P.Server(arena_bytes=16 << 20) as srv:
+        srv.wait(srv.submit(plan, x, y, meta), 30000)
+    assert np.array_equal(y, src.cpu().numpy())
 
 
 def test_applied_response_mute_sees_offset_zero_and_t0_zero():
