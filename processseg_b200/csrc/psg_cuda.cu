@@ -127,20 +127,53 @@ __global__ void __launch_bounds__(1024) panel_fold_kernel(long long rows, int co
   }
 }
 
+// The 65536-bin histogram of |x| (float32 bits >> 15, capped at 0xFEFF) over
+// the usable rows' live samples (gain/stats.nim:208-235), added into `hist`.
+// Each CTA counts its rows' samples in shared memory, the counts of bins 2k
+// and 2k + 1 as the two 16-bit halves of word k (128 KB), and adds them to
+// the global histogram before any count could pass 65535 (every 65535
+// samples it takes) and at its end: shared-memory atomics where a filtered
+// panel's samples pile onto a few hundred bins, instead of global ones.
+constexpr int kHistWords = 65536 / 2;
 template <class T>
-__global__ void __launch_bounds__(256) panel_hist_kernel(const T* __restrict__ b, long long rows, int cols,
+__global__ void __launch_bounds__(512) panel_hist_kernel(const T* __restrict__ b, long long rows, int cols,
                                                          const int* __restrict__ live, const double* __restrict__ ss,
                                                          const double* __restrict__ mx, unsigned* __restrict__ hist) {
+  extern __shared__ unsigned h2[];
+  for (int k = threadIdx.x; k < kHistWords; k += blockDim.x) h2[k] = 0;
+  __syncthreads();
+  auto flush = [&]() {
+    __syncthreads();
+    for (int k = threadIdx.x; k < kHistWords; k += blockDim.x) {
+      const unsigned w = h2[k];
+      if (w) {
+        if (w & 0xFFFFu) atomicAdd(&hist[2 * k], w & 0xFFFFu);
+        if (w >> 16) atomicAdd(&hist[2 * k + 1], w >> 16);
+        h2[k] = 0;
+      }
+    }
+    __syncthreads();
+  };
+  int pending = 0;  // samples counted since the last flush (the same in every thread)
   for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
-    int n = min(max(live[r], 0), cols);
+    const int n = min(max(live[r], 0), cols);
     if (!usable_d(ss[r], mx[r], n)) continue;
     const T* x = b + r * (long long)cols;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      float a = (float)fabs((double)x[i]);
-      unsigned key = min(__float_as_uint(a) >> 15, 0xFEFFu);
-      atomicAdd(&hist[key], 1u);
+    for (int i0 = 0; i0 < n; i0 += 65535) {
+      const int m = min(n - i0, 65535);
+      if (pending + m > 65535) {
+        flush();
+        pending = 0;
+      }
+      for (int i = i0 + (int)threadIdx.x; i < i0 + m; i += blockDim.x) {
+        const float a = (float)fabs((double)x[i]);
+        const unsigned key = min(__float_as_uint(a) >> 15, 0xFEFFu);
+        atomicAdd(&h2[key >> 1], (key & 1u) ? 0x10000u : 1u);
+      }
+      pending += m;
     }
   }
+  flush();
 }
 
 // orderStat (gain/stats.nim:237-251) for ranks j0 and j0 + 1, one CTA of
@@ -158,23 +191,26 @@ __device__ double order_stat_from(const C* hist, long long j, double mxv, int bi
 template <class C>
 __global__ void __launch_bounds__(1024) panel_clip_kernel(const C* __restrict__ hist, PanelOut* out,
                                                           double clipP, int stat, double target, int dtype) {
-  __shared__ long long pre[1024];
+  // warp w owns the bins [2048·w, 2048·w + 2048), read 32 at a time by its
+  // lanes (coalesced): their count, then the warps' exclusive prefix
+  __shared__ long long seg[32], segbase[32];
   __shared__ long long found_below[2];
   __shared__ int found_bin[2];
-  const int per = 64;  // 65536 / 1024 bins per thread
   const int maxKey = 0xFEFF;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto count = [&](int bin) -> long long { return bin <= maxKey ? (long long)hist[bin] : 0; };
   long long tot = 0;
-  for (int k = 0; k < per; k++) {
-    int bin = threadIdx.x * per + k;
-    if (bin <= maxKey) tot += (long long)hist[bin];
-  }
-  pre[threadIdx.x] = tot;
+  for (int c = 0; c < 64; c++) tot += count(warp * 2048 + c * 32 + lane);
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if (lane == 0) seg[warp] = tot;
   __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
-    long long v = threadIdx.x >= o ? pre[threadIdx.x - o] : 0;
-    __syncthreads();
-    pre[threadIdx.x] += v;
-    __syncthreads();
+  if (warp == 0) {
+    long long v = seg[lane], incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    segbase[lane] = incl - v;
   }
   double samples = out->samples, mxv = out->maxAbs;
   bool have = samples > 0 && !isnan(clipP);
@@ -187,19 +223,28 @@ __global__ void __launch_bounds__(1024) panel_clip_kernel(const C* __restrict__ 
   __syncthreads();
   if (have) {
     for (int q = 0; q < 2; q++) {
-      long long j = k0 + q;
-      long long excl = pre[threadIdx.x] - tot;
-      if (j >= excl && j < pre[threadIdx.x]) {
-        long long below = excl;
-        for (int k = 0; k < per; k++) {
-          int bin = threadIdx.x * per + k;
-          long long c = bin <= maxKey ? (long long)hist[bin] : 0;
-          if (below + c > j) {
-            found_bin[q] = bin;
-            found_below[q] = below;
+      const long long j = k0 + q;
+      // the warp whose bins hold rank j walks them 32 at a time
+      if (j >= segbase[warp] && j < segbase[warp] + seg[warp]) {
+        long long below = segbase[warp];
+        for (int c = 0; c < 64; c++) {
+          const int bin = warp * 2048 + c * 32 + lane;
+          const long long v = count(bin);
+          long long incl = v;
+          for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+          }
+          const unsigned hit = __ballot_sync(0xffffffffu, below + incl > j);
+          if (hit) {
+            const int l = __ffs(hit) - 1;
+            if (lane == l) {
+              found_bin[q] = bin;
+              found_below[q] = below + incl - v;
+            }
             break;
           }
-          below += c;
+          below += __shfl_sync(0xffffffffu, incl, 31);
         }
       }
     }
@@ -921,6 +966,17 @@ template <class F> static int guarded(F&& f) {
 // Workspace layout (bytes): [0, 512) panel outputs and factors, then
 // rows × 16 B of per-row statistics, then the 65536-bin histogram, then the
 // host-path staging (live, start_ms, samples).
+// Launches panel_hist_kernel: one CTA of 512 per SM (its 128 KB of counts).
+template <class T>
+static void launch_hist(const T* blk, long long rows, int cols, const int* live, const double* ss, const double* mx,
+                        unsigned* hist, cudaStream_t s) {
+  if (rows <= 0) return;
+  const size_t sm = (size_t)kHistWords * sizeof(unsigned);
+  CUDA_OK(cudaFuncSetAttribute((const void*)panel_hist_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int g = (int)std::min<long long>(rows, (long long)g_sm_count);
+  panel_hist_kernel<T><<<g, 512, sm, s>>>(blk, rows, cols, live, ss, mx, hist);
+}
+
 static const int64_t kHist = 65536 * 4;
 static int64_t align256(int64_t x) { return (x + 255) / 256 * 256; }
 static int64_t ws_device_bytes(int64_t rows) { return 512 + align256(rows * 16) + kHist; }
@@ -1394,7 +1450,7 @@ static const double* panel_factor_dev(const psg_plan* p, psg_workspace* ws, int 
   double clipP = ns.stat == PSG_NORM_PERCENTILE ? ns.percentile : NAN;
   if (!std::isnan(clipP)) {
     CUDA_OK(cudaMemsetAsync(hist, 0, kHist, stream));
-    if (rows > 0) panel_hist_kernel<T><<<g, 256, 0, stream>>>(blk, rows, cols, live, ss, mx, hist);
+    launch_hist<T>(blk, rows, cols, live, ss, mx, hist, stream);
   }
   panel_clip_kernel<unsigned><<<1, 1024, 0, stream>>>(hist, out, clipP, ns.stat, ns.norm_target, p->host.dtype);
   return &out->factor;
@@ -2241,10 +2297,8 @@ int psg_panel_partials(const psg_plan* plan, psg_workspace* ws, int32_t part, co
     panel_partial_head_kernel<<<1, 1, 0, s>>>(out, partial);
     if (ns.stat == PSG_NORM_PERCENTILE) {
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
-      if (rows > 0) {
-        if (f32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
-        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
-      }
+      if (f32) launch_hist<float>((const float*)block, rows, cols, live, ss, mx, hist, s);
+      else launch_hist<double>((const double*)block, rows, cols, live, ss, mx, hist, s);
       hist_to_f64_kernel<<<256, 256, 0, s>>>(hist, partial + PSG_PANEL_PARTIAL_HEAD);
     } else {
       CUDA_OK(cudaMemsetAsync(partial + PSG_PANEL_PARTIAL_HEAD, 0, 65536 * sizeof(double), s));
@@ -2413,10 +2467,8 @@ int psg_panel_stats(psg_workspace* ws, const void* block, int32_t dtype, int64_t
     panel_fold_kernel<<<1, 1024, 0, s>>>(rows, cols, live, ss, mx, po, 1);
     if (!std::isnan(clip_percentile)) {
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
-      if (rows > 0) {
-        if (dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
-        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
-      }
+      if (dtype == PSG_F32) launch_hist<float>((const float*)block, rows, cols, live, ss, mx, hist, s);
+      else launch_hist<double>((const double*)block, rows, cols, live, ss, mx, hist, s);
     }
     panel_clip_kernel<unsigned><<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
     CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -2484,10 +2536,8 @@ int psg_panel_stats_static(const void* block, int32_t dtype, int64_t rows, int32
     if (!std::isnan(clip_percentile)) {
       // The array keeps the previous call's counts: the histogram starts at zero.
       CUDA_OK(cudaMemsetAsync(hist, 0, kHist, s));
-      if (rows > 0) {
-        if (dtype == PSG_F32) panel_hist_kernel<float><<<g, 256, 0, s>>>((const float*)block, rows, cols, live, ss, mx, hist);
-        else panel_hist_kernel<double><<<g, 256, 0, s>>>((const double*)block, rows, cols, live, ss, mx, hist);
-      }
+      if (dtype == PSG_F32) launch_hist<float>((const float*)block, rows, cols, live, ss, mx, hist, s);
+      else launch_hist<double>((const double*)block, rows, cols, live, ss, mx, hist, s);
     }
     panel_clip_kernel<unsigned><<<1, 1024, 0, s>>>(hist, po, clip_percentile, -1, 1.0, dtype);
     CUDA_OK(cudaMemcpyAsync(out, po, 5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -3514,11 +3564,13 @@ void sched_loop(psg_server* S) {
       S->staged.clear();
       S->cv_done.notify_all();
     }
+    // idle: sleep until a submit; otherwise poll again at once (yielding the
+    // core), so a finished batch is seen within microseconds
     if (S->inflight.empty() && S->pending.empty() && S->staged.empty())
       S->cv.wait_for(lk, std::chrono::milliseconds(5));
     else {
       lk.unlock();
-      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      std::this_thread::yield();
       lk.lock();
     }
   }
