@@ -824,6 +824,7 @@ __global__ void trace_stats_finish(double* rms, double* mx, const int* live, lon
 struct TraceCand {
   const TracePlanInfo* tp = nullptr;
   bool pf = false, per_row = false;
+  bool row_in_buffer = false;  // the row lives in the first transform buffer (work_off 0)
   int per_sm = 0, work_off = 0;
   size_t smem = 0;
   const void* tw = nullptr;
@@ -1425,6 +1426,29 @@ template <class T> static void build_device_steps(psg_plan* p) {
           cs.push_back(c);
         }
       }
+      // The row in the first transform buffer: only the forward transform's
+      // first pass reads it, and that pass writes the other buffer. With no
+      // row buffer of its own, more CTAs fit where shared memory sets the
+      // count (the row's copy then waits for the row before it: no copy in
+      // flight); offered only when it adds CTAs per SM.
+      if ((!pf_env || atoi(pf_env) == 0) && (int64_t)p->x_bytes <= (int64_t)tb->buf * 8) {
+        int px = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&px, tb->kernel[rc][0], tb->nt, (size_t)fw));
+        if (px > std::max(per[0], per[1])) {
+          for (int per_row = 0; per_row < 2; per_row++) {
+            TraceCand c;
+            c.tp = tb;
+            c.pf = false;
+            c.per_row = per_row != 0;
+            c.per_sm = px;
+            c.work_off = 0;
+            c.smem = (size_t)fw;
+            c.tw = tw;
+            c.row_in_buffer = true;
+            cs.push_back(c);
+          }
+        }
+      }
     }
     if (cs.empty()) p->trace[part] = nullptr;
     else p->trace[part] = cs[0].tp;
@@ -1788,9 +1812,10 @@ int psg_plan_tuning(const psg_plan* plan, char* buf, int64_t cap, int64_t* neede
         }
         snprintf(tmp, sizeof tmp,
                  "%s{\"m\": %d, \"threads\": %d, \"min_blocks\": %d, \"passes\": \"%s\", \"prefetch\": %s, "
-                 "\"grid\": \"%s\", \"ctas_per_sm\": %d, \"smem\": %lld}",
+                 "\"grid\": \"%s\", \"row\": \"%s\", \"ctas_per_sm\": %d, \"smem\": %lld}",
                  i ? ", " : "", t.m, t.nt, t.min_blocks, passes.c_str(), cs[i].pf ? "true" : "false",
-                 cs[i].per_row ? "per_row" : "persistent", cs[i].per_sm, (long long)cs[i].smem);
+                 cs[i].per_row ? "per_row" : "persistent", cs[i].row_in_buffer ? "transform buffer" : "own buffer",
+                 cs[i].per_sm, (long long)cs[i].smem);
         j += tmp;
       }
       j += "]}";

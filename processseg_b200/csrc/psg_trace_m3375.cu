@@ -15,9 +15,14 @@ using A = tk::RPlan<3375, 256, 2, Grp<3, 3>, Grp<3, 5>, Grp<5, 5>>;
 // 3·3 | 3 | 5·5 | 5
 using B = tk::RPlan<3375, 256, 2, Grp<3, 3>, Grp<3>, Grp<5, 5>, Grp<5>>;
 
+// A with 85 registers: three CTAs per SM when the row shares the first
+// transform buffer (the launch shape that has no row buffer of its own)
+using C = tk::RPlan<3375, 256, 3, Grp<3, 3>, Grp<3, 5>, Grp<5, 5>>;
+
 const TracePlanInfo a = tk::info_served<A, 9>();
 const TracePlanInfo b = tk::info<B, 9>();
-const TracePlanInfo* const builds[] = {&a, &b, nullptr};
+const TracePlanInfo c = tk::info<C, 9>();
+const TracePlanInfo* const builds[] = {&a, &b, &c, nullptr};
 
 }  // namespace
 
