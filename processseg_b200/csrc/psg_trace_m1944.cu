@@ -24,12 +24,17 @@ using C = tk::RPlan<1944, 256, 3, Grp<4, 2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
 using D = tk::RPlan<1944, 512, 2, Grp<4>, Grp<2, 3>, Grp<3, 3>, Grp<3, 3>>;
 using F = tk::RPlan<1944, 512, 2, Grp<4>, Grp<2>, Grp<3, 3>, Grp<3, 3>, Grp<3>>;
 
+// A with 48 registers: five CTAs per SM when the row shares the first
+// transform buffer
+using G = tk::RPlan<1944, 256, 5, Grp<4>, Grp<2, 3>, Grp<3, 3>, Grp<3, 3>>;
+
 const TracePlanInfo a = tk::info_served<A, 5>();
 const TracePlanInfo b = tk::info<B, 5>();
 const TracePlanInfo c = tk::info<C, 5>();
 const TracePlanInfo d = tk::info<D, 5>();
 const TracePlanInfo f = tk::info<F, 5>();
-const TracePlanInfo* const builds[] = {&a, &b, &c, &d, &f, nullptr};
+const TracePlanInfo g = tk::info<G, 5>();
+const TracePlanInfo* const builds[] = {&a, &b, &c, &d, &f, &g, nullptr};
 
 }  // namespace
 
