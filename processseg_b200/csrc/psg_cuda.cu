@@ -3262,8 +3262,11 @@ void put_event(psg_server* S, cudaEvent_t e) {
 
 // Moves pending requests to staged: device requests at once; host requests
 // when their bytes fit the arena (first come, first served), starting their
-// copies in.
-void admit(psg_server* S) {
+// copies in. The copies are issued with the lock released (a copy from
+// pageable memory returns only when done), the requests in neither list
+// meanwhile (cancel then finds them started).
+void admit(psg_server* S, std::unique_lock<std::mutex>& lk) {
+  std::vector<Req*> take;
   while (!S->pending.empty()) {
     Req* r = S->pending.front();
     if (r->device) {
@@ -3288,20 +3291,37 @@ void admit(psg_server* S) {
     r->d_data = base;
     r->d_live = (const int*)(base + db);
     r->d_start = r->start ? (const double*)(base + db + lb) : nullptr;
-    CUDA_OK(cudaMemcpyAsync(base, r->src, (size_t)(r->rows * (int64_t)r->cols * r->esz), cudaMemcpyHostToDevice,
-                            S->s_in));
-    CUDA_OK(cudaMemcpyAsync(base + db, r->live, r->rows * 4, cudaMemcpyHostToDevice, S->s_in));
-    if (r->start) CUDA_OK(cudaMemcpyAsync(base + db + lb, r->start, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
     if (r->key_off) {
       r->d_off = (const double*)(base + db + lb + sb);
       r->d_t0 = (const double*)(base + db + lb + 2 * sb);
-      CUDA_OK(cudaMemcpyAsync(base + db + lb + sb, r->key_off, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
-      CUDA_OK(cudaMemcpyAsync(base + db + lb + 2 * sb, r->key_t0, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
     }
     r->in = get_event(S);
-    CUDA_OK(cudaEventRecord(r->in, S->s_in));
-    S->staged.push_back(r);
+    take.push_back(r);
   }
+  if (take.empty()) return;
+  lk.unlock();
+  try {
+    for (Req* r : take) {
+      char* base = r->d_data;
+      const int64_t db = align256(r->rows * (int64_t)r->cols * r->esz), lb = align256(r->rows * 4),
+                    sb = align256(r->rows * 8);
+      CUDA_OK(cudaMemcpyAsync(base, r->src, (size_t)(r->rows * (int64_t)r->cols * r->esz), cudaMemcpyHostToDevice,
+                              S->s_in));
+      CUDA_OK(cudaMemcpyAsync(base + db, r->live, r->rows * 4, cudaMemcpyHostToDevice, S->s_in));
+      if (r->start) CUDA_OK(cudaMemcpyAsync(base + db + lb, r->start, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+      if (r->key_off) {
+        CUDA_OK(cudaMemcpyAsync(base + db + lb + sb, r->key_off, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+        CUDA_OK(cudaMemcpyAsync(base + db + lb + 2 * sb, r->key_t0, r->rows * 8, cudaMemcpyHostToDevice, S->s_in));
+      }
+      CUDA_OK(cudaEventRecord(r->in, S->s_in));
+    }
+  } catch (...) {
+    lk.lock();
+    for (Req* r : take) S->staged.push_back(r);  // failed with the staged ones
+    throw;
+  }
+  lk.lock();
+  for (Req* r : take) S->staged.push_back(r);
 }
 
 // A staged request whose input is on the device.
@@ -3341,7 +3361,7 @@ void launch_batch_reqs(psg_server* S, Batch* b);
 // device (up to kMaxJobs, in arrival order). The generic rows go in one
 // launch, each trace build's rows in one launch, the requests run alone
 // after them part by part; then the host requests' copies out.
-void launch_batch(psg_server* S) {
+void launch_batch(psg_server* S, std::unique_lock<std::mutex>& lk) {
   int slot = -1;
   for (int i = 0; i < psg_server::kSlots; i++)
     if (!S->slot_busy[i]) {
@@ -3363,6 +3383,24 @@ void launch_batch(psg_server* S) {
   if (b->reqs.empty()) return;
   try {
     launch_batch_reqs(S, b.get());
+    // the copies out with the lock released (to pageable memory a copy
+    // returns only when done); the slot stays taken meanwhile
+    S->slot_busy[slot] = true;
+    b->done = get_event(S);
+    lk.unlock();
+    try {
+      cudaStream_t so = S->s_out[slot];
+      for (Req* r : b->reqs)
+        if (!r->device)
+          CUDA_OK(cudaMemcpyAsync(r->dst, r->d_data, (size_t)(r->rows * (int64_t)r->cols * r->esz),
+                                  cudaMemcpyDeviceToHost, so));
+      CUDA_OK(cudaEventRecord(b->done, so));
+    } catch (...) {
+      lk.lock();
+      S->slot_busy[slot] = false;
+      throw;
+    }
+    lk.lock();
   } catch (const std::exception& e) {
     // the batch's requests fail; what was queued for them finishes first,
     // so that their arena memory is free to reuse
@@ -3382,7 +3420,6 @@ void launch_batch(psg_server* S) {
     S->cv_done.notify_all();
     return;
   }
-  S->slot_busy[slot] = true;
   S->launches++;
   S->batched_reqs += (int64_t)b->reqs.size();
   S->inflight.push_back(b.release());
@@ -3515,12 +3552,6 @@ void launch_batch_reqs(psg_server* S, Batch* b) {
   b->kern = get_event(S);
   CUDA_OK(cudaEventRecord(b->kern, sc));
   CUDA_OK(cudaStreamWaitEvent(so, b->kern, 0));
-  for (Req* r : b->reqs)
-    if (!r->device)
-      CUDA_OK(cudaMemcpyAsync(r->dst, r->d_data, (size_t)(r->rows * (int64_t)r->cols * r->esz),
-                              cudaMemcpyDeviceToHost, so));
-  b->done = get_event(S);
-  CUDA_OK(cudaEventRecord(b->done, so));
 }
 
 // Retires finished batches: their requests are done and their memory free.
@@ -3566,7 +3597,7 @@ void sched_loop(psg_server* S) {
   while (true) {
     if (S->stop && S->pending.empty() && S->staged.empty() && S->inflight.empty()) break;
     try {
-      admit(S);
+      admit(S, lk);
       int running = 0;
       for (Batch* b : S->inflight) {
         if (!b->kern_done) b->kern_done = cudaEventQuery(b->kern) == cudaSuccess;
@@ -3577,7 +3608,7 @@ void sched_loop(psg_server* S) {
         if (ready(S, r)) ready_rows += std::max<int64_t>(r->rows, 1);
       if (ready_rows > 0 && (running == 0 || ready_rows >= fill_rows)) {
         if (running > 0) S->overlapped++;
-        launch_batch(S);
+        launch_batch(S, lk);
       }
       if (retire(S)) S->cv_done.notify_all();
     } catch (const std::exception& e) {
@@ -3589,13 +3620,15 @@ void sched_loop(psg_server* S) {
       S->staged.clear();
       S->cv_done.notify_all();
     }
-    // idle: sleep until a submit; otherwise poll again at once (yielding the
-    // core), so a finished batch is seen within microseconds
+    // idle: sleep until a submit; otherwise poll again within a few
+    // microseconds (a finished batch is seen at once), spinning with the lock
+    // released so that submitting and waiting threads get it meanwhile
     if (S->inflight.empty() && S->pending.empty() && S->staged.empty())
       S->cv.wait_for(lk, std::chrono::milliseconds(5));
     else {
       lk.unlock();
-      std::this_thread::yield();
+      const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(4);
+      while (std::chrono::steady_clock::now() < until) std::this_thread::yield();
       lk.lock();
     }
   }
