@@ -681,6 +681,11 @@ int psg_submit_device(psg_server* server, const psg_plan* plan, const void* src,
  * has one waiter: a second thread that waits on it while the first does
  * gets PSG_EINVAL. */
 int psg_wait(psg_server* server, uint64_t ticket, double timeout_ms);
+/* psg_wait that also gives the time the request finished (the loop saw its
+ * copies out done), in seconds of the host's monotonic clock
+ * (CLOCK_MONOTONIC: Python's time.perf_counter), so that a caller can
+ * measure latency from when the request was due. */
+int psg_wait_done(psg_server* server, uint64_t ticket, double timeout_ms, double* done_s);
 /* *done = 1 when the request has finished (or was cancelled), without
  * waiting or releasing its ticket. */
 int psg_poll(psg_server* server, uint64_t ticket, int32_t* done);

@@ -226,6 +226,7 @@ def _declare(lib):
         "psg_submit": (C.c_int, [P, P, P, P, I64, I32, P, P, DBL, C.POINTER(C.c_uint64)]),
         "psg_server_counters": (C.c_int, [P, P]),
         "psg_server_load": (C.c_int, [P, P]),
+        "psg_wait_done": (C.c_int, [P, C.c_uint64, DBL, C.POINTER(DBL)]),
         "psg_submit_keyed": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, C.POINTER(C.c_uint64)]),
         "psg_submit_device": (C.c_int, [P, P, P, P, I64, I32, P, P, C.POINTER(KeysC), DBL, P, C.POINTER(C.c_uint64)]),
         "psg_wait": (C.c_int, [P, C.c_uint64, DBL]),

@@ -3789,7 +3789,9 @@ int psg_submit_device(psg_server* S, const psg_plan* plan, const void* src, void
 // timeout the claim is dropped and the ticket can be waited on again). A
 // timeout that is not finite, or longer than about 30 years, waits until the
 // request finishes; a negative one polls once.
-int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
+int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) { return psg_wait_done(S, ticket, timeout_ms, nullptr); }
+
+int psg_wait_done(psg_server* S, uint64_t ticket, double timeout_ms, double* done_s) {
   if (!S) {
     t_err = "null argument";
     return PSG_EINVAL;
@@ -3819,6 +3821,7 @@ int psg_wait(psg_server* S, uint64_t ticket, double timeout_ms) {
     }
   }
   int st = r->status;
+  if (done_s) *done_s = r->t_done;
   S->by_ticket.erase(ticket);
   delete r;
   if (st == PSG_ECANCELED) t_err = "the request was cancelled";

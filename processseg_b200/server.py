@@ -88,15 +88,18 @@ class Server:
         self._keep[t.value] = (plan, src, dst, live, start, keys, meta)
         return t.value
 
-    def wait(self, ticket: int, timeout_ms: float = 10000.0):
+    def wait(self, ticket: int, timeout_ms: float = 10000.0) -> float:
         """Waits for a request; ``TimeoutError`` after ``timeout_ms``,
-        ``CancelledError`` for a request cancelled before it started."""
-        st = A.lib().psg_wait(self.h, ticket, timeout_ms)
+        ``CancelledError`` for a request cancelled before it started.
+        Returns when it finished, on ``time.perf_counter``'s clock."""
+        done = C.c_double(0.0)
+        st = A.lib().psg_wait_done(self.h, ticket, timeout_ms, C.byref(done))
         if st != A.ETIMEOUT:
             self._keep.pop(ticket, None)
         if st == A.ECANCELED:
             raise CancelledError(A.lib().psg_last_error().decode("utf-8", "replace"))
         A.check(st)
+        return done.value
 
     def poll(self, ticket: int) -> bool:
         """True when the request has finished (or was cancelled)."""
@@ -194,9 +197,9 @@ class ServerPool:
         s = self.loops[i]
         return i, s.submit(plan.forDevice(s.device), src, dst, meta)
 
-    def wait(self, ticket, timeout_ms: float = 10000.0):
+    def wait(self, ticket, timeout_ms: float = 10000.0) -> float:
         i, t = ticket
-        self.loops[i].wait(t, timeout_ms)
+        return self.loops[i].wait(t, timeout_ms)
 
     def poll(self, ticket) -> bool:
         i, t = ticket
