@@ -426,8 +426,9 @@ def launch_of(plan, rows):
         return None
     part = tun["parts"][0]
     rec = next((t for t in tun["tuned"] if t["part"] == part["part"] and t["class"] == int(rows).bit_length()), None)
-    return {"chosen": part["shapes"][rec["choice"] if rec else 0], "tuner_us_per_shape": rec["us"] if rec else None,
-            "shapes": part["shapes"]}
+    pick = part["pinned"] if part["pinned"] >= 0 else (rec["choice"] if rec else 0)
+    return {"chosen": part["shapes"][pick], "pinned": part["pinned"] >= 0,
+            "tuner_us_per_shape": rec["us"] if rec else None, "shapes": part["shapes"]}
 
 
 def workloads_leg(peak):
