@@ -1,26 +1,31 @@
 // psg_trace.cuh — the float32 trace kernel of libpsgcuda.so: the plan parts
 // demean → zero-phase FFT filter → AGC (→ per-trace normalization) with zero
-// pads, the chains of the benchmarked panels, with the transform's length
-// known at compile time.
+// pads, with the transform's length known at compile time, and the float32
+// correlation kernel of the same make.
 //
-// What differs from pipeline_kernel's recipe path (same inputs, same
-// outputs within the float32 rounding of a different summation order):
-//  * The FFT (FPlan): radices, strides and butterfly counts are constants, so
-//    a pass's loads and stores use immediate offsets, its butterfly index
-//    splits with a constant division, and its twiddles come from a per-pass
-//    table laid out butterfly by butterfly (two per 16-byte load).
-//  * The trace statistics fold over the CTA once, and one warp computes the
-//    scalars every step needs (the mean, the trend, the AGC's level) and
-//    hands them to the others through shared memory, instead of every warp
-//    evaluating the same float64 divisions and square roots.
-//  * The inverse transform's last pass writes the unpacked samples (and
-//    their Σx² for the AGC) straight into the row: no pass of its own.
+// What differs from pipeline_kernel's recipe path (same inputs; outputs
+// within the parity bar of both, closer to the reference's float32 bits):
+//  * The filter's transforms (RPlan) run the reference's own stages (4s, a 2,
+//    3s, 5s) with its butterflies, twiddles and roundings (no fused
+//    multiply-add), two consecutive stages fused per shared-memory pass; the
+//    split · gain · unsplit between the transforms runs once per bin pair in
+//    the reference's order. Radices, strides and butterfly counts are
+//    constants; each build groups the stages its own way (the host's tuner
+//    picks among builds and launch shapes, which give the same bits).
+//  * The demean, trend and AGC-level sums are float64, in an order that does
+//    not depend on the build (kNT lanes, then the warps in order).
+//  * One row buffer: the row is read only by the forward transform's first
+//    pass, so the next row's bulk copy goes in right after the forward
+//    transform (or the row shares the first transform buffer); the inverse
+//    transform's last pass unpacks the filtered row into the buffer it does
+//    not read, and the AGC writes its output into the other one.
 //  * The AGC's window sums come from registers: a warp takes consecutive
 //    window groups, each group's outputs needing the suffix sums of one
 //    block and the prefix sums of the next (w = 2h + 1 = the block length,
 //    so the window [i − h, i + h] spans exactly those two), scanned in
 //    registers as pipeline_kernel scans them into shared memory, with the
 //    same sums, divisors and gain arithmetic (gain/gain.nim:351-461).
+//  * BATCH: the rows of many served requests' jobs in one launch.
 #pragma once
 
 #include "psg_kernel.cuh"
