@@ -540,10 +540,12 @@ __device__ __forceinline__ void agc_block_sums(const T* X, int n, int w, bool rm
 // or the mean (mean-abs) (gain/gain.nim:392-402, :429-431). float32 uses the
 // hardware's approximate square root and division (within 2 ulp of the
 // correctly rounded ones); float64 keeps both correctly rounded.
+// The AGC's gain k / (sqrt(mean) + ε) (rms mode; mean itself otherwise) with
+// every operation correctly rounded, as the reference forms it in T
+// (gain/gain.nim:399-401).
 __device__ __forceinline__ float agc_gain(float mean, float k, float eps, bool rms_mode) {
-  float lv = mean;
-  if (rms_mode) asm("sqrt.approx.f32 %0, %1;" : "=f"(lv) : "f"(mean));
-  return __fdividef(k, lv + eps);
+  const float lv = rms_mode ? __fsqrt_rn(mean) : mean;
+  return __fdiv_rn(k, __fadd_rn(lv, eps));
 }
 __device__ __forceinline__ double agc_gain(double mean, double k, double eps, bool rms_mode) {
   const double lv = rms_mode ? sqrt(mean) : mean;
