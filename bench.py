@@ -431,7 +431,7 @@ def launch_of(plan, rows):
             "tuner_us_per_shape": rec["us"] if rec else None, "shapes": part["shapes"]}
 
 
-def workloads_leg(peak):
+def workloads_leg(peak, which=("c1", "c3", "c5", "segy", "spectrum")):
     """The other configurations, device-resident, each timed with CUDA events
     after a warm-up: C1 (48×2001, demean → band-pass 4-8-60-80 → AGC 500 ms),
     C3 (4 sweeps × 240 channels × 10001 samples correlated with a 12 s
@@ -456,92 +456,99 @@ def workloads_leg(peak):
         return e0.elapsed_time(e1) / steps * 1e-3
 
     out = {}
-    g = synth.c1()
-    meta = g.meta()
-    plan = P.initPipeline([P.demeanOp(), P.bandPassOp(P.Corners(4, 8, 60, 80)), P.agcOp(500)]).compile(P.float32, 2.0, 2001)
-    ws = P.initWorkspace()
-    ws.reserve(plan, rows=48, cols=2001)
-    src = torch.from_numpy(g.data).cuda()
-    dst = torch.empty_like(src)
-    t = timed(lambda: plan.apply(src, dst, meta, ws), 200)
-    # the same apply captured once and replayed: one host call per panel
-    gr = plan.capture(src, dst, meta, ws)
-    tg = timed(gr.replay, 200)
-    del gr
-    out["c1"] = {"workload": "48x2001 f32 @2ms: demean -> bandpass 4-8-60-80 -> AGC 500 ms", "us_per_panel": t * 1e6,
-                 "msamples_per_s": 48 * 2001 / t / 1e6, "hbm_frac": 2 * 48 * 2001 * 4 / t / 1e9 / peak,
-                 "us_per_panel_graph_replay": tg * 1e6, "launch": launch_of(plan, 48)}
+    if "c1" in which:
+        g = synth.c1()
+        meta = g.meta()
+        plan = P.initPipeline([P.demeanOp(), P.bandPassOp(P.Corners(4, 8, 60, 80)), P.agcOp(500)]).compile(P.float32, 2.0, 2001)
+        ws = P.initWorkspace()
+        ws.reserve(plan, rows=48, cols=2001)
+        src = torch.from_numpy(g.data).cuda()
+        dst = torch.empty_like(src)
+        t = timed(lambda: plan.apply(src, dst, meta, ws), 200)
+        # the same apply captured once and replayed: one host call per panel
+        gr = plan.capture(src, dst, meta, ws)
+        tg = timed(gr.replay, 200)
+        del gr
+        out["c1"] = {"workload": "48x2001 f32 @2ms: demean -> bandpass 4-8-60-80 -> AGC 500 ms", "us_per_panel": t * 1e6,
+                     "msamples_per_s": 48 * 2001 / t / 1e6, "hbm_frac": 2 * 48 * 2001 * 4 / t / 1e9 / peak,
+                     "us_per_panel_graph_replay": tg * 1e6, "launch": launch_of(plan, 48)}
 
-    spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
-    pilot = P.generatePilot(spec, np.float64)
-    recs = synth.vibroseis_records(pilot.samples, channels=240, sweeps=4)
-    sweeps, ch, ns = recs.shape
-    cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=3000)
-    stack = P.initRecordStack(ch, 3000, 2.0)
-    # the gather's sweeps as one block of records, each stacked on its channel
-    x = torch.from_numpy(recs.reshape(sweeps * ch, ns)).cuda()
-    rmap = (torch.arange(sweeps * ch, dtype=torch.int32, device="cuda") % ch).contiguous()
-    cmeta = P.initChunkMeta(np.full(sweeps * ch, P.tsLive, np.int32), np.full(sweeps * ch, ns, np.int32), 2.0)
-    d = torch.empty(sweeps * ch, 3000, device="cuda")
-    so = torch.empty(ch, 3000, device="cuda")
+    if "c3" in which:
+        spec = P.linearSweep(8, 80, 12000, 2, P.initSweepTaper(300, 300, P.tpCos2))
+        pilot = P.generatePilot(spec, np.float64)
+        recs = synth.vibroseis_records(pilot.samples, channels=240, sweeps=4)
+        sweeps, ch, ns = recs.shape
+        cplan = P.initCorrelationPlan(P.float32, pilot, 2.0, ns, outSamples=3000)
+        stack = P.initRecordStack(ch, 3000, 2.0)
+        # the gather's sweeps as one block of records, each stacked on its channel
+        x = torch.from_numpy(recs.reshape(sweeps * ch, ns)).cuda()
+        rmap = (torch.arange(sweeps * ch, dtype=torch.int32, device="cuda") % ch).contiguous()
+        cmeta = P.initChunkMeta(np.full(sweeps * ch, P.tsLive, np.int32), np.full(sweeps * ch, ns, np.int32), 2.0)
+        d = torch.empty(sweeps * ch, 3000, device="cuda")
+        so = torch.empty(ch, 3000, device="cuda")
 
-    def c3():
-        stack.clear()
-        cplan.correlateInto(x, d, cmeta, stack=stack, rowMap=rmap)
-        stack.stackInto(so)
-    t = timed(c3, 20)
-    inb = sweeps * ch * ns * 4
-    outb = sweeps * ch * 3000 * 4 + ch * 3000 * 4
-    out["c3"] = {"workload": "4 sweeps x 240 channels x 10001 f32 @2ms, 12 s 8-80 Hz pilot, nfft 16200, 6 s out, vertical stack (one call of 960 records, rowMap to the channels)",
-                 "ms_per_gather": t * 1e3, "msamples_per_s": sweeps * ch * ns / t / 1e6,
-                 "hbm_frac": (inb + outb) / t / 1e9 / peak}
+        def c3():
+            stack.clear()
+            cplan.correlateInto(x, d, cmeta, stack=stack, rowMap=rmap)
+            stack.stackInto(so)
+        t = timed(c3, 20)
+        inb = sweeps * ch * ns * 4
+        outb = sweeps * ch * 3000 * 4 + ch * 3000 * 4
+        out["c3"] = {"workload": "4 sweeps x 240 channels x 10001 f32 @2ms, 12 s 8-80 Hz pilot, nfft 16200, 6 s out, vertical stack (one call of 960 records, rowMap to the channels)",
+                     "ms_per_gather": t * 1e3, "msamples_per_s": sweeps * ch * ns / t / 1e6,
+                     "hbm_frac": (inb + outb) / t / 1e9 / peak}
 
-    g = synth.c5()
-    meta = g.meta()
-    flow = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(2, 5, 120, 150))), P.agcOp(250),
-            P.normalizeOp(P.normPercentile, P.perTrace, percentile=99.0)]
-    plan = P.initPipeline(flow).compile(P.float32, 1.0, 6001)
-    ws = P.initWorkspace()
-    ws.reserve(plan, rows=50000, cols=6001)
-    src = torch.from_numpy(g.data).cuda()
-    dst = torch.empty_like(src)
-    t = timed(lambda: plan.apply(src, dst, meta, ws), 3)
-    out["c5"] = {"workload": "50000x6001 f32 @1ms (1.2 GB), live U{4000..6001}: demean -> bandpass 2/5/120/150 -> AGC 250 ms -> per-trace p99",
-                 "ms_per_panel": t * 1e3, "msamples_per_s": 50000 * 6001 / t / 1e6,
-                 "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak, "launch": launch_of(plan, 50000)}
-    del src, dst
-    torch.cuda.empty_cache()
+    if "c5" in which:
+        g = synth.c5()
+        meta = g.meta()
+        flow = [P.demeanOp(), P.filterOp(P.bandPass(P.Corners(2, 5, 120, 150))), P.agcOp(250),
+                P.normalizeOp(P.normPercentile, P.perTrace, percentile=99.0)]
+        plan = P.initPipeline(flow).compile(P.float32, 1.0, 6001)
+        ws = P.initWorkspace()
+        ws.reserve(plan, rows=50000, cols=6001)
+        src = torch.from_numpy(g.data).cuda()
+        dst = torch.empty_like(src)
+        t = timed(lambda: plan.apply(src, dst, meta, ws), 3)
+        out["c5"] = {"workload": "50000x6001 f32 @1ms (1.2 GB), live U{4000..6001}: demean -> bandpass 2/5/120/150 -> AGC 250 ms -> per-trace p99",
+                     "ms_per_panel": t * 1e3, "msamples_per_s": 50000 * 6001 / t / 1e6,
+                     "hbm_frac": 2 * 50000 * 6001 * 4 / t / 1e9 / peak, "launch": launch_of(plan, 50000)}
+        del src, dst
+        torch.cuda.empty_cache()
 
-    # SEG-Y decode: 20000 records of 3001 IBM-float samples (random words)
-    # to a float32 block, and a viewer's spectrum panel (501-sample windows
-    # of the C2 panel, power-averaged)
-    from processseg_b200 import _abi as A
-    rows, n = 20000, 3001
-    st = torch.cuda.current_stream().cuda_stream
-    blk = torch.empty(rows, n, dtype=torch.float32, device="cuda")
-    out["segy"] = {"workload": "20000 SEG-Y records x 3001 samples (random words) -> f32 block"}
-    for fmt, name, sz in ((1, "ibm", 4), (3, "int16", 2), (5, "ieee32", 4)):
-        rec = torch.randint(0, 256, (rows, 240 + sz * n), dtype=torch.uint8, device="cuda")
-        t = timed(lambda: A.check(A.lib().psg_segy_decode(rec.data_ptr(), rows, 240 + sz * n, 240, n, fmt, 0, A.F32,
-                                                          blk.data_ptr(), n, st)), 10)
-        nbytes = rec.numel() + blk.numel() * 4
-        out["segy"][name] = {"us_per_block": t * 1e6, "gb_per_s": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / peak}
-        del rec
-    del blk
-    g = synth.c2()
-    meta = g.meta()
-    sp = P.initSpectrumPlan(P.float32, 2.0, 501)
-    ws = P.initWorkspace()
-    src = torch.from_numpy(g.data).cuda()
-    amp = [0.0] * sp.bins
-    live, _ = meta.device(3001)
-    avg = torch.empty(sp.bins, dtype=torch.float64, device="cuda")
-    t = timed(lambda: A.check(A.lib().psg_spectrum_average(sp.h, ws.h, src.data_ptr(), 2000, 3001, live.data_ptr(), 2.0,
-                                                           500, 0, 1999, avg.data_ptr(), None, st)), 20)
-    out["spectrum"] = {"workload": "spectrum panel: 2000 traces x 501-sample windows from sample 500, nfft 512",
-                       "us_per_panel": t * 1e6, "msamples_per_s": 2000 * 501 / t / 1e6}
-    del src
-    torch.cuda.empty_cache()
+    if "segy" in which:
+        # SEG-Y decode: 20000 records of 3001 IBM-float samples (random words)
+        # to a float32 block, and a viewer's spectrum panel (501-sample windows
+        # of the C2 panel, power-averaged)
+        from processseg_b200 import _abi as A
+        rows, n = 20000, 3001
+        st = torch.cuda.current_stream().cuda_stream
+        blk = torch.empty(rows, n, dtype=torch.float32, device="cuda")
+        out["segy"] = {"workload": "20000 SEG-Y records x 3001 samples (random words) -> f32 block"}
+        for fmt, name, sz in ((1, "ibm", 4), (3, "int16", 2), (5, "ieee32", 4)):
+            rec = torch.randint(0, 256, (rows, 240 + sz * n), dtype=torch.uint8, device="cuda")
+            t = timed(lambda: A.check(A.lib().psg_segy_decode(rec.data_ptr(), rows, 240 + sz * n, 240, n, fmt, 0, A.F32,
+                                                              blk.data_ptr(), n, st)), 10)
+            nbytes = rec.numel() + blk.numel() * 4
+            out["segy"][name] = {"us_per_block": t * 1e6, "gb_per_s": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / peak}
+            del rec
+        del blk
+    if "spectrum" in which:
+        from processseg_b200 import _abi as A
+        st = torch.cuda.current_stream().cuda_stream
+        g = synth.c2()
+        meta = g.meta()
+        sp = P.initSpectrumPlan(P.float32, 2.0, 501)
+        ws = P.initWorkspace()
+        src = torch.from_numpy(g.data).cuda()
+        amp = [0.0] * sp.bins
+        live, _ = meta.device(3001)
+        avg = torch.empty(sp.bins, dtype=torch.float64, device="cuda")
+        t = timed(lambda: A.check(A.lib().psg_spectrum_average(sp.h, ws.h, src.data_ptr(), 2000, 3001, live.data_ptr(), 2.0,
+                                                               500, 0, 1999, avg.data_ptr(), None, st)), 20)
+        out["spectrum"] = {"workload": "spectrum panel: 2000 traces x 501-sample windows from sample 500, nfft 512",
+                           "us_per_panel": t * 1e6, "msamples_per_s": 2000 * 501 / t / 1e6}
+        del src
+        torch.cuda.empty_cache()
     return out
 
 
@@ -711,7 +718,7 @@ def run_ours(args):
         if world == 1 and not args.no_serving:
             line["serving"] = serving_leg()
         if world == 1 and not args.no_workloads:
-            line["workloads"] = workloads_leg(peak)
+            line["workloads"] = workloads_leg(peak, args.workloads.split(","))
         if world == 1 and not args.no_errors:
             line["error_vs_fp64"] = error_report(dsts[0])
         if world == 1 and not args.no_cpu:
@@ -731,6 +738,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-load leg")
     ap.add_argument("--no-multi", action="store_true", help="skip the split-panel and by-channel legs")
+    ap.add_argument("--workloads", default="c1,c3,c5,segy,spectrum",
+                    help="the other configurations to time (comma-separated: c1, c3, c5, segy, spectrum)")
     ap.add_argument("--trace-shape", type=int, default=None,
                     help="run the headline panel with this trace-kernel launch shape (PipelinePlan.tuning lists them)")
     ap.add_argument("--no-workloads", action="store_true", help="skip the C1/C3/C5 legs")
