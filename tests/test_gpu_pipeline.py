@@ -1,5 +1,5 @@
 """Parity of the device pipeline (libpsgcuda.so through its C ABI) with the
-CPU oracle, on seeded synthetic panels. The bar: each
+CPU oracle, on seeded synthetic panels. The bar (the parity tolerance): each
 output trace within 1e-5 of its RMS of the oracle's float32 apply, and
 within 1e-12 of its RMS for float64 plans. Non-live rows and samples past a
 row's live length are copied bit for bit."""
