@@ -940,8 +940,10 @@ __global__ void __launch_bounds__(P::NT, P::MINB) trace_kernel(PipeArgs a) {
 struct RecLd {
   const float* __restrict__ x;
   int n;
+  bool al8;  // x is 8-byte aligned: a pair of samples in one load
   __device__ __forceinline__ float2 operator()(int c, int) const {
     const int k = 2 * c;
+    if (al8 && k + 1 < n) return __ldg(reinterpret_cast<const float2*>(x) + c);
     return make_float2(k < n ? __ldg(x + k) : 0.f, k + 1 < n ? __ldg(x + k + 1) : 0.f);
   }
 };
@@ -971,7 +973,8 @@ __global__ void __launch_bounds__(P::NT, P::MINB) corr_trace_kernel(CorrArgs a) 
     const int n = min(max(a.live[r], 0), a.cols);
     const float2* y = nullptr;
     if (n > 0) {
-      fft<P>(0, M, tw, RecLd{src + r * (long long)a.cols, n}, BufSt{zo});
+      const float* rx = src + r * (long long)a.cols;
+      fft<P>(0, M, tw, RecLd{rx, n, ((uintptr_t)rx & 7) == 0}, BufSt{zo});
       __syncthreads();
       fft<P>(zo, za, tw, BridgeLd{zo, M, ab}, BufSt{yo});
       __syncthreads();
