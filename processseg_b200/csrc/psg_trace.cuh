@@ -986,14 +986,49 @@ __global__ void __launch_bounds__(P::NT, P::MINB) corr_trace_kernel(CorrArgs a) 
       const float2 v = y[idx >> 1];
       return (idx & 1) ? v.x : v.y;
     };
+    const int o = a.stack_on ? (a.row_map ? a.row_map[r] : (int)r) : -1;
+    const int sn = !a.stack_on ? 0
+                   : a.stack_live ? min(max(a.stack_live[r], 0), a.stack_samples) : min(a.out, a.stack_samples);
+    const bool take = a.stack_on && o >= 0 && o < a.stack_rows && sn > 0;
+    constexpr int KV = 8;  // output samples a thread keeps in registers
+    if (max(a.out, sn) <= KV * NT) {
+      // one pass over the lags: the output row, the finite check and the
+      // values the stack adds, kept in registers
+      float vals[KV];
+      double bad = 0;
+      float* d = dst ? dst + r * (long long)a.out : nullptr;
+#pragma unroll
+      for (int k = 0; k < KV; k++) {
+        const int c = threadIdx.x + k * NT;
+        const float v = value(c);
+        vals[k] = v;
+        if (d && c < a.out) d[c] = v;
+        if (take && c < sn) bad += (double)v - (double)v;  // allFinite: x − x is 0 for finite x
+      }
+      if (take) {
+        bad = block_sum(bad, S.red[0][0]);
+        if (bad == 0) {
+          double* nm = a.num + (long long)o * a.stack_samples;
+          int* ct = a.cnt + (long long)o * a.stack_samples;
+#pragma unroll
+          for (int k = 0; k < KV; k++) {
+            const int c = threadIdx.x + k * NT;
+            if (c < sn) {
+              atomicAdd(nm + c, (double)vals[k]);
+              atomicAdd(ct + c, 1);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     if (dst) {
       float* d = dst + r * (long long)a.out;
       for (int c = threadIdx.x; c < a.out; c += NT) d[c] = value(c);
     }
     if (a.stack_on) {
-      const int o = a.row_map ? a.row_map[r] : (int)r;
-      const int sn = a.stack_live ? min(max(a.stack_live[r], 0), a.stack_samples) : min(a.out, a.stack_samples);
-      if (o >= 0 && o < a.stack_rows && sn > 0) {
+      if (take) {
         double bad = 0;
         for (int c = threadIdx.x; c < sn; c += NT) {
           const double v = (double)value(c);
