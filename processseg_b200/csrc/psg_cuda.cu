@@ -1502,8 +1502,8 @@ static void launch_trace(const psg_plan* p, int part, const TraceCand& c, PipeAr
 // a scratch block on `stream`, each timed launch with events after a write
 // of twice the L2's size has flushed the input from it (the panel comes
 // from HBM, as a fresh one does); one warm-up launch per shape, then the
-// least time of four launches (two rounds over the shapes) wins, and the
-// choice is kept for the class. The shapes give the same bits, so the choice
+// least mean time of six launches (three rounds over the shapes) wins, and
+// the choice is kept for the class. The shapes give the same bits, so the choice
 // never changes a result. No tuning under stream capture, with tuning off
 // (PSG_TUNE=0), or when the scratch block cannot be had: the first shape.
 static int trace_choice(const psg_plan* p, int part, const PipeArgs& a, int64_t rows, int32_t cols, size_t esz,
@@ -1553,20 +1553,25 @@ static int trace_choice(const psg_plan* p, int part, const PipeArgs& a, int64_t 
   try {
     CUDA_OK(cudaEventCreate(&e0));
     CUDA_OK(cudaEventCreate(&e1));
-    for (int round = 0; round < 2; round++)
+    std::vector<float> sum(cs.size(), 0.f);
+    constexpr int kRounds = 3, kPer = 2;
+    for (int round = 0; round < kRounds; round++)
       for (size_t i = 0; i < cs.size(); i++) {
         if (round == 0) launch_trace(p, part, cs[i], t, trows, stream);
-        for (int k = 0; k < 2; k++) {
-          if (flush) CUDA_OK(cudaMemsetAsync(flush, 2 * round + k, flush_bytes, stream));
+        for (int k = 0; k < kPer; k++) {
+          if (flush) CUDA_OK(cudaMemsetAsync(flush, kPer * round + k, flush_bytes, stream));
           CUDA_OK(cudaEventRecord(e0, stream));
           launch_trace(p, part, cs[i], t, trows, stream);
           CUDA_OK(cudaEventRecord(e1, stream));
           CUDA_OK(cudaEventSynchronize(e1));
           float ms = 0;
           CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
-          res.us[i] = std::min(res.us[i], ms * 1000.f);
+          sum[i] += ms * 1000.f;
         }
       }
+    // the mean of the samples: the event clock ticks in steps of a few
+    // microseconds at these durations, which a minimum would keep
+    for (size_t i = 0; i < cs.size(); i++) res.us[i] = sum[i] / (kRounds * kPer);
   } catch (...) {
     done();
     throw;
