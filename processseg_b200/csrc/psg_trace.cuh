@@ -166,6 +166,42 @@ template <class P> __device__ __forceinline__ int last_out(int a, int b) { retur
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+// Sums and differences on a complex value's two parts at once (sm_100's
+// paired float32 instructions, written in PTX with the rounding stated), each
+// part rounded as the scalar form is. ppm gives (a.x + b.x, a.y − b.y) and pmp
+// (a.x − b.x, a.y + b.y) as fma.rn.f32x2(b, (±1, ∓1), a), whose products are
+// exact, so the one rounding is the sum's or difference's, zero signs
+// included. Products stay scalar (pm): a paired multiply feeding a paired add
+// came out fused into one rounding on sm_100a even with .rn stated (a third
+// of radix-5 butterflies differed), scalar products into paired sums do not.
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 pa(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 ps(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 pm(float c, float2 b) { return make_float2(fm(c, b.x), fm(c, b.y)); }
+template <int SX> __device__ __forceinline__ float2 pmix(float2 a, float2 b) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pk2(b)), "l"(pk2(make_float2((float)SX, (float)-SX))), "l"(pk2(a)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 ppm(float2 a, float2 b) { return pmix<1>(a, b); }
+__device__ __forceinline__ float2 pmp(float2 a, float2 b) { return pmix<-1>(a, b); }
 
 // MULTW (fft/plan.nim:203-206): re = yr·wr − yi·wi, im = yr·wi + yi·wr.
 __device__ __forceinline__ float2 mul_tw(float2 y, float2 w) {
@@ -173,39 +209,37 @@ __device__ __forceinline__ float2 mul_tw(float2 y, float2 w) {
 }
 
 // The reference's butterfly of radix R on v[0 .. R) (outputs in place, k-th
-// output at v[k], before its twiddle).
+// output at v[k], before its twiddle); every operation the reference applies
+// to both parts alike runs on the pair.
 template <int R> struct RefDft;
 template <> struct RefDft<2> {
   static __device__ __forceinline__ void run(float2* v) {
     const float2 u = v[0], w = v[1];
-    v[0] = make_float2(fa(u.x, w.x), fa(u.y, w.y));
-    v[1] = make_float2(fs(u.x, w.x), fs(u.y, w.y));
+    v[0] = pa(u, w);
+    v[1] = ps(u, w);
   }
 };
 template <> struct RefDft<3> {
   static __device__ __forceinline__ void run(float2* v) {
     const float c = -0.5f, s = (float)0.8660254037844386467637231707529362;
     const float2 a = v[0];
-    const float t1r = fa(v[1].x, v[2].x), t1i = fa(v[1].y, v[2].y);
-    const float t2r = fs(v[1].x, v[2].x), t2i = fs(v[1].y, v[2].y);
-    const float m1r = fa(a.x, fm(c, t1r)), m1i = fa(a.y, fm(c, t1i));
-    const float m2r = fm(s, t2i), m2i = fm(-s, t2r);
-    v[0] = make_float2(fa(a.x, t1r), fa(a.y, t1i));
-    v[1] = make_float2(fa(m1r, m2r), fa(m1i, m2i));
-    v[2] = make_float2(fs(m1r, m2r), fs(m1i, m2i));
+    const float2 t1 = pa(v[1], v[2]), t2 = ps(v[1], v[2]);
+    const float2 m1 = pa(a, pm(c, t1));
+    const float2 m2 = make_float2(fm(s, t2.y), fm(-s, t2.x));
+    v[0] = pa(a, t1);
+    v[1] = pa(m1, m2);
+    v[2] = ps(m1, m2);
   }
 };
 template <> struct RefDft<4> {
   static __device__ __forceinline__ void run(float2* v) {
     const float2 x0 = v[0], x1 = v[1], x2 = v[2], x3 = v[3];
-    const float t0r = fa(x0.x, x2.x), t0i = fa(x0.y, x2.y);
-    const float t1r = fs(x0.x, x2.x), t1i = fs(x0.y, x2.y);
-    const float t2r = fa(x1.x, x3.x), t2i = fa(x1.y, x3.y);
-    const float t3r = fs(x1.y, x3.y), t3i = fs(x3.x, x1.x);
-    v[0] = make_float2(fa(t0r, t2r), fa(t0i, t2i));
-    v[1] = make_float2(fa(t1r, t3r), fa(t1i, t3i));
-    v[2] = make_float2(fs(t0r, t2r), fs(t0i, t2i));
-    v[3] = make_float2(fs(t1r, t3r), fs(t1i, t3i));
+    const float2 t0 = pa(x0, x2), t1 = ps(x0, x2), t2 = pa(x1, x3);
+    const float2 t3 = make_float2(fs(x1.y, x3.y), fs(x3.x, x1.x));
+    v[0] = pa(t0, t2);
+    v[1] = pa(t1, t3);
+    v[2] = ps(t0, t2);
+    v[3] = ps(t1, t3);
   }
 };
 template <> struct RefDft<5> {
@@ -213,19 +247,19 @@ template <> struct RefDft<5> {
     const float c1 = (float)0.3090169943749474241022934171828191, c2 = (float)-0.8090169943749474241022934171828191;
     const float s1 = (float)0.9510565162951535721164393333793821, s2 = (float)0.5877852522924731291687059546390728;
     const float2 a = v[0];
-    const float t1r = fa(v[1].x, v[4].x), t1i = fa(v[1].y, v[4].y);
-    const float t2r = fa(v[2].x, v[3].x), t2i = fa(v[2].y, v[3].y);
-    const float t3r = fs(v[1].x, v[4].x), t3i = fs(v[1].y, v[4].y);
-    const float t4r = fs(v[2].x, v[3].x), t4i = fs(v[2].y, v[3].y);
-    const float b1r = fa(fa(a.x, fm(c1, t1r)), fm(c2, t2r)), b1i = fa(fa(a.y, fm(c1, t1i)), fm(c2, t2i));
-    const float b2r = fa(fa(a.x, fm(c2, t1r)), fm(c1, t2r)), b2i = fa(fa(a.y, fm(c2, t1i)), fm(c1, t2i));
-    const float d1r = fa(fm(s1, t3r), fm(s2, t4r)), d1i = fa(fm(s1, t3i), fm(s2, t4i));
-    const float d2r = fs(fm(s2, t3r), fm(s1, t4r)), d2i = fs(fm(s2, t3i), fm(s1, t4i));
-    v[0] = make_float2(fa(fa(a.x, t1r), t2r), fa(fa(a.y, t1i), t2i));
-    v[1] = make_float2(fa(b1r, d1i), fs(b1i, d1r));
-    v[4] = make_float2(fs(b1r, d1i), fa(b1i, d1r));
-    v[2] = make_float2(fa(b2r, d2i), fs(b2i, d2r));
-    v[3] = make_float2(fs(b2r, d2i), fa(b2i, d2r));
+    const float2 t1 = pa(v[1], v[4]), t2 = pa(v[2], v[3]);
+    const float2 t3 = ps(v[1], v[4]), t4 = ps(v[2], v[3]);
+    const float2 b1 = pa(pa(a, pm(c1, t1)), pm(c2, t2));
+    const float2 b2 = pa(pa(a, pm(c2, t1)), pm(c1, t2));
+    const float2 d1 = pa(pm(s1, t3), pm(s2, t4));
+    const float2 d2 = ps(pm(s2, t3), pm(s1, t4));
+    // (b.x + d.y, b.y − d.x) and (b.x − d.y, b.y + d.x)
+    const float2 e1 = make_float2(d1.y, d1.x), e2 = make_float2(d2.y, d2.x);
+    v[0] = pa(pa(a, t1), t2);
+    v[1] = ppm(b1, e1);
+    v[4] = pmp(b1, e1);
+    v[2] = ppm(b2, e2);
+    v[3] = pmp(b2, e2);
   }
 };
 
