@@ -203,9 +203,10 @@ template <int SX> __device__ __forceinline__ float2 pmix(float2 a, float2 b) {
 __device__ __forceinline__ float2 ppm(float2 a, float2 b) { return pmix<1>(a, b); }
 __device__ __forceinline__ float2 pmp(float2 a, float2 b) { return pmix<-1>(a, b); }
 
-// MULTW (fft/plan.nim:203-206): re = yr·wr − yi·wi, im = yr·wi + yi·wr.
+// MULTW (fft/plan.nim:203-206): re = yr·wr − yi·wi, im = yr·wi + yi·wr
+// (four scalar products, then the difference and the sum as one pair).
 __device__ __forceinline__ float2 mul_tw(float2 y, float2 w) {
-  return make_float2(fs(fm(y.x, w.x), fm(y.y, w.y)), fa(fm(y.x, w.y), fm(y.y, w.x)));
+  return pmp(make_float2(fm(y.x, w.x), fm(y.x, w.y)), make_float2(fm(y.y, w.y), fm(y.y, w.x)));
 }
 
 // The reference's butterfly of radix R on v[0 .. R) (outputs in place, k-th
